@@ -1,0 +1,286 @@
+"""Benchmark: particle-timesteps/s of the DEM time step on the periodic
+inclined chute workload (200,000 bidisperse flowing spheres, size ratio 2,
+two HGrid levels, rough base of fixed spheres, periodic 100 x 50 small
+diameters, 24 deg, LinearViscoelasticSlidingFriction, dt = tc/50).
+
+One bench "step" is one dem_step call that advances the whole system by
+STEPS_PER_CALL time steps (inputs resident in HBM). `value` counts moving
+particles x time steps over all ranks / the slowest rank's device time.
+`e2e` is the same metric through the public C ABI with host buffers: every
+bench step uploads the state from pinned host memory, runs the same batch and
+downloads the state.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs an independent replica (the time step does not
+shard across GPUs on this path: replicas only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-timesteps/s"
+STEPS_PER_CALL = 200
+WORKLOAD = dict(workload="periodic_chute_200k", n_flowing=200_000, size_ratio=2, hgrid_levels=2,
+                periodic="xy", domain_small_diameters=[100, 50], angle_deg=24, species="LinearViscoelasticSlidingFriction",
+                restitution=0.88, friction=0.5, dt="tc/50", time_steps_per_bench_step=STEPS_PER_CALL,
+                l2="working set >= L2; 256 MiB L2 flush before every timed dem_step call")
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0:
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and s[3 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def workload():
+    from mercurydpm_fork_b200 import scenarios
+    return scenarios.periodic_chute(n_flow=200_000, seed=2)
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def force_kernel_bytes(n, nwords, entries, contacts, wall_contacts, ncomp=3):
+    """Algorithmic bytes of one time-step force kernel launch (compulsory traffic).
+
+    per particle: read pr, vm, wi, qo (4 x 32 B) + info (16 B) + caller (4 B),
+                  write the same 6 arrays to the other buffer (148 B),
+                  active-bit words read + written (8 B x words), wall bits (8 B);
+    per neighbour-list entry: its index (4 B);
+    per contact side (a particle pair has two sides, a wall contact one):
+                  spring history read + written (2 x 8 B x ncomp).
+    Neighbour state gathers are cache hits (sorted order) and not counted.
+    """
+    per_particle = (4 * 32 + 16 + 4) + (4 * 32 + 16 + 4) + 8 * nwords + 8
+    return n * per_particle + 4 * entries + (2 * contacts + wall_contacts) * 2 * 8 * ncomp
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = rank_info()
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    from mercurydpm_fork_b200 import DemEngine, _abi
+    sc = workload()
+    n_moving = sc.n_moving
+    eng = DemEngine(sc.time_step, [sc.instance], sc.species, sc.walls, rotation=True, device=local)
+    eng.upload(sc.position, sc.velocity, sc.radius, sc.inv_mass, sc.inv_inertia, sc.species_index, sc.ids)
+    eng.step(0)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        eng.step(STEPS_PER_CALL)
+    barrier()
+    total_ms = 0.0
+    launches = 0
+    rebuilds = 0
+    t0 = time.perf_counter()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            eng.step(STEPS_PER_CALL)
+            st = eng.stats()
+            total_ms += st["ms"]
+            launches += st["kernel_launches"]
+            rebuilds += st["rebuilds"]
+    barrier()
+    wall = time.perf_counter() - t0
+    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    max_ms = float(t.item())
+    steps_total = args.steps * STEPS_PER_CALL
+    value = n_moving * steps_total * world / (max_ms / 1e3)
+
+    # roofline of the dominant kernel (time-step force + integration)
+    info = eng.stats()
+    cnt = eng.counts()
+    nwords = info["max_neighbors"] // 32
+    fk_ms = eng.time_force_kernel(20)
+    fk_bytes = force_kernel_bytes(sc.n, nwords, cnt["list_entries"], cnt["contacts"], cnt["wall_contacts"])
+    peak, peak_kind = measured_peak()
+    achieved = fk_bytes / (fk_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "force_kernel_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            tj = json.load(open(tpath))
+            traffic = tj.get("bytes_per_launch_scaled")
+        except Exception:
+            traffic = None
+
+    # end to end through the public API with host buffers
+    pos = torch.from_numpy(np.ascontiguousarray(sc.position)).pin_memory().numpy()
+    vel = torch.from_numpy(np.ascontiguousarray(sc.velocity)).pin_memory().numpy()
+    e2e_ms = 0.0
+    e2e_steps = max(1, min(args.steps, 3))
+    h2d = d2h = 0
+    barrier()
+    for _ in range(e2e_steps):
+        t1 = time.perf_counter()
+        eng.upload(pos, vel, sc.radius, sc.inv_mass, sc.inv_inertia, sc.species_index, sc.ids)
+        eng.step(STEPS_PER_CALL)
+        out = eng.download()
+        e2e_ms += (time.perf_counter() - t1) * 1e3
+        h2d = sc.n * (4 * 32 + 16 + 4)
+        d2h = sc.n * (4 * 32 + 16 + 4)
+    e2e_value = n_moving * e2e_steps * STEPS_PER_CALL / (e2e_ms / 1e3) * world
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(sc)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-timesteps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded periodic-chute packing)",
+        "config": dict(WORKLOAD, parallelism=f"replicas{world}", n_total=sc.n, n_moving=n_moving),
+        "e2e": {"value": e2e_value, "unit": "particle-timesteps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "k_force<1> (force + integration)", "peak_source": peak_kind,
+                     "bytes_per_launch": fk_bytes, "launch_ms": fk_ms},
+        "cpu_baseline": cpu,
+        "gpu_launches": launches,
+        "rebuilds": rebuilds,
+        "clocks": clocks.summary(),
+        "wall_s": wall,
+        "contacts": cnt,
+    }
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def cpu_baseline(sc, target_s: float = 15.0):
+    """The reference's own OpenMP build on this host's cores, on a bounded
+    sample of the same workload (a few time steps of the full system)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import harness as H
+    if not H.reference_available("omp"):
+        return None
+    threads = os.cpu_count() or 1
+    # calibrate on a short window, then time a window of about target_s seconds
+    t = H.time_reference(sc, 1, 2, threads, "omp")
+    nsteps = int(max(2, min(400, target_s / max(t / 2, 1e-6))))
+    t = H.time_reference(sc, 2, nsteps, threads, "omp")
+    return {"value": sc.n_moving * nsteps / t, "unit": "particle-timesteps/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{nsteps} time steps of the full workload after 2 warm-up steps (MercuryDPM OpenMP build, "
+                      f"{threads} threads, std::chrono around computeOneTimeStep)"}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import harness as H
+    if not H.reference_available("omp"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref not present"}))
+        return
+    sc = workload()
+    threads = os.cpu_count() or 1
+    per_step = max(1, STEPS_PER_CALL // 20)
+    t = H.time_reference(sc, args.warmup, per_step * args.steps, threads, "omp")
+    value = sc.n_moving * per_step * args.steps / t
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-timesteps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded periodic-chute packing)",
+        "config": dict(WORKLOAD, parallelism="cpu", time_steps_per_bench_step=per_step), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "particle-timesteps/s", "cores": threads, "kind": "reference",
+                         "sample": f"{per_step} time steps per bench step of the full workload"},
+        "e2e": {"value": value, "unit": "particle-timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

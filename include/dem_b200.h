@@ -1,0 +1,257 @@
+/*
+ * dem_b200.h -- C ABI of the B200 DEM time-step engine.
+ *
+ * The engine replaces the serial force/broad-phase loop of a MercuryDPM
+ * driver (DPMBase::computeOneTimeStep, Kernel/DPMBase.cc:4315-4389) with
+ * device-resident state and sm_100a kernels. A driver keeps its
+ * Mercury3D/DPMBase set-up code (species, particles, walls, periodic
+ * boundaries), hands the result to the engine once through this interface,
+ * and advances it in batches of time steps.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (DEM_OK == 0); no exceptions
+ *    cross the ABI. dem_last_error() gives the message of the last failure.
+ *  - The caller owns every host buffer; the engine owns all device memory.
+ *  - One host thread per handle. Calls on one handle are serialised on the
+ *    handle's own CUDA stream.
+ *  - Arrays are structure-of-arrays, FP64, indexed by the caller's particle
+ *    order at upload (the engine reorders internally and restores the
+ *    caller's order on download).
+ *  - Units and sign conventions are MercuryDPM's: the force stored on a
+ *    particle-particle contact acts on the particle with the lower id (P),
+ *    its normal points from I to P (Kernel/Particles/BaseParticle.cc:688-710);
+ *    for a wall contact P is the particle and the normal is minus the wall's
+ *    outward normal (Kernel/Walls/BaseWall.cc:367-437).
+ */
+#ifndef DEM_B200_H
+#define DEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define DEM_OK             0
+#define DEM_ERR_CAPACITY   1  /* neighbour-list or cell capacity exceeded          */
+#define DEM_ERR_TIMEOUT    2  /* a bounded device wait gave up                      */
+#define DEM_ERR_NAN        3  /* non-finite force or position detected              */
+#define DEM_ERR_BAD_INPUT  4  /* invalid argument (sizes, indices, parameters)      */
+#define DEM_ERR_CUDA       5  /* CUDA runtime failure                               */
+#define DEM_ERR_STATE      6  /* call out of order (e.g. step before upload)        */
+#define DEM_ERR_DOMAIN     7  /* a particle left the instance's bounding box        */
+
+/* ---- contact laws (the Species typedef headers in Kernel/Species) ----- */
+#define DEM_NORMAL_LINEAR_VISCOELASTIC   0 /* LinearViscoelasticInteraction.cc:105-135  */
+#define DEM_NORMAL_HERTZIAN_VISCOELASTIC 1 /* HertzianViscoelasticInteraction.cc:106-141 */
+
+#define DEM_FRICTION_NONE                0
+#define DEM_FRICTION_SLIDING             1 /* SlidingFrictionInteraction.cc:106-193      */
+#define DEM_FRICTION_ROLLING_TORSION     2 /* FrictionInteraction.cc:108-232             */
+#define DEM_FRICTION_MINDLIN             3 /* MindlinInteraction.cc:279-344              */
+#define DEM_FRICTION_MINDLIN_ROLLING_TORSION 4 /* MindlinRollingTorsionInteraction.cc:109-208 */
+
+/* ---- wall types ------------------------------------------------------- */
+#define DEM_WALL_INFINITE        0 /* InfiniteWall.cc:151-175                       */
+#define DEM_WALL_AXISYMMETRIC    1 /* AxisymmetricIntersectionOfWalls.cc:93-124     */
+
+#define DEM_MAX_LEVELS      4
+#define DEM_MAX_WALL_FACES  8
+#define DEM_MAX_WALLS_PER_INSTANCE 32
+
+/* Parameters of one (mixed) species pair, as held by the reference's
+ * Species<Normal,Friction,Adhesive> objects and the mixed-species triangle
+ * (SpeciesHandler::getMixedObject, Kernel/SpeciesHandler.cc:901-937).
+ * Values are the ones the reference species getters return, so the device
+ * law evaluates the same expressions on the same numbers. */
+typedef struct dem_species_pair {
+    int32_t normal_law;            /* DEM_NORMAL_*                                   */
+    int32_t friction_law;          /* DEM_FRICTION_*                                 */
+    int32_t constant_restitution;  /* LinearViscoelasticNormalSpecies constantRestitution */
+    int32_t reserved;
+    double  stiffness;             /* linear k                                       */
+    double  dissipation;           /* linear gamma; Hertz: dimensionless damping     */
+    double  elastic_modulus;       /* Hertz effective elastic modulus                */
+    double  shear_modulus;         /* Mindlin effective shear modulus                */
+    double  sliding_stiffness, sliding_dissipation;
+    double  sliding_mu, sliding_mu_static;
+    double  rolling_stiffness, rolling_dissipation;
+    double  rolling_mu, rolling_mu_static;
+    double  torsion_stiffness, torsion_dissipation;
+    double  torsion_mu, torsion_mu_static;
+    double  interaction_distance;  /* mixed-species interaction distance (0: none)   */
+} dem_species_pair;
+
+/* A wall. Infinite walls keep the reference's own representation: the
+ * orientation quaternion set by BaseInteractable::setOrientationViaNormal
+ * and the position (a point on the plane); the distance is evaluated with
+ * Quaternion::getDistance (Kernel/Math/Quaternion.cc:658-670).
+ * Axisymmetric walls hold up to DEM_MAX_WALL_FACES half-planes in the
+ * wall's (r, axial) frame, as AxisymmetricIntersectionOfWalls::addObject
+ * stores them: face k has normal (faces[k][0], 0, faces[k][2]) and a point
+ * (faces[k][3], 0, faces[k][5]) in (r, -, a) coordinates. */
+typedef struct dem_wall {
+    int32_t type;                  /* DEM_WALL_*                                     */
+    int32_t species;               /* species index of the wall                      */
+    int32_t instance;              /* owning instance (0 for a single simulation)    */
+    int32_t n_faces;               /* axisymmetric: number of half-planes            */
+    double  position[3];
+    double  orientation[4];        /* quaternion q0..q3                              */
+    double  velocity[3];
+    double  angular_velocity[3];
+    double  faces[DEM_MAX_WALL_FACES][6];
+} dem_wall;
+
+/* Host-side particle arrays (structure of arrays, caller order).
+ * position/velocity/angular_velocity: 3*n doubles, xyz interleaved per particle.
+ * orientation: 4*n doubles (q0..q3) or NULL (identity).
+ * inv_mass/inv_inertia: 0 for fixed particles (BaseParticle::fixParticle).
+ * inv_inertia is the isotropic diagonal of BaseParticle::invInertia_
+ * (Kernel/Particles/BaseParticle.cc:874-883). id is the reference's
+ * BaseParticle::getId(); it orders each pair (lower id is P). */
+typedef struct dem_particles_soa {
+    int64_t  n;
+    double  *position;
+    double  *velocity;
+    double  *angular_velocity;
+    double  *orientation;
+    double  *radius;
+    double  *inv_mass;
+    double  *inv_inertia;
+    int32_t *species;
+    int32_t *id;
+    int32_t *instance;             /* NULL: all in instance 0                        */
+} dem_particles_soa;
+
+/* Contact list with history, one row per live contact, for download,
+ * restart and oracle injection (the content of InteractionHandler,
+ * Kernel/InteractionHandler.cc:146-174, 433-500).
+ * For particle-wall contacts id_i is the wall index and is_wall is 1.
+ * springs: 9 doubles per contact: sliding(3), rolling(3), torsion(3).
+ * force/contact_point: 3 doubles per contact (may be NULL on upload). */
+typedef struct dem_contacts_soa {
+    int64_t  n;
+    int32_t *id_p;
+    int32_t *id_i;
+    int32_t *is_wall;
+    int32_t *periodic;             /* 1: the pair meets across a periodic boundary   */
+    double  *springs;
+    double  *force;
+    double  *overlap;
+} dem_contacts_soa;
+
+/* Per-instance description. A single simulation is one instance. */
+typedef struct dem_instance_desc {
+    double   domain_min[3];        /* bounding box of the cell grid (DPMBase::setDomain) */
+    double   domain_max[3];
+    double   gravity[3];           /* DPMBase::setGravity                            */
+    uint32_t periodic_mask;        /* bit d: dimension d is periodic                 */
+    int32_t  species_offset;       /* first species of this instance                 */
+    int32_t  n_species;            /* species table of this instance is n_species^2  */
+    int32_t  reserved;
+    double   periodic_min[3];      /* PeriodicBoundary left/right positions          */
+    double   periodic_max[3];
+} dem_instance_desc;
+
+typedef struct dem_config {
+    double   time_step;            /* DPMBase::setTimeStep                           */
+    double   background_drag;      /* DPMBase::setBackgroundDrag                     */
+    int32_t  rotation;             /* DPMBase::setRotation (1: integrate omega, q)   */
+    int32_t  device;               /* CUDA device ordinal                            */
+    int32_t  max_neighbors;        /* neighbour-list capacity per particle (0: auto) */
+    int32_t  use_graphs;           /* capture the step loop in CUDA graphs           */
+    double   skin;                 /* Verlet skin distance (0: auto)                 */
+    int32_t  n_instances;          /* >= 1                                           */
+    int32_t  reserved;
+} dem_config;
+
+/* Global balances (DPMBase::getKineticEnergy ... getCentreOfMass,
+ * Kernel/DPMBase.cc:1528-1640; writeEneTimeStep :2100-2123). */
+typedef struct dem_globals {
+    double  kinetic_energy;
+    double  rotational_energy;
+    double  gravitational_energy;
+    double  elastic_energy;
+    double  momentum[3];
+    double  angular_momentum[3];
+    double  mass;
+    double  centre_of_mass[3];
+    int64_t n_contacts;
+    int64_t n_wall_contacts;
+    double  time;
+    int64_t n_steps;
+} dem_globals;
+
+/* Gaussian coarse-graining grid (CG<XZ|XYZ|O, Gauss, StandardFields>,
+ * Kernel/CG/CG.hcc:233-528). Fields per grid point, in this order:
+ * density, momentum(3), kinetic stress(6: xx xy xz yy yz zz),
+ * contact stress(9: row-major), volume fraction. 20 doubles per point. */
+#define DEM_CG_NFIELDS 20
+#define DEM_CG_O   0
+#define DEM_CG_XZ  1
+#define DEM_CG_XYZ 2
+typedef struct dem_cg_grid {
+    int32_t coordinates;           /* DEM_CG_*                                       */
+    int32_t instance;
+    int32_t n[3];                  /* points per dimension (unused dims: 1)          */
+    int32_t reserved;
+    double  min[3];                /* CG domain (CG::setMin/setMax)                  */
+    double  max[3];
+    double  width;                 /* Gaussian standard deviation (Gauss::setWidth)  */
+    double  cutoff_factor;         /* cutoff = cutoff_factor * width (reference: 3)  */
+} dem_cg_grid;
+
+typedef struct dem_handle dem_handle;
+
+/* DPMBase construction + setTimeStep/setGravity/setDomain. */
+int  dem_create(const dem_config *config, const dem_instance_desc *instances,
+                dem_handle **out);
+/* Species table: n_species^2 entries per instance, row-major (i*n+j), the
+ * mixed entries symmetric (SpeciesHandler::getMixedObject). */
+int  dem_set_species(dem_handle *h, const dem_species_pair *table, int n_entries);
+/* WallHandler contents. */
+int  dem_set_walls(dem_handle *h, const dem_wall *walls, int n);
+/* ParticleHandler contents; triggers the first force evaluation on the next
+ * dem_step (the one DPMBase::initialiseSolve performs, DPMBase.cc:4180). */
+int  dem_upload_particles(dem_handle *h, const dem_particles_soa *p);
+/* Inject contact history (restart / oracle states). Call after upload. */
+int  dem_upload_contacts(dem_handle *h, const dem_contacts_soa *c);
+/* Advance n time steps (n >= 0; n == 0 only performs a pending initial
+ * force evaluation). Equivalent to n calls of DPMBase::computeOneTimeStep
+ * without output. Returns DEM_ERR_* on a device-side status. */
+int  dem_step(dem_handle *h, int nsteps);
+int  dem_download_particles(dem_handle *h, dem_particles_soa *p);
+/* Total force and torque on every particle from the last force evaluation
+ * (3*n doubles each, caller order). */
+int  dem_download_forces(dem_handle *h, double *force, double *torque);
+/* Live contacts (one row per contact as the reference keeps them).
+ * capacity: rows available in c; *count receives the number of contacts
+ * (rows beyond capacity are not written). */
+int  dem_download_contacts(dem_handle *h, dem_contacts_soa *c, int64_t capacity,
+                           int64_t *count);
+int  dem_reduce(dem_handle *h, int instance, dem_globals *out);
+int  dem_cg_eval(dem_handle *h, const dem_cg_grid *grid, double *fields_out);
+/* Device time of the last dem_step call in milliseconds (CUDA events on the
+ * handle's stream) and how many kernels it launched. */
+int  dem_last_step_stats(dem_handle *h, double *ms, int64_t *kernel_launches,
+                         int64_t *rebuilds);
+int  dem_get_info(dem_handle *h, int64_t *n_particles, int64_t *max_neighbors,
+                  int64_t *n_cells);
+/* Neighbour-list entries, live particle contacts and wall contacts of the
+ * current state (the sizes the per-step byte count is made of). */
+int  dem_get_counts(dem_handle *h, int64_t *list_entries, int64_t *contacts,
+                    int64_t *wall_contacts);
+/* Profiling aid (no reference counterpart): launches the time-step force
+ * kernel `reps` times on the current state, writing into the spare state and
+ * history buffers without committing them, and returns the mean device time
+ * of one launch in milliseconds (CUDA events on the handle's stream). The
+ * simulation state is unchanged. */
+int  dem_time_force_kernel(dem_handle *h, int reps, double *ms_per_launch);
+const char *dem_last_error(dem_handle *h);
+void dem_destroy(dem_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DEM_B200_H */

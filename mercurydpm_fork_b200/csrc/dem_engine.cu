@@ -1,0 +1,958 @@
+// dem_engine.cu -- host side of the C ABI (include/dem_b200.h) and the
+// device buffers, kernel launches and CUDA graphs of the DEM engine.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dem_engine.cuh"
+#include "dem_walls.cuh"
+#include "dem_kernels.cuh"
+
+using namespace dem;
+
+namespace {
+
+constexpr unsigned FATAL_STATUS = (1u << DEM_ERR_CAPACITY) | (1u << DEM_ERR_NAN) | (1u << DEM_ERR_TIMEOUT);
+constexpr int GRAPH_STEPS = 16;
+
+struct Handle {
+    dem_config cfg{};
+    std::vector<dem_instance_desc> inst_desc;
+    std::vector<InstanceDev> inst;
+    std::vector<dem_species_pair> species;
+    std::vector<dem_wall> walls;
+    std::string err;
+    int device = 0;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevPtrs d{};
+    // device allocations
+    std::vector<void*> allocs;
+    InstanceDev* d_inst = nullptr;
+    dem_species_pair* d_species = nullptr;
+    dem_wall* d_walls = nullptr;
+    Control* d_ctl = nullptr;
+    ContactRecord* d_records = nullptr;
+    unsigned record_capacity = 0;
+    int nblocks_scan = 0;
+    bool uploaded = false;
+    bool initial_pending = false;
+    bool records_valid = false;
+    unsigned n_records = 0;
+    long long steps_total = 0;
+    double last_ms = 0.0;
+    long long last_launches = 0;
+    long long last_rebuilds = 0;
+    long long launches_per_step = 0;
+    cudaGraphExec_t graph1 = nullptr, graphK = nullptr;
+    int ncomp = 3;
+};
+
+int fail(Handle* h, int code, const std::string& msg)
+{
+    if (h) h->err = msg;
+    return code;
+}
+
+#define CU(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(h, DEM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+template <typename T>
+int dalloc(Handle* h, T** p, size_t count)
+{
+    void* ptr = nullptr;
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    cudaError_t e = cudaMalloc(&ptr, bytes);
+    if (e != cudaSuccess) return fail(h, DEM_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    e = cudaMemsetAsync(ptr, 0, bytes, h->stream);
+    if (e != cudaSuccess) return fail(h, DEM_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    h->allocs.push_back(ptr);
+    *p = static_cast<T*>(ptr);
+    return DEM_OK;
+}
+
+void free_graphs(Handle* h)
+{
+    if (h->graph1) cudaGraphExecDestroy(h->graph1);
+    if (h->graphK) cudaGraphExecDestroy(h->graphK);
+    h->graph1 = h->graphK = nullptr;
+}
+
+void free_particle_arrays(Handle* h)
+{
+    free_graphs(h);
+    for (void* p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    h->d_records = nullptr;
+    h->record_capacity = 0;
+}
+
+inline unsigned grid_for(long long n, int block) { return (unsigned)std::max<long long>(1, (n + block - 1) / block); }
+
+// ---- kernel launch sequences ------------------------------------------------
+void launch_rebuild(Handle* h, cudaStream_t s)
+{
+    DevPtrs& d = h->d;
+    k_keys<<<grid_for(d.n, 256), 256, 0, s>>>(d);
+    k_scan_blocks<<<h->nblocks_scan, 1024, 0, s>>>(d);
+    k_scan_sums<<<1, 1024, 0, s>>>(d, h->nblocks_scan);
+    k_scan_add<<<grid_for(d.ncells, 256), 256, 0, s>>>(d);
+    k_scatter<<<grid_for(d.n, 256), 256, 0, s>>>(d);
+    k_cell_sort<<<grid_for(d.ncells, 128), 128, 0, s>>>(d);
+    k_gather<<<grid_for(d.n, 256), 256, 0, s>>>(d);
+    k_build<<<grid_for(d.n, 128), 128, 0, s>>>(d);
+    k_rb_finish<<<1, 32, 0, s>>>(d);
+}
+constexpr int REBUILD_LAUNCHES = 9;
+
+void launch_force(Handle* h, cudaStream_t s, int mode)
+{
+    DevPtrs& d = h->d;
+    if (mode == 0)
+        k_force<0><<<grid_for(d.n, 128), 128, 0, s>>>(d);
+    else
+        k_force<1><<<grid_for(d.n, 128), 128, 0, s>>>(d);
+}
+
+// Captures `steps` time steps: control -> (if rebuild) rebuild body -> force.
+int build_graph(Handle* h, int steps, cudaGraphExec_t* out)
+{
+    cudaStream_t s = h->stream;
+    CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < steps; ++k) {
+        cudaStreamCaptureStatus st;
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr));
+        cudaGraphConditionalHandle handle;
+        CU(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
+        k_control<<<1, 32, 0, s>>>(h->d_ctl, handle, 1);
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CU(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps));
+        // cudaGraphNodeParams has no default constructor; build it in zeroed storage
+        alignas(cudaGraphNodeParams) unsigned char storage[sizeof(cudaGraphNodeParams)];
+        std::memset(storage, 0, sizeof(storage));
+        cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(storage);
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode;
+        CU(cudaGraphAddNode(&cnode, g, deps, ndeps, &cp));
+        CU(cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CU(cudaStreamBeginCaptureToGraph(h->stream2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        launch_rebuild(h, h->stream2);
+        cudaGraph_t body_out = nullptr;
+        CU(cudaStreamEndCapture(h->stream2, &body_out));
+        launch_force(h, s, 1);
+    }
+    cudaGraph_t graph = nullptr;
+    CU(cudaStreamEndCapture(s, &graph));
+    cudaError_t e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(h, DEM_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return DEM_OK;
+}
+
+int read_control(Handle* h, Control* c)
+{
+    CU(cudaMemcpyAsync(c, h->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return DEM_OK;
+}
+
+int check_status(Handle* h, const Control& c)
+{
+    const unsigned st = c.status & FATAL_STATUS;
+    if (!st) return DEM_OK;
+    if (st & (1u << DEM_ERR_CAPACITY))
+        return fail(h, DEM_ERR_CAPACITY, "neighbour-list capacity exceeded (max_neighbors=" +
+                                             std::to_string(h->d.cap) + "); raise dem_config.max_neighbors");
+    if (st & (1u << DEM_ERR_NAN)) return fail(h, DEM_ERR_NAN, "non-finite force detected");
+    return fail(h, DEM_ERR_TIMEOUT, "device wait timed out");
+}
+
+// Levels and cell grid of one instance (MercuryBase::hGridRebuild,
+// MercuryBase.cc:204-306, restated as dense per-level grids): radii are
+// grouped in geometric bands of ratio 2 starting at the smallest radius; a
+// level's cell edge is at least 2 r_max(level) + interaction distance + skin.
+void setup_instance_grid(const dem_instance_desc& in, const std::vector<double>& radii, double skin, double dmax,
+                         InstanceDev& I, std::vector<int>& level_of, int& cell_base)
+{
+    double rmin = 1e300, rmax = 0.0;
+    for (double r : radii) { rmin = std::min(rmin, r); rmax = std::max(rmax, r); }
+    if (radii.empty()) { rmin = rmax = 1.0; }
+    int nl = 1;
+    while (nl < DEM_MAX_LEVELS && rmax >= rmin * std::pow(2.0, nl)) ++nl;
+    std::vector<double> lrmax(nl, 0.0);
+    std::vector<int> used(nl, 0);
+    level_of.resize(radii.size());
+    for (size_t i = 0; i < radii.size(); ++i) {
+        int l = (int)std::floor(std::log2(radii[i] / rmin));
+        l = std::max(0, std::min(nl - 1, l));
+        level_of[i] = l;
+        lrmax[l] = std::max(lrmax[l], radii[i]);
+        used[l] = 1;
+    }
+    // drop empty levels
+    std::vector<int> remap(nl, -1);
+    int nu = 0;
+    std::vector<double> lr;
+    for (int l = 0; l < nl; ++l)
+        if (used[l] || radii.empty()) { remap[l] = nu++; lr.push_back(lrmax[l] > 0 ? lrmax[l] : rmax); }
+    for (auto& l : level_of) l = remap[l];
+    I.n_levels = nu;
+    for (int l = 0; l < nu; ++l) {
+        const double cs = 2.0 * lr[l] + dmax + skin;
+        I.level_rmax[l] = lr[l];
+        I.cell_base[l] = cell_base;
+        int total = 1;
+        for (int k = 0; k < 3; ++k) {
+            const bool per = (in.periodic_mask >> k) & 1u;
+            int dim;
+            if (per) {
+                const double L = in.periodic_max[k] - in.periodic_min[k];
+                dim = std::max(1, (int)std::floor(L / cs));
+                I.inv_cell[l][k] = (double)dim / L;
+            } else {
+                const double ext = in.domain_max[k] - in.domain_min[k];
+                dim = std::max(1, (int)std::ceil(ext / cs));
+                I.inv_cell[l][k] = 1.0 / cs;
+            }
+            I.dims[l][k] = dim;
+            total *= dim;
+        }
+        cell_base += total;
+    }
+}
+
+} // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+int dem_create(const dem_config* config, const dem_instance_desc* instances, dem_handle** out)
+{
+    Handle* h = nullptr;
+    if (!config || !out || !instances) return DEM_ERR_BAD_INPUT;
+    if (config->n_instances < 1 || !(config->time_step > 0.0)) return DEM_ERR_BAD_INPUT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DEM_ERR_CUDA;
+    if (config->device < 0 || config->device >= ndev) return DEM_ERR_BAD_INPUT;
+    h = new Handle();
+    h->cfg = *config;
+    h->device = config->device;
+    h->inst_desc.assign(instances, instances + config->n_instances);
+    for (const auto& in : h->inst_desc) {
+        for (int k = 0; k < 3; ++k) {
+            if ((in.periodic_mask >> k) & 1u) {
+                if (!(in.periodic_max[k] > in.periodic_min[k])) {
+                    delete h;
+                    return DEM_ERR_BAD_INPUT;
+                }
+            } else if (!(in.domain_max[k] > in.domain_min[k])) {
+                delete h;
+                return DEM_ERR_BAD_INPUT;
+            }
+        }
+    }
+    if (cudaSetDevice(h->device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+        delete h;
+        return DEM_ERR_CUDA;
+    }
+    *out = reinterpret_cast<dem_handle*>(h);
+    return DEM_OK;
+}
+
+int dem_set_species(dem_handle* hh, const dem_species_pair* table, int n_entries)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !table || n_entries <= 0) return fail(h, DEM_ERR_BAD_INPUT, "dem_set_species: empty table");
+    size_t need = 0;
+    for (const auto& in : h->inst_desc) {
+        if (in.n_species <= 0 || in.species_offset < 0) return fail(h, DEM_ERR_BAD_INPUT, "instance without species");
+        need = std::max(need, (size_t)in.species_offset + (size_t)in.n_species * in.n_species);
+    }
+    if ((size_t)n_entries < need) return fail(h, DEM_ERR_BAD_INPUT, "species table smaller than the instances need");
+    h->species.assign(table, table + n_entries);
+    h->ncomp = 3;
+    for (const auto& s : h->species) {
+        if (s.friction_law == DEM_FRICTION_ROLLING_TORSION || s.friction_law == DEM_FRICTION_MINDLIN_ROLLING_TORSION)
+            h->ncomp = 9;
+        if (s.normal_law < 0 || s.normal_law > 1 || s.friction_law < 0 || s.friction_law > 4)
+            return fail(h, DEM_ERR_BAD_INPUT, "unknown contact law");
+    }
+    return DEM_OK;
+}
+
+int dem_set_walls(dem_handle* hh, const dem_wall* walls, int n)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || n < 0 || (n > 0 && !walls)) return fail(h, DEM_ERR_BAD_INPUT, "dem_set_walls: bad arguments");
+    std::vector<dem_wall> w(walls, walls + n);
+    std::stable_sort(w.begin(), w.end(), [](const dem_wall& a, const dem_wall& b) { return a.instance < b.instance; });
+    for (const auto& x : w) {
+        if (x.instance < 0 || x.instance >= (int)h->inst_desc.size())
+            return fail(h, DEM_ERR_BAD_INPUT, "wall instance out of range");
+        if (x.type != DEM_WALL_INFINITE && x.type != DEM_WALL_AXISYMMETRIC)
+            return fail(h, DEM_ERR_BAD_INPUT, "unknown wall type");
+        if (x.n_faces < 0 || x.n_faces > DEM_MAX_WALL_FACES) return fail(h, DEM_ERR_BAD_INPUT, "too many wall faces");
+        if (x.species < 0 || x.species >= h->inst_desc[x.instance].n_species)
+            return fail(h, DEM_ERR_BAD_INPUT, "wall species out of range");
+    }
+    h->walls = w;
+    return DEM_OK;
+}
+
+int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !p || p->n < 0 || p->n > (1ll << 30)) return fail(h, DEM_ERR_BAD_INPUT, "dem_upload_particles: bad arguments");
+    if (h->species.empty()) return fail(h, DEM_ERR_STATE, "dem_set_species must come before dem_upload_particles");
+    const long long n = p->n;
+    if (n > 0 && (!p->position || !p->velocity || !p->radius || !p->inv_mass || !p->species || !p->id))
+        return fail(h, DEM_ERR_BAD_INPUT, "missing particle arrays");
+    CU(cudaSetDevice(h->device));
+    const int ninst = (int)h->inst_desc.size();
+    // ---- validate and collect per-instance radii
+    std::vector<std::vector<double>> radii(ninst);
+    std::vector<std::vector<long long>> members(ninst);
+    double rmin_all = 1e300;
+    for (long long i = 0; i < n; ++i) {
+        const int in = p->instance ? p->instance[i] : 0;
+        if (in < 0 || in >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "particle instance out of range");
+        const double r = p->radius[i];
+        if (!(r > 0.0) || !std::isfinite(r)) return fail(h, DEM_ERR_BAD_INPUT, "particle radius must be positive");
+        if (p->species[i] < 0 || p->species[i] >= h->inst_desc[in].n_species)
+            return fail(h, DEM_ERR_BAD_INPUT, "particle species out of range");
+        if (!(p->inv_mass[i] >= 0.0)) return fail(h, DEM_ERR_BAD_INPUT, "inverse mass must be >= 0");
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(p->position[3 * i + k]) || !std::isfinite(p->velocity[3 * i + k]))
+                return fail(h, DEM_ERR_BAD_INPUT, "non-finite particle state");
+        radii[in].push_back(r);
+        members[in].push_back(i);
+        rmin_all = std::min(rmin_all, r);
+    }
+    // ---- walls per instance
+    std::vector<int> wbegin(ninst, 0), wend(ninst, 0);
+    {
+        int w = 0;
+        for (int in = 0; in < ninst; ++in) {
+            wbegin[in] = w;
+            while (w < (int)h->walls.size() && h->walls[w].instance == in) ++w;
+            wend[in] = w;
+            if (wend[in] - wbegin[in] > DEM_MAX_WALLS_PER_INSTANCE)
+                return fail(h, DEM_ERR_BAD_INPUT, "more than 32 walls in one instance");
+        }
+    }
+    int wmax = 1;
+    for (int in = 0; in < ninst; ++in) wmax = std::max(wmax, wend[in] - wbegin[in]);
+    // ---- skin and levels
+    double skin = h->cfg.skin;
+    if (!(skin > 0.0)) skin = (n > 0) ? 0.2 * rmin_all : 1e-3;
+    h->inst.assign(ninst, InstanceDev{});
+    std::vector<int> level(n, 0);
+    int cell_base = 0;
+    for (int in = 0; in < ninst; ++in) {
+        const auto& D = h->inst_desc[in];
+        InstanceDev& I = h->inst[in];
+        double dmax = 0.0;
+        for (int a = 0; a < D.n_species; ++a)
+            for (int b = 0; b < D.n_species; ++b)
+                dmax = std::max(dmax, h->species[D.species_offset + a * D.n_species + b].interaction_distance);
+        I.max_interaction_distance = dmax;
+        for (int k = 0; k < 3; ++k) {
+            I.gravity[k] = D.gravity[k];
+            const bool per = (D.periodic_mask >> k) & 1u;
+            I.origin[k] = per ? D.periodic_min[k] : D.domain_min[k];
+            I.per_lo[k] = D.periodic_min[k];
+            I.per_hi[k] = D.periodic_max[k];
+            I.per_L[k] = D.periodic_max[k] - D.periodic_min[k];
+            I.per_half[k] = 0.5 * I.per_L[k];
+        }
+        I.per_mask = D.periodic_mask;
+        I.species_offset = D.species_offset;
+        I.n_species = D.n_species;
+        I.wall_begin = wbegin[in];
+        I.wall_end = wend[in];
+        std::vector<int> lv;
+        setup_instance_grid(D, radii[in], skin, dmax, I, lv, cell_base);
+        for (size_t k = 0; k < members[in].size(); ++k) level[members[in][k]] = lv[k];
+        // a periodic dimension must be longer than twice the largest reach
+        for (int k = 0; k < 3; ++k)
+            if ((D.periodic_mask >> k) & 1u) {
+                double rm = 0.0;
+                for (double r : radii[in]) rm = std::max(rm, r);
+                if (I.per_L[k] <= 2.0 * (2.0 * rm + dmax + skin))
+                    return fail(h, DEM_ERR_BAD_INPUT, "periodic box too small for the particle size");
+            }
+    }
+    const long long ncells = cell_base;
+    // ---- neighbour capacity
+    int cap = h->cfg.max_neighbors;
+    if (cap <= 0) {
+        // auto: 48 for monodisperse-like packings, more when radii spread
+        double rmax_all = 0.0;
+        for (int in = 0; in < ninst; ++in) for (double r : radii[in]) rmax_all = std::max(rmax_all, r);
+        const double ratio = (n > 0) ? rmax_all / rmin_all : 1.0;
+        cap = ratio < 1.5 ? 48 : (ratio < 2.5 ? 96 : 128);
+    }
+    cap = ((cap + 31) / 32) * 32;
+    if (cap > 128) return fail(h, DEM_ERR_BAD_INPUT, "max_neighbors above 128 is not supported");
+
+    // ---- (re)allocate
+    free_particle_arrays(h);
+    h->d = DevPtrs{};
+    DevPtrs& d = h->d;
+    d.n = (int)n;
+    d.ncap = (int)std::max<long long>(32, ((n + 31) / 32) * 32);
+    d.cap = cap;
+    d.nwords = cap / 32;
+    d.ncomp = h->ncomp;
+    d.wmax = wmax;
+    d.ncells = (int)ncells;
+    d.rotation = h->cfg.rotation;
+    d.dt = h->cfg.time_step;
+    d.drag = h->cfg.background_drag;
+    h->nblocks_scan = (int)grid_for(ncells, 1024);
+    const size_t NC = d.ncap;
+    int rc;
+    for (int b = 0; b < 2; ++b) {
+        if ((rc = dalloc(h, &d.pr[b], NC))) return rc;
+        if ((rc = dalloc(h, &d.vm[b], NC))) return rc;
+        if ((rc = dalloc(h, &d.wi[b], NC))) return rc;
+        if ((rc = dalloc(h, &d.qo[b], NC))) return rc;
+        if ((rc = dalloc(h, &d.info[b], NC))) return rc;
+        if ((rc = dalloc(h, &d.caller[b], NC))) return rc;
+        if ((rc = dalloc(h, &d.nbr[b], (size_t)cap * NC))) return rc;
+        if ((rc = dalloc(h, &d.cnt[b], NC))) return rc;
+        if ((rc = dalloc(h, &d.hist[b], (size_t)d.ncomp * cap * NC))) return rc;
+        if ((rc = dalloc(h, &d.act[b], (size_t)d.nwords * NC))) return rc;
+        if ((rc = dalloc(h, &d.whist[b], (size_t)d.ncomp * wmax * NC))) return rc;
+        if ((rc = dalloc(h, &d.wact[b], NC))) return rc;
+    }
+    if ((rc = dalloc(h, &d.force, 3 * NC))) return rc;
+    if ((rc = dalloc(h, &d.torque, 3 * NC))) return rc;
+    if ((rc = dalloc(h, &d.key, NC))) return rc;
+    if ((rc = dalloc(h, &d.perm, NC))) return rc;
+    if ((rc = dalloc(h, &d.newidx, NC))) return rc;
+    if ((rc = dalloc(h, &d.cell_count, (size_t)ncells + 1))) return rc;
+    if ((rc = dalloc(h, &d.cell_start, (size_t)ncells + 1))) return rc;
+    if ((rc = dalloc(h, &d.cell_cursor, (size_t)ncells + 1))) return rc;
+    if ((rc = dalloc(h, &d.block_sums, (size_t)h->nblocks_scan + 1))) return rc;
+    if ((rc = dalloc(h, &h->d_inst, h->inst.size()))) return rc;
+    if ((rc = dalloc(h, &h->d_species, h->species.size()))) return rc;
+    if ((rc = dalloc(h, &h->d_walls, std::max<size_t>(1, h->walls.size())))) return rc;
+    if ((rc = dalloc(h, &h->d_ctl, 1))) return rc;
+    h->record_capacity = (unsigned)std::min<long long>(2000000000ll, 8 * n + 1024 + (long long)n * std::min(wmax, 4));
+    if ((rc = dalloc(h, &h->d_records, h->record_capacity))) return rc;
+    d.inst = h->d_inst;
+    d.species = h->d_species;
+    d.walls = h->d_walls;
+    d.ctl = h->d_ctl;
+    d.records = h->d_records;
+
+    // ---- host staging in caller order
+    std::vector<double4> pr(n), vm(n), wi(n), qo(n);
+    std::vector<int4> info(n);
+    std::vector<int> caller(n);
+    for (long long i = 0; i < n; ++i) {
+        pr[i] = make_double4(p->position[3 * i], p->position[3 * i + 1], p->position[3 * i + 2], p->radius[i]);
+        vm[i] = make_double4(p->velocity[3 * i], p->velocity[3 * i + 1], p->velocity[3 * i + 2], p->inv_mass[i]);
+        const double* w = p->angular_velocity;
+        wi[i] = make_double4(w ? w[3 * i] : 0.0, w ? w[3 * i + 1] : 0.0, w ? w[3 * i + 2] : 0.0,
+                             p->inv_inertia ? p->inv_inertia[i] : 0.0);
+        const double* q = p->orientation;
+        qo[i] = q ? make_double4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]) : make_double4(1.0, 0.0, 0.0, 0.0);
+        const int in = p->instance ? p->instance[i] : 0;
+        const int flags = (p->inv_mass[i] == 0.0 ? FLAG_FIXED : 0) | (level[i] << LEVEL_SHIFT);
+        info[i] = make_int4(p->id[i], p->species[i], in, flags);
+        caller[i] = (int)i;
+    }
+    CU(cudaMemcpyAsync(d.pr[0], pr.data(), n * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(d.vm[0], vm.data(), n * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(d.wi[0], wi.data(), n * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(d.qo[0], qo.data(), n * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(d.info[0], info.data(), n * sizeof(int4), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(d.caller[0], caller.data(), n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->d_inst, h->inst.data(), h->inst.size() * sizeof(InstanceDev), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->d_species, h->species.data(), h->species.size() * sizeof(dem_species_pair),
+                       cudaMemcpyHostToDevice, h->stream));
+    if (!h->walls.empty())
+        CU(cudaMemcpyAsync(h->d_walls, h->walls.data(), h->walls.size() * sizeof(dem_wall), cudaMemcpyHostToDevice,
+                           h->stream));
+    Control c{};
+    c.cur = 0;
+    c.lbuf = 0;
+    c.skin = skin;
+    c.force_rebuild = 1;
+    c.record = 1;
+    c.record_capacity = h->record_capacity;
+    CU(cudaMemcpyAsync(h->d_ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    h->uploaded = true;
+    h->initial_pending = true;
+    h->records_valid = false;
+    h->steps_total = 0;
+    return DEM_OK;
+}
+
+// Runs the forced rebuild that a pending initial evaluation needs (without
+// the force evaluation itself); used by dem_upload_contacts.
+static int ensure_lists(Handle* h)
+{
+    Control c;
+    int rc = read_control(h, &c);
+    if (rc) return rc;
+    if (!c.force_rebuild) return DEM_OK;
+    c.rebuild = 1;
+    c.force_rebuild = 0;
+    CU(cudaMemcpyAsync(h->d_ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+    launch_rebuild(h, h->stream);
+    CU(cudaGetLastError());
+    return read_control(h, &c);
+}
+
+int dem_upload_contacts(dem_handle* hh, const dem_contacts_soa* cs)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !cs || cs->n < 0) return fail(h, DEM_ERR_BAD_INPUT, "dem_upload_contacts: bad arguments");
+    if (!h->uploaded) return fail(h, DEM_ERR_STATE, "upload particles first");
+    if (!h->initial_pending) return fail(h, DEM_ERR_STATE, "contacts can only be injected before the first step");
+    int rc = ensure_lists(h);
+    if (rc) return rc;
+    Control c;
+    if ((rc = read_control(h, &c))) return rc;
+    DevPtrs& d = h->d;
+    const int n = d.n, cur = c.cur, l = c.lbuf;
+    const size_t NC = d.ncap;
+    std::vector<int4> info(n);
+    std::vector<double4> pr(n);
+    std::vector<int> cnt(n), nbr((size_t)d.cap * NC);
+    std::vector<unsigned> act((size_t)d.nwords * NC), wact(NC);
+    std::vector<double> hist((size_t)d.ncomp * d.cap * NC), whist((size_t)d.ncomp * d.wmax * NC);
+    CU(cudaMemcpyAsync(info.data(), d.info[cur], n * sizeof(int4), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(pr.data(), d.pr[cur], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(cnt.data(), d.cnt[l], n * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(nbr.data(), d.nbr[l], nbr.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(act.data(), d.act[cur], act.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(wact.data(), d.wact[cur], wact.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(hist.data(), d.hist[cur], hist.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(whist.data(), d.whist[cur], whist.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    // id -> sorted slot
+    std::vector<std::pair<int, int>> ids(n);
+    for (int s = 0; s < n; ++s) ids[s] = {info[s].x, s};
+    std::sort(ids.begin(), ids.end());
+    auto slot_of = [&](int id) -> int {
+        auto it = std::lower_bound(ids.begin(), ids.end(), std::make_pair(id, -1));
+        return (it != ids.end() && it->first == id) ? it->second : -1;
+    };
+    auto set_entry = [&](int s, int t, const double* spr, double sign) -> bool {
+        for (int k = 0; k < cnt[s]; ++k) {
+            if (nbr[(size_t)k * NC + s] != t) continue;
+            for (int comp = 0; comp < d.ncomp; ++comp)
+                hist[((size_t)comp * d.cap + k) * NC + s] = sign * spr[comp];
+            act[(size_t)(k >> 5) * NC + s] |= 1u << (k & 31);
+            return true;
+        }
+        return false;
+    };
+    for (long long r = 0; r < cs->n; ++r) {
+        const double* spr = cs->springs ? cs->springs + 9 * r : nullptr;
+        double zero[9] = {0};
+        if (!spr) spr = zero;
+        const int sp = slot_of(cs->id_p[r]);
+        if (sp < 0) return fail(h, DEM_ERR_BAD_INPUT, "contact refers to an unknown particle id");
+        if (cs->is_wall && cs->is_wall[r]) {
+            const int in = info[sp].z;
+            const int w = cs->id_i[r] - h->inst[in].wall_begin;
+            if (w < 0 || w >= h->inst[in].wall_end - h->inst[in].wall_begin)
+                return fail(h, DEM_ERR_BAD_INPUT, "contact refers to a wall outside the particle's instance");
+            for (int comp = 0; comp < d.ncomp; ++comp) whist[((size_t)comp * d.wmax + w) * NC + sp] = spr[comp];
+            wact[sp] |= 1u << w;
+            continue;
+        }
+        const int si = slot_of(cs->id_i[r]);
+        if (si < 0) return fail(h, DEM_ERR_BAD_INPUT, "contact refers to an unknown particle id");
+        const bool per = cs->periodic && cs->periodic[r];
+        // P's own entry carries the spring; I's entry carries the same spring for
+        // a direct pair and the reversed one for a periodic pair
+        // (BaseInteraction::copySwitchPointer / reverseHistory).
+        if (!set_entry(sp, si, spr, 1.0) || !set_entry(si, sp, spr, per ? -1.0 : 1.0))
+            return fail(h, DEM_ERR_BAD_INPUT, "injected contact is not within the neighbour list");
+    }
+    CU(cudaMemcpyAsync(d.act[cur], act.data(), act.size() * sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(d.wact[cur], wact.data(), wact.size() * sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(d.hist[cur], hist.data(), hist.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(d.whist[cur], whist.data(), whist.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return DEM_OK;
+}
+
+int dem_step(dem_handle* hh, int nsteps)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h) return DEM_ERR_BAD_INPUT;
+    if (nsteps < 0) return fail(h, DEM_ERR_BAD_INPUT, "nsteps must be >= 0");
+    if (!h->uploaded) return fail(h, DEM_ERR_STATE, "dem_upload_particles must come before dem_step");
+    CU(cudaSetDevice(h->device));
+    DevPtrs& d = h->d;
+    long long launches = 0;
+    Control c0;
+    int rc = read_control(h, &c0);
+    if (rc) return rc;
+    const long long rebuilds0 = c0.n_rebuilds;
+    const bool evaluates = d.n > 0 && (h->initial_pending || nsteps > 0);
+    c0.status = 0;
+    if (evaluates) c0.n_records = 0;
+    if (h->initial_pending && d.n > 0) {
+        // DPMBase::initialiseSolve: first force evaluation at the uploaded state.
+        // If dem_upload_contacts already built the lists, they are kept.
+        c0.rebuild = c0.force_rebuild ? 1 : 0;
+        c0.force_rebuild = 0;
+        c0.pending_flip = 1;
+    }
+    CU(cudaMemcpyAsync(h->d_ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaEventRecord(h->ev0, h->stream));
+    if (d.n > 0) {
+        if (h->initial_pending) {
+            if (c0.rebuild) {
+                launch_rebuild(h, h->stream);
+                launches += REBUILD_LAUNCHES;
+            }
+            launch_force(h, h->stream, 0);
+            k_flip<<<1, 32, 0, h->stream>>>(h->d_ctl);
+            launches += 2;
+            CU(cudaGetLastError());
+            h->initial_pending = false;
+        }
+        if (nsteps > 0) {
+            long long sl = nsteps;
+            CU(cudaMemcpyAsync(&h->d_ctl->steps_left, &sl, sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+            k_kick_drift<<<grid_for(d.n, 256), 256, 0, h->stream>>>(d);
+            launches += 1;
+            if (h->cfg.use_graphs) {
+                if (!h->graph1) {
+                    if ((rc = build_graph(h, 1, &h->graph1))) return rc;
+                    if ((rc = build_graph(h, GRAPH_STEPS, &h->graphK))) return rc;
+                }
+                int left = nsteps;
+                while (left >= GRAPH_STEPS) {
+                    CU(cudaGraphLaunch(h->graphK, h->stream));
+                    left -= GRAPH_STEPS;
+                }
+                while (left-- > 0) CU(cudaGraphLaunch(h->graph1, h->stream));
+                launches += 2ll * nsteps;
+            } else {
+                for (int k = 0; k < nsteps; ++k) {
+                    k_control<<<1, 32, 0, h->stream>>>(h->d_ctl, cudaGraphConditionalHandle{}, 0);
+                    launch_rebuild(h, h->stream);
+                    launch_force(h, h->stream, 1);
+                }
+                CU(cudaGetLastError());
+                launches += (2ll + REBUILD_LAUNCHES) * nsteps;
+            }
+            k_flip<<<1, 32, 0, h->stream>>>(h->d_ctl);
+            launches += 1;
+        }
+    }
+    CU(cudaEventRecord(h->ev1, h->stream));
+    Control c;
+    if ((rc = read_control(h, &c))) return rc;
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->last_ms = ms;
+    const long long rb = c.n_rebuilds - rebuilds0;
+    h->last_rebuilds = rb;
+    h->last_launches = launches + (h->cfg.use_graphs ? rb * REBUILD_LAUNCHES : 0);
+    h->steps_total += nsteps;
+    if (evaluates) {
+        h->n_records = c.n_records;
+        h->records_valid = c.n_records <= c.record_capacity;
+        if (!h->records_valid) {
+            // grow the record buffer so that the next evaluation keeps every contact
+            const unsigned need = (unsigned)std::min<unsigned long long>(2000000000ull, 2ull * c.n_records);
+            void* p = nullptr;
+            if (cudaMalloc(&p, (size_t)need * sizeof(ContactRecord)) == cudaSuccess) {
+                h->allocs.push_back(p);
+                h->d_records = static_cast<ContactRecord*>(p);
+                h->record_capacity = need;
+                d.records = h->d_records;
+                free_graphs(h); // the captured kernels hold the old pointer
+                c.record_capacity = need;
+                c.n_records = 0;
+                CU(cudaMemcpyAsync(h->d_ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+                CU(cudaStreamSynchronize(h->stream));
+            }
+        }
+    }
+    return check_status(h, c);
+}
+
+int dem_download_particles(dem_handle* hh, dem_particles_soa* p)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !p) return fail(h, DEM_ERR_BAD_INPUT, "dem_download_particles: bad arguments");
+    if (!h->uploaded) return fail(h, DEM_ERR_STATE, "nothing uploaded");
+    if (p->n != h->d.n) return fail(h, DEM_ERR_BAD_INPUT, "dem_download_particles: n does not match the upload");
+    CU(cudaSetDevice(h->device));
+    Control c;
+    int rc = read_control(h, &c);
+    if (rc) return rc;
+    const int n = h->d.n, b = c.cur;
+    std::vector<double4> pr(n), vm(n), wi(n), qo(n);
+    std::vector<int4> info(n);
+    std::vector<int> caller(n);
+    CU(cudaMemcpyAsync(pr.data(), h->d.pr[b], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(vm.data(), h->d.vm[b], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(wi.data(), h->d.wi[b], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(qo.data(), h->d.qo[b], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(info.data(), h->d.info[b], n * sizeof(int4), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(caller.data(), h->d.caller[b], n * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    for (int s = 0; s < n; ++s) {
+        const int i = caller[s];
+        if (p->position) { p->position[3 * i] = pr[s].x; p->position[3 * i + 1] = pr[s].y; p->position[3 * i + 2] = pr[s].z; }
+        if (p->velocity) { p->velocity[3 * i] = vm[s].x; p->velocity[3 * i + 1] = vm[s].y; p->velocity[3 * i + 2] = vm[s].z; }
+        if (p->angular_velocity) {
+            p->angular_velocity[3 * i] = wi[s].x;
+            p->angular_velocity[3 * i + 1] = wi[s].y;
+            p->angular_velocity[3 * i + 2] = wi[s].z;
+        }
+        if (p->orientation) {
+            p->orientation[4 * i] = qo[s].x; p->orientation[4 * i + 1] = qo[s].y;
+            p->orientation[4 * i + 2] = qo[s].z; p->orientation[4 * i + 3] = qo[s].w;
+        }
+        if (p->radius) p->radius[i] = pr[s].w;
+        if (p->inv_mass) p->inv_mass[i] = vm[s].w;
+        if (p->inv_inertia) p->inv_inertia[i] = wi[s].w;
+        if (p->species) p->species[i] = info[s].y;
+        if (p->id) p->id[i] = info[s].x;
+        if (p->instance) p->instance[i] = info[s].z;
+    }
+    return DEM_OK;
+}
+
+int dem_download_forces(dem_handle* hh, double* force, double* torque)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h) return DEM_ERR_BAD_INPUT;
+    if (!h->uploaded || h->initial_pending) return fail(h, DEM_ERR_STATE, "no force evaluation yet (call dem_step)");
+    CU(cudaSetDevice(h->device));
+    Control c;
+    int rc = read_control(h, &c);
+    if (rc) return rc;
+    const int n = h->d.n;
+    std::vector<double> f(3 * (size_t)n), t(3 * (size_t)n);
+    std::vector<int> caller(n);
+    CU(cudaMemcpyAsync(f.data(), h->d.force, f.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(t.data(), h->d.torque, t.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(caller.data(), h->d.caller[c.cur], n * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    for (int s = 0; s < n; ++s) {
+        const int i = caller[s];
+        for (int k = 0; k < 3; ++k) {
+            if (force) force[3 * i + k] = f[3 * (size_t)s + k];
+            if (torque) torque[3 * i + k] = t[3 * (size_t)s + k];
+        }
+    }
+    return DEM_OK;
+}
+
+int dem_download_contacts(dem_handle* hh, dem_contacts_soa* cs, int64_t capacity, int64_t* count)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !count || capacity < 0) return fail(h, DEM_ERR_BAD_INPUT, "dem_download_contacts: bad arguments");
+    if (!h->uploaded || h->initial_pending) return fail(h, DEM_ERR_STATE, "no force evaluation yet (call dem_step)");
+    if (!h->records_valid)
+        return fail(h, DEM_ERR_CAPACITY, "contact records of the last evaluation overflowed; the buffer has grown, "
+                                         "the next dem_step records all contacts");
+    CU(cudaSetDevice(h->device));
+    const unsigned nr = h->n_records;
+    std::vector<ContactRecord> rec(nr);
+    if (nr) CU(cudaMemcpyAsync(rec.data(), h->d_records, nr * sizeof(ContactRecord), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    std::sort(rec.begin(), rec.end(), [](const ContactRecord& a, const ContactRecord& b) {
+        if (a.is_wall != b.is_wall) return a.is_wall < b.is_wall;
+        if (a.id_p != b.id_p) return a.id_p < b.id_p;
+        return a.id_i < b.id_i;
+    });
+    *count = nr;
+    if (!cs) return DEM_OK;
+    const int64_t m = std::min<int64_t>(capacity, nr);
+    for (int64_t r = 0; r < m; ++r) {
+        const ContactRecord& x = rec[r];
+        if (cs->id_p) cs->id_p[r] = x.id_p;
+        if (cs->id_i) cs->id_i[r] = x.id_i;
+        if (cs->is_wall) cs->is_wall[r] = x.is_wall;
+        if (cs->periodic) cs->periodic[r] = x.periodic;
+        if (cs->overlap) cs->overlap[r] = x.overlap;
+        for (int k = 0; k < 3; ++k)
+            if (cs->force) cs->force[3 * r + k] = x.force[k];
+        for (int k = 0; k < 9; ++k)
+            if (cs->springs) cs->springs[9 * r + k] = x.springs[k];
+    }
+    cs->n = m;
+    return DEM_OK;
+}
+
+int dem_reduce(dem_handle* hh, int instance, dem_globals* out)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !out) return DEM_ERR_BAD_INPUT;
+    if (!h->uploaded) return fail(h, DEM_ERR_STATE, "nothing uploaded");
+    if (instance < 0 || instance >= (int)h->inst.size()) return fail(h, DEM_ERR_BAD_INPUT, "instance out of range");
+    CU(cudaSetDevice(h->device));
+    std::memset(out, 0, sizeof(*out));
+    const int n = h->d.n;
+    const unsigned nb = grid_for(n, 256);
+    const unsigned nr = h->records_valid && !h->initial_pending ? h->n_records : 0;
+    const unsigned nbr = grid_for(nr, 256);
+    double* dpart = nullptr;
+    const size_t slots = (size_t)nb * RED_SLOTS + (size_t)nbr * 3;
+    CU(cudaMallocAsync((void**)&dpart, slots * sizeof(double), h->stream));
+    k_reduce_particles<<<nb, 256, 0, h->stream>>>(h->d, instance, dpart);
+    if (nr) k_reduce_records<<<nbr, 256, 0, h->stream>>>(h->d, instance, nr, dpart + (size_t)nb * RED_SLOTS);
+    std::vector<double> part(slots);
+    CU(cudaMemcpyAsync(part.data(), dpart, slots * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaFreeAsync(dpart, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    double acc[RED_SLOTS] = {0};
+    for (unsigned b = 0; b < nb; ++b)
+        for (int k = 0; k < RED_SLOTS; ++k) acc[k] += part[(size_t)b * RED_SLOTS + k];
+    double racc[3] = {0, 0, 0};
+    for (unsigned b = 0; b < (nr ? nbr : 0); ++b)
+        for (int k = 0; k < 3; ++k) racc[k] += part[(size_t)nb * RED_SLOTS + (size_t)b * 3 + k];
+    out->kinetic_energy = acc[0];
+    out->rotational_energy = acc[1];
+    out->gravitational_energy = acc[2];
+    out->mass = acc[3];
+    for (int k = 0; k < 3; ++k) {
+        out->momentum[k] = acc[4 + k];
+        out->centre_of_mass[k] = acc[3] > 0 ? acc[7 + k] / acc[3] : 0.0;
+        out->angular_momentum[k] = acc[10 + k];
+    }
+    out->elastic_energy = racc[0];
+    out->n_contacts = (int64_t)llround(racc[1]);
+    out->n_wall_contacts = (int64_t)llround(racc[2]);
+    out->time = h->steps_total * h->cfg.time_step;
+    out->n_steps = h->steps_total;
+    return DEM_OK;
+}
+
+int dem_last_step_stats(dem_handle* hh, double* ms, int64_t* kernel_launches, int64_t* rebuilds)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h) return DEM_ERR_BAD_INPUT;
+    if (ms) *ms = h->last_ms;
+    if (kernel_launches) *kernel_launches = h->last_launches;
+    if (rebuilds) *rebuilds = h->last_rebuilds;
+    return DEM_OK;
+}
+
+int dem_get_info(dem_handle* hh, int64_t* n_particles, int64_t* max_neighbors, int64_t* n_cells)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h) return DEM_ERR_BAD_INPUT;
+    if (n_particles) *n_particles = h->d.n;
+    if (max_neighbors) *max_neighbors = h->d.cap;
+    if (n_cells) *n_cells = h->d.ncells;
+    return DEM_OK;
+}
+
+int dem_get_counts(dem_handle* hh, int64_t* list_entries, int64_t* contacts, int64_t* wall_contacts)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h) return DEM_ERR_BAD_INPUT;
+    if (!h->uploaded || h->initial_pending) return fail(h, DEM_ERR_STATE, "no force evaluation yet (call dem_step)");
+    CU(cudaSetDevice(h->device));
+    Control c;
+    int rc = read_control(h, &c);
+    if (rc) return rc;
+    std::vector<int> cnt(h->d.n);
+    CU(cudaMemcpyAsync(cnt.data(), h->d.cnt[c.lbuf], cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<ContactRecord> rec(h->records_valid ? h->n_records : 0);
+    if (!rec.empty())
+        CU(cudaMemcpyAsync(rec.data(), h->d_records, rec.size() * sizeof(ContactRecord), cudaMemcpyDeviceToHost,
+                           h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    long long e = 0, pc = 0, wc = 0;
+    for (int v : cnt) e += v;
+    for (const auto& r : rec) (r.is_wall ? wc : pc) += 1;
+    if (list_entries) *list_entries = e;
+    if (contacts) *contacts = pc;
+    if (wall_contacts) *wall_contacts = wc;
+    return DEM_OK;
+}
+
+int dem_time_force_kernel(dem_handle* hh, int reps, double* ms_per_launch)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || reps <= 0 || !ms_per_launch) return fail(h, DEM_ERR_BAD_INPUT, "dem_time_force_kernel: bad arguments");
+    if (!h->uploaded || h->initial_pending) return fail(h, DEM_ERR_STATE, "no force evaluation yet (call dem_step)");
+    CU(cudaSetDevice(h->device));
+    Control saved;
+    int rc = read_control(h, &saved);
+    if (rc) return rc;
+    // a mid-batch step: second half-kick, next half-kick and drift, written to
+    // the spare buffers; nothing is flipped, so the state stays as it was
+    Control probe = saved;
+    probe.final_step = 0;
+    probe.first_step = 0;
+    probe.pending_flip = 0;
+    probe.record = 0;
+    CU(cudaMemcpyAsync(h->d_ctl, &probe, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+    launch_force(h, h->stream, 1); // warm-up
+    CU(cudaEventRecord(h->ev0, h->stream));
+    for (int r = 0; r < reps; ++r) launch_force(h, h->stream, 1);
+    CU(cudaEventRecord(h->ev1, h->stream));
+    CU(cudaGetLastError());
+    CU(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    *ms_per_launch = ms / reps;
+    CU(cudaMemcpyAsync(h->d_ctl, &saved, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return DEM_OK;
+}
+
+const char* dem_last_error(dem_handle* hh)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    return h ? h->err.c_str() : "null handle";
+}
+
+void dem_destroy(dem_handle* hh)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_particle_arrays(h);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->stream2) cudaStreamDestroy(h->stream2);
+    delete h;
+}
+
+int dem_cg_eval(dem_handle* hh, const dem_cg_grid* grid, double* fields_out);
+
+} // extern "C"
+
+#include "dem_cg.cuh"

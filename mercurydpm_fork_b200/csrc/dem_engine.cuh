@@ -1,0 +1,126 @@
+// dem_engine.cuh -- device data layout shared by the DEM kernels.
+//
+// Layout in HBM (all arrays indexed by the engine's sorted particle order,
+// which is (instance, level, cell, id) after every neighbour-list rebuild):
+//   pr[b][i]   double4 (x, y, z, radius)         b = state buffer 0/1
+//   vm[b][i]   double4 (vx, vy, vz, invMass)
+//   wi[b][i]   double4 (wx, wy, wz, invInertia)
+//   qo[b][i]   double4 orientation quaternion (q0..q3)
+//   info[b][i] int4    (id, species, instance, flags)
+//   caller[b][i] int   index of the particle in the caller's upload order
+// The 32-byte records let a neighbour's position+radius, velocity+mass and
+// angular velocity+inertia each arrive in one 32-byte sector.
+// Neighbour lists are ELL, entry-major: nbr[l][k*ncap + i] (k < count[l][i]),
+// so the k-th entries of 32 consecutive particles are one coalesced load;
+// l = Control::lbuf flips at every rebuild.
+// Contact history is stored per neighbour entry in the same layout,
+// hist[b][(c*cap + k)*ncap + i] for history component c (3 per spring), and
+// an active bit per entry, act[b][w*ncap + i] (bit k%32 of word k/32). The
+// history is double-buffered together with the state (b = Control::cur): a
+// force evaluation reads buffer b and writes b^1, so a thread may read its
+// partner's history of the previous step (needed for periodic pairs) while
+// the partner writes the next one. Reading b and writing b^1 moves the same
+// bytes as an in-place update.
+#pragma once
+#include <cstdint>
+#include "dem_math.cuh"
+#include "../../include/dem_b200.h"
+
+namespace dem {
+
+constexpr int FLAG_FIXED = 1;
+constexpr int LEVEL_SHIFT = 8;
+
+struct InstanceDev {
+    double origin[3];
+    double gravity[3];
+    double per_lo[3];
+    double per_hi[3];
+    double per_L[3];
+    double per_half[3];
+    uint32_t per_mask;
+    int species_offset;
+    int n_species;
+    int wall_begin;
+    int wall_end;
+    int n_levels;
+    int cell_base[DEM_MAX_LEVELS];
+    int dims[DEM_MAX_LEVELS][3];
+    double inv_cell[DEM_MAX_LEVELS][3];
+    double level_rmax[DEM_MAX_LEVELS];
+    double max_interaction_distance;
+};
+
+// Contact record written at the last force evaluation of a dem_step call:
+// one row per contact (particle pairs once, from P's side; wall contacts).
+struct ContactRecord {
+    int id_p, id_i;
+    int is_wall, periodic;
+    int slot_p, slot_i;         // sorted indices (slot_i = wall index for walls)
+    double overlap;
+    double elastic_energy;
+    double force[3];
+    double contact_point[3];
+    double branch[3];           // x_P - x_I (image position for periodic pairs); wall: 0
+    double springs[9];
+};
+
+struct Control {
+    int cur;               // state buffer holding the current state
+    int lbuf;              // neighbour-list buffer in use
+    int pending_flip;      // the last force kernel wrote the other state buffer
+    int rebuild;           // this step rebuilds the neighbour list
+    int final_step;        // this step is the last of the dem_step call
+    int force_rebuild;     // rebuild at the next control point regardless of displacement
+    int record;            // record contacts at final/initial evaluations
+    int pad0;
+    long long steps_left;
+    long long n_rebuilds;
+    long long steps_done;  // time steps since the upload
+    int first_step;        // this step is the first after the initial evaluation
+    int pad1;
+    double disp_acc;       // sum of per-step maximum displacements since the last rebuild
+    double skin;
+    unsigned long long step_disp2_bits; // max |dx|^2 this step (bits of a non-negative double)
+    unsigned int status;   // OR of (1u << DEM_ERR_*)
+    unsigned int n_records;
+    unsigned int record_capacity;
+    unsigned int lost_history;
+};
+
+struct DevPtrs {
+    // particle state, two buffers
+    double4 *pr[2], *vm[2], *wi[2], *qo[2];
+    int4 *info[2];
+    int *caller[2];
+    // forces of the last force evaluation (3 per particle, sorted order)
+    double *force, *torque;
+    // neighbour lists, two buffers
+    int *nbr[2];
+    int *cnt[2];
+    double *hist[2];
+    unsigned int *act[2];
+    double *whist[2];
+    unsigned int *wact[2];
+    // broad phase scratch
+    int *key, *perm, *newidx, *cell_count, *cell_start, *cell_cursor, *block_sums;
+    // tables
+    const InstanceDev *inst;
+    const dem_species_pair *species;
+    const dem_wall *walls;
+    Control *ctl;
+    ContactRecord *records;
+    // sizes
+    int n;            // particles
+    int ncap;         // allocated particle slots (ELL stride)
+    int cap;          // neighbour capacity per particle (multiple of 32)
+    int nwords;       // cap / 32
+    int ncomp;        // history components per contact (3 or 9)
+    int wmax;         // max walls per instance
+    int ncells;
+    int rotation;
+    double dt;
+    double drag;
+};
+
+} // namespace dem

@@ -1,0 +1,859 @@
+// dem_kernels.cuh -- the DEM time-step kernels.
+//
+// Per time step (captured in a CUDA graph):
+//   k_control   one thread: applies the pending state-buffer flip, adds the
+//               last step's maximum displacement to the skin budget and sets
+//               the graph condition that runs the rebuild body
+//               (MercuryBase::hGridNeedsRebuilding, MercuryBase.cc:496-535,
+//               turned into a Verlet-skin test).
+//   rebuild     k_keys -> scan -> k_scatter -> k_cell_sort -> k_gather ->
+//               k_build -> k_rb_finish: cell keys per HGrid level, counting
+//               sort, per-cell ordering by particle id, permutation gather of
+//               the state, neighbour lists with contact-history carry-over
+//               (replaces HGrid buckets + InteractionHandler lookup,
+//               Mercury3D.cc:224-416, InteractionHandler.cc:103-174).
+//   k_force     one thread per particle: every neighbour-list entry is tested
+//               with the reference's exact FP64 contact predicate
+//               (BaseParticle::getInteractionWith, BaseParticle.cc:688-710),
+//               the contact law runs with the entry's spring history, walls
+//               and body forces are added, and the particle is integrated
+//               (second half-kick of this step, then first half-kick and
+//               drift of the next one: BaseParticle.cc:718-776) into the
+//               other state buffer.
+#pragma once
+#include "dem_engine.cuh"
+#include "dem_laws.cuh"
+
+namespace dem {
+
+__device__ __forceinline__ V3 xyz(double4 a) { return V3{a.x, a.y, a.z}; }
+
+// ---------------------------------------------------------------------------
+// control
+// ---------------------------------------------------------------------------
+__global__ void k_control(Control* ctl, cudaGraphConditionalHandle handle, int use_handle)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (ctl->pending_flip) {
+        ctl->cur ^= 1;
+        ctl->pending_flip = 0;
+    }
+    const double d = sqrt(__longlong_as_double((long long)ctl->step_disp2_bits));
+    ctl->step_disp2_bits = 0ull;
+    ctl->disp_acc += d;
+    const int rebuild = ctl->force_rebuild || (2.0 * ctl->disp_acc >= ctl->skin);
+    ctl->rebuild = rebuild;
+    ctl->force_rebuild = 0;
+    ctl->final_step = (ctl->steps_left <= 1);
+    ctl->steps_left -= 1;
+    ctl->first_step = (ctl->steps_done == 0);
+    ctl->steps_done += 1;
+    ctl->pending_flip = 1; // the force kernel of this step writes the other buffer
+    if (use_handle) cudaGraphSetConditional(handle, rebuild ? 1u : 0u);
+}
+
+__global__ void k_flip(Control* ctl)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (ctl->pending_flip) {
+        ctl->cur ^= 1;
+        ctl->pending_flip = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// broad phase
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ int cell_coord(double x, double origin, double inv, int dim)
+{
+    const double f = floor((x - origin) * inv);
+    // positions far outside the grid are clamped into the edge cells
+    if (!(f >= 0.0)) return 0;
+    if (f >= (double)(dim - 1)) return dim - 1;
+    return (int)f;
+}
+
+__global__ void k_keys(DevPtrs d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!d.ctl->rebuild || i >= d.n) return;
+    const int c = d.ctl->cur;
+    const double4 p = d.pr[c][i];
+    const int4 inf = d.info[c][i];
+    const InstanceDev& I = d.inst[inf.z];
+    const int lvl = (inf.w >> LEVEL_SHIFT) & 0xff;
+    const int cx = cell_coord(p.x, I.origin[0], I.inv_cell[lvl][0], I.dims[lvl][0]);
+    const int cy = cell_coord(p.y, I.origin[1], I.inv_cell[lvl][1], I.dims[lvl][1]);
+    const int cz = cell_coord(p.z, I.origin[2], I.inv_cell[lvl][2], I.dims[lvl][2]);
+    const int key = I.cell_base[lvl] + (cz * I.dims[lvl][1] + cy) * I.dims[lvl][0] + cx;
+    d.key[i] = key;
+    atomicAdd(&d.cell_count[key], 1);
+}
+
+// Exclusive scan of cell_count into cell_start, 1024 cells per block.
+__device__ __forceinline__ int block_inclusive_scan_1024(int v, int* warp_sums)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) warp_sums[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int w = warp_sums[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        warp_sums[lane] = w;
+    }
+    __syncthreads();
+    if (wid > 0) v += warp_sums[wid - 1];
+    return v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_blocks(DevPtrs d)
+{
+    __shared__ int ws[32];
+    if (!d.ctl->rebuild) return;
+    const int i = blockIdx.x * 1024 + threadIdx.x;
+    const int v = (i < d.ncells) ? d.cell_count[i] : 0;
+    const int inc = block_inclusive_scan_1024(v, ws);
+    if (i < d.ncells) d.cell_start[i] = inc - v;
+    if (threadIdx.x == 1023) d.block_sums[blockIdx.x] = inc;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_sums(DevPtrs d, int nblocks)
+{
+    __shared__ int ws[32];
+    __shared__ int carry;
+    if (!d.ctl->rebuild) return;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nblocks; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int v = (i < nblocks) ? d.block_sums[i] : 0;
+        const int inc = block_inclusive_scan_1024(v, ws);
+        const int c0 = carry;
+        if (i < nblocks) d.block_sums[i] = c0 + inc - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = c0 + inc;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) d.cell_start[d.ncells] = carry;
+}
+
+__global__ void k_scan_add(DevPtrs d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!d.ctl->rebuild || i >= d.ncells) return;
+    d.cell_start[i] += d.block_sums[i >> 10];
+}
+
+__global__ void k_scatter(DevPtrs d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!d.ctl->rebuild || i >= d.n) return;
+    const int key = d.key[i];
+    const int slot = d.cell_start[key] + atomicAdd(&d.cell_cursor[key], 1);
+    d.perm[slot] = i;
+}
+
+// Orders the members of every cell by particle id, so the sorted order (and
+// with it every neighbour list and force sum) does not depend on the order in
+// which the atomics above were served. Resets the counters for the next rebuild.
+__global__ void k_cell_sort(DevPtrs d)
+{
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!d.ctl->rebuild || cell >= d.ncells) return;
+    const int b = d.cell_start[cell], e = d.cell_start[cell + 1];
+    const int c = d.ctl->cur;
+    d.cell_count[cell] = 0;
+    d.cell_cursor[cell] = 0;
+    if (e - b < 2) return;
+    if (e - b > 512) { // pathological pile-up (e.g. particles far outside the grid)
+        atomicOr(&d.ctl->status, 1u << DEM_ERR_DOMAIN);
+        return;
+    }
+    for (int a = b + 1; a < e; ++a) {
+        const int v = d.perm[a];
+        const int id = d.info[c][v].x;
+        int k = a - 1;
+        while (k >= b && d.info[c][d.perm[k]].x > id) {
+            d.perm[k + 1] = d.perm[k];
+            --k;
+        }
+        d.perm[k + 1] = v;
+    }
+}
+
+__global__ void k_gather(DevPtrs d)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!d.ctl->rebuild || s >= d.n) return;
+    const int c = d.ctl->cur, nb = c ^ 1;
+    const int o = d.perm[s];
+    d.pr[nb][s] = d.pr[c][o];
+    d.vm[nb][s] = d.vm[c][o];
+    d.wi[nb][s] = d.wi[c][o];
+    d.qo[nb][s] = d.qo[c][o];
+    d.info[nb][s] = d.info[c][o];
+    d.caller[nb][s] = d.caller[c][o];
+    d.newidx[o] = s;
+}
+
+// Minimum-image position of particle t as seen from position xs, with the
+// rounding of a periodic ghost: x_t +- L (PeriodicBoundary::shiftPosition,
+// PeriodicBoundary.cc:219-229).
+__device__ __forceinline__ V3 image_of(const InstanceDev& I, V3 xs, V3 xt, bool& periodic)
+{
+    periodic = false;
+    if (I.per_mask) {
+        double* c = &xt.x;
+        const double* s = &xs.x;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if ((I.per_mask >> k) & 1u) {
+                const double raw = s[k] - c[k];
+                if (raw > I.per_half[k]) {
+                    c[k] = c[k] + I.per_L[k];
+                    periodic = true;
+                } else if (raw < -I.per_half[k]) {
+                    c[k] = c[k] - I.per_L[k];
+                    periodic = true;
+                }
+            }
+        }
+    }
+    return xt;
+}
+
+__device__ __forceinline__ void cell_range(const InstanceDev& I, int lvl, int k, double x, double reach, int& lo,
+                                           int& hi)
+{
+    const int dim = I.dims[lvl][k];
+    const double inv = I.inv_cell[lvl][k];
+    const double flo = floor((x - reach - I.origin[k]) * inv);
+    const double fhi = floor((x + reach - I.origin[k]) * inv);
+    if ((I.per_mask >> k) & 1u) {
+        // periodic: wrap, but visit each cell at most once
+        double span = fhi - flo + 1.0;
+        if (span > (double)dim) {
+            lo = 0;
+            hi = dim - 1;
+        } else {
+            lo = (int)flo;
+            hi = (int)fhi;
+        }
+    } else {
+        lo = (flo < 0.0) ? 0 : ((flo > (double)(dim - 1)) ? dim - 1 : (int)flo);
+        hi = (fhi < 0.0) ? 0 : ((fhi > (double)(dim - 1)) ? dim - 1 : (int)fhi);
+    }
+}
+
+__device__ __forceinline__ int wrap_cell(int c, int dim)
+{
+    c %= dim;
+    return c < 0 ? c + dim : c;
+}
+
+__global__ void __launch_bounds__(128) k_build(DevPtrs d)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!d.ctl->rebuild || s >= d.n) return;
+    const int hc = d.ctl->cur;         // old state order and its history
+    const int nb = hc ^ 1;             // gathered (new) state; new history
+    const int lo_ = d.ctl->lbuf;       // old lists
+    const int ln = lo_ ^ 1;            // new lists
+    const double4 ps = d.pr[nb][s];
+    const int4 is = d.info[nb][s];
+    const InstanceDev& I = d.inst[is.z];
+    const V3 xs = xyz(ps);
+    const bool fixed_s = (is.w & FLAG_FIXED) != 0;
+    const double extra = I.max_interaction_distance + d.ctl->skin;
+    int count = 0;
+    bool overflow = false;
+    for (int lvl = 0; lvl < I.n_levels; ++lvl) {
+        const double reach = ps.w + I.level_rmax[lvl] + extra;
+        int lo[3], hi[3];
+        cell_range(I, lvl, 0, xs.x, reach, lo[0], hi[0]);
+        cell_range(I, lvl, 1, xs.y, reach, lo[1], hi[1]);
+        cell_range(I, lvl, 2, xs.z, reach, lo[2], hi[2]);
+        const int dx = I.dims[lvl][0], dy = I.dims[lvl][1], dz = I.dims[lvl][2];
+        for (int cz = lo[2]; cz <= hi[2]; ++cz) {
+            const int wz = ((I.per_mask >> 2) & 1u) ? wrap_cell(cz, dz) : cz;
+            for (int cy = lo[1]; cy <= hi[1]; ++cy) {
+                const int wy = ((I.per_mask >> 1) & 1u) ? wrap_cell(cy, dy) : cy;
+                for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+                    const int wx = (I.per_mask & 1u) ? wrap_cell(cx, dx) : cx;
+                    const int cell = I.cell_base[lvl] + (wz * dy + wy) * dx + wx;
+                    const int b = d.cell_start[cell], e = d.cell_start[cell + 1];
+                    for (int t = b; t < e; ++t) {
+                        if (t == s) continue;
+                        const int4 it = d.info[nb][t];
+                        if (fixed_s && (it.w & FLAG_FIXED)) continue; // DPMBase.cc:3116-3120
+                        const double4 pt = d.pr[nb][t];
+                        bool per;
+                        const V3 xt = image_of(I, xs, xyz(pt), per);
+                        const V3 br = xs - xt;
+                        const double cut = ps.w + pt.w + extra;
+                        if (len2(br) < cut * cut) {
+                            if (count < d.cap) {
+                                d.nbr[ln][(size_t)count * d.ncap + s] = t;
+                            } else {
+                                overflow = true;
+                            }
+                            ++count;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (overflow) {
+        atomicOr(&d.ctl->status, 1u << DEM_ERR_CAPACITY);
+        count = d.cap;
+    }
+    d.cnt[ln][s] = count;
+
+    // carry contact history from the old list (old order) to the new one
+    const int o = d.perm[s];
+    const int ocnt = d.cnt[lo_][o];
+    unsigned int neww[4] = {0u, 0u, 0u, 0u};
+    for (int w = 0; w < d.nwords; ++w) {
+        unsigned int bits = d.act[hc][(size_t)w * d.ncap + o];
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const int k = w * 32 + b;
+            if (k >= ocnt) break;
+            const int tnew = d.newidx[d.nbr[lo_][(size_t)k * d.ncap + o]];
+            int m = -1;
+            for (int q = 0; q < count; ++q) {
+                if (d.nbr[ln][(size_t)q * d.ncap + s] == tnew) {
+                    m = q;
+                    break;
+                }
+            }
+            if (m < 0) {
+                atomicAdd(&d.ctl->lost_history, 1u);
+                continue;
+            }
+            for (int comp = 0; comp < d.ncomp; ++comp)
+                d.hist[nb][((size_t)comp * d.cap + m) * d.ncap + s] =
+                    d.hist[hc][((size_t)comp * d.cap + k) * d.ncap + o];
+            neww[m >> 5] |= 1u << (m & 31);
+        }
+    }
+    for (int w = 0; w < d.nwords; ++w) d.act[nb][(size_t)w * d.ncap + s] = neww[w];
+    // wall history moves with the particle
+    const unsigned int wbits = d.wact[hc][o];
+    d.wact[nb][s] = wbits;
+    unsigned int bits = wbits;
+    while (bits) {
+        const int w = __ffs(bits) - 1;
+        bits &= bits - 1;
+        for (int comp = 0; comp < d.ncomp; ++comp)
+            d.whist[nb][((size_t)comp * d.wmax + w) * d.ncap + s] =
+                d.whist[hc][((size_t)comp * d.wmax + w) * d.ncap + o];
+    }
+}
+
+__global__ void k_rb_finish(DevPtrs d)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Control* ctl = d.ctl;
+    if (!ctl->rebuild) return;
+    ctl->cur ^= 1;
+    ctl->lbuf ^= 1;
+    ctl->disp_acc = 0.0;
+    ctl->n_rebuilds += 1;
+}
+
+// ---------------------------------------------------------------------------
+// force + integration
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void load_springs(const double* h, size_t base, size_t stride, int ncomp, Springs& s)
+{
+    s.slide = v3(h[base], h[base + stride], h[base + 2 * stride]);
+    if (ncomp > 3) {
+        s.roll = v3(h[base + 3 * stride], h[base + 4 * stride], h[base + 5 * stride]);
+        s.tors = v3(h[base + 6 * stride], h[base + 7 * stride], h[base + 8 * stride]);
+    } else {
+        s.roll = zero3();
+        s.tors = zero3();
+    }
+}
+
+__device__ __forceinline__ void store_springs(double* h, size_t base, size_t stride, int ncomp, const Springs& s)
+{
+    h[base] = s.slide.x;
+    h[base + stride] = s.slide.y;
+    h[base + 2 * stride] = s.slide.z;
+    if (ncomp > 3) {
+        h[base + 3 * stride] = s.roll.x;
+        h[base + 4 * stride] = s.roll.y;
+        h[base + 5 * stride] = s.roll.z;
+        h[base + 6 * stride] = s.tors.x;
+        h[base + 7 * stride] = s.tors.y;
+        h[base + 8 * stride] = s.tors.z;
+    }
+}
+
+__device__ __forceinline__ void write_record(const DevPtrs& d, int id_p, int id_i, int is_wall, int periodic,
+                                             int slot_p, int slot_i, const ContactGeom& g, const ContactOut& out,
+                                             const Springs& s, double spring_energy)
+{
+    const unsigned int idx = atomicAdd(&d.ctl->n_records, 1u);
+    if (idx >= d.ctl->record_capacity) return;
+    ContactRecord& r = d.records[idx];
+    r.id_p = id_p;
+    r.id_i = id_i;
+    r.is_wall = is_wall;
+    r.periodic = periodic;
+    r.slot_p = slot_p;
+    r.slot_i = slot_i;
+    r.overlap = g.overlap;
+    r.elastic_energy = out.normal_stiffness_energy + spring_energy;
+    r.force[0] = out.force.x; r.force[1] = out.force.y; r.force[2] = out.force.z;
+    r.contact_point[0] = g.c.x; r.contact_point[1] = g.c.y; r.contact_point[2] = g.c.z;
+    const V3 br = is_wall ? zero3() : g.xp - g.xi;
+    r.branch[0] = br.x; r.branch[1] = br.y; r.branch[2] = br.z;
+    r.springs[0] = s.slide.x; r.springs[1] = s.slide.y; r.springs[2] = s.slide.z;
+    r.springs[3] = s.roll.x; r.springs[4] = s.roll.y; r.springs[5] = s.roll.z;
+    r.springs[6] = s.tors.x; r.springs[7] = s.tors.y; r.springs[8] = s.tors.z;
+}
+
+// Elastic energy of the tangential springs (SlidingFrictionInteraction.cc:239-246,
+// FrictionInteraction / Mindlin getElasticEnergy): used for the energy balance only.
+__device__ __forceinline__ double spring_energy(const dem_species_pair& sp, const Springs& s, double meff)
+{
+    if (sp.friction_law == DEM_FRICTION_SLIDING || sp.friction_law == DEM_FRICTION_ROLLING_TORSION) {
+        double e = sp.constant_restitution ? meff * sp.sliding_stiffness * len2(s.slide)
+                                           : 0.5 * sp.sliding_stiffness * len2(s.slide);
+        if (sp.friction_law == DEM_FRICTION_ROLLING_TORSION) {
+            e += sp.constant_restitution ? meff * sp.rolling_stiffness * len2(s.roll)
+                                         : 0.5 * sp.rolling_stiffness * len2(s.roll);
+            e += sp.constant_restitution ? meff * sp.torsion_stiffness * len2(s.tors)
+                                         : 0.5 * sp.torsion_stiffness * len2(s.tors);
+        }
+        return e;
+    }
+    return 0.0;
+}
+
+// Evaluates a wall's signed distance and outward normal for a particle at x.
+// Returns false when there is no contact within r + interaction distance.
+__device__ bool wall_distance(const dem_wall& w, V3 x, double wall_radius, double& dist, V3& normal);
+
+template <int MODE> // 0: initial force evaluation, 1: time step
+__global__ void __launch_bounds__(128) k_force(DevPtrs d)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    Control* ctl = d.ctl;
+    double disp2 = 0.0;
+    if (s < d.n) {
+        const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
+        const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
+        const bool record = final_step && ctl->record;
+        const double4 ps = d.pr[c][s];
+        const double4 vs = d.vm[c][s];
+        const double4 ws = d.wi[c][s];
+        double4 qs = d.qo[c][s];
+        const int4 is = d.info[c][s];
+        const InstanceDev& I = d.inst[is.z];
+        const V3 xs = xyz(ps), vel = xyz(vs), om = xyz(ws);
+        const bool fixed_s = (is.w & FLAG_FIXED) != 0;
+        const int ns = I.n_species;
+        const double dt = d.dt;
+        V3 F = zero3(), T = zero3();
+
+        const int count = d.cnt[l][s];
+        // first time step after the initial evaluation: the reference's
+        // initialiseSolve and step 0 stamp contacts with the same time stamp
+        // (DPMBase.cc:4180-4259, :4315-4389); see the two uses below
+        const bool first = (MODE == 1) && ctl->first_step;
+        unsigned int actw[4] = {0u, 0u, 0u, 0u};
+        unsigned int neww[4] = {0u, 0u, 0u, 0u};
+        for (int w = 0; w < d.nwords; ++w) actw[w] = d.act[c][(size_t)w * d.ncap + s];
+        const size_t hstride = (size_t)d.cap * d.ncap;
+        const double* hin = d.hist[c];
+        double* hout = d.hist[nb];
+
+        for (int k = 0; k < count; ++k) {
+            const int t = d.nbr[l][(size_t)k * d.ncap + s];
+            const double4 pt = d.pr[c][t];
+            const int4 it = d.info[c][t];
+            bool periodic;
+            const V3 xt = image_of(I, xs, xyz(pt), periodic);
+            // P is the lower id (DPMBase.cc:3129-3139); against a periodic
+            // ghost the real particle is P (ghosts carry higher ids)
+            const bool selfP = periodic || (is.x < it.x);
+            const V3 branch = selfP ? xs - xt : xt - xs;
+            const double d2 = len2(branch);
+            const dem_species_pair& sp =
+                d.species[I.species_offset + (selfP ? is.y * ns + it.y : it.y * ns + is.y)];
+            const double rP = selfP ? ps.w : pt.w;
+            const double rI = selfP ? pt.w : ps.w;
+            const double sum = rI + rP + sp.interaction_distance;
+            const bool was_active = (actw[k >> 5] >> (k & 31)) & 1u;
+            const size_t hb = (size_t)k * d.ncap + s;
+            // the higher-id side of a periodic pair restarts every step from the
+            // reversed spring of the lower-id side (InteractionHandler.cc:316-368,
+            // BaseInteraction::copySwitchPointer / reverseHistory)
+            const bool derived = periodic && (is.x > it.x);
+            if (d2 >= sum * sum) { // BaseParticle.cc:695-697: no contact
+                if (first && was_active && !derived) {
+                    // an interaction of the initial evaluation outlives step 0
+                    // (InteractionHandler::eraseOldInteractions, stamps <= 0 only)
+                    Springs keep;
+                    load_springs(hin, hb, hstride, d.ncomp, keep);
+                    store_springs(hout, hb, hstride, d.ncomp, keep);
+                    neww[k >> 5] |= 1u << (k & 31);
+                }
+                continue;
+            }
+            const double4 vt4 = d.vm[c][t];
+            const double4 wt4 = d.wi[c][t];
+            ContactGeom g;
+            g.distance = sqrt(d2);
+            g.n = branch / g.distance;
+            g.overlap = rP + rI - g.distance;
+            if (selfP) {
+                g.xp = xs; g.vp = vel; g.wp = om; g.inv_mass_p = vs.w;
+                g.xi = xt; g.vi = xyz(vt4); g.wi = xyz(wt4); g.inv_mass_i = vt4.w;
+            } else {
+                g.xp = xt; g.vp = xyz(vt4); g.wp = xyz(wt4); g.inv_mass_p = vt4.w;
+                g.xi = xs; g.vi = vel; g.wi = om; g.inv_mass_i = vs.w;
+            }
+            g.c = g.xp - (rP - 0.5 * g.overlap) * g.n;
+            g.curv_p = 1.0 / rP;
+            g.curv_i = 1.0 / rI;
+            g.i_is_wall = false;
+            Springs spr;
+            spr.slide = zero3(); spr.roll = zero3(); spr.tors = zero3();
+            if (derived) {
+                const int tc = d.cnt[l][t];
+                for (int m = 0; m < tc; ++m) {
+                    if (d.nbr[l][(size_t)m * d.ncap + t] != s) continue;
+                    if ((d.act[c][(size_t)(m >> 5) * d.ncap + t] >> (m & 31)) & 1u) {
+                        load_springs(hin, (size_t)m * d.ncap + t, hstride, d.ncomp, spr);
+                        spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
+                    }
+                    break;
+                }
+            } else if (was_active) {
+                load_springs(hin, hb, hstride, d.ncomp, spr);
+            }
+            const Springs before = spr;
+            ContactOut out;
+            evaluate_contact(sp, g, spr, dt, out);
+            // step 0 keeps the lower-id side's old spring of a periodic pair
+            // that existed at the initial evaluation (equal stamps,
+            // InteractionHandler.cc:339-352)
+            store_springs(hout, hb, hstride, d.ncomp, (first && periodic && !derived && was_active) ? before : spr);
+            neww[k >> 5] |= 1u << (k & 31);
+            if (selfP) {
+                F += out.force;
+                T += out.torque - cross(xs - g.c, out.force);
+            } else {
+                F += -out.force;
+                T += -out.torque + cross(xs - g.c, out.force);
+            }
+            if (record && (periodic ? (is.x < it.x) : selfP)) {
+                const double meff = 1.0 / (g.inv_mass_p + g.inv_mass_i);
+                write_record(d, is.x, it.x, 0, periodic ? 1 : 0, s, t, g, out, spr, spring_energy(sp, spr, meff));
+            }
+        }
+        for (int w = 0; w < d.nwords; ++w) d.act[nb][(size_t)w * d.ncap + s] = neww[w];
+
+        if (!fixed_s) {
+            // body forces: DPMBase::computeExternalForces (DPMBase.cc:3168-3179)
+            const double m = 1.0 / vs.w;
+            const V3 g3 = v3(I.gravity[0], I.gravity[1], I.gravity[2]);
+            F += g3 * m - d.drag * vel;
+            // walls: DPMBase::computeForcesDueToWalls (DPMBase.cc:3188-3215)
+            unsigned int wact = d.wact[c][s];
+            unsigned int wnew = 0u;
+            const size_t wstride = (size_t)d.wmax * d.ncap;
+            for (int w = I.wall_begin; w < I.wall_end; ++w) {
+                const int wl = w - I.wall_begin;
+                const dem_wall& wall = d.walls[w];
+                const dem_species_pair& sp = d.species[I.species_offset + is.y * ns + wall.species];
+                double dist;
+                V3 nrm;
+                const size_t hb = (size_t)wl * d.ncap + s;
+                if (!wall_distance(wall, xs, ps.w + sp.interaction_distance, dist, nrm)) {
+                    if (first && ((wact >> wl) & 1u)) { // survives step 0, as for particle pairs
+                        Springs keep;
+                        load_springs(d.whist[c], hb, wstride, d.ncomp, keep);
+                        store_springs(d.whist[nb], hb, wstride, d.ncomp, keep);
+                        wnew |= 1u << wl;
+                    }
+                    continue;
+                }
+                ContactGeom g;
+                g.n = -nrm;
+                g.distance = dist;
+                g.overlap = ps.w - dist;
+                g.c = xs - (ps.w - 0.5 * g.overlap) * g.n;
+                g.xp = xs; g.vp = vel; g.wp = om; g.inv_mass_p = vs.w; g.curv_p = 1.0 / ps.w;
+                g.xi = v3(wall.position[0], wall.position[1], wall.position[2]);
+                g.vi = v3(wall.velocity[0], wall.velocity[1], wall.velocity[2]);
+                g.wi = v3(wall.angular_velocity[0], wall.angular_velocity[1], wall.angular_velocity[2]);
+                g.inv_mass_i = 0.0;
+                g.curv_i = 0.0;
+                g.i_is_wall = true;
+                Springs spr;
+                if ((wact >> wl) & 1u) {
+                    load_springs(d.whist[c], hb, wstride, d.ncomp, spr);
+                } else {
+                    spr.slide = zero3(); spr.roll = zero3(); spr.tors = zero3();
+                }
+                ContactOut out;
+                evaluate_contact(sp, g, spr, dt, out);
+                store_springs(d.whist[nb], hb, wstride, d.ncomp, spr);
+                wnew |= 1u << wl;
+                F += out.force;
+                T += out.torque - cross(xs - g.c, out.force);
+                if (record) {
+                    const double meff = 1.0 / vs.w;
+                    write_record(d, is.x, w, 1, 0, s, w, g, out, spr, spring_energy(sp, spr, meff));
+                }
+            }
+            d.wact[nb][s] = wnew;
+        } else {
+            d.wact[nb][s] = 0u;
+        }
+        if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z))) atomicOr(&ctl->status, 1u << DEM_ERR_NAN);
+
+        // ---- integration ----
+        double4 pn = ps, vn = vs, wn = ws;
+        if (final_step) {
+            d.force[3 * (size_t)s + 0] = F.x;
+            d.force[3 * (size_t)s + 1] = F.y;
+            d.force[3 * (size_t)s + 2] = F.z;
+            d.torque[3 * (size_t)s + 0] = T.x;
+            d.torque[3 * (size_t)s + 1] = T.y;
+            d.torque[3 * (size_t)s + 2] = T.z;
+        }
+        if (MODE == 1) {
+            V3 x = xs, v = vel, w = om;
+            Q4 q{qs.x, qs.y, qs.z, qs.w};
+            if (vs.w != 0.0) {
+                const V3 a = ((F * vs.w) * 0.5) * dt;
+                v += a; // BaseParticle::integrateAfterForceComputation
+                V3 aw = zero3();
+                if (d.rotation) {
+                    const S33 Ib{ws.w, 0.0, 0.0, ws.w, 0.0, ws.w};
+                    aw = ((rotate_inverse_inertia(q, Ib) * T) * 0.5) * dt;
+                    w += aw;
+                }
+                if (!final_step) { // BaseParticle::integrateBeforeForceComputation of the next step
+                    v += a;
+                    const V3 disp = v * dt;
+                    x += disp;
+                    disp2 = len2(disp);
+                    if (d.rotation) {
+                        w += aw;
+                        q = quat_rotate(q, w * dt);
+                    }
+                }
+            } else if (!final_step) { // BaseInteractable::integrateBeforeForceComputation
+                const V3 disp = v * dt;
+                x += disp;
+                disp2 = len2(disp);
+                q = quat_rotate(q, w * dt);
+            }
+            if (!final_step && I.per_mask) { // PeriodicBoundary::checkBoundaryAfterParticlesMove
+                double* xc = &x.x;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if ((I.per_mask >> k) & 1u) {
+                        const double dl = xc[k] - I.per_lo[k], dr = I.per_hi[k] - xc[k];
+                        if ((dl < dr ? dl : dr) < 0) {
+                            if (I.per_hi[k] - xc[k] > xc[k] - I.per_lo[k])
+                                xc[k] = xc[k] + I.per_L[k];
+                            else
+                                xc[k] = xc[k] - I.per_L[k];
+                        }
+                    }
+                }
+            }
+            pn = make_double4(x.x, x.y, x.z, ps.w);
+            vn = make_double4(v.x, v.y, v.z, vs.w);
+            wn = make_double4(w.x, w.y, w.z, ws.w);
+            qs = make_double4(q.q0, q.q1, q.q2, q.q3);
+        }
+        d.pr[nb][s] = pn;
+        d.vm[nb][s] = vn;
+        d.wi[nb][s] = wn;
+        d.qo[nb][s] = qs;
+        d.info[nb][s] = is;
+        d.caller[nb][s] = d.caller[c][s];
+    }
+    // maximum displacement of this step (for the skin test)
+    if (MODE == 1) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) disp2 = fmax(disp2, __shfl_xor_sync(0xffffffffu, disp2, o));
+        if ((threadIdx.x & 31) == 0 && disp2 > 0.0)
+            atomicMax(&ctl->step_disp2_bits, (unsigned long long)__double_as_longlong(disp2));
+    }
+}
+
+// First half-kick and drift from the stored forces: the
+// integrateBeforeForceComputation that opens every dem_step call. It only
+// touches each particle's own record, so it updates the current buffer in place.
+__global__ void __launch_bounds__(256) k_kick_drift(DevPtrs d)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    Control* ctl = d.ctl;
+    double disp2 = 0.0;
+    if (s < d.n) {
+        const int c = ctl->cur;
+        const double4 ps = d.pr[c][s];
+        const double4 vs = d.vm[c][s];
+        const double4 ws = d.wi[c][s];
+        const double4 qs = d.qo[c][s];
+        const int4 is = d.info[c][s];
+        const InstanceDev& I = d.inst[is.z];
+        const double dt = d.dt;
+        V3 x = xyz(ps), v = xyz(vs), w = xyz(ws);
+        Q4 q{qs.x, qs.y, qs.z, qs.w};
+        const V3 F = v3(d.force[3 * (size_t)s], d.force[3 * (size_t)s + 1], d.force[3 * (size_t)s + 2]);
+        const V3 T = v3(d.torque[3 * (size_t)s], d.torque[3 * (size_t)s + 1], d.torque[3 * (size_t)s + 2]);
+        if (vs.w != 0.0) {
+            v += ((F * vs.w) * 0.5) * dt;
+            const V3 disp = v * dt;
+            x += disp;
+            disp2 = len2(disp);
+            if (d.rotation) {
+                const S33 Ib{ws.w, 0.0, 0.0, ws.w, 0.0, ws.w};
+                w += ((rotate_inverse_inertia(q, Ib) * T) * 0.5) * dt;
+                q = quat_rotate(q, w * dt);
+            }
+        } else {
+            const V3 disp = v * dt;
+            x += disp;
+            disp2 = len2(disp);
+            q = quat_rotate(q, w * dt);
+        }
+        if (I.per_mask) {
+            double* xc = &x.x;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if ((I.per_mask >> k) & 1u) {
+                    const double dl = xc[k] - I.per_lo[k], dr = I.per_hi[k] - xc[k];
+                    if ((dl < dr ? dl : dr) < 0) {
+                        if (I.per_hi[k] - xc[k] > xc[k] - I.per_lo[k])
+                            xc[k] = xc[k] + I.per_L[k];
+                        else
+                            xc[k] = xc[k] - I.per_L[k];
+                    }
+                }
+            }
+        }
+        d.pr[c][s] = make_double4(x.x, x.y, x.z, ps.w);
+        d.vm[c][s] = make_double4(v.x, v.y, v.z, vs.w);
+        d.wi[c][s] = make_double4(w.x, w.y, w.z, ws.w);
+        d.qo[c][s] = make_double4(q.q0, q.q1, q.q2, q.q3);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) disp2 = fmax(disp2, __shfl_xor_sync(0xffffffffu, disp2, o));
+    if ((threadIdx.x & 31) == 0 && disp2 > 0.0)
+        atomicMax(&ctl->step_disp2_bits, (unsigned long long)__double_as_longlong(disp2));
+}
+
+} // namespace dem
+
+namespace dem {
+
+// ---------------------------------------------------------------------------
+// global balances (DPMBase.cc:1528-1640); per-block partial sums, summed on
+// the host in block order so the result does not depend on scheduling.
+// slots: 0 kinetic, 1 rotational, 2 gravitational, 3 mass, 4-6 momentum,
+//        7-9 mass*position, 10-12 angular momentum (I omega)
+// ---------------------------------------------------------------------------
+constexpr int RED_SLOTS = 13;
+
+__global__ void __launch_bounds__(256) k_reduce_particles(DevPtrs d, int instance, double* partial)
+{
+    __shared__ double sh[RED_SLOTS][8];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[RED_SLOTS];
+#pragma unroll
+    for (int k = 0; k < RED_SLOTS; ++k) v[k] = 0.0;
+    if (s < d.n) {
+        const int c = d.ctl->cur;
+        const int4 is = d.info[c][s];
+        if (is.z == instance && !(is.w & FLAG_FIXED)) {
+            const double4 p = d.pr[c][s];
+            const double4 vm = d.vm[c][s];
+            const double4 w = d.wi[c][s];
+            const InstanceDev& I = d.inst[is.z];
+            const double m = 1.0 / vm.w;
+            const V3 vel = xyz(vm), om = xyz(w), x = xyz(p);
+            v[0] = .5 * m * len2(vel);
+            const double inertia = 1.0 / w.w; // isotropic sphere: getInertia() = 1/invInertia
+            v[1] = .5 * dot(om, om * inertia);
+            const V3 g = v3(-I.gravity[0], -I.gravity[1], -I.gravity[2]);
+            v[2] = m * dot(g, x);
+            v[3] = m;
+            v[4] = m * vel.x; v[5] = m * vel.y; v[6] = m * vel.z;
+            v[7] = m * x.x; v[8] = m * x.y; v[9] = m * x.z;
+            v[10] = inertia * om.x; v[11] = inertia * om.y; v[12] = inertia * om.z;
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < RED_SLOTS; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[k][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < RED_SLOTS) {
+        double x = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += sh[threadIdx.x][w];
+        partial[(size_t)blockIdx.x * RED_SLOTS + threadIdx.x] = x;
+    }
+}
+
+// elastic energy and contact counts from the contact records of the last
+// force evaluation; slots: 0 energy, 1 particle contacts, 2 wall contacts
+__global__ void __launch_bounds__(256) k_reduce_records(DevPtrs d, int instance, unsigned n_records, double* partial)
+{
+    __shared__ double sh[3][8];
+    const unsigned r = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[3] = {0.0, 0.0, 0.0};
+    if (r < n_records) {
+        const ContactRecord& rec = d.records[r];
+        const int c = d.ctl->cur;
+        if (d.info[c][rec.slot_p].z == instance) {
+            v[0] = rec.elastic_energy;
+            if (rec.is_wall) v[2] = 1.0; else v[1] = 1.0;
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[k][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double x = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += sh[threadIdx.x][w];
+        partial[(size_t)blockIdx.x * 3 + threadIdx.x] = x;
+    }
+}
+
+} // namespace dem

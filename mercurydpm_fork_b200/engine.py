@@ -1,0 +1,264 @@
+"""Python view of the C ABI: one :class:`DemEngine` per ``dem_handle``.
+
+The engine state lives on the GPU; this class only converts numpy arrays to
+the ABI's structure-of-arrays layout and raises :class:`DemError` on any
+non-zero status. It is the interface the tests and ``bench.py`` use; C and
+C++ callers use ``include/dem_b200.h`` directly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = _abi.load()
+    return _lib
+
+
+class DemError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{_abi.STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def _dp(a: np.ndarray | None):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a: np.ndarray | None):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _f64(a, shape=None):
+    if a is None:
+        return None
+    out = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        out = out.reshape(shape)
+    return out
+
+
+def _i32(a):
+    if a is None:
+        return None
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+@dataclass
+class Instance:
+    """One independent simulation inside a handle (dem_instance_desc)."""
+    domain_min: tuple
+    domain_max: tuple
+    gravity: tuple = (0.0, 0.0, -9.81)
+    n_species: int = 1
+    species_offset: int = 0
+    periodic_mask: int = 0
+    periodic_min: tuple = (0.0, 0.0, 0.0)
+    periodic_max: tuple = (0.0, 0.0, 0.0)
+
+    def to_c(self) -> _abi.InstanceDesc:
+        d = _abi.InstanceDesc()
+        d.domain_min[:] = list(map(float, self.domain_min))
+        d.domain_max[:] = list(map(float, self.domain_max))
+        d.gravity[:] = list(map(float, self.gravity))
+        d.periodic_mask = int(self.periodic_mask)
+        d.species_offset = int(self.species_offset)
+        d.n_species = int(self.n_species)
+        d.periodic_min[:] = list(map(float, self.periodic_min))
+        d.periodic_max[:] = list(map(float, self.periodic_max))
+        return d
+
+
+def species_pair(**kw) -> _abi.SpeciesPair:
+    s = _abi.SpeciesPair()
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def infinite_wall(normal, point, species=0, instance=0, velocity=(0, 0, 0), angular_velocity=(0, 0, 0),
+                  orientation=None) -> _abi.Wall:
+    """An InfiniteWall with outward normal `normal` through `point`.
+
+    The orientation is the reference's quaternion for that normal
+    (BaseInteractable::setOrientationViaNormal); pass it explicitly to reuse
+    the exact quaternion a reference object holds.
+    """
+    from .host import quaternion_from_normal
+    w = _abi.Wall()
+    w.type = _abi.DEM_WALL_INFINITE
+    w.species = species
+    w.instance = instance
+    w.position[:] = list(map(float, point))
+    q = orientation if orientation is not None else quaternion_from_normal(normal)
+    w.orientation[:] = list(map(float, q))
+    w.velocity[:] = list(map(float, velocity))
+    w.angular_velocity[:] = list(map(float, angular_velocity))
+    return w
+
+
+class DemEngine:
+    def __init__(self, time_step: float, instances: list[Instance], species: list[_abi.SpeciesPair],
+                 walls: list[_abi.Wall] | None = None, rotation: bool = True, background_drag: float = 0.0,
+                 max_neighbors: int = 0, skin: float = 0.0, use_graphs: bool = True, device: int = 0):
+        self._h = C.c_void_p()
+        cfg = _abi.Config()
+        cfg.time_step = time_step
+        cfg.background_drag = background_drag
+        cfg.rotation = 1 if rotation else 0
+        cfg.device = device
+        cfg.max_neighbors = max_neighbors
+        cfg.use_graphs = 1 if use_graphs else 0
+        cfg.skin = skin
+        cfg.n_instances = len(instances)
+        arr = (_abi.InstanceDesc * len(instances))(*[i.to_c() for i in instances])
+        rc = lib().dem_create(C.byref(cfg), arr, C.byref(self._h))
+        if rc:
+            raise DemError(rc, "dem_create failed")
+        self.n_instances = len(instances)
+        sp = (_abi.SpeciesPair * len(species))(*species)
+        self._check(lib().dem_set_species(self._h, sp, len(species)))
+        walls = walls or []
+        wa = (_abi.Wall * max(1, len(walls)))(*walls)
+        self._check(lib().dem_set_walls(self._h, wa, len(walls)))
+        self.n = 0
+
+    # ------------------------------------------------------------------
+    def _check(self, rc: int):
+        if rc:
+            msg = lib().dem_last_error(self._h)
+            raise DemError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if self._h:
+            lib().dem_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------
+    def upload(self, position, velocity, radius, inv_mass, inv_inertia, species, ids=None, angular_velocity=None,
+               orientation=None, instance=None):
+        n = len(radius)
+        self._keep = dict(
+            position=_f64(position, (n, 3)), velocity=_f64(velocity, (n, 3)),
+            angular_velocity=_f64(angular_velocity, (n, 3)) if angular_velocity is not None else None,
+            orientation=_f64(orientation, (n, 4)) if orientation is not None else None,
+            radius=_f64(radius), inv_mass=_f64(inv_mass), inv_inertia=_f64(inv_inertia), species=_i32(species),
+            id=_i32(ids if ids is not None else np.arange(n)), instance=_i32(instance))
+        k = self._keep
+        p = _abi.ParticlesSoA(n, _dp(k["position"]), _dp(k["velocity"]), _dp(k["angular_velocity"]),
+                              _dp(k["orientation"]), _dp(k["radius"]), _dp(k["inv_mass"]), _dp(k["inv_inertia"]),
+                              _ip(k["species"]), _ip(k["id"]), _ip(k["instance"]))
+        self._check(lib().dem_upload_particles(self._h, C.byref(p)))
+        self.n = n
+
+    def upload_contacts(self, id_p, id_i, springs, is_wall=None, periodic=None):
+        m = len(id_p)
+        keep = dict(id_p=_i32(id_p), id_i=_i32(id_i), is_wall=_i32(is_wall) if is_wall is not None else None,
+                    periodic=_i32(periodic) if periodic is not None else None,
+                    springs=_f64(springs, (m, 9)))
+        c = _abi.ContactsSoA(m, _ip(keep["id_p"]), _ip(keep["id_i"]), _ip(keep["is_wall"]), _ip(keep["periodic"]),
+                             _dp(keep["springs"]), None, None)
+        self._check(lib().dem_upload_contacts(self._h, C.byref(c)))
+
+    def step(self, n: int = 1):
+        self._check(lib().dem_step(self._h, int(n)))
+
+    def download(self) -> dict:
+        n = self.n
+        out = dict(position=np.zeros((n, 3)), velocity=np.zeros((n, 3)), angular_velocity=np.zeros((n, 3)),
+                   orientation=np.zeros((n, 4)), radius=np.zeros(n), inv_mass=np.zeros(n), inv_inertia=np.zeros(n),
+                   species=np.zeros(n, np.int32), id=np.zeros(n, np.int32), instance=np.zeros(n, np.int32))
+        p = _abi.ParticlesSoA(n, _dp(out["position"]), _dp(out["velocity"]), _dp(out["angular_velocity"]),
+                              _dp(out["orientation"]), _dp(out["radius"]), _dp(out["inv_mass"]),
+                              _dp(out["inv_inertia"]), _ip(out["species"]), _ip(out["id"]), _ip(out["instance"]))
+        self._check(lib().dem_download_particles(self._h, C.byref(p)))
+        return out
+
+    def forces(self):
+        f = np.zeros((self.n, 3))
+        t = np.zeros((self.n, 3))
+        self._check(lib().dem_download_forces(self._h, _dp(f), _dp(t)))
+        return f, t
+
+    def contacts(self) -> dict:
+        cnt = C.c_int64(0)
+        self._check(lib().dem_download_contacts(self._h, None, 0, C.byref(cnt)))
+        m = cnt.value
+        out = dict(id_p=np.zeros(m, np.int32), id_i=np.zeros(m, np.int32), is_wall=np.zeros(m, np.int32),
+                   periodic=np.zeros(m, np.int32), springs=np.zeros((m, 9)), force=np.zeros((m, 3)),
+                   overlap=np.zeros(m))
+        c = _abi.ContactsSoA(m, _ip(out["id_p"]), _ip(out["id_i"]), _ip(out["is_wall"]), _ip(out["periodic"]),
+                             _dp(out["springs"]), _dp(out["force"]), _dp(out["overlap"]))
+        self._check(lib().dem_download_contacts(self._h, C.byref(c), m, C.byref(cnt)))
+        return out
+
+    def reduce(self, instance: int = 0) -> dict:
+        g = _abi.Globals()
+        self._check(lib().dem_reduce(self._h, instance, C.byref(g)))
+        return dict(kinetic_energy=g.kinetic_energy, rotational_energy=g.rotational_energy,
+                    gravitational_energy=g.gravitational_energy, elastic_energy=g.elastic_energy,
+                    momentum=np.array(g.momentum[:]), angular_momentum=np.array(g.angular_momentum[:]),
+                    mass=g.mass, centre_of_mass=np.array(g.centre_of_mass[:]), n_contacts=g.n_contacts,
+                    n_wall_contacts=g.n_wall_contacts, time=g.time, n_steps=g.n_steps)
+
+    def cg(self, coordinates: int, n, lo, hi, width: float, cutoff_factor: float = 3.0, instance: int = 0):
+        g = _abi.CGGrid()
+        g.coordinates = coordinates
+        g.instance = instance
+        g.n[:] = list(map(int, n))
+        g.min[:] = list(map(float, lo))
+        g.max[:] = list(map(float, hi))
+        g.width = width
+        g.cutoff_factor = cutoff_factor
+        npts = int(np.prod(n))
+        out = np.zeros((npts, _abi.DEM_CG_NFIELDS))
+        self._check(lib().dem_cg_eval(self._h, C.byref(g), _dp(out)))
+        return out
+
+    def counts(self) -> dict:
+        e, c, w = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        self._check(lib().dem_get_counts(self._h, C.byref(e), C.byref(c), C.byref(w)))
+        return dict(list_entries=e.value, contacts=c.value, wall_contacts=w.value)
+
+    def time_force_kernel(self, reps: int = 20) -> float:
+        """Mean device milliseconds of one time-step force-kernel launch."""
+        ms = C.c_double(0)
+        self._check(lib().dem_time_force_kernel(self._h, int(reps), C.byref(ms)))
+        return ms.value
+
+    def stats(self) -> dict:
+        ms = C.c_double(0)
+        launches = C.c_int64(0)
+        rebuilds = C.c_int64(0)
+        self._check(lib().dem_last_step_stats(self._h, C.byref(ms), C.byref(launches), C.byref(rebuilds)))
+        n = C.c_int64(0)
+        cap = C.c_int64(0)
+        cells = C.c_int64(0)
+        self._check(lib().dem_get_info(self._h, C.byref(n), C.byref(cap), C.byref(cells)))
+        return dict(ms=ms.value, kernel_launches=launches.value, rebuilds=rebuilds.value, n=n.value,
+                    max_neighbors=cap.value, n_cells=cells.value)

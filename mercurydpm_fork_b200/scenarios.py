@@ -1,0 +1,217 @@
+"""Seeded synthetic DEM workloads with the shapes of the benchmark set-ups.
+
+Each builder returns a :class:`Scenario`: ABI structures (config, instance,
+species table, walls) plus particle arrays in the caller order. The same
+Scenario feeds the GPU engine, the CPU oracle and the reference build, so
+all three start from bit-identical inputs.
+
+* :func:`settling_box` -- monodisperse spheres on a jittered simple-cubic
+  lattice in a closed box of six InfiniteWalls under gravity
+  (LinearViscoelasticSlidingFrictionSpecies).
+* :func:`periodic_chute` -- bidisperse (size ratio 2) spheres over a rough
+  base of fixed spheres, periodic in x and y, gravity inclined like
+  Chute::setChuteAngleAndMagnitudeOfGravity (Kernel/Chute.cc:789-805).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from .engine import Instance, infinite_wall, species_pair
+from .host import linear_collision_time_restitution, sphere_inv_mass_inertia, PI
+
+
+@dataclass
+class Scenario:
+    name: str
+    time_step: float
+    instance: Instance
+    species: list
+    density: np.ndarray
+    walls: list
+    position: np.ndarray
+    velocity: np.ndarray
+    radius: np.ndarray
+    inv_mass: np.ndarray
+    inv_inertia: np.ndarray
+    species_index: np.ndarray
+    ids: np.ndarray
+    rotation: bool = True
+    info: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return len(self.radius)
+
+    @property
+    def n_moving(self) -> int:
+        return int(np.count_nonzero(self.inv_mass))
+
+    def config(self, **kw) -> _abi.Config:
+        c = _abi.Config()
+        c.time_step = self.time_step
+        c.background_drag = 0.0
+        c.rotation = 1 if self.rotation else 0
+        c.device = kw.get("device", 0)
+        c.max_neighbors = kw.get("max_neighbors", 0)
+        c.use_graphs = kw.get("use_graphs", 1)
+        c.skin = kw.get("skin", 0.0)
+        c.n_instances = 1
+        return c
+
+    def engine(self, **kw):
+        from .engine import DemEngine
+        e = DemEngine(self.time_step, [self.instance], self.species, self.walls, rotation=self.rotation, **kw)
+        e.upload(self.position, self.velocity, self.radius, self.inv_mass, self.inv_inertia, self.species_index,
+                 self.ids)
+        return e
+
+
+def linear_sliding_species(tc: float, eps: float, mass: float, mu: float, kt_ratio: float = 2.0 / 7.0,
+                           gt_ratio: float = 0.0, constant_restitution: bool = False) -> _abi.SpeciesPair:
+    k, g = linear_collision_time_restitution(tc, eps, mass)
+    return species_pair(normal_law=_abi.DEM_NORMAL_LINEAR_VISCOELASTIC, friction_law=_abi.DEM_FRICTION_SLIDING,
+                        constant_restitution=1 if constant_restitution else 0, stiffness=k, dissipation=g,
+                        sliding_stiffness=kt_ratio * k, sliding_dissipation=gt_ratio * g, sliding_mu=mu,
+                        sliding_mu_static=mu)
+
+
+def settling_box(n: int = 5000, seed: int = 1, d: float = 1e-3, density: float = 2000.0, tc: float = 1e-4,
+                 eps: float = 0.8, mu: float = 0.5, box=(20, 20, 40), spacing: float = 1.1,
+                 jitter: float = 0.05, vstd: float = 0.01) -> Scenario:
+    """Monodisperse settling box: simple-cubic lattice (spacing 1.1 d), first
+    n sites in x-fastest order, positions jittered U[-0.05, 0.05] d,
+    velocities N(0, 0.01 m/s), six walls, gravity -9.81 z, dt = tc/50."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    r = 0.5 * d
+    Lx, Ly, Lz = (b * d for b in box)
+    nx = int(Lx / (spacing * d))
+    ny = int(Ly / (spacing * d))
+    nz = int(Lz / (spacing * d))
+    if n > nx * ny * nz:
+        raise ValueError("too many particles for the lattice")
+    i = np.arange(n)
+    ix, iy, iz = i % nx, (i // nx) % ny, i // (nx * ny)
+    off = np.array([(Lx - nx * spacing * d) / 2, (Ly - ny * spacing * d) / 2, (Lz - nz * spacing * d) / 2])
+    pos = (np.stack([ix, iy, iz], 1) + 0.5) * spacing * d + off
+    pos = pos + rng.uniform(-jitter * d, jitter * d, size=(n, 3))
+    vel = rng.normal(0.0, vstd, size=(n, 3))
+    radius = np.full(n, r)
+    inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
+    mass = 1.0 / inv_mass[0]
+    sp = linear_sliding_species(tc, eps, mass, mu)
+    walls = [
+        infinite_wall((-1, 0, 0), (0, 0, 0)), infinite_wall((1, 0, 0), (Lx, 0, 0)),
+        infinite_wall((0, -1, 0), (0, 0, 0)), infinite_wall((0, 1, 0), (0, Ly, 0)),
+        infinite_wall((0, 0, -1), (0, 0, 0)), infinite_wall((0, 0, 1), (0, 0, Lz)),
+    ]
+    inst = Instance(domain_min=(0, 0, 0), domain_max=(Lx, Ly, Lz), gravity=(0, 0, -9.81), n_species=1)
+    return Scenario("settling_box", tc / 50, inst, [sp], np.array([density]), walls, pos, vel, radius, inv_mass,
+                    inv_inertia, np.zeros(n, np.int32), np.arange(n, dtype=np.int32),
+                    info=dict(n=n, d=d, seed=seed, box=box))
+
+
+def chute_gravity(angle_deg: float, g: float = 9.81):
+    """Chute::setChuteAngleAndMagnitudeOfGravity: (sin a, 0, -cos a) g."""
+    a = angle_deg * PI / 180.
+    return (math.sin(a) * g, 0.0, -math.cos(a) * g)
+
+
+def _rough_base(rng, Lx, Ly, r_lo, r_hi, area_fraction):
+    """Fixed spheres at random non-overlapping xy positions on z = 0."""
+    mean_area = PI * (r_lo * r_lo + r_lo * r_hi + r_hi * r_hi) / 3.0
+    target = int(round(area_fraction * Lx * Ly / mean_area))
+    cell = 2.0 * r_hi
+    nxc, nyc = max(1, int(Lx / cell)), max(1, int(Ly / cell))
+    grid = {}
+    pos, rad = [], []
+    attempts = 0
+    while len(pos) < target and attempts < 200 * target:
+        attempts += 1
+        x, y = rng.uniform(0, Lx), rng.uniform(0, Ly)
+        rr = rng.uniform(r_lo, r_hi)
+        cx, cy = int(x / Lx * nxc) % nxc, int(y / Ly * nyc) % nyc
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for j in grid.get(((cx + dx) % nxc, (cy + dy) % nyc), ()):
+                    ddx = x - pos[j][0]
+                    ddy = y - pos[j][1]
+                    ddx -= Lx * round(ddx / Lx)
+                    ddy -= Ly * round(ddy / Ly)
+                    if ddx * ddx + ddy * ddy < (rr + rad[j]) ** 2:
+                        ok = False
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if ok:
+            grid.setdefault((cx, cy), []).append(len(pos))
+            pos.append((x, y, 0.0))
+            rad.append(rr)
+    return np.array(pos), np.array(rad)
+
+
+def periodic_chute(n_flow: int = 200_000, seed: int = 2, ds: float = 1e-3, density: float = 2000.0,
+                   tc: float = 1e-4, eps: float = 0.88, mu: float = 0.5, angle: float = 24.0,
+                   lx: float = 100.0, ly: float = 50.0, base_fraction: float = 0.6, vstd: float = 0.01,
+                   site_scale: float = 1.0, base_gap: float = 1.2) -> Scenario:
+    """Periodic inclined chute: n_flow spheres, 50:50 by number, small radii
+    U[0.45, 0.55] ds, large = 2x; periodic 100 x 50 small diameters; rough
+    base of fixed small spheres (area fraction 0.6); 24 deg; dt = tc/50.
+    Flowing spheres start on a lattice of 2.2 ds sites (times site_scale),
+    each holding one large sphere or a 2x2x2 block of small ones, base_gap ds
+    above the base; site_scale < 1 starts the bed pre-compressed."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    Lx, Ly = lx * ds, ly * ds
+    r_lo, r_hi = 0.45 * ds, 0.55 * ds
+    bpos, brad = _rough_base(rng, Lx, Ly, r_lo, r_hi, base_fraction)
+    n_large = n_flow // 2
+    n_small = n_flow - n_large
+    site = 2.2 * ds * site_scale
+    # a pre-compressed bed also closes the gaps across the periodic boundaries
+    fit = math.ceil if site_scale < 1.0 else int
+    sx, sy = fit(Lx / site), fit(Ly / site)
+    n_small_sites = (n_small + 7) // 8
+    n_sites = n_large + n_small_sites
+    kinds = np.zeros(n_sites, np.int8)
+    kinds[rng.permutation(n_sites)[:n_small_sites]] = 1
+    pos, rad = [], []
+    small_left = n_small
+    z0 = r_hi + base_gap * ds
+    for s in range(n_sites):
+        ix, iy, iz = s % sx, (s // sx) % sy, s // (sx * sy)
+        base = np.array([(ix + 0.5) * (Lx / sx), (iy + 0.5) * (Ly / sy), z0 + (iz + 0.5) * site])
+        if kinds[s] == 0:
+            pos.append(base)
+            rad.append(2.0 * rng.uniform(r_lo, r_hi))
+        else:
+            for k in range(8):
+                if small_left == 0:
+                    break
+                o = (np.array([k & 1, (k >> 1) & 1, (k >> 2) & 1]) - 0.5) * (site / 2)
+                pos.append(base + o)
+                rad.append(rng.uniform(r_lo, r_hi))
+                small_left -= 1
+    fpos = np.array(pos)
+    frad = np.array(rad)
+    top = float(fpos[:, 2].max()) + 2 * ds
+    position = np.concatenate([bpos, fpos])
+    radius = np.concatenate([brad, frad])
+    n = len(radius)
+    velocity = np.zeros((n, 3))
+    velocity[len(brad):] = rng.normal(0.0, vstd, size=(len(frad), 3))
+    inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
+    inv_mass[: len(brad)] = 0.0
+    inv_inertia[: len(brad)] = 0.0
+    m_small = 4.0 / 3.0 * PI * (0.5 * ds) ** 3 * density
+    sp = linear_sliding_species(tc, eps, m_small, mu)
+    inst = Instance(domain_min=(0, 0, -2 * ds), domain_max=(Lx, Ly, top + 20 * ds), gravity=chute_gravity(angle),
+                    n_species=1, periodic_mask=0b011, periodic_min=(0, 0, 0), periodic_max=(Lx, Ly, 0))
+    return Scenario("periodic_chute", tc / 50, inst, [sp], np.array([density]), [], position, velocity, radius,
+                    inv_mass, inv_inertia, np.zeros(n, np.int32), np.arange(n, dtype=np.int32),
+                    info=dict(n_flow=len(frad), n_base=len(brad), seed=seed, angle=angle, lx=lx, ly=ly))

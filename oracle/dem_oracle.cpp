@@ -1,0 +1,468 @@
+// dem_oracle.cpp -- TEST INFRASTRUCTURE ONLY (the oracle).
+//
+// A CPU, FP64, single-threaded restatement of MercuryDPM's DEM time step for
+// the paths the GPU engine implements. It is the checker the parity tests
+// compare the CUDA path against; nothing in the product links or calls it.
+// It is itself pinned against the reference build in oracle/_ref (see
+// tests/test_oracle_vs_reference.py) and the reference's own known-answer
+// tests (tests/test_oracle_known_answers.py).
+//
+// Step order follows DPMBase::computeOneTimeStep (Kernel/DPMBase.cc:4315-4389):
+//   integrateBeforeForceComputation (BaseParticle.cc:718-752, BaseInteractable.cc:538-600)
+//   checkInteractionWithBoundaries  (PeriodicBoundary.cc:374-395)
+//   computeAllForces                (DPMBase.cc:3397-3526, :3113-3162, :3168-3215)
+//   integrateAfterForceComputation  (BaseParticle.cc:760-776)
+//   eraseOldInteractions            (InteractionHandler.cc:377-393)
+// Periodic boundaries are restated with the reference's ghost semantics:
+// a pair that meets across a boundary is evaluated twice, once from each real
+// particle against the other's ghost (DPMBase.cc:3124-3127: ghost-ghost pairs
+// are skipped, a real-ghost pair has the real particle as P because ghosts
+// carry higher ids), and after the step the lower-index particle's view is
+// kept while the other's view restarts from the reversed spring
+// (InteractionHandler::removeObjectKeepingPeriodics, InteractionHandler.cc:316-368;
+// BaseInteraction::copySwitchPointer, BaseInteraction.cc:340-356).
+// The contact-law arithmetic is shared with the device code
+// (mercurydpm_fork_b200/csrc/dem_laws.cuh), compiled here for the host.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "../mercurydpm_fork_b200/csrc/dem_laws.cuh"
+#include "../mercurydpm_fork_b200/csrc/dem_math.cuh"
+
+using namespace dem;
+
+namespace {
+
+struct Particle {
+    V3 x, v, w;
+    Q4 q;
+    double r, invm, invI;
+    int species, id;
+    bool fixed;
+    V3 F, T;
+};
+
+// Persistent interaction (InteractionHandler object). Key: (kind, P id, I id)
+// kind 0: particle pair (P, I real ids); 1: P real vs ghost of I (P's view);
+// 2: wall (P particle, I wall index).
+struct Inter {
+    Springs s;
+    unsigned stamp;
+    double overlap;
+    V3 force;
+    double energy;
+    bool periodic;
+};
+
+struct Sim {
+    dem_config cfg;
+    dem_instance_desc inst;
+    std::vector<dem_species_pair> species;
+    std::vector<dem_wall> walls;
+    std::vector<Particle> p;
+    std::map<std::tuple<int, int, int>, Inter> inter;
+    unsigned nt = 0; // DPMBase::numberOfTimeSteps_
+    double L[3], half[3];
+
+    const dem_species_pair& sp(int a, int b) const
+    {
+        return species[inst.species_offset + a * inst.n_species + b];
+    }
+
+    void integrate_before()
+    {
+        const double dt = cfg.time_step;
+        for (auto& q : p) {
+            if (q.invm == 0.0) {
+                q.x += q.v * dt;
+                q.q = quat_rotate(q.q, q.w * dt);
+            } else {
+                q.v += ((q.F * q.invm) * 0.5) * dt;
+                q.x += q.v * dt;
+                if (cfg.rotation) {
+                    const S33 I{q.invI, 0.0, 0.0, q.invI, 0.0, q.invI};
+                    q.w += ((rotate_inverse_inertia(q.q, I) * q.T) * 0.5) * dt;
+                    q.q = quat_rotate(q.q, q.w * dt);
+                }
+            }
+        }
+    }
+
+    void integrate_after()
+    {
+        const double dt = cfg.time_step;
+        for (auto& q : p) {
+            if (q.invm == 0.0) continue;
+            q.v += ((q.F * q.invm) * 0.5) * dt;
+            if (cfg.rotation) {
+                const S33 I{q.invI, 0.0, 0.0, q.invI, 0.0, q.invI};
+                q.w += ((rotate_inverse_inertia(q.q, I) * q.T) * 0.5) * dt;
+            }
+        }
+    }
+
+    void wrap()
+    {
+        for (int k = 0; k < 3; ++k) {
+            if (!((inst.periodic_mask >> k) & 1u)) continue;
+            const double lo = inst.periodic_min[k], hi = inst.periodic_max[k];
+            for (auto& q : p) {
+                double* xc = &q.x.x;
+                if (std::min(xc[k] - lo, hi - xc[k]) < 0) {
+                    if (hi - xc[k] > xc[k] - lo)
+                        xc[k] = xc[k] + L[k];
+                    else
+                        xc[k] = xc[k] - L[k];
+                }
+            }
+        }
+    }
+
+    // One evaluation of DPMBase::computeInternalForce for P (real) against I
+    // at position xi (I's real position or a ghost image).
+    void pair(Particle& P, Particle& I, V3 xi, bool ghost)
+    {
+        const V3 branch = P.x - xi;
+        const double d2 = len2(branch);
+        const dem_species_pair& s = sp(P.species, I.species);
+        const double sum = I.r + P.r + s.interaction_distance;
+        if (d2 >= sum * sum) return;
+        const auto key = std::make_tuple(ghost ? 1 : 0, P.id, I.id);
+        auto it = inter.find(key);
+        if (it == inter.end()) {
+            Inter n{};
+            n.s = Springs{zero3(), zero3(), zero3()};
+            it = inter.emplace(key, n).first;
+        }
+        Inter& c = it->second;
+        c.stamp = nt + 1;
+        c.periodic = ghost;
+        ContactGeom g;
+        g.distance = std::sqrt(d2);
+        g.n = branch / g.distance;
+        g.overlap = P.r + I.r - g.distance;
+        g.c = P.x - (P.r - 0.5 * g.overlap) * g.n;
+        g.xp = P.x; g.vp = P.v; g.wp = P.w; g.inv_mass_p = P.invm; g.curv_p = 1.0 / P.r;
+        g.xi = xi; g.vi = I.v; g.wi = I.w; g.inv_mass_i = I.invm; g.curv_i = 1.0 / I.r;
+        g.i_is_wall = false;
+        ContactOut out;
+        evaluate_contact(s, g, c.s, cfg.time_step, out);
+        c.overlap = g.overlap;
+        c.force = out.force;
+        c.energy = out.normal_stiffness_energy;
+        P.F += out.force;
+        P.T += out.torque - cross(P.x - g.c, out.force);
+        if (!ghost) {
+            I.F += -out.force;
+            I.T += -out.torque + cross(I.x - g.c, out.force);
+        }
+    }
+
+    bool wall_dist(const dem_wall& w, V3 x, double radius, double& dist, V3& nrm) const
+    {
+        if (w.type != DEM_WALL_INFINITE) return false;
+        const Q4 q{w.orientation[0], w.orientation[1], w.orientation[2], w.orientation[3]};
+        dist = quat_plane_distance(q, x, v3(w.position[0], w.position[1], w.position[2]));
+        if (dist >= radius) return false;
+        nrm = quat_axis(q);
+        return true;
+    }
+
+    void compute_forces()
+    {
+        for (auto& q : p) { q.F = zero3(); q.T = zero3(); }
+        const int n = (int)p.size();
+        // candidate pairs: uniform grid over the box (exact FP64 predicate decides)
+        double rmax = 0.0;
+        for (auto& q : p) rmax = std::max(rmax, q.r);
+        double dmax = 0.0;
+        for (auto& s : species) dmax = std::max(dmax, s.interaction_distance);
+        const double cs = 2.0 * rmax + dmax + 1e-12;
+        double lo[3], hi[3];
+        int dim[3];
+        for (int k = 0; k < 3; ++k) {
+            const bool per = (inst.periodic_mask >> k) & 1u;
+            lo[k] = per ? inst.periodic_min[k] : inst.domain_min[k];
+            hi[k] = per ? inst.periodic_max[k] : inst.domain_max[k];
+            for (auto& q : p) { lo[k] = std::min(lo[k], (&q.x.x)[k]); hi[k] = std::max(hi[k], (&q.x.x)[k]); }
+            dim[k] = std::max(1, (int)std::floor((hi[k] - lo[k]) / cs));
+        }
+        auto cell_of = [&](V3 x, int k) {
+            int c = (int)std::floor(((&x.x)[k] - lo[k]) / (hi[k] - lo[k]) * dim[k]);
+            return std::max(0, std::min(dim[k] - 1, c));
+        };
+        std::vector<std::vector<int>> cells((size_t)dim[0] * dim[1] * dim[2]);
+        for (int i = 0; i < n; ++i) {
+            const V3 x = p[i].x;
+            cells[((size_t)cell_of(x, 2) * dim[1] + cell_of(x, 1)) * dim[0] + cell_of(x, 0)].push_back(i);
+        }
+        std::vector<int> cand;
+        for (int i = 0; i < n; ++i) {
+            cand.clear();
+            int c[3];
+            for (int k = 0; k < 3; ++k) c[k] = cell_of(p[i].x, k);
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        int cc[3] = {c[0] + dx, c[1] + dy, c[2] + dz};
+                        bool ok = true;
+                        for (int k = 0; k < 3; ++k) {
+                            if (cc[k] < 0 || cc[k] >= dim[k]) {
+                                if ((inst.periodic_mask >> k) & 1u)
+                                    cc[k] = (cc[k] + dim[k]) % dim[k];
+                                else
+                                    ok = false;
+                            }
+                        }
+                        if (!ok) continue;
+                        for (int j : cells[((size_t)cc[2] * dim[1] + cc[1]) * dim[0] + cc[0]]) cand.push_back(j);
+                    }
+            std::sort(cand.begin(), cand.end());
+            cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+            for (int j : cand) {
+                if (j == i) continue;
+                Particle& A = p[i];
+                Particle& B = p[j];
+                if (A.fixed && B.fixed) continue;
+                // image of B seen from A
+                V3 xb = B.x;
+                bool per = false;
+                for (int k = 0; k < 3; ++k) {
+                    if (!((inst.periodic_mask >> k) & 1u)) continue;
+                    const double raw = (&A.x.x)[k] - (&xb.x)[k];
+                    if (raw > half[k]) { (&xb.x)[k] = (&xb.x)[k] + L[k]; per = true; }
+                    else if (raw < -half[k]) { (&xb.x)[k] = (&xb.x)[k] - L[k]; per = true; }
+                }
+                if (per) {
+                    pair(A, B, xb, true); // A real, B's ghost
+                } else if (A.id < B.id) {
+                    pair(A, B, B.x, false);
+                }
+            }
+        }
+        // body forces
+        for (auto& q : p) {
+            if (q.fixed) continue;
+            const double m = 1.0 / q.invm;
+            q.F += v3(inst.gravity[0], inst.gravity[1], inst.gravity[2]) * m - cfg.background_drag * q.v;
+        }
+        // walls
+        for (int w = 0; w < (int)walls.size(); ++w) {
+            for (auto& q : p) {
+                if (q.fixed) continue;
+                const dem_wall& wall = walls[w];
+                const dem_species_pair& s = sp(q.species, wall.species);
+                double dist;
+                V3 nrm;
+                if (!wall_dist(wall, q.x, q.r + s.interaction_distance, dist, nrm)) continue;
+                const auto key = std::make_tuple(2, q.id, w);
+                auto it = inter.find(key);
+                if (it == inter.end()) {
+                    Inter n{};
+                    n.s = Springs{zero3(), zero3(), zero3()};
+                    it = inter.emplace(key, n).first;
+                }
+                Inter& c = it->second;
+                c.stamp = nt + 1;
+                c.periodic = false;
+                ContactGeom g;
+                g.n = -nrm;
+                g.distance = dist;
+                g.overlap = q.r - dist;
+                g.c = q.x - (q.r - 0.5 * g.overlap) * g.n;
+                g.xp = q.x; g.vp = q.v; g.wp = q.w; g.inv_mass_p = q.invm; g.curv_p = 1.0 / q.r;
+                g.xi = v3(wall.position[0], wall.position[1], wall.position[2]);
+                g.vi = v3(wall.velocity[0], wall.velocity[1], wall.velocity[2]);
+                g.wi = v3(wall.angular_velocity[0], wall.angular_velocity[1], wall.angular_velocity[2]);
+                g.inv_mass_i = 0.0; g.curv_i = 0.0; g.i_is_wall = true;
+                ContactOut out;
+                evaluate_contact(s, g, c.s, cfg.time_step, out);
+                c.overlap = g.overlap;
+                c.force = out.force;
+                c.energy = out.normal_stiffness_energy;
+                q.F += out.force;
+                q.T += out.torque - cross(q.x - g.c, out.force);
+            }
+        }
+    }
+
+    // Springs and stamps of the lower-id views of periodic pairs before an
+    // evaluation (see periodic_handover).
+    std::map<std::tuple<int, int, int>, std::pair<unsigned, Springs>> before;
+
+    void snapshot_periodic()
+    {
+        before.clear();
+        for (auto& kv : inter)
+            if (std::get<0>(kv.first) == 1 && std::get<1>(kv.first) < std::get<2>(kv.first))
+                before[kv.first] = {kv.second.stamp, kv.second.s};
+    }
+
+    // removeDuplicatePeriodicParticles: keep the lower-id particle's view of a
+    // periodic pair; the other view restarts from the reversed spring. When the
+    // real-real interaction carries the same stamp as the new view (the first
+    // time step after initialiseSolve, whose stamps coincide), the reference
+    // keeps the old interaction and drops this evaluation's spring update
+    // (InteractionHandler.cc:339-352).
+    void periodic_handover()
+    {
+        for (auto& kv : inter) {
+            if (std::get<0>(kv.first) != 1) continue;
+            const int a = std::get<1>(kv.first), b = std::get<2>(kv.first);
+            if (a > b) continue;
+            auto pb = before.find(kv.first);
+            if (pb != before.end() && pb->second.first == kv.second.stamp) kv.second.s = pb->second.second;
+            auto other = inter.find(std::make_tuple(1, b, a));
+            if (other == inter.end()) continue;
+            other->second.s.slide = -kv.second.s.slide;
+            other->second.s.roll = -kv.second.s.roll;
+            other->second.s.tors = -kv.second.s.tors;
+        }
+    }
+
+    void erase_old(unsigned current)
+    {
+        for (auto it = inter.begin(); it != inter.end();) {
+            if (it->second.stamp <= current)
+                it = inter.erase(it);
+            else
+                ++it;
+        }
+    }
+};
+
+} // namespace
+
+extern "C" {
+
+// Runs nsteps reference time steps from the given state (after the initial
+// force evaluation of DPMBase::initialiseSolve) and returns the final state
+// (caller order), the forces of the last evaluation and the live contacts.
+int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species, int nspecies,
+               const dem_wall* walls, int nwalls, const dem_particles_soa* in, const dem_contacts_soa* contacts_in,
+               int nsteps, dem_particles_soa* out, double* force, double* torque, dem_contacts_soa* contacts_out,
+               int64_t contacts_capacity, int64_t* contacts_count)
+{
+    Sim S;
+    S.cfg = *cfg;
+    S.inst = *inst;
+    S.species.assign(species, species + nspecies);
+    S.walls.assign(walls, walls + nwalls);
+    for (int k = 0; k < 3; ++k) {
+        S.L[k] = inst->periodic_max[k] - inst->periodic_min[k];
+        S.half[k] = 0.5 * S.L[k];
+    }
+    const int64_t n = in->n;
+    S.p.resize(n);
+    for (int64_t i = 0; i < n; ++i) {
+        Particle& q = S.p[i];
+        q.x = v3(in->position[3 * i], in->position[3 * i + 1], in->position[3 * i + 2]);
+        q.v = v3(in->velocity[3 * i], in->velocity[3 * i + 1], in->velocity[3 * i + 2]);
+        q.w = in->angular_velocity ? v3(in->angular_velocity[3 * i], in->angular_velocity[3 * i + 1],
+                                        in->angular_velocity[3 * i + 2])
+                                   : zero3();
+        q.q = in->orientation ? Q4{in->orientation[4 * i], in->orientation[4 * i + 1], in->orientation[4 * i + 2],
+                                   in->orientation[4 * i + 3]}
+                              : Q4{1.0, 0.0, 0.0, 0.0};
+        q.r = in->radius[i];
+        q.invm = in->inv_mass[i];
+        q.invI = in->inv_inertia ? in->inv_inertia[i] : 0.0;
+        q.species = in->species[i];
+        q.id = in->id[i];
+        q.fixed = q.invm == 0.0;
+        q.F = q.T = zero3();
+    }
+    std::map<int, int> index_of;
+    for (int64_t i = 0; i < n; ++i) index_of[S.p[i].id] = (int)i;
+    if (contacts_in) {
+        for (int64_t r = 0; r < contacts_in->n; ++r) {
+            Inter c{};
+            const double* s = contacts_in->springs + 9 * r;
+            c.s = Springs{v3(s[0], s[1], s[2]), v3(s[3], s[4], s[5]), v3(s[6], s[7], s[8])};
+            c.stamp = 0;
+            const bool wall = contacts_in->is_wall && contacts_in->is_wall[r];
+            const bool per = contacts_in->periodic && contacts_in->periodic[r];
+            if (wall) {
+                S.inter[std::make_tuple(2, contacts_in->id_p[r], contacts_in->id_i[r])] = c;
+            } else if (per) {
+                S.inter[std::make_tuple(1, contacts_in->id_p[r], contacts_in->id_i[r])] = c;
+                Inter o = c;
+                o.s.slide = -c.s.slide; o.s.roll = -c.s.roll; o.s.tors = -c.s.tors;
+                S.inter[std::make_tuple(1, contacts_in->id_i[r], contacts_in->id_p[r])] = o;
+            } else {
+                S.inter[std::make_tuple(0, contacts_in->id_p[r], contacts_in->id_i[r])] = c;
+            }
+        }
+    }
+    // DPMBase::initialiseSolve: numberOfTimeSteps_ = 0, one force evaluation
+    S.nt = 0;
+    S.snapshot_periodic();
+    S.compute_forces();
+    S.periodic_handover();
+    for (int step = 0; step < nsteps; ++step) {
+        S.integrate_before();
+        S.wrap();
+        S.snapshot_periodic();
+        S.compute_forces();
+        S.periodic_handover();
+        S.integrate_after();
+        S.erase_old(S.nt);
+        S.nt += 1;
+    }
+    if (out) {
+        for (int64_t i = 0; i < n; ++i) {
+            const Particle& q = S.p[i];
+            if (out->position) { out->position[3 * i] = q.x.x; out->position[3 * i + 1] = q.x.y; out->position[3 * i + 2] = q.x.z; }
+            if (out->velocity) { out->velocity[3 * i] = q.v.x; out->velocity[3 * i + 1] = q.v.y; out->velocity[3 * i + 2] = q.v.z; }
+            if (out->angular_velocity) {
+                out->angular_velocity[3 * i] = q.w.x; out->angular_velocity[3 * i + 1] = q.w.y; out->angular_velocity[3 * i + 2] = q.w.z;
+            }
+            if (out->orientation) {
+                out->orientation[4 * i] = q.q.q0; out->orientation[4 * i + 1] = q.q.q1;
+                out->orientation[4 * i + 2] = q.q.q2; out->orientation[4 * i + 3] = q.q.q3;
+            }
+        }
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        const Particle& q = S.p[i];
+        if (force) { force[3 * i] = q.F.x; force[3 * i + 1] = q.F.y; force[3 * i + 2] = q.F.z; }
+        if (torque) { torque[3 * i] = q.T.x; torque[3 * i + 1] = q.T.y; torque[3 * i + 2] = q.T.z; }
+    }
+    // live contacts as the reference keeps them after the step
+    int64_t cnt = 0;
+    for (const auto& kv : S.inter) {
+        const int kind = std::get<0>(kv.first), a = std::get<1>(kv.first), b = std::get<2>(kv.first);
+        const unsigned last_stamp = nsteps > 0 ? (unsigned)nsteps : 1u; // stamp of the last evaluation
+        if (kv.second.stamp != last_stamp) continue;
+        if (kind == 1 && a > b) continue; // the kept view of a periodic pair
+        if (contacts_out && cnt < contacts_capacity) {
+            contacts_out->id_p[cnt] = a;
+            contacts_out->id_i[cnt] = b;
+            if (contacts_out->is_wall) contacts_out->is_wall[cnt] = kind == 2;
+            if (contacts_out->periodic) contacts_out->periodic[cnt] = kind == 1;
+            if (contacts_out->overlap) contacts_out->overlap[cnt] = kv.second.overlap;
+            if (contacts_out->force) {
+                contacts_out->force[3 * cnt] = kv.second.force.x;
+                contacts_out->force[3 * cnt + 1] = kv.second.force.y;
+                contacts_out->force[3 * cnt + 2] = kv.second.force.z;
+            }
+            if (contacts_out->springs) {
+                const Springs& s = kv.second.s;
+                const double v[9] = {s.slide.x, s.slide.y, s.slide.z, s.roll.x, s.roll.y, s.roll.z,
+                                     s.tors.x, s.tors.y, s.tors.z};
+                std::memcpy(contacts_out->springs + 9 * cnt, v, sizeof(v));
+            }
+        }
+        ++cnt;
+    }
+    if (contacts_count) *contacts_count = cnt;
+    if (contacts_out) contacts_out->n = std::min(cnt, contacts_capacity);
+    return 0;
+}
+
+} // extern "C"

@@ -1,0 +1,188 @@
+"""Test harness: runs one Scenario through the CPU oracle (oracle/), the
+reference build (oracle/_ref) and the GPU engine, returning comparable dicts.
+
+Only tests import this module; the oracle and the reference are checkers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from mercurydpm_fork_b200 import _abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_LIB = os.path.join(ROOT, "oracle", "libdem_oracle.so")
+REF_LIBS = {v: os.path.join(ROOT, "oracle", "_ref", f"libmdpm_ref_{v}.so") for v in ("serial", "omp")}
+
+_pd = C.POINTER(C.c_double)
+_pi = C.POINTER(C.c_int32)
+_oracle = None
+_ref = {}
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(_pd)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(_pi)
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_LIB):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+        lib = C.CDLL(ORACLE_LIB)
+        lib.oracle_run.restype = C.c_int
+        lib.oracle_run.argtypes = [C.POINTER(_abi.Config), C.POINTER(_abi.InstanceDesc), C.POINTER(_abi.SpeciesPair),
+                                   C.c_int, C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA),
+                                   C.POINTER(_abi.ContactsSoA), C.c_int, C.POINTER(_abi.ParticlesSoA), _pd, _pd,
+                                   C.POINTER(_abi.ContactsSoA), C.c_int64, C.POINTER(C.c_int64)]
+        _oracle = lib
+    return _oracle
+
+
+def reference_available(variant="serial") -> bool:
+    return os.path.exists(REF_LIBS[variant])
+
+
+def ref_lib(variant="serial"):
+    if variant not in _ref:
+        lib = C.CDLL(REF_LIBS[variant])
+        common = [C.POINTER(_abi.Config), C.POINTER(_abi.InstanceDesc), C.POINTER(_abi.SpeciesPair), _pd,
+                  C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA)]
+        lib.mdpm_ref_run.restype = C.c_int
+        lib.mdpm_ref_run.argtypes = common + [C.c_int, C.POINTER(_abi.ParticlesSoA), _pd, _pd,
+                                              C.POINTER(_abi.ContactsSoA), C.c_int64, C.POINTER(C.c_int64), _pd]
+        lib.mdpm_ref_time.restype = C.c_int
+        lib.mdpm_ref_time.argtypes = common + [C.c_int, C.c_int, C.c_int, _pd]
+        _ref[variant] = lib
+    return _ref[variant]
+
+
+class _Inputs:
+    """Keeps the ctypes views of a Scenario alive."""
+
+    def __init__(self, sc, contacts=None):
+        n = sc.n
+        self.pos = np.ascontiguousarray(sc.position, np.float64)
+        self.vel = np.ascontiguousarray(sc.velocity, np.float64)
+        self.rad = np.ascontiguousarray(sc.radius, np.float64)
+        self.im = np.ascontiguousarray(sc.inv_mass, np.float64)
+        self.ii = np.ascontiguousarray(sc.inv_inertia, np.float64)
+        self.sp = np.ascontiguousarray(sc.species_index, np.int32)
+        self.ids = np.ascontiguousarray(sc.ids, np.int32)
+        self.soa = _abi.ParticlesSoA(n, _dp(self.pos), _dp(self.vel), None, None, _dp(self.rad), _dp(self.im),
+                                     _dp(self.ii), _ip(self.sp), _ip(self.ids), None)
+        self.cfg = sc.config()
+        self.inst = sc.instance.to_c()
+        self.species = (_abi.SpeciesPair * len(sc.species))(*sc.species)
+        self.walls = (_abi.Wall * max(1, len(sc.walls)))(*sc.walls)
+        self.nwalls = len(sc.walls)
+        self.density = np.ascontiguousarray(sc.density, np.float64)
+        self.contacts_in = None
+        if contacts is not None:
+            m = len(contacts["id_p"])
+            self._c = {k: np.ascontiguousarray(v) for k, v in contacts.items()}
+            self.contacts_in = _abi.ContactsSoA(m, _ip(self._c["id_p"].astype(np.int32)), None, None, None, None,
+                                                None, None)
+            self._cid = [self._c["id_p"].astype(np.int32), self._c["id_i"].astype(np.int32),
+                         self._c.get("is_wall", np.zeros(m)).astype(np.int32),
+                         self._c.get("periodic", np.zeros(m)).astype(np.int32),
+                         np.ascontiguousarray(self._c["springs"], np.float64)]
+            self.contacts_in = _abi.ContactsSoA(m, _ip(self._cid[0]), _ip(self._cid[1]), _ip(self._cid[2]),
+                                                _ip(self._cid[3]), _dp(self._cid[4]), None, None)
+
+
+def _outputs(n, cap):
+    o = dict(position=np.zeros((n, 3)), velocity=np.zeros((n, 3)), angular_velocity=np.zeros((n, 3)),
+             orientation=np.zeros((n, 4)), inv_mass=np.zeros(n), inv_inertia=np.zeros(n),
+             force=np.zeros((n, 3)), torque=np.zeros((n, 3)))
+    c = dict(id_p=np.zeros(cap, np.int32), id_i=np.zeros(cap, np.int32), is_wall=np.zeros(cap, np.int32),
+             periodic=np.zeros(cap, np.int32), springs=np.zeros((cap, 9)), force=np.zeros((cap, 3)),
+             overlap=np.zeros(cap))
+    soa = _abi.ParticlesSoA(n, _dp(o["position"]), _dp(o["velocity"]), _dp(o["angular_velocity"]),
+                            _dp(o["orientation"]), None, _dp(o["inv_mass"]), _dp(o["inv_inertia"]), None, None, None)
+    csoa = _abi.ContactsSoA(cap, _ip(c["id_p"]), _ip(c["id_i"]), _ip(c["is_wall"]), _ip(c["periodic"]),
+                            _dp(c["springs"]), _dp(c["force"]), _dp(c["overlap"]))
+    return o, c, soa, csoa
+
+
+def _trim(c, m):
+    return {k: v[:m] for k, v in c.items()}
+
+
+def sort_contacts(c):
+    order = np.lexsort((c["id_i"], c["id_p"], c["is_wall"]))
+    return {k: v[order] for k, v in c.items()}
+
+
+def run_oracle(sc, nsteps: int, contacts=None) -> dict:
+    inp = _Inputs(sc, contacts)
+    cap = 16 * sc.n + 64
+    o, c, soa, csoa = _outputs(sc.n, cap)
+    cnt = C.c_int64(0)
+    rc = oracle_lib().oracle_run(C.byref(inp.cfg), C.byref(inp.inst), inp.species, len(sc.species), inp.walls,
+                                 inp.nwalls, C.byref(inp.soa), C.byref(inp.contacts_in) if inp.contacts_in else None,
+                                 nsteps, C.byref(soa), _dp(o["force"]), _dp(o["torque"]), C.byref(csoa), cap,
+                                 C.byref(cnt))
+    assert rc == 0
+    o["contacts"] = sort_contacts(_trim(c, cnt.value))
+    return o
+
+
+def run_reference(sc, nsteps: int, variant: str = "serial") -> dict:
+    inp = _Inputs(sc)
+    cap = 16 * sc.n + 64
+    o, c, soa, csoa = _outputs(sc.n, cap)
+    cnt = C.c_int64(0)
+    ene = np.zeros(4)
+    rc = ref_lib(variant).mdpm_ref_run(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density), inp.walls,
+                                       inp.nwalls, C.byref(inp.soa), nsteps, C.byref(soa), _dp(o["force"]),
+                                       _dp(o["torque"]), C.byref(csoa), cap, C.byref(cnt), _dp(ene))
+    assert rc == 0
+    o["contacts"] = sort_contacts(_trim(c, cnt.value))
+    o["energies"] = dict(kinetic=ene[0], rotational=ene[1], gravitational=ene[2], elastic=ene[3])
+    return o
+
+
+def time_reference(sc, warmup: int, nsteps: int, threads: int, variant: str = "omp") -> float:
+    inp = _Inputs(sc)
+    sec = C.c_double(0)
+    rc = ref_lib(variant).mdpm_ref_time(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density),
+                                        inp.walls, inp.nwalls, C.byref(inp.soa), warmup, nsteps, threads,
+                                        C.byref(sec))
+    assert rc == 0
+    return sec.value
+
+
+def run_gpu(sc, nsteps: int, contacts=None, **kw) -> dict:
+    e = sc.engine(**kw)
+    if contacts is not None:
+        e.upload_contacts(contacts["id_p"], contacts["id_i"], contacts["springs"], contacts.get("is_wall"),
+                          contacts.get("periodic"))
+    e.step(nsteps)
+    out = e.download()
+    out["force"], out["torque"] = e.forces()
+    out["contacts"] = sort_contacts(e.contacts())
+    out["globals"] = e.reduce()
+    out["stats"] = e.stats()
+    e.close()
+    return out
+
+
+def pair_set(c) -> set:
+    return {(int(a), int(b), int(w)) for a, b, w in zip(c["id_p"], c["id_i"], c["is_wall"])}
+
+
+def rel_err(a, b, scale=None):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    s = np.max(np.abs(b)) if scale is None else scale
+    if s == 0:
+        return float(np.max(np.abs(a - b)))
+    return float(np.max(np.abs(a - b)) / s)

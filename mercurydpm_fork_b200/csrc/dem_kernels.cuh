@@ -241,9 +241,11 @@ __device__ __forceinline__ void cell_range(const InstanceDev& I, int lvl, int k,
     const double flo = floor((x - reach - I.origin[k]) * inv);
     const double fhi = floor((x + reach - I.origin[k]) * inv);
     if ((I.per_mask >> k) & 1u) {
-        // periodic: wrap, but visit each cell at most once
+        // periodic: wrap, but visit each cell at most once; non-finite or far
+        // away coordinates (a diverging run) fall back to the whole row, so
+        // the loop bounds always stay small integers
         double span = fhi - flo + 1.0;
-        if (span > (double)dim) {
+        if (!(span <= (double)dim) || !(fabs(flo) < 1e9) || !(fabs(fhi) < 1e9)) {
             lo = 0;
             hi = dim - 1;
         } else {

@@ -46,6 +46,7 @@ __global__ void k_control(Control* ctl, cudaGraphConditionalHandle handle, int u
     ctl->force_rebuild = 0;
     ctl->final_step = (ctl->steps_left <= 1);
     ctl->steps_left -= 1;
+    if (ctl->final_step) ctl->n_records = 0; // records describe the last evaluation only
     ctl->first_step = (ctl->steps_done == 0);
     ctl->steps_done += 1;
     ctl->pending_flip = 1; // the force kernel of this step writes the other buffer

@@ -53,6 +53,7 @@ struct Particle {
 struct Inter {
     Springs s;
     unsigned stamp;
+    unsigned eval;    // index of the last force evaluation that touched it
     double overlap;
     V3 force;
     double energy;
@@ -67,6 +68,7 @@ struct Sim {
     std::vector<Particle> p;
     std::map<std::tuple<int, int, int>, Inter> inter;
     unsigned nt = 0; // DPMBase::numberOfTimeSteps_
+    unsigned evals = 0; // force evaluations so far
     double L[3], half[3];
 
     const dem_species_pair& sp(int a, int b) const
@@ -141,6 +143,7 @@ struct Sim {
         }
         Inter& c = it->second;
         c.stamp = nt + 1;
+        c.eval = evals;
         c.periodic = ghost;
         ContactGeom g;
         g.distance = std::sqrt(d2);
@@ -175,6 +178,7 @@ struct Sim {
 
     void compute_forces()
     {
+        ++evals;
         for (auto& q : p) { q.F = zero3(); q.T = zero3(); }
         const int n = (int)p.size();
         // candidate pairs: uniform grid over the box (exact FP64 predicate decides)
@@ -269,6 +273,7 @@ struct Sim {
                 }
                 Inter& c = it->second;
                 c.stamp = nt + 1;
+        c.eval = evals;
                 c.periodic = false;
                 ContactGeom g;
                 g.n = -nrm;
@@ -338,7 +343,15 @@ struct Sim {
 
 } // namespace
 
+static int g_report_handler = 0;
+
 extern "C" {
+
+// 0: report the contacts of the last force evaluation (what the engine
+// records); 1: report every interaction the reference's handler still holds
+// after the step (after step 0 this includes interactions of the initial
+// evaluation that step 0 did not touch: both carry time stamp 1).
+void oracle_set_contact_report(int mode) { g_report_handler = mode; }
 
 // Runs nsteps reference time steps from the given state (after the initial
 // force evaluation of DPMBase::initialiseSolve) and returns the final state
@@ -437,8 +450,13 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
     int64_t cnt = 0;
     for (const auto& kv : S.inter) {
         const int kind = std::get<0>(kv.first), a = std::get<1>(kv.first), b = std::get<2>(kv.first);
-        const unsigned last_stamp = nsteps > 0 ? (unsigned)nsteps : 1u; // stamp of the last evaluation
-        if (kv.second.stamp != last_stamp) continue;
+        if (g_report_handler) {
+            // every interaction the reference's InteractionHandler still holds
+            const unsigned last_stamp = nsteps > 0 ? (unsigned)nsteps : 1u;
+            if (kv.second.stamp != last_stamp) continue;
+        } else if (kv.second.eval != S.evals) {
+            continue; // only contacts of the last force evaluation
+        }
         if (kind == 1 && a > b) continue; // the kept view of a periodic pair
         if (contacts_out && cnt < contacts_capacity) {
             contacts_out->id_p[cnt] = a;

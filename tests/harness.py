@@ -42,6 +42,8 @@ def oracle_lib():
                                    C.c_int, C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA),
                                    C.POINTER(_abi.ContactsSoA), C.c_int, C.POINTER(_abi.ParticlesSoA), _pd, _pd,
                                    C.POINTER(_abi.ContactsSoA), C.c_int64, C.POINTER(C.c_int64)]
+        lib.oracle_set_contact_report.restype = None
+        lib.oracle_set_contact_report.argtypes = [C.c_int]
         _oracle = lib
     return _oracle
 
@@ -121,7 +123,10 @@ def sort_contacts(c):
     return {k: v[order] for k, v in c.items()}
 
 
-def run_oracle(sc, nsteps: int, contacts=None) -> dict:
+def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated") -> dict:
+    """report="evaluated": contacts of the last force evaluation (what the
+    engine records); "handler": every interaction the reference still holds."""
+    oracle_lib().oracle_set_contact_report(1 if report == "handler" else 0)
     inp = _Inputs(sc, contacts)
     cap = 16 * sc.n + 64
     o, c, soa, csoa = _outputs(sc.n, cap)

@@ -25,7 +25,7 @@ def test_oracle_tangential_spring_known_answer():
 @pytest.mark.parametrize("nsteps", [0, 1, 10])
 def test_oracle_matches_reference_short(nsteps):
     sc = cases.compressed_box()
-    o = H.run_oracle(sc, nsteps)
+    o = H.run_oracle(sc, nsteps, report="handler")
     r = H.run_reference(sc, nsteps)
     assert H.pair_set(o["contacts"]) == H.pair_set(r["contacts"])
     assert len(o["contacts"]["id_p"]) > 1000
@@ -43,7 +43,7 @@ def test_oracle_matches_reference_short(nsteps):
 @needs_ref
 def test_oracle_matches_reference_walls_horizon():
     sc = cases.compressed_box()
-    o = H.run_oracle(sc, 300)
+    o = H.run_oracle(sc, 300, report="handler")
     r = H.run_reference(sc, 300)
     assert H.pair_set(o["contacts"]) == H.pair_set(r["contacts"])
     assert int(o["contacts"]["is_wall"].sum()) > 100
@@ -55,7 +55,7 @@ def test_oracle_matches_reference_walls_horizon():
 @pytest.mark.parametrize("nsteps", [0, 5])
 def test_oracle_matches_reference_periodic_chute(nsteps):
     sc = cases.small_chute(n_flow=1500)
-    o = H.run_oracle(sc, nsteps)
+    o = H.run_oracle(sc, nsteps, report="handler")
     r = H.run_reference(sc, nsteps)
     assert H.pair_set(o["contacts"]) == H.pair_set(r["contacts"])
     assert int(o["contacts"]["periodic"].sum()) > 0

@@ -32,7 +32,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-timesteps/s"
 STEPS_PER_CALL = 200
-WORKLOAD = dict(workload="periodic_chute_200k", n_flowing=200_000, size_ratio=2, hgrid_levels=2,
+WORKLOAD = dict(workload="periodic_chute_200k", packing="close-packed layers (LLLLS), spacing = mean diameter",
+                n_flowing=200_000, size_ratio=2, hgrid_levels=2,
                 periodic="xy", domain_small_diameters=[100, 50], angle_deg=24, species="LinearViscoelasticSlidingFriction",
                 restitution=0.88, friction=0.5, dt="tc/50", time_steps_per_bench_step=STEPS_PER_CALL,
                 l2="working set >= L2; 256 MiB L2 flush before every timed dem_step call")
@@ -89,7 +90,8 @@ class ClockSampler:
 
 def workload():
     from mercurydpm_fork_b200 import scenarios
-    return scenarios.periodic_chute(n_flow=200_000, seed=2)
+    # dense start: close-packed layers at the mean diameter (about 3.7 contacts per particle)
+    return scenarios.periodic_chute(n_flow=200_000, seed=2, packing="layers", spacing_factor=1.0)
 
 
 def measured_peak():

@@ -51,6 +51,7 @@ struct Handle {
     long long launches_per_step = 0;
     cudaGraphExec_t graph1 = nullptr, graphK = nullptr;
     int ncomp = 3;
+    int law_variant = 0;
 };
 
 int fail(Handle* h, int code, const std::string& msg)
@@ -114,13 +115,42 @@ void launch_rebuild(Handle* h, cudaStream_t s)
 }
 constexpr int REBUILD_LAUNCHES = 9;
 
-void launch_force(Handle* h, cudaStream_t s, int mode)
+// Law variants the force kernel is instantiated for; the handle uses a
+// specialised one when every species pair shares the same law pair.
+enum LawVariant { LAW_GENERIC = 0, LAW_LINEAR_SLIDING, LAW_LINEAR_ROLLING, LAW_HERTZ_MINDLIN, LAW_HERTZ_MINDLIN_RT };
+
+template <int MODE>
+void launch_force_mode(Handle* h, cudaStream_t s)
 {
     DevPtrs& d = h->d;
+    const unsigned g = grid_for(d.n, 128);
+    switch (h->law_variant) {
+    case LAW_LINEAR_SLIDING:
+        k_force<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_SLIDING, 3><<<g, 128, 0, s>>>(d);
+        break;
+    case LAW_LINEAR_ROLLING:
+        k_force<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_ROLLING_TORSION, 9><<<g, 128, 0, s>>>(d);
+        break;
+    case LAW_HERTZ_MINDLIN:
+        k_force<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN, 3><<<g, 128, 0, s>>>(d);
+        break;
+    case LAW_HERTZ_MINDLIN_RT:
+        k_force<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN_ROLLING_TORSION, 9><<<g, 128, 0, s>>>(d);
+        break;
+    default:
+        if (d.ncomp == 3)
+            k_force<MODE, -1, -1, 3><<<g, 128, 0, s>>>(d);
+        else
+            k_force<MODE, -1, -1, 9><<<g, 128, 0, s>>>(d);
+    }
+}
+
+void launch_force(Handle* h, cudaStream_t s, int mode)
+{
     if (mode == 0)
-        k_force<0><<<grid_for(d.n, 128), 128, 0, s>>>(d);
+        launch_force_mode<0>(h, s);
     else
-        k_force<1><<<grid_for(d.n, 128), 128, 0, s>>>(d);
+        launch_force_mode<1>(h, s);
 }
 
 // Captures `steps` time steps: control -> (if rebuild) rebuild body -> force.
@@ -290,6 +320,17 @@ int dem_set_species(dem_handle* hh, const dem_species_pair* table, int n_entries
     if ((size_t)n_entries < need) return fail(h, DEM_ERR_BAD_INPUT, "species table smaller than the instances need");
     h->species.assign(table, table + n_entries);
     h->ncomp = 3;
+    const int n0 = table[0].normal_law, f0 = table[0].friction_law;
+    bool same = true;
+    for (const auto& s : h->species) same = same && s.normal_law == n0 && s.friction_law == f0;
+    h->law_variant = LAW_GENERIC;
+    if (same) {
+        if (n0 == DEM_NORMAL_LINEAR_VISCOELASTIC && f0 == DEM_FRICTION_SLIDING) h->law_variant = LAW_LINEAR_SLIDING;
+        if (n0 == DEM_NORMAL_LINEAR_VISCOELASTIC && f0 == DEM_FRICTION_ROLLING_TORSION) h->law_variant = LAW_LINEAR_ROLLING;
+        if (n0 == DEM_NORMAL_HERTZIAN_VISCOELASTIC && f0 == DEM_FRICTION_MINDLIN) h->law_variant = LAW_HERTZ_MINDLIN;
+        if (n0 == DEM_NORMAL_HERTZIAN_VISCOELASTIC && f0 == DEM_FRICTION_MINDLIN_ROLLING_TORSION)
+            h->law_variant = LAW_HERTZ_MINDLIN_RT;
+    }
     for (const auto& s : h->species) {
         if (s.friction_law == DEM_FRICTION_ROLLING_TORSION || s.friction_law == DEM_FRICTION_MINDLIN_ROLLING_TORSION)
             h->ncomp = 9;

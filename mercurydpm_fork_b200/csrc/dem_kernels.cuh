@@ -454,8 +454,11 @@ __device__ __forceinline__ double spring_energy(const dem_species_pair& sp, cons
 // Returns false when there is no contact within r + interaction distance.
 __device__ bool wall_distance(const dem_wall& w, V3 x, double wall_radius, double& dist, V3& normal);
 
-template <int MODE> // 0: initial force evaluation, 1: time step
-__global__ void __launch_bounds__(128) k_force(DevPtrs d)
+// MODE 0: initial force evaluation, 1: time step. NLAW/FLAW: the contact
+// law pair when every species pair of the simulation uses the same one
+// (-1: dispatch per contact); NCOMP: spring history doubles per contact.
+template <int MODE, int NLAW, int FLAW, int NCOMP>
+__global__ void __launch_bounds__(128, 3) k_force(DevPtrs d)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     Control* ctl = d.ctl;
@@ -515,8 +518,8 @@ __global__ void __launch_bounds__(128) k_force(DevPtrs d)
                     // an interaction of the initial evaluation outlives step 0
                     // (InteractionHandler::eraseOldInteractions, stamps <= 0 only)
                     Springs keep;
-                    load_springs(hin, hb, hstride, d.ncomp, keep);
-                    store_springs(hout, hb, hstride, d.ncomp, keep);
+                    load_springs(hin, hb, hstride, NCOMP, keep);
+                    store_springs(hout, hb, hstride, NCOMP, keep);
                     neww[k >> 5] |= 1u << (k & 31);
                 }
                 continue;
@@ -545,21 +548,21 @@ __global__ void __launch_bounds__(128) k_force(DevPtrs d)
                 for (int m = 0; m < tc; ++m) {
                     if (d.nbr[l][(size_t)m * d.ncap + t] != s) continue;
                     if ((d.act[c][(size_t)(m >> 5) * d.ncap + t] >> (m & 31)) & 1u) {
-                        load_springs(hin, (size_t)m * d.ncap + t, hstride, d.ncomp, spr);
+                        load_springs(hin, (size_t)m * d.ncap + t, hstride, NCOMP, spr);
                         spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
                     }
                     break;
                 }
             } else if (was_active) {
-                load_springs(hin, hb, hstride, d.ncomp, spr);
+                load_springs(hin, hb, hstride, NCOMP, spr);
             }
             const Springs before = spr;
             ContactOut out;
-            evaluate_contact(sp, g, spr, dt, out);
+            evaluate_contact<NLAW, FLAW>(sp, g, spr, dt, out);
             // step 0 keeps the lower-id side's old spring of a periodic pair
             // that existed at the initial evaluation (equal stamps,
             // InteractionHandler.cc:339-352)
-            store_springs(hout, hb, hstride, d.ncomp, (first && periodic && !derived && was_active) ? before : spr);
+            store_springs(hout, hb, hstride, NCOMP, (first && periodic && !derived && was_active) ? before : spr);
             neww[k >> 5] |= 1u << (k & 31);
             if (selfP) {
                 F += out.force;
@@ -594,8 +597,8 @@ __global__ void __launch_bounds__(128) k_force(DevPtrs d)
                 if (!wall_distance(wall, xs, ps.w + sp.interaction_distance, dist, nrm)) {
                     if (first && ((wact >> wl) & 1u)) { // survives step 0, as for particle pairs
                         Springs keep;
-                        load_springs(d.whist[c], hb, wstride, d.ncomp, keep);
-                        store_springs(d.whist[nb], hb, wstride, d.ncomp, keep);
+                        load_springs(d.whist[c], hb, wstride, NCOMP, keep);
+                        store_springs(d.whist[nb], hb, wstride, NCOMP, keep);
                         wnew |= 1u << wl;
                     }
                     continue;
@@ -614,13 +617,13 @@ __global__ void __launch_bounds__(128) k_force(DevPtrs d)
                 g.i_is_wall = true;
                 Springs spr;
                 if ((wact >> wl) & 1u) {
-                    load_springs(d.whist[c], hb, wstride, d.ncomp, spr);
+                    load_springs(d.whist[c], hb, wstride, NCOMP, spr);
                 } else {
                     spr.slide = zero3(); spr.roll = zero3(); spr.tors = zero3();
                 }
                 ContactOut out;
-                evaluate_contact(sp, g, spr, dt, out);
-                store_springs(d.whist[nb], hb, wstride, d.ncomp, spr);
+                evaluate_contact<NLAW, FLAW>(sp, g, spr, dt, out);
+                store_springs(d.whist[nb], hb, wstride, NCOMP, spr);
                 wnew |= 1u << wl;
                 F += out.force;
                 T += out.torque - cross(xs - g.c, out.force);

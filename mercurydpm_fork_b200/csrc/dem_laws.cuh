@@ -51,9 +51,14 @@ __device__ __host__ __forceinline__ V3 velocity_at_contact(V3 v, V3 x, V3 w, V3 
 
 __device__ __host__ __forceinline__ double sq(double a) { return a * a; }
 
+// NLAW / FLAW fix the normal and friction law at compile time (-1: read them
+// from the species pair at run time); the kernels instantiate the law pair a
+// simulation uses so that unused branches cost neither registers nor code.
+template <int NLAW = -1, int FLAW = -1>
 __device__ __host__ __forceinline__ void evaluate_contact(const dem_species_pair& sp, const ContactGeom& g,
                                                           Springs& s, double dt, ContactOut& out)
 {
+    const int nl = NLAW >= 0 ? NLAW : sp.normal_law;
     const V3 vrel = velocity_at_contact(g.vp, g.xp, g.wp, g.c) - velocity_at_contact(g.vi, g.xi, g.wi, g.c);
     const double vn = dot(vrel, g.n);
     const double meff = 1.0 / (g.inv_mass_p + g.inv_mass_i);   // BaseInteraction.cc:810-816
@@ -67,7 +72,7 @@ __device__ __host__ __forceinline__ void evaluate_contact(const dem_species_pair
     // ---- normal force ----
     if (g.overlap > 0) {
         double fn;
-        if (sp.normal_law == DEM_NORMAL_HERTZIAN_VISCOELASTIC) {
+        if (nl == DEM_NORMAL_HERTZIAN_VISCOELASTIC) {
             const double k = 4. / 3. * sp.elastic_modulus * sqrt(reff * g.overlap);
             const double diss = sp.dissipation * sqrt(meff * k);
             fn = k * g.overlap - diss * vn;
@@ -84,7 +89,7 @@ __device__ __host__ __forceinline__ void evaluate_contact(const dem_species_pair
     }
 
     // ---- friction ----
-    const int fl = sp.friction_law;
+    const int fl = FLAW >= 0 ? FLAW : sp.friction_law;
     if (abs_fn != 0.0 && fl != DEM_FRICTION_NONE) {
         if (fl == DEM_FRICTION_SLIDING || fl == DEM_FRICTION_ROLLING_TORSION) {
             // SlidingFrictionInteraction::computeFrictionForce

@@ -156,10 +156,52 @@ def _rough_base(rng, Lx, Ly, r_lo, r_hi, area_fraction):
     return np.array(pos), np.array(rad)
 
 
+def _hcp_layers(rng, Lx, Ly, z0, counts_radii, spacing_factor, pattern):
+    """Close-packed triangular layers with ABC stacking, periodic in x and y.
+
+    counts_radii: {"L": (n, sampler), "S": (n, sampler)}; pattern: the layer
+    type sequence that repeats ("LLLLS"). A layer's nearest-neighbour spacing
+    is spacing_factor x the mean diameter of its type, stretched so that an
+    integer number of rows and columns fills the periodic box exactly."""
+    left = {k: v[0] for k, v in counts_radii.items()}
+    pos, rad = [], []
+    z = z0
+    prev_r = None
+    layer = 0
+    while any(v > 0 for v in left.values()):
+        kind = pattern[layer % len(pattern)]
+        layer += 1
+        if left[kind] <= 0:
+            continue
+        n_kind, sampler, r_mean = counts_radii[kind]
+        s = 2.0 * r_mean * spacing_factor
+        nx = max(3, int(round(Lx / s)))
+        ny = max(4, 2 * int(round(Ly / (s * math.sqrt(3.0) / 2.0) / 2.0)))
+        ax, ay = Lx / nx, Ly / ny
+        if prev_r is None:
+            z = z0 + r_mean
+        elif prev_r == r_mean:  # same kind: close-packed layer distance
+            z += 2.0 * r_mean * spacing_factor * math.sqrt(2.0 / 3.0)
+        else:  # change of kind: centres may sit on top of each other
+            z += (prev_r + r_mean) * spacing_factor
+        k3 = layer % 3  # ABC stacking: shift by the hollow-site offset (a1 + a2) / 3
+        take = min(left[kind], nx * ny)
+        j = np.arange(take)
+        ix, iy = j % nx, j // nx
+        x = (ix + 0.5 * (iy % 2) + 0.5 * k3) * ax
+        y = (iy + k3 / 3.0) * ay
+        pos.append(np.stack([np.mod(x, Lx), np.mod(y, Ly), np.full(take, z)], 1))
+        rad.append(sampler(take))
+        left[kind] -= take
+        prev_r = r_mean
+    return np.concatenate(pos), np.concatenate(rad)
+
+
 def periodic_chute(n_flow: int = 200_000, seed: int = 2, ds: float = 1e-3, density: float = 2000.0,
                    tc: float = 1e-4, eps: float = 0.88, mu: float = 0.5, angle: float = 24.0,
                    lx: float = 100.0, ly: float = 50.0, base_fraction: float = 0.6, vstd: float = 0.01,
-                   site_scale: float = 1.0, base_gap: float = 1.2) -> Scenario:
+                   site_scale: float = 1.0, base_gap: float = 1.2, packing: str = "sites",
+                   spacing_factor: float = 1.0) -> Scenario:
     """Periodic inclined chute: n_flow spheres, 50:50 by number, small radii
     U[0.45, 0.55] ds, large = 2x; periodic 100 x 50 small diameters; rough
     base of fixed small spheres (area fraction 0.6); 24 deg; dt = tc/50.
@@ -183,6 +225,13 @@ def periodic_chute(n_flow: int = 200_000, seed: int = 2, ds: float = 1e-3, densi
     pos, rad = [], []
     small_left = n_small
     z0 = r_hi + base_gap * ds
+    if packing == "layers":
+        fpos, frad = _hcp_layers(
+            rng, Lx, Ly, r_hi * spacing_factor,
+            {"L": (n_large, lambda k: 2.0 * rng.uniform(r_lo, r_hi, k), r_lo + r_hi),
+             "S": (n_small, lambda k: rng.uniform(r_lo, r_hi, k), 0.5 * (r_lo + r_hi))},
+            spacing_factor, "LLLLS")
+        n_sites = 0
     for s in range(n_sites):
         ix, iy, iz = s % sx, (s // sx) % sy, s // (sx * sy)
         base = np.array([(ix + 0.5) * (Lx / sx), (iy + 0.5) * (Ly / sy), z0 + (iz + 0.5) * site])
@@ -197,8 +246,9 @@ def periodic_chute(n_flow: int = 200_000, seed: int = 2, ds: float = 1e-3, densi
                 pos.append(base + o)
                 rad.append(rng.uniform(r_lo, r_hi))
                 small_left -= 1
-    fpos = np.array(pos)
-    frad = np.array(rad)
+    if packing != "layers":
+        fpos = np.array(pos)
+        frad = np.array(rad)
     top = float(fpos[:, 2].max()) + 2 * ds
     position = np.concatenate([bpos, fpos])
     radius = np.concatenate([brad, frad])

@@ -270,6 +270,25 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_profile_target(args):
+    """Small, self-terminating run for ncu captures: the bench workload, a
+    few time steps, then `--profile-launches` extra launches of the time-step
+    force kernel (dem_time_force_kernel). Prints the kernel-launch plan."""
+    from mercurydpm_fork_b200 import DemEngine
+    sc = workload()
+    # direct launches: ncu cannot profile kernel nodes of graphs with conditional nodes
+    eng = DemEngine(sc.time_step, [sc.instance], sc.species, sc.walls, rotation=True, use_graphs=False)
+    eng.upload(sc.position, sc.velocity, sc.radius, sc.inv_mass, sc.inv_inertia, sc.species_index, sc.ids)
+    eng.step(args.profile_steps)
+    st = eng.stats()
+    ms = eng.time_force_kernel(args.profile_launches)
+    cnt = eng.counts()
+    print(json.dumps({"profile_steps": args.profile_steps, "force_launches_before_timing": 1 + args.profile_steps,
+                      "timed_force_launches": 1 + args.profile_launches, "force_ms": ms, "stats": st,
+                      "counts": cnt}))
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -277,8 +296,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-target", action="store_true", help="run the small ncu capture target and exit")
+    ap.add_argument("--profile-steps", type=int, default=20)
+    ap.add_argument("--profile-launches", type=int, default=2)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_target:
+        run_profile_target(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -467,6 +467,10 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     d.wmax = wmax;
     d.ncells = (int)ncells;
     d.rotation = h->cfg.rotation;
+    d.single_instance = ninst == 1;
+    d.n_species_table = (int)h->species.size();
+    d.zero_idist = 1;
+    for (const auto& sp : h->species) d.zero_idist = d.zero_idist && sp.interaction_distance == 0.0;
     d.dt = h->cfg.time_step;
     d.drag = h->cfg.background_drag;
     h->nblocks_scan = (int)grid_for(ncells, 1024);

@@ -119,6 +119,9 @@ struct DevPtrs {
     int wmax;         // max walls per instance
     int ncells;
     int rotation;
+    int single_instance;   // one instance: its record is staged in shared memory
+    int n_species_table;   // entries of the species table
+    int zero_idist;        // every species pair has interaction distance 0
     double dt;
     double drag;
 };

@@ -44,9 +44,9 @@ __device__ __forceinline__ V3 quat_rotate_vec(Q4 q, V3 p)
 // Intersection of half-planes in the (r, 0, a) plane; a point is inside when
 // it is on the negative side of every face normal. Returns the distance to
 // the closest face (with edge/corner handling as in IntersectionOfWalls).
-__device__ bool intersection_distance(const dem_wall& w, V3 p, double wall_radius, double& distance, V3& normal);
+__device__ __forceinline__ bool intersection_distance(const dem_wall& w, V3 p, double wall_radius, double& distance, V3& normal);
 
-__device__ bool wall_distance(const dem_wall& w, V3 x, double wall_radius, double& dist, V3& normal)
+__device__ __forceinline__ bool wall_distance(const dem_wall& w, V3 x, double wall_radius, double& dist, V3& normal)
 {
     if (w.type == DEM_WALL_INFINITE) {
         const Q4 q = wall_q(w);
@@ -84,7 +84,7 @@ __device__ bool wall_distance(const dem_wall& w, V3 x, double wall_radius, doubl
     return false;
 }
 
-__device__ bool intersection_distance(const dem_wall& w, V3 p, double wall_radius, double& distance, V3& normal)
+__device__ __forceinline__ bool intersection_distance(const dem_wall& w, V3 p, double wall_radius, double& distance, V3& normal)
 {
     // Signed distance to each face: faces[k] = (nx, ny, nz, px, py, pz), outward normal n,
     // the wall occupies {x : dot(x - p, n) <= 0 for all faces} complement... The

@@ -10,12 +10,13 @@
 //   caller[b][i] int   index of the particle in the caller's upload order
 // The 32-byte records let a neighbour's position+radius, velocity+mass and
 // angular velocity+inertia each arrive in one 32-byte sector.
-// Neighbour lists are ELL, entry-major: nbr[l][k*ncap + i] (k < count[l][i]),
-// so the k-th entries of 32 consecutive particles are one coalesced load;
-// l = Control::lbuf flips at every rebuild.
-// Contact history is stored per neighbour entry in the same layout,
-// hist[b][(c*cap + k)*ncap + i] for history component c (3 per spring), and
-// an active bit per entry, act[b][w*ncap + i] (bit k%32 of word k/32). The
+// Neighbour lists are fixed-capacity rows, one per particle: nbr[l][i*cap + k]
+// (k < count[l][i]); l = Control::lbuf flips at every rebuild. The force
+// kernel walks a warp's entries particle by particle, so a particle's entries
+// are contiguous. Contact history is stored per neighbour entry in the same
+// row order with its components contiguous, hist[b][(i*cap + k)*ncomp + c]
+// (3 components per spring), and an active bit per entry,
+// act[b][w*ncap + i] (bit k%32 of word k/32). The
 // history is double-buffered together with the state (b = Control::cur): a
 // force evaluation reads buffer b and writes b^1, so a thread may read its
 // partner's history of the previous step (needed for periodic pairs) while
@@ -87,6 +88,16 @@ struct Control {
     unsigned int record_capacity;
     unsigned int lost_history;
 };
+
+__host__ __device__ __forceinline__ size_t nbr_at(int cap, int i, int k) { return (size_t)i * cap + k; }
+__host__ __device__ __forceinline__ size_t hist_at(int cap, int ncomp, int i, int k)
+{
+    return ((size_t)i * cap + k) * ncomp;
+}
+__host__ __device__ __forceinline__ size_t whist_at(int wmax, int ncomp, int i, int w)
+{
+    return ((size_t)i * wmax + w) * ncomp;
+}
 
 struct DevPtrs {
     // particle state, two buffers

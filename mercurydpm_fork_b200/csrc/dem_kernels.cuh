@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
                         const double cut = ps.w + pt.w + extra;
                         if (len2(br) < cut * cut) {
                             if (count < d.cap) {
-                                d.nbr[ln][(size_t)count * d.ncap + s] = t;
+                                d.nbr[ln][nbr_at(d.cap, s, count)] = t;
                             } else {
                                 overflow = true;
                             }
@@ -335,10 +335,10 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
             bits &= bits - 1;
             const int k = w * 32 + b;
             if (k >= ocnt) break;
-            const int tnew = d.newidx[d.nbr[lo_][(size_t)k * d.ncap + o]];
+            const int tnew = d.newidx[d.nbr[lo_][nbr_at(d.cap, o, k)]];
             int m = -1;
             for (int q = 0; q < count; ++q) {
-                if (d.nbr[ln][(size_t)q * d.ncap + s] == tnew) {
+                if (d.nbr[ln][nbr_at(d.cap, s, q)] == tnew) {
                     m = q;
                     break;
                 }
@@ -348,8 +348,7 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
                 continue;
             }
             for (int comp = 0; comp < d.ncomp; ++comp)
-                d.hist[nb][((size_t)comp * d.cap + m) * d.ncap + s] =
-                    d.hist[hc][((size_t)comp * d.cap + k) * d.ncap + o];
+                d.hist[nb][hist_at(d.cap, d.ncomp, s, m) + comp] = d.hist[hc][hist_at(d.cap, d.ncomp, o, k) + comp];
             neww[m >> 5] |= 1u << (m & 31);
         }
     }
@@ -362,8 +361,7 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
         const int w = __ffs(bits) - 1;
         bits &= bits - 1;
         for (int comp = 0; comp < d.ncomp; ++comp)
-            d.whist[nb][((size_t)comp * d.wmax + w) * d.ncap + s] =
-                d.whist[hc][((size_t)comp * d.wmax + w) * d.ncap + o];
+            d.whist[nb][whist_at(d.wmax, d.ncomp, s, w) + comp] = d.whist[hc][whist_at(d.wmax, d.ncomp, o, w) + comp];
     }
 }
 
@@ -538,8 +536,8 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
     const InstanceDev* inst_sm = d.single_instance ? &s_inst : nullptr;
     const dem_species_pair* sp_sm = d.n_species_table <= FORCE_SPECIES_SMEM ? s_species : nullptr;
     const double dt = d.dt;
-    const size_t hstride = (size_t)d.cap * d.ncap;
-    const size_t wstride = (size_t)d.wmax * d.ncap;
+    constexpr size_t hstride = 1; // spring components are contiguous
+    constexpr size_t wstride = 1;
     const double* hin = d.hist[c];
     double* hout = d.hist[nb];
 
@@ -611,7 +609,7 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
                 }
                 oo[h] = lo;
                 kk[h] = j - pre[wid][lo];
-                tt[h] = (j < total) ? d.nbr[l][(size_t)kk[h] * d.ncap + wbase + lo] : -1;
+                tt[h] = (j < total) ? d.nbr[l][nbr_at(d.cap, wbase + lo, kk[h])] : -1;
             }
             double4 pt2[2];
             int4 it2[2];
@@ -655,7 +653,7 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
                         // an interaction of the initial evaluation outlives step 0
                         // (InteractionHandler::eraseOldInteractions, stamps <= 0 only)
                         Springs keep;
-                        const size_t hb = (size_t)k * d.ncap + wbase + o;
+                        const size_t hb = hist_at(d.cap, NCOMP, wbase + o, k);
                         load_springs(hin, hb, hstride, NCOMP, keep);
                         store_springs(hout, hb, hstride, NCOMP, keep);
                         atomicOr(&newbits[wid][k >> 5][o], 1u << (k & 31));
@@ -692,7 +690,7 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
                     hit = wall_distance(wall, xo, own_d[wid][9][o] + sp.interaction_distance, dist, nrm);
                     if (!hit && first && ((own_wa[wid][o] >> wl) & 1u)) { // survives step 0, as for pairs
                         Springs keep;
-                        const size_t hb = (size_t)wl * d.ncap + wbase + o;
+                        const size_t hb = whist_at(d.wmax, NCOMP, wbase + o, wl);
                         load_springs(d.whist[c], hb, wstride, NCOMP, keep);
                         store_springs(d.whist[nb], hb, wstride, NCOMP, keep);
                         atomicOr(&wnewbits[wid][o], 1u << wl);
@@ -756,7 +754,7 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
                     g.inv_mass_i = 0.0;
                     g.curv_i = 0.0;
                     g.i_is_wall = true;
-                    hb = (size_t)wl * d.ncap + so;
+                    hb = whist_at(d.wmax, NCOMP, so, wl);
                     hs = wstride;
                     hdst = d.whist[nb];
                     was_active = (own_wa[wid][oq] >> wl) & 1u;
@@ -789,7 +787,7 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
                     g.curv_p = 1.0 / rP;
                     g.curv_i = 1.0 / rI;
                     g.i_is_wall = false;
-                    hb = (size_t)kq * d.ncap + so;
+                    hb = hist_at(d.cap, NCOMP, so, kq);
                     hs = hstride;
                     hdst = hout;
                     was_active = (own_a[wid][kq >> 5][oq] >> (kq & 31)) & 1u;
@@ -800,9 +798,9 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
                     if (derived) {
                         const int tc = d.cnt[l][tq];
                         for (int m = 0; m < tc; ++m) {
-                            if (d.nbr[l][(size_t)m * d.ncap + tq] != so) continue;
+                            if (d.nbr[l][nbr_at(d.cap, tq, m)] != so) continue;
                             if ((d.act[c][(size_t)(m >> 5) * d.ncap + tq] >> (m & 31)) & 1u) {
-                                load_springs(hin, (size_t)m * d.ncap + tq, hstride, NCOMP, spr);
+                                load_springs(hin, hist_at(d.cap, NCOMP, tq, m), hstride, NCOMP, spr);
                                 spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
                             }
                             break;

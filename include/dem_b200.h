@@ -231,6 +231,21 @@ int  dem_download_forces(dem_handle *h, double *force, double *torque);
 int  dem_download_contacts(dem_handle *h, dem_contacts_soa *c, int64_t capacity,
                            int64_t *count);
 int  dem_reduce(dem_handle *h, int instance, dem_globals *out);
+/* The balances of dem_reduce, computed without allocating any device memory.
+ * It has no counterpart in the reference. It is for callers that may not
+ * allocate GPU memory at the point where they need the balances, e.g. a
+ * coupled solver that has reserved the whole device memory budget up front,
+ * or a monitoring hook run between time steps of a host application that
+ * forbids allocation there. dem_reduce allocates a small temporary buffer for
+ * its per-block partial sums; this entry point keeps them in a static device
+ * array of 1 MiB instead (held by every GPU that loads the library until the
+ * process exits) and therefore accepts at most 2,097,152 particles and
+ * 2,097,152 contact records (DEM_ERR_CAPACITY above that). The first call on
+ * a device looks up the array's device address; make that first call before
+ * any stream capture. All calls share the array: calls that overlap on the
+ * GPU (several handles on concurrent streams of one device) race. Results are
+ * the same sums, in the same order, as dem_reduce. */
+int  dem_reduce_noalloc(dem_handle *h, int instance, dem_globals *out);
 int  dem_cg_eval(dem_handle *h, const dem_cg_grid *grid, double *fields_out);
 /* Device time of the last dem_step call in milliseconds (CUDA events on the
  * handle's stream) and how many kernels it launched. */

@@ -124,6 +124,7 @@ _SIGNATURES = {
     "dem_download_forces": (C.c_int, [C.c_void_p, _pd, _pd]),
     "dem_download_contacts": (C.c_int, [C.c_void_p, C.POINTER(ContactsSoA), _i64, C.POINTER(_i64)]),
     "dem_reduce": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Globals)]),
+    "dem_reduce_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Globals)]),
     "dem_cg_eval": (C.c_int, [C.c_void_p, C.POINTER(CGGrid), _pd]),
     "dem_last_step_stats": (C.c_int, [C.c_void_p, _pd, C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_get_info": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),

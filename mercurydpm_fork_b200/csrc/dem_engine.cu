@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -895,6 +896,99 @@ int dem_reduce(dem_handle* hh, int instance, dem_globals* out)
     out->elastic_energy = racc[0];
     out->n_contacts = (int64_t)llround(racc[1]);
     out->n_wall_contacts = (int64_t)llround(racc[2]);
+    out->time = h->steps_total * h->cfg.time_step;
+    out->n_steps = h->steps_total;
+    return DEM_OK;
+}
+
+} // extern "C"
+
+// ---- balances without device allocation ------------------------------------
+// The partial sums of dem_reduce_noalloc live in this file-scope array, which
+// every GPU that loads the library holds until the process exits. One block
+// of 256 particles (or contact records) leaves one partial row, so the array
+// bounds the sizes the entry point accepts.
+namespace {
+constexpr unsigned NOALLOC_MAX_BLOCKS = 8192;  // 2,097,152 particles / contact records
+constexpr size_t NOALLOC_PART_ROWS = (size_t)NOALLOC_MAX_BLOCKS * RED_SLOTS;
+constexpr size_t NOALLOC_REC_ROWS = (size_t)NOALLOC_MAX_BLOCKS * 3;
+constexpr size_t NOALLOC_RESULT = NOALLOC_PART_ROWS + NOALLOC_REC_ROWS; // 16 result slots follow
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_scratch[NOALLOC_MAX_DEVICES] = {nullptr};
+} // namespace
+
+static __device__ __align__(256) double g_reduce_scratch[NOALLOC_RESULT + 16];
+
+// Sums the per-block rows in block order, exactly as dem_reduce does on the host.
+__global__ void k_reduce_finish(const double* part, unsigned nb, unsigned nbr, double* result)
+{
+    const int k = threadIdx.x;
+    if (k < RED_SLOTS) {
+        double a = 0.0;
+        for (unsigned b = 0; b < nb; ++b) a += part[(size_t)b * RED_SLOTS + k];
+        result[k] = a;
+    } else if (k < RED_SLOTS + 3) {
+        double a = 0.0;
+        for (unsigned b = 0; b < nbr; ++b) a += part[NOALLOC_PART_ROWS + (size_t)b * 3 + (k - RED_SLOTS)];
+        result[k] = a;
+    }
+}
+
+extern "C" {
+
+int dem_reduce_noalloc(dem_handle* hh, int instance, dem_globals* out)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !out) return DEM_ERR_BAD_INPUT;
+    if (!h->uploaded) return fail(h, DEM_ERR_STATE, "nothing uploaded");
+    if (instance < 0 || instance >= (int)h->inst.size()) return fail(h, DEM_ERR_BAD_INPUT, "instance out of range");
+    if (h->device < 0 || h->device >= NOALLOC_MAX_DEVICES)
+        return fail(h, DEM_ERR_BAD_INPUT, "dem_reduce_noalloc: device ordinal above 63");
+    const int n = h->d.n;
+    const unsigned nb = grid_for(n, 256);
+    const unsigned nr = h->records_valid && !h->initial_pending ? h->n_records : 0;
+    const unsigned nbr = grid_for(nr, 256);
+    if (nb > NOALLOC_MAX_BLOCKS || nbr > NOALLOC_MAX_BLOCKS)
+        return fail(h, DEM_ERR_CAPACITY,
+                    "dem_reduce_noalloc: more than 2,097,152 particles or contact records (the size of its "
+                    "static scratch array); use dem_reduce");
+    CU(cudaSetDevice(h->device));
+    double* scratch = nullptr;
+    {
+        // set-up, once per device with that device current: the host-side name
+        // of a __device__ array is not a device address
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_scratch[h->device]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_reduce_scratch);
+            if (e != cudaSuccess)
+                return fail(h, DEM_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_noalloc_scratch[h->device] = static_cast<double*>(p);
+        }
+        scratch = g_noalloc_scratch[h->device];
+    }
+    // every row the kernels write is overwritten before it is read: nothing to clear
+    k_reduce_particles<<<nb, 256, 0, h->stream>>>(h->d, instance, scratch);
+    if (nr) k_reduce_records<<<nbr, 256, 0, h->stream>>>(h->d, instance, nr, scratch + NOALLOC_PART_ROWS);
+    k_reduce_finish<<<1, 32, 0, h->stream>>>(scratch, nb, nr ? nbr : 0, scratch + NOALLOC_RESULT);
+    CU(cudaGetLastError());
+    double res[16];
+    CU(cudaMemcpyAsync(res, scratch + NOALLOC_RESULT, sizeof(res), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    std::memset(out, 0, sizeof(*out));
+    out->kinetic_energy = res[0];
+    out->rotational_energy = res[1];
+    out->gravitational_energy = res[2];
+    out->mass = res[3];
+    for (int k = 0; k < 3; ++k) {
+        out->momentum[k] = res[4 + k];
+        out->centre_of_mass[k] = res[3] > 0 ? res[7 + k] / res[3] : 0.0;
+        out->angular_momentum[k] = res[10 + k];
+    }
+    out->elastic_energy = res[RED_SLOTS];
+    out->n_contacts = (int64_t)llround(res[RED_SLOTS + 1]);
+    out->n_wall_contacts = (int64_t)llround(res[RED_SLOTS + 2]);
     out->time = h->steps_total * h->cfg.time_step;
     out->n_steps = h->steps_total;
     return DEM_OK;

@@ -184,10 +184,18 @@ typedef struct dem_globals {
 } dem_globals;
 
 /* Gaussian coarse-graining grid (CG<XZ|XYZ|O, Gauss, StandardFields>,
- * Kernel/CG/CG.hcc:233-528). Fields per grid point, in this order:
- * density, momentum(3), kinetic stress(6: xx xy xz yy yz zz),
- * contact stress(9: row-major), volume fraction. 20 doubles per point. */
-#define DEM_CG_NFIELDS 20
+ * Kernel/CG/CG.hcc:233-528, Kernel/CG/Fields/StandardFields.cc:184-250).
+ * The fields of StandardFields per grid point, in this order (29 doubles):
+ *   0      volume fraction          sum V phi
+ *   1      density                  sum m phi
+ *   2-4    momentum                 sum m v phi
+ *   5-10   momentum flux            sum m v(x)v phi     (xx xy xz yy yz zz)
+ *   11-19  contact stress           sum F(x)branch psi  (row-major)
+ *   20-22  interaction force density (contacts with fixed particles / walls)
+ *   23-28  particle size density    sum r^k phi, k = 0..5
+ * all divided by the volume of the averaged dimensions (CG::volumeAverageVariables).
+ * Points are ordered (i*nY + j)*nZ + k over the resolved dimensions (unresolved: 1). */
+#define DEM_CG_NFIELDS 29
 #define DEM_CG_O   0
 #define DEM_CG_XZ  1
 #define DEM_CG_XYZ 2

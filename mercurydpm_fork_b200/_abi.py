@@ -36,7 +36,7 @@ DEM_WALL_AXISYMMETRIC = 1
 DEM_MAX_LEVELS = 4
 DEM_MAX_WALL_FACES = 8
 
-DEM_CG_NFIELDS = 20
+DEM_CG_NFIELDS = 29
 DEM_CG_O = 0
 DEM_CG_XZ = 1
 DEM_CG_XYZ = 2

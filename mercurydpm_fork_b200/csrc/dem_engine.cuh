@@ -63,6 +63,7 @@ struct ContactRecord {
     double force[3];
     double contact_point[3];
     double branch[3];           // x_P - x_I (image position for periodic pairs); wall: 0
+    double normal[3];           // unit normal of the contact (from I towards P)
     double springs[9];
 };
 

@@ -14,6 +14,12 @@
 #include <vector>
 
 #include "Boundaries/PeriodicBoundary.h"
+#include "CG/CG.h"
+#include "CG/Coordinates/O.h"
+#include "CG/Coordinates/XYZ.h"
+#include "CG/Coordinates/XZ.h"
+#include "CG/Fields/StandardFields.h"
+#include "CG/Functions/Gauss.h"
 #include "Interactions/FrictionForceInteractions/FrictionInteraction.h"
 #include "Interactions/FrictionForceInteractions/MindlinRollingTorsionInteraction.h"
 #include "Interactions/FrictionForceInteractions/SlidingFrictionInteraction.h"
@@ -262,6 +268,66 @@ int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem
         energies[2] = d.getGravitationalEnergy();
         energies[3] = d.getElasticEnergy();
     }
+    return 0;
+}
+
+} // extern "C"
+
+namespace {
+
+template <class Coordinates>
+void reference_cg(RefDriver& d, const dem_cg_grid* grid, double* out)
+{
+    CG<Coordinates, CGFunctions::Gauss, CGFields::StandardFields> cg;
+    cg.setNX(grid->n[0]);
+    cg.setNY(grid->n[1]);
+    cg.setNZ(grid->n[2]);
+    cg.setMin(Vec3D(grid->min[0], grid->min[1], grid->min[2]));
+    cg.setMax(Vec3D(grid->max[0], grid->max[1], grid->max[2]));
+    cg.setWidth(grid->width);
+    auto* p = d.cgHandler.copyAndAddObject(cg);
+    p->statFile.setFileType(FileType::NO_FILE);
+    p->initialise();
+    p->evaluate();
+    size_t k = 0;
+    for (const auto& pt : p->getPoints()) {
+        double* f = out + 29 * k++;
+        f[0] = pt.getVolumeFraction();
+        f[1] = pt.getDensity();
+        const Vec3D m = pt.getMomentum();
+        f[2] = m.X; f[3] = m.Y; f[4] = m.Z;
+        const MatrixSymmetric3D mf = pt.getMomentumFlux();
+        f[5] = mf.XX; f[6] = mf.XY; f[7] = mf.XZ; f[8] = mf.YY; f[9] = mf.YZ; f[10] = mf.ZZ;
+        const Matrix3D cs = pt.getContactStress();
+        f[11] = cs.XX; f[12] = cs.XY; f[13] = cs.XZ; f[14] = cs.YX; f[15] = cs.YY; f[16] = cs.YZ;
+        f[17] = cs.ZX; f[18] = cs.ZY; f[19] = cs.ZZ;
+        const Vec3D ifd = pt.getInteractionForceDensity();
+        f[20] = ifd.X; f[21] = ifd.Y; f[22] = ifd.Z;
+        for (size_t i = 0; i < 6; ++i) f[23 + i] = pt.getParticleSizeDensity(i);
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+// The reference's own CG<Coordinates, Gauss, StandardFields> evaluated after
+// `nsteps` time steps (what writeOutputFiles would compute at the start of the
+// next step). coordinates: 0 = O, 1 = XZ, 2 = XYZ; 29 fields per point.
+int mdpm_ref_cg(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
+                const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in, int nsteps,
+                const dem_cg_grid* grid, double* fields_out)
+{
+    RefDriver d;
+    setup(d, cfg, inst, species, density, walls, nwalls, in, 1);
+    d.initialiseSolve();
+    for (int k = 0; k < nsteps; ++k) d.computeOneTimeStep();
+    if (grid->coordinates == DEM_CG_O)
+        reference_cg<CGCoordinates::O>(d, grid, fields_out);
+    else if (grid->coordinates == DEM_CG_XZ)
+        reference_cg<CGCoordinates::XZ>(d, grid, fields_out);
+    else
+        reference_cg<CGCoordinates::XYZ>(d, grid, fields_out);
     return 0;
 }
 

@@ -39,6 +39,35 @@ def small_chute(n_flow=3000, seed=7):
     return sc
 
 
+def cubic_packing(n=5, distance=0.99):
+    """Drivers/UnitTests/CG3DPackingUnitTest.cpp: n^3 spheres (r = 0.5) on a
+    cubic lattice of spacing 0.99 in a triply periodic box; every contact
+    carries a unit force, so CG<O> gives density n^3/V and contact stress
+    n^3 0.99 / V on the diagonal."""
+    from mercurydpm_fork_b200 import _abi
+    from mercurydpm_fork_b200.engine import species_pair
+    k = 100.0
+    eps = 0.5
+    mass = 1.0
+    log_eps = np.log(eps)
+    diss = -np.sqrt(2.0 * mass * k / (PI * PI + log_eps * log_eps)) * log_eps
+    sp = species_pair(normal_law=_abi.DEM_NORMAL_LINEAR_VISCOELASTIC, friction_law=_abi.DEM_FRICTION_NONE,
+                      stiffness=k, dissipation=diss)
+    density = 6.0 / PI
+    ijk = np.array([(i, j, l) for i in range(n) for j in range(n) for l in range(n)], dtype=np.float64)
+    pos = distance * (ijk + 0.5)
+    m = len(pos)
+    radius = np.full(m, 0.5)
+    inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
+    L = n * distance
+    inst = Instance(domain_min=(0, 0, 0), domain_max=(L, L, L), gravity=(0, 0, 0), n_species=1, periodic_mask=0b111,
+                    periodic_min=(0, 0, 0), periodic_max=(L, L, L))
+    tc = PI / np.sqrt(k / (.5 * mass) - (diss / mass) ** 2)  # getCollisionTime(1.0)
+    sc = Scenario("cubic_packing", 0.02 * tc, inst, [sp], np.array([density]), [], pos, np.zeros((m, 3)), radius,
+                  inv_mass, inv_inertia, np.zeros(m, np.int32), np.arange(m, dtype=np.int32), rotation=False)
+    return sc, dict(n=n, distance=distance, volume=L ** 3)
+
+
 def tangential_spring():
     """Drivers/UnitTests/TangentialSpringUnitTest.cpp: a sphere rolling off a
     fixed sphere under gravity (0, 0, -1); returns (scenario, steps, golden)."""

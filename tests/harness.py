@@ -155,6 +155,36 @@ def run_reference(sc, nsteps: int, variant: str = "serial") -> dict:
     return o
 
 
+def cg_grid(coordinates: int, n, lo, hi, width: float, cutoff_factor: float = 3.0) -> _abi.CGGrid:
+    g = _abi.CGGrid()
+    g.coordinates = coordinates
+    g.n[:] = list(map(int, n))
+    g.min[:] = list(map(float, lo))
+    g.max[:] = list(map(float, hi))
+    g.width = width
+    g.cutoff_factor = cutoff_factor
+    return g
+
+
+def reference_cg(sc, nsteps: int, grid: _abi.CGGrid, variant: str = "serial") -> np.ndarray:
+    """The reference's CG<Coordinates, Gauss, StandardFields> after nsteps steps (29 fields per point)."""
+    inp = _Inputs(sc)
+    npts = 1
+    for k, res in enumerate((grid.coordinates != _abi.DEM_CG_O, grid.coordinates == _abi.DEM_CG_XYZ,
+                             grid.coordinates != _abi.DEM_CG_O)):
+        npts *= grid.n[k] if res else 1
+    out = np.zeros((npts, _abi.DEM_CG_NFIELDS))
+    lib = ref_lib(variant)
+    fn = lib.mdpm_ref_cg
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(_abi.Config), C.POINTER(_abi.InstanceDesc), C.POINTER(_abi.SpeciesPair), _pd,
+                   C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA), C.c_int, C.POINTER(_abi.CGGrid), _pd]
+    rc = fn(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density), inp.walls, inp.nwalls,
+            C.byref(inp.soa), nsteps, C.byref(grid), _dp(out))
+    assert rc == 0
+    return out
+
+
 def time_reference(sc, warmup: int, nsteps: int, threads: int, variant: str = "omp") -> float:
     inp = _Inputs(sc)
     sec = C.c_double(0)

@@ -287,6 +287,8 @@ void reference_cg(RefDriver& d, const dem_cg_grid* grid, double* out)
     cg.setWidth(grid->width);
     auto* p = d.cgHandler.copyAndAddObject(cg);
     p->statFile.setFileType(FileType::NO_FILE);
+    // CG::initialise opens the stat file whatever its type (CG.hcc:179): send it nowhere
+    p->statFile.setName("/dev/null");
     p->initialise();
     p->evaluate();
     size_t k = 0;

@@ -185,12 +185,32 @@ def reference_cg(sc, nsteps: int, grid: _abi.CGGrid, variant: str = "serial") ->
     return out
 
 
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null while the reference runs (its
+    logger prints thread and time-step lines to stdout)."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self._saved = os.dup(1)
+        self._null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self._null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        os.close(self._null)
+        return False
+
+
 def time_reference(sc, warmup: int, nsteps: int, threads: int, variant: str = "omp") -> float:
     inp = _Inputs(sc)
     sec = C.c_double(0)
-    rc = ref_lib(variant).mdpm_ref_time(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density),
-                                        inp.walls, inp.nwalls, C.byref(inp.soa), warmup, nsteps, threads,
-                                        C.byref(sec))
+    with quiet_stdout():
+        rc = ref_lib(variant).mdpm_ref_time(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density),
+                                            inp.walls, inp.nwalls, C.byref(inp.soa), warmup, nsteps, threads,
+                                            C.byref(sec))
     assert rc == 0
     return sec.value
 

@@ -55,6 +55,7 @@ extern "C" {
 /* ---- wall types ------------------------------------------------------- */
 #define DEM_WALL_INFINITE        0 /* InfiniteWall.cc:151-175                       */
 #define DEM_WALL_AXISYMMETRIC    1 /* AxisymmetricIntersectionOfWalls.cc:93-124     */
+#define DEM_WALL_INTERSECTION    2 /* IntersectionOfWalls.cc:532-547, 567-712       */
 
 #define DEM_MAX_LEVELS      4
 #define DEM_MAX_WALL_FACES  8
@@ -83,19 +84,27 @@ typedef struct dem_species_pair {
     double  interaction_distance;  /* mixed-species interaction distance (0: none)   */
 } dem_species_pair;
 
-/* A wall. Infinite walls keep the reference's own representation: the
- * orientation quaternion set by BaseInteractable::setOrientationViaNormal
- * and the position (a point on the plane); the distance is evaluated with
- * Quaternion::getDistance (Kernel/Math/Quaternion.cc:658-670).
- * Axisymmetric walls hold up to DEM_MAX_WALL_FACES half-planes in the
- * wall's (r, axial) frame, as AxisymmetricIntersectionOfWalls::addObject
- * stores them: face k has normal (faces[k][0], 0, faces[k][2]) and a point
- * (faces[k][3], 0, faces[k][5]) in (r, -, a) coordinates. */
+/* A wall. Every wall keeps the reference's own representation: the
+ * orientation quaternion (BaseInteractable::setOrientationViaNormal for an
+ * InfiniteWall's normal, AxisymmetricIntersectionOfWalls::setAxis for an
+ * axisymmetric wall's axis) and the position.
+ *  - DEM_WALL_INFINITE: position is a point on the plane; the distance is
+ *    Quaternion::getDistance (Kernel/Math/Quaternion.cc:658-670).
+ *  - DEM_WALL_INTERSECTION / DEM_WALL_AXISYMMETRIC: faces[k] =
+ *    (normal xyz, point xyz) exactly as passed to
+ *    IntersectionOfWalls::addObject(normal, point), in the wall's frame
+ *    (IntersectionOfWalls: the frame given by position and orientation;
+ *    axisymmetric: (r, 0, a) about the axis through position). The engine
+ *    derives the faces' quaternions, edges and corners as the reference does.
+ * Walls move every time step as BaseInteractable::integrateBeforeForceComputation
+ * does without prescribed motion: position += velocity dt, orientation
+ * rotated by angular_velocity dt. Wall indices in contacts are indices into
+ * the array given to dem_set_walls. */
 typedef struct dem_wall {
     int32_t type;                  /* DEM_WALL_*                                     */
     int32_t species;               /* species index of the wall                      */
     int32_t instance;              /* owning instance (0 for a single simulation)    */
-    int32_t n_faces;               /* axisymmetric: number of half-planes            */
+    int32_t n_faces;               /* intersection walls: number of faces            */
     double  position[3];
     double  orientation[4];        /* quaternion q0..q3                              */
     double  velocity[3];
@@ -218,7 +227,7 @@ int  dem_create(const dem_config *config, const dem_instance_desc *instances,
 /* Species table: n_species^2 entries per instance, row-major (i*n+j), the
  * mixed entries symmetric (SpeciesHandler::getMixedObject). */
 int  dem_set_species(dem_handle *h, const dem_species_pair *table, int n_entries);
-/* WallHandler contents. */
+/* WallHandler contents (before dem_upload_particles). */
 int  dem_set_walls(dem_handle *h, const dem_wall *walls, int n);
 /* ParticleHandler contents; triggers the first force evaluation on the next
  * dem_step (the one DPMBase::initialiseSolve performs, DPMBase.cc:4180). */
@@ -233,6 +242,10 @@ int  dem_download_particles(dem_handle *h, dem_particles_soa *p);
 /* Total force and torque on every particle from the last force evaluation
  * (3*n doubles each, caller order). */
 int  dem_download_forces(dem_handle *h, double *force, double *torque);
+/* Current wall states (n must equal the count given to dem_set_walls; the
+ * caller's order), after the motion of the steps taken so far
+ * (BaseWall::getPosition / getOrientation). */
+int  dem_download_walls(dem_handle *h, dem_wall *walls, int n);
 /* Live contacts (one row per contact as the reference keeps them).
  * capacity: rows available in c; *count receives the number of contacts
  * (rows beyond capacity are not written). */

@@ -33,6 +33,7 @@ DEM_FRICTION_MINDLIN_ROLLING_TORSION = 4
 
 DEM_WALL_INFINITE = 0
 DEM_WALL_AXISYMMETRIC = 1
+DEM_WALL_INTERSECTION = 2
 DEM_MAX_LEVELS = 4
 DEM_MAX_WALL_FACES = 8
 
@@ -122,6 +123,7 @@ _SIGNATURES = {
     "dem_step": (C.c_int, [C.c_void_p, C.c_int]),
     "dem_download_particles": (C.c_int, [C.c_void_p, C.POINTER(ParticlesSoA)]),
     "dem_download_forces": (C.c_int, [C.c_void_p, _pd, _pd]),
+    "dem_download_walls": (C.c_int, [C.c_void_p, C.POINTER(Wall), C.c_int]),
     "dem_download_contacts": (C.c_int, [C.c_void_p, C.POINTER(ContactsSoA), _i64, C.POINTER(_i64)]),
     "dem_reduce": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Globals)]),
     "dem_reduce_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Globals)]),

@@ -20,13 +20,17 @@ namespace {
 
 constexpr unsigned FATAL_STATUS = (1u << DEM_ERR_CAPACITY) | (1u << DEM_ERR_NAN) | (1u << DEM_ERR_TIMEOUT);
 constexpr int GRAPH_STEPS = 16;
+constexpr int CONTROL_THREADS = 128;
 
 struct Handle {
     dem_config cfg{};
     std::vector<dem_instance_desc> inst_desc;
     std::vector<InstanceDev> inst;
     std::vector<dem_species_pair> species;
-    std::vector<dem_wall> walls;
+    std::vector<dem_wall> walls;       // grouped by instance (stable)
+    std::vector<WallGeom> wgeom;       // per wall, for intersection walls
+    std::vector<int> wall_caller;      // grouped index -> caller index
+    std::vector<int> wall_grouped;     // caller index -> grouped index
     std::string err;
     int device = 0;
     cudaStream_t stream = nullptr, stream2 = nullptr;
@@ -37,6 +41,7 @@ struct Handle {
     InstanceDev* d_inst = nullptr;
     dem_species_pair* d_species = nullptr;
     dem_wall* d_walls = nullptr;
+    WallGeom* d_wgeom = nullptr;
     Control* d_ctl = nullptr;
     ContactRecord* d_records = nullptr;
     unsigned record_capacity = 0;
@@ -165,7 +170,7 @@ int build_graph(Handle* h, int steps, cudaGraphExec_t* out)
         CU(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr));
         cudaGraphConditionalHandle handle;
         CU(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
-        k_control<<<1, 32, 0, s>>>(h->d_ctl, handle, 1);
+        k_control<<<1, CONTROL_THREADS, 0, s>>>(h->d_ctl, h->d.walls, h->d.n_walls, h->d.dt, handle, 1);
         const cudaGraphNode_t* deps = nullptr;
         size_t ndeps = 0;
         CU(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps));
@@ -345,18 +350,45 @@ int dem_set_walls(dem_handle* hh, const dem_wall* walls, int n)
 {
     Handle* h = reinterpret_cast<Handle*>(hh);
     if (!h || n < 0 || (n > 0 && !walls)) return fail(h, DEM_ERR_BAD_INPUT, "dem_set_walls: bad arguments");
-    std::vector<dem_wall> w(walls, walls + n);
-    std::stable_sort(w.begin(), w.end(), [](const dem_wall& a, const dem_wall& b) { return a.instance < b.instance; });
-    for (const auto& x : w) {
+    if (h->uploaded) return fail(h, DEM_ERR_STATE, "dem_set_walls must come before dem_upload_particles");
+    std::vector<int> order(n);
+    for (int k = 0; k < n; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return walls[a].instance < walls[b].instance; });
+    std::vector<dem_wall> w(n);
+    std::vector<WallGeom> g(n);
+    std::vector<int> grouped(n);
+    for (int k = 0; k < n; ++k) {
+        const dem_wall& x = walls[order[k]];
         if (x.instance < 0 || x.instance >= (int)h->inst_desc.size())
             return fail(h, DEM_ERR_BAD_INPUT, "wall instance out of range");
-        if (x.type != DEM_WALL_INFINITE && x.type != DEM_WALL_AXISYMMETRIC)
+        if (x.type != DEM_WALL_INFINITE && x.type != DEM_WALL_AXISYMMETRIC && x.type != DEM_WALL_INTERSECTION)
             return fail(h, DEM_ERR_BAD_INPUT, "unknown wall type");
         if (x.n_faces < 0 || x.n_faces > DEM_MAX_WALL_FACES) return fail(h, DEM_ERR_BAD_INPUT, "too many wall faces");
         if (x.species < 0 || x.species >= h->inst_desc[x.instance].n_species)
             return fail(h, DEM_ERR_BAD_INPUT, "wall species out of range");
+        bool finite = true;
+        for (int a = 0; a < 3; ++a)
+            finite = finite && std::isfinite(x.position[a]) && std::isfinite(x.velocity[a]) &&
+                     std::isfinite(x.angular_velocity[a]);
+        for (int a = 0; a < 4; ++a) finite = finite && std::isfinite(x.orientation[a]);
+        if (!finite) return fail(h, DEM_ERR_BAD_INPUT, "non-finite wall state");
+        if (x.type != DEM_WALL_INFINITE) {
+            for (int f = 0; f < x.n_faces; ++f) {
+                const double l2 = x.faces[f][0] * x.faces[f][0] + x.faces[f][1] * x.faces[f][1] +
+                                  x.faces[f][2] * x.faces[f][2];
+                if (!(l2 > 0.0) || !std::isfinite(l2)) return fail(h, DEM_ERR_BAD_INPUT, "wall face normal of length 0");
+            }
+            build_wall_geom(x, g[k]);
+        } else {
+            std::memset(&g[k], 0, sizeof(WallGeom));
+        }
+        w[k] = x;
+        grouped[order[k]] = k;
     }
-    h->walls = w;
+    h->walls = std::move(w);
+    h->wgeom = std::move(g);
+    h->wall_caller = std::move(order);
+    h->wall_grouped = std::move(grouped);
     return DEM_OK;
 }
 
@@ -503,12 +535,15 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     if ((rc = dalloc(h, &h->d_inst, h->inst.size()))) return rc;
     if ((rc = dalloc(h, &h->d_species, h->species.size()))) return rc;
     if ((rc = dalloc(h, &h->d_walls, std::max<size_t>(1, h->walls.size())))) return rc;
+    if ((rc = dalloc(h, &h->d_wgeom, std::max<size_t>(1, h->wgeom.size())))) return rc;
     if ((rc = dalloc(h, &h->d_ctl, 1))) return rc;
     h->record_capacity = (unsigned)std::min<long long>(2000000000ll, 8 * n + 1024 + (long long)n * std::min(wmax, 4));
     if ((rc = dalloc(h, &h->d_records, h->record_capacity))) return rc;
     d.inst = h->d_inst;
     d.species = h->d_species;
     d.walls = h->d_walls;
+    d.wgeom = h->d_wgeom;
+    d.n_walls = (int)h->walls.size();
     d.ctl = h->d_ctl;
     d.records = h->d_records;
 
@@ -538,9 +573,12 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     CU(cudaMemcpyAsync(h->d_inst, h->inst.data(), h->inst.size() * sizeof(InstanceDev), cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(h->d_species, h->species.data(), h->species.size() * sizeof(dem_species_pair),
                        cudaMemcpyHostToDevice, h->stream));
-    if (!h->walls.empty())
+    if (!h->walls.empty()) {
         CU(cudaMemcpyAsync(h->d_walls, h->walls.data(), h->walls.size() * sizeof(dem_wall), cudaMemcpyHostToDevice,
                            h->stream));
+        CU(cudaMemcpyAsync(h->d_wgeom, h->wgeom.data(), h->wgeom.size() * sizeof(WallGeom), cudaMemcpyHostToDevice,
+                           h->stream));
+    }
     Control c{};
     c.cur = 0;
     c.lbuf = 0;
@@ -626,7 +664,9 @@ int dem_upload_contacts(dem_handle* hh, const dem_contacts_soa* cs)
         if (sp < 0) return fail(h, DEM_ERR_BAD_INPUT, "contact refers to an unknown particle id");
         if (cs->is_wall && cs->is_wall[r]) {
             const int in = info[sp].z;
-            const int w = cs->id_i[r] - h->inst[in].wall_begin;
+            const int wc = cs->id_i[r];
+            if (wc < 0 || wc >= (int)h->walls.size()) return fail(h, DEM_ERR_BAD_INPUT, "contact refers to an unknown wall");
+            const int w = h->wall_grouped[wc] - h->inst[in].wall_begin;
             if (w < 0 || w >= h->inst[in].wall_end - h->inst[in].wall_begin)
                 return fail(h, DEM_ERR_BAD_INPUT, "contact refers to a wall outside the particle's instance");
             for (int comp = 0; comp < d.ncomp; ++comp) whist[whist_at(d.wmax, d.ncomp, sp, w) + comp] = spr[comp];
@@ -706,7 +746,8 @@ int dem_step(dem_handle* hh, int nsteps)
                 launches += 2ll * nsteps;
             } else {
                 for (int k = 0; k < nsteps; ++k) {
-                    k_control<<<1, 32, 0, h->stream>>>(h->d_ctl, cudaGraphConditionalHandle{}, 0);
+                    k_control<<<1, CONTROL_THREADS, 0, h->stream>>>(h->d_ctl, d.walls, d.n_walls, d.dt,
+                                                                     cudaGraphConditionalHandle{}, 0);
                     launch_rebuild(h, h->stream);
                     launch_force(h, h->stream, 1);
                 }
@@ -820,6 +861,22 @@ int dem_download_forces(dem_handle* hh, double* force, double* torque)
     return DEM_OK;
 }
 
+int dem_download_walls(dem_handle* hh, dem_wall* walls, int n)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || n < 0 || (n > 0 && !walls)) return fail(h, DEM_ERR_BAD_INPUT, "dem_download_walls: bad arguments");
+    if (n != (int)h->walls.size()) return fail(h, DEM_ERR_BAD_INPUT, "dem_download_walls: wrong wall count");
+    if (n == 0) return DEM_OK;
+    std::vector<dem_wall> w(h->walls);
+    if (h->uploaded) {
+        CU(cudaSetDevice(h->device));
+        CU(cudaMemcpyAsync(w.data(), h->d_walls, n * sizeof(dem_wall), cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+    }
+    for (int k = 0; k < n; ++k) walls[h->wall_caller[k]] = w[k];
+    return DEM_OK;
+}
+
 int dem_download_contacts(dem_handle* hh, dem_contacts_soa* cs, int64_t capacity, int64_t* count)
 {
     Handle* h = reinterpret_cast<Handle*>(hh);
@@ -833,6 +890,8 @@ int dem_download_contacts(dem_handle* hh, dem_contacts_soa* cs, int64_t capacity
     std::vector<ContactRecord> rec(nr);
     if (nr) CU(cudaMemcpyAsync(rec.data(), h->d_records, nr * sizeof(ContactRecord), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
+    for (auto& x : rec)
+        if (x.is_wall) x.id_i = h->wall_caller[x.id_i]; // report the caller's wall index
     std::sort(rec.begin(), rec.end(), [](const ContactRecord& a, const ContactRecord& b) {
         if (a.is_wall != b.is_wall) return a.is_wall < b.is_wall;
         if (a.id_p != b.id_p) return a.id_p < b.id_p;

@@ -25,6 +25,7 @@
 #pragma once
 #include <cstdint>
 #include "dem_math.cuh"
+#include "dem_walls.cuh"
 #include "../../include/dem_b200.h"
 
 namespace dem {
@@ -119,7 +120,9 @@ struct DevPtrs {
     // tables
     const InstanceDev *inst;
     const dem_species_pair *species;
-    const dem_wall *walls;
+    dem_wall *walls;         // moved by k_control every step
+    const WallGeom *wgeom;   // per wall; faces, edges and corners of intersection walls
+    int n_walls;
     Control *ctl;
     ContactRecord *records;
     // sizes

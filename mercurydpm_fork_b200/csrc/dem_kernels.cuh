@@ -1,11 +1,11 @@
 // dem_kernels.cuh -- the DEM time-step kernels.
 //
 // Per time step (captured in a CUDA graph):
-//   k_control   one thread: applies the pending state-buffer flip, adds the
-//               last step's maximum displacement to the skin budget and sets
-//               the graph condition that runs the rebuild body
-//               (MercuryBase::hGridNeedsRebuilding, MercuryBase.cc:496-535,
-//               turned into a Verlet-skin test).
+//   k_control   moves the walls (one thread per wall); one thread applies
+//               the pending state-buffer flip, adds the last step's maximum
+//               displacement to the skin budget and sets the graph condition
+//               that runs the rebuild body (MercuryBase::hGridNeedsRebuilding,
+//               MercuryBase.cc:496-535, turned into a Verlet-skin test).
 //   rebuild     k_keys -> scan -> k_scatter -> k_cell_sort -> k_gather ->
 //               k_build -> k_rb_finish: cell keys per HGrid level, counting
 //               sort, per-cell ordering by particle id, permutation gather of
@@ -31,8 +31,20 @@ __device__ __forceinline__ V3 xyz(double4 a) { return V3{a.x, a.y, a.z}; }
 // ---------------------------------------------------------------------------
 // control
 // ---------------------------------------------------------------------------
-__global__ void k_control(Control* ctl, cudaGraphConditionalHandle handle, int use_handle)
+__global__ void k_control(Control* ctl, dem_wall* walls, int n_walls, double dt, cudaGraphConditionalHandle handle,
+                          int use_handle)
 {
+    // Walls move before the force evaluation of every step, after the particles
+    // (DPMBase::integrateBeforeForceComputation, DPMBase.cc:3228-3261, through
+    // BaseInteractable::integrateBeforeForceComputation, BaseInteractable.cc:538-600:
+    // move(v dt), then rotate(omega dt) = Quaternion::updateAngularDisplacement).
+    for (int k = threadIdx.x; k < n_walls; k += blockDim.x) {
+        dem_wall& w = walls[k];
+        for (int a = 0; a < 3; ++a) w.position[a] += w.velocity[a] * dt;
+        const Q4 q = quat_rotate(Q4{w.orientation[0], w.orientation[1], w.orientation[2], w.orientation[3]},
+                                 v3(w.angular_velocity[0] * dt, w.angular_velocity[1] * dt, w.angular_velocity[2] * dt));
+        w.orientation[0] = q.q0; w.orientation[1] = q.q1; w.orientation[2] = q.q2; w.orientation[3] = q.q3;
+    }
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (ctl->pending_flip) {
         ctl->cur ^= 1;
@@ -449,10 +461,6 @@ __device__ __forceinline__ double spring_energy(const dem_species_pair& sp, cons
     return 0.0;
 }
 
-// Evaluates a wall's signed distance and outward normal for a particle at x.
-// Returns false when there is no contact within r + interaction distance.
-__device__ __forceinline__ bool wall_distance(const dem_wall& w, V3 x, double wall_radius, double& dist, V3& normal);
-
 constexpr int FORCE_BLOCK = 128;  // threads (particles) per block, 4 warps
 constexpr int FORCE_QUEUE = 112;  // contacts a warp buffers before evaluating them (>= 64 + 48)
 constexpr int FORCE_SPECIES_SMEM = 16; // species tables up to this size are staged in shared memory
@@ -688,7 +696,8 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
                     const V3 xo = v3(own_d[wid][0][o], own_d[wid][1][o], own_d[wid][2][o]);
                     double dist;
                     V3 nrm;
-                    hit = wall_distance(wall, xo, own_d[wid][9][o] + sp.interaction_distance, dist, nrm);
+                    hit = wall_distance(wall, d.wgeom + I.wall_begin + wl, xo, own_d[wid][9][o] + sp.interaction_distance,
+                                        dist, nrm);
                     if (!hit && first && ((own_wa[wid][o] >> wl) & 1u)) { // survives step 0, as for pairs
                         Springs keep;
                         const size_t hb = whist_at(d.wmax, NCOMP, wbase + o, wl);
@@ -743,7 +752,7 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
                     spp = &species_at(d, sp_sm, I.species_offset + spq * ns + wall.species);
                     double dist;
                     V3 nrm;
-                    wall_distance(wall, xq, rq + spp->interaction_distance, dist, nrm);
+                    wall_distance(wall, d.wgeom + wg, xq, rq + spp->interaction_distance, dist, nrm);
                     g.n = -nrm;
                     g.distance = dist;
                     g.overlap = rq - dist;

@@ -1,111 +1,288 @@
-// dem_walls.cuh -- wall geometry on the device.
+// dem_walls.cuh -- wall geometry on the device (and its host-side set-up).
 //
 // InfiniteWall::getDistanceAndNormal (Kernel/Walls/InfiniteWall.cc:151-175):
 // distance from Quaternion::getDistance of the wall's orientation and
 // position, normal = Quaternion::getAxis.
-// AxisymmetricIntersectionOfWalls::getDistanceAndNormal
-// (Kernel/Walls/AxisymmetricIntersectionOfWalls.cc:93-124) maps the particle
-// to the wall's axis frame (r, 0, axial) and evaluates
-// IntersectionOfWalls::getDistanceAndNormal (IntersectionOfWalls.cc:567-700)
-// on the half-planes stored in faces[].
+//
+// IntersectionOfWalls (Kernel/Walls/IntersectionOfWalls.cc): a set of
+// half-spaces ("faces", each an InfiniteWall built by addObject(normal,
+// point), :138-149); a particle touches the wall where it lies inside every
+// face but within the interaction radius of the boundary. Faces, edge lines
+// (A_, AB_) and corner points (C_) are precomputed on the host exactly as
+// setPointsAndLines (:351-450) does, and the device evaluates the face /
+// edge / corner selection of getDistanceAndNormal(Vec3D, ...) (:567-712).
+// The plain IntersectionOfWalls maps the particle into the wall frame with
+// Quaternion::rotateBack and the normal back with Quaternion::rotate
+// (:532-547); AxisymmetricIntersectionOfWalls maps it to (r, 0, a) about the
+// wall's axis (AxisymmetricIntersectionOfWalls.cc:93-124).
 #pragma once
+#include <cstring>
+
 #include "dem_math.cuh"
 #include "../../include/dem_b200.h"
 
 namespace dem {
 
-__device__ __forceinline__ Q4 wall_q(const dem_wall& w)
+constexpr int WALL_PAIRS = DEM_MAX_WALL_FACES * (DEM_MAX_WALL_FACES - 1) / 2;
+constexpr int WALL_TRIPLES = DEM_MAX_WALL_FACES * (DEM_MAX_WALL_FACES - 1) * (DEM_MAX_WALL_FACES - 2) / 6;
+
+// Derived geometry of one intersection wall (unused for infinite walls).
+struct WallGeom {
+    double fq[DEM_MAX_WALL_FACES][4]; // face orientation (InfiniteWall::setNormal)
+    double fp[DEM_MAX_WALL_FACES][3]; // face position
+    double fn[DEM_MAX_WALL_FACES][3]; // face normal = Quaternion::getAxis(fq)
+    double A[WALL_PAIRS][3];          // a point on the edge of faces (m, n)
+    double AB[WALL_PAIRS][3];         // unit direction of that edge
+    double C[WALL_TRIPLES][3];        // the corner of faces (l, m, n)
+};
+
+__host__ __device__ __forceinline__ Q4 wall_q(const dem_wall& w)
 {
     return Q4{w.orientation[0], w.orientation[1], w.orientation[2], w.orientation[3]};
 }
 
-// Quaternion::rotateBack (Quaternion.cc): lab -> body frame, R^T p.
-__device__ __forceinline__ V3 quat_rotate_back(Q4 q, V3 p)
+__host__ __device__ __forceinline__ V3 row3(const double* a) { return V3{a[0], a[1], a[2]}; }
+
+// Rotation matrix entries of a unit quaternion with the reference's rounding
+// (Quaternion::rotate / rotateBack, Quaternion.cc:570-640).
+struct QRot {
+    double q00, q01, q02, q03, q11, q12, q13, q22, q23, q33;
+};
+
+__host__ __device__ __forceinline__ QRot qrot(Q4 q)
 {
-    const double q00 = q.q0 * q.q0, q11 = q.q1 * q.q1, q22 = q.q2 * q.q2, q33 = q.q3 * q.q3;
-    const double q01 = q.q0 * q.q1, q02 = q.q0 * q.q2, q03 = q.q0 * q.q3;
-    const double q12 = q.q1 * q.q2, q13 = q.q1 * q.q3, q23 = q.q2 * q.q3;
-    return V3{(q00 + q11 - q22 - q33) * p.x + 2.0 * (q12 + q03) * p.y + 2.0 * (q13 - q02) * p.z,
-              2.0 * (q12 - q03) * p.x + (q00 - q11 + q22 - q33) * p.y + 2.0 * (q23 + q01) * p.z,
-              2.0 * (q13 + q02) * p.x + 2.0 * (q23 - q01) * p.y + (q00 - q11 - q22 + q33) * p.z};
+    QRot r;
+    r.q00 = q.q0 * q.q0;
+    r.q01 = 2 * q.q0 * q.q1;
+    r.q02 = 2 * q.q0 * q.q2;
+    r.q03 = 2 * q.q0 * q.q3;
+    r.q11 = q.q1 * q.q1;
+    r.q12 = 2 * q.q1 * q.q2;
+    r.q13 = 2 * q.q1 * q.q3;
+    r.q22 = q.q2 * q.q2;
+    r.q23 = 2 * q.q2 * q.q3;
+    r.q33 = q.q3 * q.q3;
+    return r;
 }
 
-// Quaternion::rotate (Quaternion.cc): body -> lab frame, R p.
-__device__ __forceinline__ V3 quat_rotate_vec(Q4 q, V3 p)
+// body -> lab (Quaternion::rotate)
+__host__ __device__ __forceinline__ V3 quat_to_lab(Q4 q, V3 p)
 {
-    const double q00 = q.q0 * q.q0, q11 = q.q1 * q.q1, q22 = q.q2 * q.q2, q33 = q.q3 * q.q3;
-    const double q01 = q.q0 * q.q1, q02 = q.q0 * q.q2, q03 = q.q0 * q.q3;
-    const double q12 = q.q1 * q.q2, q13 = q.q1 * q.q3, q23 = q.q2 * q.q3;
-    return V3{(q00 + q11 - q22 - q33) * p.x + 2.0 * (q12 - q03) * p.y + 2.0 * (q13 + q02) * p.z,
-              2.0 * (q12 + q03) * p.x + (q00 - q11 + q22 - q33) * p.y + 2.0 * (q23 - q01) * p.z,
-              2.0 * (q13 - q02) * p.x + 2.0 * (q23 + q01) * p.y + (q00 - q11 - q22 + q33) * p.z};
+    const QRot r = qrot(q);
+    const double m00 = r.q00 + r.q11 - r.q22 - r.q33, m01 = r.q12 - r.q03, m02 = r.q13 + r.q02;
+    const double m10 = r.q12 + r.q03, m11 = r.q00 - r.q11 + r.q22 - r.q33, m12 = r.q23 - r.q01;
+    const double m20 = r.q13 - r.q02, m21 = r.q23 + r.q01, m22 = r.q00 - r.q11 - r.q22 + r.q33;
+    return V3{m00 * p.x + m01 * p.y + m02 * p.z, m10 * p.x + m11 * p.y + m12 * p.z, m20 * p.x + m21 * p.y + m22 * p.z};
 }
 
-// Intersection of half-planes in the (r, 0, a) plane; a point is inside when
-// it is on the negative side of every face normal. Returns the distance to
-// the closest face (with edge/corner handling as in IntersectionOfWalls).
-__device__ __forceinline__ bool intersection_distance(const dem_wall& w, V3 p, double wall_radius, double& distance, V3& normal);
-
-__device__ __forceinline__ bool wall_distance(const dem_wall& w, V3 x, double wall_radius, double& dist, V3& normal)
+// lab -> body (Quaternion::rotateBack)
+__host__ __device__ __forceinline__ V3 quat_to_body(Q4 q, V3 p)
 {
+    const QRot r = qrot(q);
+    const double m00 = r.q00 + r.q11 - r.q22 - r.q33, m01 = r.q12 + r.q03, m02 = r.q13 - r.q02;
+    const double m10 = r.q12 - r.q03, m11 = r.q00 - r.q11 + r.q22 - r.q33, m12 = r.q23 + r.q01;
+    const double m20 = r.q13 + r.q02, m21 = r.q23 - r.q01, m22 = r.q00 - r.q11 - r.q22 + r.q33;
+    return V3{m00 * p.x + m01 * p.y + m02 * p.z, m10 * p.x + m11 * p.y + m12 * p.z, m20 * p.x + m21 * p.y + m22 * p.z};
+}
+
+__host__ __device__ __forceinline__ double face_distance(const WallGeom& g, unsigned k, V3 x)
+{
+    return quat_plane_distance(Q4{g.fq[k][0], g.fq[k][1], g.fq[k][2], g.fq[k][3]}, x, row3(g.fp[k]));
+}
+
+// IntersectionOfWalls::getDistanceAndNormal(const Vec3D&, ...): the face with
+// the largest signed distance decides, unless the closest point on it lies
+// outside a second (edge: distance to the line A + t AB) or a third face
+// (corner: distance to C). Face, edge and corner indices and the NaN
+// fall-through (the corner of three faces whose normals are coplanar has no
+// finite C) follow the reference.
+__host__ __device__ __forceinline__ bool intersection_distance(const WallGeom& g, int nf, V3 position, double R,
+                                                               double& distance, V3& normal)
+{
+    if (nf <= 0) return false;
+    distance = -1e20;
+    double distance2 = -1e20, distance3 = -1e20;
+    unsigned id = 0, id2 = 0, id3 = 0;
+    for (unsigned i = 0; i < (unsigned)nf; ++i) {
+        const double dc = face_distance(g, i, position);
+        if (dc >= R) return false;
+        if (dc > distance) {
+            if (distance > -R) {
+                if (distance2 > -R) {
+                    distance3 = distance2;
+                    id3 = id2;
+                }
+                distance2 = distance;
+                id2 = id;
+            }
+            distance = dc;
+            id = i;
+        } else if (dc < -R) {
+            continue;
+        } else if (dc > distance2) {
+            if (distance2 > -R) {
+                distance3 = distance2;
+                id3 = id2;
+            }
+            distance2 = dc;
+            id2 = i;
+        } else if (dc > distance3) {
+            distance3 = dc;
+            id3 = i;
+        }
+    }
+    if (distance2 > -R) {
+        const V3 D = position + row3(g.fn[id]) * distance; // closest point on face id
+        bool edge2 = face_distance(g, id2, D) > 0.0;
+        if (distance3 > -R && face_distance(g, id3, D) > 0.0) {
+            const V3 E = position + row3(g.fn[id2]) * distance2;
+            const bool edge3 = face_distance(g, id3, E) > 0.0;
+            if (edge2) {
+                if (edge3) {
+                    if (id2 > id3) {
+                        const unsigned t = id2;
+                        id2 = id3;
+                        id3 = t;
+                    }
+                    const unsigned index = (id < id2)   ? ((id3 - 2) * (id3 - 1) * id3 / 6 + (id2 - 1) * id2 / 2 + id)
+                                           : (id < id3) ? ((id3 - 2) * (id3 - 1) * id3 / 6 + (id - 1) * id / 2 + id2)
+                                                        : ((id - 2) * (id - 1) * id / 6 + (id3 - 1) * id3 / 2 + id2);
+                    normal = position - row3(g.C[index]);
+                    distance = sqrt(len2(normal));
+                    if (distance <= R) {
+                        normal = normal / (-distance);
+                        return true;
+                    }
+                    if (distance == distance) return false;
+                }
+            } else {
+                edge2 = true;
+                distance2 = distance3;
+                id2 = id3;
+            }
+        }
+        if (edge2) {
+            const unsigned index = (id > id2) ? ((id - 1) * id / 2 + id2) : ((id2 - 1) * id2 / 2 + id);
+            const V3 AB = row3(g.AB[index]);
+            const V3 AC = position - row3(g.A[index]);
+            normal = AC - AB * dot(AC, AB);
+            distance = sqrt(len2(normal));
+            if (distance <= R) {
+                normal = normal / (-distance);
+                return true;
+            }
+            if (distance == distance) return false;
+        }
+    }
+    normal = row3(g.fn[id]);
+    return true;
+}
+
+// BaseWall::getDistanceNormalOverlap for the supported wall types: signed
+// distance of x from the wall and the wall's outward normal at the contact;
+// false when x is not within R of the wall.
+__host__ __device__ __forceinline__ bool wall_distance(const dem_wall& w, const WallGeom* geom, V3 x, double R,
+                                                       double& dist, V3& normal)
+{
+    const Q4 q = wall_q(w);
+    const V3 wp = v3(w.position[0], w.position[1], w.position[2]);
     if (w.type == DEM_WALL_INFINITE) {
-        const Q4 q = wall_q(w);
-        dist = quat_plane_distance(q, x, v3(w.position[0], w.position[1], w.position[2]));
-        if (dist >= wall_radius) return false;
+        dist = quat_plane_distance(q, x, wp);
+        if (dist >= R) return false;
         normal = quat_axis(q);
         return true;
     }
     if (w.type == DEM_WALL_AXISYMMETRIC) {
-        // AxisymmetricIntersectionOfWalls::getDistanceAndNormal
-        const Q4 q = wall_q(w);
-        V3 pos = x - v3(w.position[0], w.position[1], w.position[2]);
-        pos = quat_rotate_back(q, pos);
-        // the wall axis is the body-frame x axis after rotateBack (orientation of (1,0,0))
-        const V3 axis = v3(1.0, 0.0, 0.0);
-        const double a = dot(pos, axis);
-        const V3 radial = pos - a * axis;
-        const double rr = len(radial);
-        const V3 rp = v3(rr, 0.0, a);
-        double d;
+        const V3 po = x - wp;
+        const V3 axis = quat_axis(q);
+        const double a = dot(po, axis);
+        V3 radial = po - a * axis;
+        const double r = sqrt(len2(radial));
         V3 nrz;
-        if (!intersection_distance(w, rp, wall_radius, d, nrz)) return false;
-        dist = d;
-        // map the (r, 0, a) normal back: radial component along the radial unit vector
-        V3 nb;
-        if (rr != 0.0) {
-            const V3 ur = radial / rr;
-            nb = nrz.x * ur + nrz.z * axis;
-        } else {
-            nb = nrz.z * axis;
-        }
-        normal = quat_rotate_vec(q, nb);
+        if (!intersection_distance(*geom, w.n_faces, v3(r, 0.0, a), R, dist, nrz)) return false;
+        if (r != 0) radial = radial / r;
+        normal = nrz.z * axis + nrz.x * radial;
         return true;
     }
-    return false;
+    // DEM_WALL_INTERSECTION
+    const V3 pb = quat_to_body(q, x - wp);
+    V3 nb;
+    if (!intersection_distance(*geom, w.n_faces, pb, R, dist, nb)) return false;
+    normal = quat_to_lab(q, nb);
+    return true;
 }
 
-__device__ __forceinline__ bool intersection_distance(const dem_wall& w, V3 p, double wall_radius, double& distance, V3& normal)
+// ---- host-side set-up --------------------------------------------------
+
+// Quaternion::setOrientationViaNormal (Quaternion.cc:543-567), which first
+// normalises the normal: the rotation taking (1, 0, 0) to the normal.
+__host__ inline Q4 orientation_from_normal(V3 n)
 {
-    // Signed distance to each face: faces[k] = (nx, ny, nz, px, py, pz), outward normal n,
-    // the wall occupies {x : dot(x - p, n) <= 0 for all faces} complement... The
-    // particle is in contact with the face whose distance is largest (least negative
-    // penetration) among faces that bound the wall.
-    const int nf = w.n_faces;
-    double dmax = -1e300;
-    int imax = -1;
-    for (int k = 0; k < nf; ++k) {
-        const V3 n = v3(w.faces[k][0], w.faces[k][1], w.faces[k][2]);
-        const V3 q = v3(w.faces[k][3], w.faces[k][4], w.faces[k][5]);
-        const double dk = dot(q - p, n);
-        if (dk > dmax) {
-            dmax = dk;
-            imax = k;
+    n = n / sqrt(len2(n));
+    if (n.x <= -1 + 1e-14) return Q4{0.0, 0.0, 1.0, 0.0};
+    const V3 half = V3{1.0 + n.x, 0.0 + n.y, 0.0 + n.z};
+    Q4 q{half.x, 0.0, -half.z, half.y};
+    const double l = sqrt(q.q0 * q.q0 + q.q1 * q.q1 + q.q2 * q.q2 + q.q3 * q.q3);
+    q.q0 /= l;
+    q.q1 /= l;
+    q.q2 /= l;
+    q.q3 /= l;
+    return q;
+}
+
+// The point where three planes {x : x . n_k = b_k} meet, by Cramer's rule
+// with the cofactor order of IntersectionOfWalls::setPointsAndLines
+// (IntersectionOfWalls.cc:365-389 for the edge point, with the edge
+// direction as third plane and b = 0; :399-433 for a corner).
+__host__ inline V3 three_plane_point(V3 a, V3 b, V3 c, double ba, double bb, double bc)
+{
+    const double invdet = 1.0 / (+a.x * (b.y * c.z - c.y * b.z) - a.y * (b.x * c.z - b.z * c.x) +
+                                 a.z * (b.x * c.y - b.y * c.x));
+    const V3 r{+(b.y * c.z - c.y * b.z) * ba - (a.y * c.z - a.z * c.y) * bb + (a.y * b.z - a.z * b.y) * bc,
+               -(b.x * c.z - b.z * c.x) * ba + (a.x * c.z - a.z * c.x) * bb - (a.x * b.z - b.x * a.z) * bc,
+               +(b.x * c.y - c.x * b.y) * ba - (a.x * c.y - c.x * a.y) * bb + (a.x * b.y - b.x * a.y) * bc};
+    return r * invdet;
+}
+
+// Vec3D::cross (Vector.cc:164-167)
+__host__ inline V3 cross_ref(V3 a, V3 b)
+{
+    return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// Faces are added one at a time, each followed by its edges with the earlier
+// faces and its corners with every earlier pair (IntersectionOfWalls::addObject
+// then setPointsAndLines).
+__host__ inline void build_wall_geom(const dem_wall& w, WallGeom& g)
+{
+    std::memset(&g, 0, sizeof(g));
+    for (int n = 0; n < w.n_faces; ++n) {
+        V3 nrm = row3(w.faces[n]);
+        nrm = nrm / sqrt(len2(nrm)); // addObject normalises, setNormal normalises again
+        const Q4 q = orientation_from_normal(nrm);
+        g.fq[n][0] = q.q0; g.fq[n][1] = q.q1; g.fq[n][2] = q.q2; g.fq[n][3] = q.q3;
+        for (int k = 0; k < 3; ++k) g.fp[n][k] = w.faces[n][3 + k];
+        const V3 ax = quat_axis(q);
+        g.fn[n][0] = ax.x; g.fn[n][1] = ax.y; g.fn[n][2] = ax.z;
+        const V3 Nn = ax, Pn = row3(g.fp[n]);
+        for (int m = 0; m < n; ++m) {
+            const int id = (n - 1) * n / 2 + m;
+            const V3 Nm = row3(g.fn[m]), Pm = row3(g.fp[m]);
+            V3 AB = cross_ref(Nm, Nn);
+            AB = AB / sqrt(len2(AB));
+            const V3 A = three_plane_point(Nn, Nm, AB, dot(Pn, Nn), dot(Pm, Nm), 0.0);
+            g.AB[id][0] = AB.x; g.AB[id][1] = AB.y; g.AB[id][2] = AB.z;
+            g.A[id][0] = A.x; g.A[id][1] = A.y; g.A[id][2] = A.z;
         }
+        for (int m = 0; m < n; ++m)
+            for (int l = 0; l < m; ++l) {
+                const int id = (n - 2) * (n - 1) * n / 6 + (m - 1) * m / 2 + l;
+                const V3 Nm = row3(g.fn[m]), Pm = row3(g.fp[m]);
+                const V3 Nl = row3(g.fn[l]), Pl = row3(g.fp[l]);
+                const V3 C = three_plane_point(Nn, Nm, Nl, dot(Pn, Nn), dot(Pm, Nm), dot(Pl, Nl));
+                g.C[id][0] = C.x; g.C[id][1] = C.y; g.C[id][2] = C.z;
+            }
     }
-    if (imax < 0 || dmax >= wall_radius) return false;
-    distance = dmax;
-    normal = v3(w.faces[imax][0], w.faces[imax][1], w.faces[imax][2]);
-    return true;
 }
 
 } // namespace dem

@@ -110,6 +110,38 @@ def infinite_wall(normal, point, species=0, instance=0, velocity=(0, 0, 0), angu
     return w
 
 
+def intersection_wall(faces, position=(0, 0, 0), orientation=(1, 0, 0, 0), species=0, instance=0,
+                      velocity=(0, 0, 0), angular_velocity=(0, 0, 0), axisymmetric=False) -> _abi.Wall:
+    """IntersectionOfWalls (or, with axisymmetric=True,
+    AxisymmetricIntersectionOfWalls) built from `faces`, a list of
+    (normal, point) pairs as given to IntersectionOfWalls::addObject, in the
+    wall's frame (position, orientation quaternion)."""
+    if len(faces) > _abi.DEM_MAX_WALL_FACES:
+        raise ValueError(f"at most {_abi.DEM_MAX_WALL_FACES} faces")
+    w = _abi.Wall()
+    w.type = _abi.DEM_WALL_AXISYMMETRIC if axisymmetric else _abi.DEM_WALL_INTERSECTION
+    w.species = species
+    w.instance = instance
+    w.n_faces = len(faces)
+    w.position[:] = list(map(float, position))
+    w.orientation[:] = list(map(float, orientation))
+    w.velocity[:] = list(map(float, velocity))
+    w.angular_velocity[:] = list(map(float, angular_velocity))
+    for k, (nrm, pt) in enumerate(faces):
+        w.faces[k][:] = list(map(float, nrm)) + list(map(float, pt))
+    return w
+
+
+def axisymmetric_wall(axis, faces, position=(0, 0, 0), species=0, instance=0, velocity=(0, 0, 0),
+                      angular_velocity=(0, 0, 0)) -> _abi.Wall:
+    """AxisymmetricIntersectionOfWalls with setAxis(axis), setPosition(position)
+    and addObject(normal, point) for each (normal, point) of `faces`, given
+    in (r, 0, a) coordinates."""
+    from .host import quaternion_from_normal
+    return intersection_wall(faces, position, quaternion_from_normal(axis), species, instance, velocity,
+                             angular_velocity, axisymmetric=True)
+
+
 class DemEngine:
     def __init__(self, time_step: float, instances: list[Instance], species: list[_abi.SpeciesPair],
                  walls: list[_abi.Wall] | None = None, rotation: bool = True, background_drag: float = 0.0,
@@ -134,6 +166,7 @@ class DemEngine:
         walls = walls or []
         wa = (_abi.Wall * max(1, len(walls)))(*walls)
         self._check(lib().dem_set_walls(self._h, wa, len(walls)))
+        self._nwalls = len(walls)
         self.n = 0
 
     # ------------------------------------------------------------------
@@ -198,6 +231,13 @@ class DemEngine:
                               _dp(out["inv_inertia"]), _ip(out["species"]), _ip(out["id"]), _ip(out["instance"]))
         self._check(lib().dem_download_particles(self._h, C.byref(p)))
         return out
+
+    def walls(self) -> list:
+        """Current wall states (position and orientation after the steps taken)."""
+        n = self._nwalls
+        arr = (_abi.Wall * max(1, n))()
+        self._check(lib().dem_download_walls(self._h, arr, n))
+        return [arr[k] for k in range(n)]
 
     def forces(self):
         f = np.zeros((self.n, 3))

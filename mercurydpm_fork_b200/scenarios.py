@@ -11,6 +11,9 @@ all three start from bit-identical inputs.
 * :func:`periodic_chute` -- bidisperse (size ratio 2) spheres over a rough
   base of fixed spheres, periodic in x and y, gravity inclined like
   Chute::setChuteAngleAndMagnitudeOfGravity (Kernel/Chute.cc:789-805).
+* :func:`rotating_drum` -- bidisperse (size ratio 3, 90 % small by number)
+  spheres in a cylinder (AxisymmetricIntersectionOfWalls) with two flat end
+  caps, rotating about x, Hertz-Mindlin with rolling and torsion friction.
 """
 from __future__ import annotations
 
@@ -20,8 +23,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from .engine import Instance, infinite_wall, species_pair
-from .host import linear_collision_time_restitution, sphere_inv_mass_inertia, PI
+from .engine import Instance, axisymmetric_wall, infinite_wall, species_pair
+from .host import hertz_dissipation_from_restitution, linear_collision_time_restitution, sphere_inv_mass_inertia, PI
 
 
 @dataclass
@@ -265,3 +268,110 @@ def periodic_chute(n_flow: int = 200_000, seed: int = 2, ds: float = 1e-3, densi
     return Scenario("periodic_chute", tc / 50, inst, [sp], np.array([density]), [], position, velocity, radius,
                     inv_mass, inv_inertia, np.zeros(n, np.int32), np.arange(n, dtype=np.int32),
                     info=dict(n_flow=len(frad), n_base=len(brad), seed=seed, angle=angle, lx=lx, ly=ly))
+
+
+def hertz_mindlin_species(E: float, G: float, eps: float, mu: float, mu_r: float = 0.0, mu_o: float = 0.0,
+                          sliding_dissipation: float = 0.0, rolling_dissipation: float = 0.0,
+                          torsion_dissipation: float = 0.0, rolling_torsion: bool = True) -> _abi.SpeciesPair:
+    """HertzianViscoelasticMindlin(RollingTorsion)Species: effective elastic
+    modulus E and restitution eps
+    (setEffectiveElasticModulusAndRestitutionCoefficient,
+    HertzianViscoelasticNormalSpecies.cc:109-140), effective shear modulus G
+    (MindlinSpecies::setEffectiveShearModulus), Coulomb coefficients
+    mu (sliding), mu_r (rolling), mu_o (torsion), static = dynamic."""
+    law = _abi.DEM_FRICTION_MINDLIN_ROLLING_TORSION if rolling_torsion else _abi.DEM_FRICTION_MINDLIN
+    return species_pair(normal_law=_abi.DEM_NORMAL_HERTZIAN_VISCOELASTIC, friction_law=law, elastic_modulus=E,
+                        dissipation=hertz_dissipation_from_restitution(eps), shear_modulus=G,
+                        sliding_dissipation=sliding_dissipation, sliding_mu=mu, sliding_mu_static=mu,
+                        rolling_dissipation=rolling_dissipation, rolling_mu=mu_r, rolling_mu_static=mu_r,
+                        torsion_dissipation=torsion_dissipation, torsion_mu=mu_o, torsion_mu_static=mu_o)
+
+
+def hertz_collision_time(d: float, density: float, E: float, v: float = 1.0) -> float:
+    """HertzianViscoelasticNormalSpecies::getCollisionTime(d, rho, v)
+    (HertzianViscoelasticNormalSpecies.cc:290-300): 2.214 (rho^2/E^2/v)^0.2 d."""
+    return 2.214 * ((density / E) ** 2 / v) ** 0.2 * d
+
+
+def rotating_drum(n: int = 1_000_000, seed: int = 3, ds: float = 1e-3, size_ratio: float = 3.0,
+                  frac_small: float = 0.9, radius_d: float = 120.0, length_d: float = 60.0, omega: float = 1.0,
+                  E: float = 1e7, nu: float = 0.3, mu: float = 0.4, mu_r: float = 0.05, eps: float = 0.7,
+                  density: float = 2000.0, dt_factor: float = 0.02, site_spacing: float = 1.02,
+                  jitter: float = 0.005, vstd: float = 0.0, touch_wall: float = 0.0, gravity: float = 9.81,
+                  mu_o: float = 0.0, sliding_dissipation: float = 0.0, rolling_dissipation: float = 0.0,
+                  torsion_dissipation: float = 0.0) -> Scenario:
+    """Rotating drum: n spheres, frac_small of them small (diameter ds), the
+    rest size_ratio x larger, in a cylinder of radius radius_d ds and length
+    length_d ds along x (AxisymmetricIntersectionOfWalls with setAxis(1,0,0)
+    and one face addObject((1,0,0), (R,0,0))) closed by two InfiniteWall
+    caps; the cylinder rotates at omega rad/s about x, gravity -z.
+
+    Species: Hertz-Mindlin with rolling and torsion friction, effective
+    E and G = E/2 (1 + nu) (the reference's
+    setEffectiveElasticModulusAndPoissonRatio, HertzianViscoelasticNormalSpecies.cc:158),
+    restitution eps; dt = dt_factor x the Hertz collision time of two small
+    spheres at 1 m/s.
+
+    Packing: cubes of 3 x 3 x 3 lattice sites (site_spacing ds apart), each
+    holding one large sphere or up to 27 small ones, filled from the bottom of
+    the drum upwards, large cubes chosen in seeded random order, positions
+    jittered by +-jitter ds. site_spacing < 1 starts the bed pre-compressed.
+    touch_wall > 0 moves every sphere within touch_wall ds of the cylinder
+    radially onto it with an overlap of 0.1 touch_wall ds."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    R, L = radius_d * ds, length_d * ds
+    r_s, r_l = 0.5 * ds, 0.5 * ds * size_ratio
+    n_small = int(round(frac_small * n))
+    n_large = n - n_small
+    b = int(math.ceil(size_ratio - 1e-9))
+    s = site_spacing * ds
+    B = b * s
+    per_block = b ** 3
+    n_blocks = n_large + (n_small + per_block - 1) // per_block
+    nx = int(L // B)
+    nyz = int(2 * R // B)
+    xs = (np.arange(nx) - (nx - 1) / 2) * B
+    ys = (np.arange(nyz) - (nyz - 1) / 2) * B
+    X, Y, Z = np.meshgrid(xs, ys, ys, indexing="ij")
+    cen = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    reach = np.hypot(np.abs(cen[:, 1]) + B / 2, np.abs(cen[:, 2]) + B / 2)
+    cen = cen[reach <= R]
+    if len(cen) < n_blocks:
+        raise ValueError(f"{n} spheres do not fit: {n_blocks} blocks needed, {len(cen)} available")
+    order = np.lexsort((cen[:, 0], cen[:, 1], cen[:, 2]))
+    cen = cen[order[:n_blocks]]
+    large_block = np.zeros(n_blocks, bool)
+    large_block[rng.permutation(n_blocks)[:n_large]] = True
+    sub = (np.stack(np.meshgrid(np.arange(b), np.arange(b), np.arange(b), indexing="ij"), -1).reshape(-1, 3)
+           - (b - 1) / 2) * s
+    small_pos = (cen[~large_block][:, None, :] + sub[None, :, :]).reshape(-1, 3)[:n_small]
+    large_pos = cen[large_block]
+    position = np.concatenate([small_pos, large_pos])
+    radius = np.concatenate([np.full(n_small, r_s), np.full(n_large, r_l)])
+    species_index = np.concatenate([np.zeros(n_small, np.int32), np.ones(n_large, np.int32)])
+    perm = rng.permutation(n)
+    position, radius, species_index = position[perm], radius[perm], species_index[perm]
+    position = position + rng.uniform(-jitter * ds, jitter * ds, size=position.shape)
+    if touch_wall > 0.0:
+        rho = np.hypot(position[:, 1], position[:, 2])
+        near = rho + radius > R - touch_wall * ds
+        target = R - radius[near] + 0.1 * touch_wall * ds
+        position[near, 1:] *= (target / rho[near])[:, None]
+    velocity = rng.normal(0.0, vstd, size=(n, 3)) if vstd > 0 else np.zeros((n, 3))
+    inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
+    G = E / 2 * (1 + nu)
+    sp = hertz_mindlin_species(E, G, eps, mu, mu_r, mu_o, sliding_dissipation, rolling_dissipation,
+                               torsion_dissipation)
+    table = [sp] * 9  # species 0 small, 1 large, 2 wall; identical mixed entries
+    walls = [axisymmetric_wall((1, 0, 0), [((1, 0, 0), (R, 0, 0))], species=2, angular_velocity=(omega, 0, 0)),
+             infinite_wall((-1, 0, 0), (-L / 2, 0, 0), species=2),
+             infinite_wall((1, 0, 0), (L / 2, 0, 0), species=2)]
+    m = 2 * R + 4 * r_l
+    inst = Instance(domain_min=(-L / 2 - 2 * r_l, -m / 2, -m / 2), domain_max=(L / 2 + 2 * r_l, m / 2, m / 2),
+                    gravity=(0.0, 0.0, -gravity), n_species=3)
+    dt = dt_factor * hertz_collision_time(ds, density, E, 1.0)
+    return Scenario("rotating_drum", dt, inst, table, np.array([density] * 3), walls, position, velocity, radius,
+                    inv_mass, inv_inertia, species_index, np.arange(n, dtype=np.int32),
+                    info=dict(n=n, n_small=n_small, n_large=n_large, seed=seed, radius_d=radius_d,
+                              length_d=length_d, omega=omega, shear_modulus=G,
+                              solid_fraction_of_drum=float(np.sum(4 / 3 * PI * radius ** 3) / (PI * R * R * L))))

@@ -3,12 +3,12 @@
 // A CPU, FP64, single-threaded restatement of MercuryDPM's DEM time step for
 // the paths the GPU engine implements. It is the checker the parity tests
 // compare the CUDA path against; nothing in the product links or calls it.
-// It is itself pinned against the reference build in oracle/_ref (see
-// tests/test_oracle_vs_reference.py) and the reference's own known-answer
-// tests (tests/test_oracle_known_answers.py).
+// It is itself pinned against the reference build in oracle/_ref and the
+// reference's own known-answer tests (tests/test_oracle.py).
 //
 // Step order follows DPMBase::computeOneTimeStep (Kernel/DPMBase.cc:4315-4389):
-//   integrateBeforeForceComputation (BaseParticle.cc:718-752, BaseInteractable.cc:538-600)
+//   integrateBeforeForceComputation (BaseParticle.cc:718-752, then the walls:
+//                                    BaseInteractable.cc:538-600)
 //   checkInteractionWithBoundaries  (PeriodicBoundary.cc:374-395)
 //   computeAllForces                (DPMBase.cc:3397-3526, :3113-3162, :3168-3215)
 //   integrateAfterForceComputation  (BaseParticle.cc:760-776)
@@ -60,11 +60,161 @@ struct Inter {
     bool periodic;
 };
 
+// One face of an IntersectionOfWalls: the InfiniteWall that
+// IntersectionOfWalls::addObject(normal, point) creates (IntersectionOfWalls.cc:138-149).
+struct Face {
+    Q4 q;  // InfiniteWall orientation from the twice-normalised normal
+    V3 p;  // point
+    V3 n() const { return quat_axis(q); }
+    double dist(V3 x) const { return quat_plane_distance(q, x, p); }
+};
+
+Q4 face_orientation(V3 n)
+{
+    // addObject's Vec3D::normalise, then Quaternion::setOrientationViaNormal
+    // (Quaternion.cc:543-567), which normalises again
+    for (int k = 0; k < 2; ++k) {
+        const double l = sqrt(n.x * n.x + n.y * n.y + n.z * n.z);
+        n = v3(n.x / l, n.y / l, n.z / l);
+    }
+    if (n.x <= -1 + 1e-14) return Q4{0, 0, 1, 0};
+    const double h0 = 1.0 + n.x, h1 = 0.0 + n.y, h2 = 0.0 + n.z;
+    const Q4 q{h0, 0.0, -h2, h1};
+    const double l = sqrt(q.q0 * q.q0 + q.q1 * q.q1 + q.q2 * q.q2 + q.q3 * q.q3);
+    return Q4{q.q0 / l, q.q1 / l, q.q2 / l, q.q3 / l};
+}
+
+// Solution of the 3x3 system with rows r0, r1, r2 and right-hand side b by
+// cofactors, in the term order of IntersectionOfWalls::setPointsAndLines
+// (IntersectionOfWalls.cc:365-389, 399-433).
+V3 cramer(V3 r0, V3 r1, V3 r2, double b0, double b1, double b2)
+{
+    const double c00 = r1.y * r2.z - r2.y * r1.z;
+    const double c01 = r1.x * r2.z - r1.z * r2.x;
+    const double c02 = r1.x * r2.y - r1.y * r2.x;
+    const double inv = 1.0 / (+r0.x * c00 - r0.y * c01 + r0.z * c02);
+    const double x = +c00 * b0 - (r0.y * r2.z - r0.z * r2.y) * b1 + (r0.y * r1.z - r0.z * r1.y) * b2;
+    const double y = -c01 * b0 + (r0.x * r2.z - r0.z * r2.x) * b1 - (r0.x * r1.z - r1.x * r0.z) * b2;
+    const double z = +(r1.x * r2.y - r2.x * r1.y) * b0 - (r0.x * r2.y - r2.x * r0.y) * b1 +
+                     (r0.x * r1.y - r1.x * r0.y) * b2;
+    return v3(x * inv, y * inv, z * inv);
+}
+
+struct Intersection {
+    std::vector<Face> f;
+    std::vector<V3> A, AB, C; // indexed as the reference's A_, AB_, C_
+
+    void build(const dem_wall& w)
+    {
+        for (int n = 0; n < w.n_faces; ++n) {
+            Face fc;
+            fc.q = face_orientation(v3(w.faces[n][0], w.faces[n][1], w.faces[n][2]));
+            fc.p = v3(w.faces[n][3], w.faces[n][4], w.faces[n][5]);
+            f.push_back(fc);
+            A.resize((size_t)(n + 1) * n / 2);
+            AB.resize(A.size());
+            for (int m = 0; m < n; ++m) {
+                const V3 a = f[m].n(), b = f[n].n();
+                V3 ab = v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+                const double l = sqrt(ab.x * ab.x + ab.y * ab.y + ab.z * ab.z);
+                ab = v3(ab.x / l, ab.y / l, ab.z / l);
+                const size_t id = (size_t)(n - 1) * n / 2 + m;
+                AB[id] = ab;
+                A[id] = cramer(b, a, ab, dot(f[n].p, b), dot(f[m].p, a), 0.0);
+            }
+            C.resize((size_t)(n + 1) * n * (n > 0 ? n - 1 : 0) / 6);
+            for (int m = 0; m < n; ++m)
+                for (int l = 0; l < m; ++l) {
+                    const size_t id = (size_t)(n - 2) * (n - 1) * n / 6 + (size_t)(m - 1) * m / 2 + l;
+                    C[id] = cramer(f[n].n(), f[m].n(), f[l].n(), dot(f[n].p, f[n].n()), dot(f[m].p, f[m].n()),
+                                   dot(f[l].p, f[l].n()));
+                }
+        }
+    }
+
+    // IntersectionOfWalls::getDistanceAndNormal(const Vec3D&, ...) (IntersectionOfWalls.cc:567-712)
+    bool distance(V3 x, double R, double& d, V3& nrm) const
+    {
+        if (f.empty()) return false;
+        double d1 = -1e20, d2 = -1e20, d3 = -1e20;
+        unsigned i1 = 0, i2 = 0, i3 = 0;
+        for (unsigned i = 0; i < f.size(); ++i) {
+            const double dc = f[i].dist(x);
+            if (dc >= R) return false;
+            if (dc > d1) {
+                if (d1 > -R) {
+                    if (d2 > -R) { d3 = d2; i3 = i2; }
+                    d2 = d1; i2 = i1;
+                }
+                d1 = dc; i1 = i;
+            } else if (dc < -R) {
+                continue;
+            } else if (dc > d2) {
+                if (d2 > -R) { d3 = d2; i3 = i2; }
+                d2 = dc; i2 = i;
+            } else if (dc > d3) {
+                d3 = dc; i3 = i;
+            }
+        }
+        d = d1;
+        if (d2 > -R) {
+            const V3 D = x + f[i1].n() * d1;
+            bool with2 = f[i2].dist(D) > 0.0;
+            if (d3 > -R && f[i3].dist(D) > 0.0) {
+                const V3 E = x + f[i2].n() * d2;
+                const bool with3 = f[i3].dist(E) > 0.0;
+                if (with2) {
+                    if (with3) {
+                        if (i2 > i3) std::swap(i2, i3);
+                        auto tri = [](unsigned a) { return (a - 2) * (a - 1) * a / 6; };
+                        auto pr = [](unsigned a) { return (a - 1) * a / 2; };
+                        const unsigned idx = i1 < i2 ? tri(i3) + pr(i2) + i1
+                                                     : (i1 < i3 ? tri(i3) + pr(i1) + i2 : tri(i1) + pr(i3) + i2);
+                        nrm = x - C[idx];
+                        d = sqrt(len2(nrm));
+                        if (d <= R) { nrm = nrm / (-d); return true; }
+                        if (d == d) return false;
+                    }
+                } else {
+                    with2 = true;
+                    d2 = d3;
+                    i2 = i3;
+                }
+            }
+            if (with2) {
+                const unsigned idx = i1 > i2 ? (i1 - 1) * i1 / 2 + i2 : (i2 - 1) * i2 / 2 + i1;
+                const V3 ac = x - A[idx];
+                nrm = ac - AB[idx] * dot(ac, AB[idx]);
+                d = sqrt(len2(nrm));
+                if (d <= R) { nrm = nrm / (-d); return true; }
+                if (d == d) return false;
+            }
+        }
+        nrm = f[i1].n();
+        return true;
+    }
+};
+
+// Quaternion::rotate (back = false) / rotateBack (back = true), Quaternion.cc:570-640;
+// the off-diagonal signs flip between the two (transpose)
+V3 q_apply(Q4 q, V3 v, bool back)
+{
+    const double a = q.q0 * q.q0, b = q.q1 * q.q1, c = q.q2 * q.q2, e = q.q3 * q.q3;
+    const double q01 = 2 * q.q0 * q.q1, q02 = 2 * q.q0 * q.q2, q03 = 2 * q.q0 * q.q3;
+    const double q12 = 2 * q.q1 * q.q2, q13 = 2 * q.q1 * q.q3, q23 = 2 * q.q2 * q.q3;
+    const double m01 = back ? q12 + q03 : q12 - q03, m02 = back ? q13 - q02 : q13 + q02;
+    const double m10 = back ? q12 - q03 : q12 + q03, m12 = back ? q23 + q01 : q23 - q01;
+    const double m20 = back ? q13 + q02 : q13 - q02, m21 = back ? q23 - q01 : q23 + q01;
+    const double m00 = a + b - c - e, m11 = a - b + c - e, m22 = a - b - c + e;
+    return v3(m00 * v.x + m01 * v.y + m02 * v.z, m10 * v.x + m11 * v.y + m12 * v.z, m20 * v.x + m21 * v.y + m22 * v.z);
+}
+
 struct Sim {
     dem_config cfg;
     dem_instance_desc inst;
     std::vector<dem_species_pair> species;
     std::vector<dem_wall> walls;
+    std::vector<Intersection> wgeo;
     std::vector<Particle> p;
     std::map<std::tuple<int, int, int>, Inter> inter;
     unsigned nt = 0; // DPMBase::numberOfTimeSteps_
@@ -92,6 +242,13 @@ struct Sim {
                     q.q = quat_rotate(q.q, q.w * dt);
                 }
             }
+        }
+        for (auto& w : walls) { // BaseInteractable::integrateBeforeForceComputation: move, rotate
+            const V3 dx = v3(w.velocity[0], w.velocity[1], w.velocity[2]) * dt;
+            w.position[0] += dx.x; w.position[1] += dx.y; w.position[2] += dx.z;
+            const Q4 q = quat_rotate(Q4{w.orientation[0], w.orientation[1], w.orientation[2], w.orientation[3]},
+                                     v3(w.angular_velocity[0], w.angular_velocity[1], w.angular_velocity[2]) * dt);
+            w.orientation[0] = q.q0; w.orientation[1] = q.q1; w.orientation[2] = q.q2; w.orientation[3] = q.q3;
         }
     }
 
@@ -166,13 +323,33 @@ struct Sim {
         }
     }
 
-    bool wall_dist(const dem_wall& w, V3 x, double radius, double& dist, V3& nrm) const
+    bool wall_dist(int wi, V3 x, double radius, double& dist, V3& nrm) const
     {
-        if (w.type != DEM_WALL_INFINITE) return false;
+        const dem_wall& w = walls[wi];
         const Q4 q{w.orientation[0], w.orientation[1], w.orientation[2], w.orientation[3]};
-        dist = quat_plane_distance(q, x, v3(w.position[0], w.position[1], w.position[2]));
-        if (dist >= radius) return false;
-        nrm = quat_axis(q);
+        const V3 wp = v3(w.position[0], w.position[1], w.position[2]);
+        if (w.type == DEM_WALL_INFINITE) {
+            dist = quat_plane_distance(q, x, wp);
+            if (dist >= radius) return false;
+            nrm = quat_axis(q);
+            return true;
+        }
+        if (w.type == DEM_WALL_AXISYMMETRIC) { // AxisymmetricIntersectionOfWalls.cc:93-124
+            const V3 po = x - wp;
+            const V3 axis = quat_axis(q);
+            const double a = dot(po, axis);
+            V3 rad = po - axis * a;
+            const double r = sqrt(len2(rad));
+            V3 n2;
+            if (!wgeo[wi].distance(v3(r, 0.0, a), radius, dist, n2)) return false;
+            if (r != 0) rad = rad / r;
+            nrm = axis * n2.z + rad * n2.x;
+            return true;
+        }
+        // IntersectionOfWalls::getDistanceAndNormal(const BaseParticle&, ...) (:532-547)
+        V3 nb;
+        if (!wgeo[wi].distance(q_apply(q, x - wp, true), radius, dist, nb)) return false;
+        nrm = q_apply(q, nb, false);
         return true;
     }
 
@@ -263,7 +440,7 @@ struct Sim {
                 const dem_species_pair& s = sp(q.species, wall.species);
                 double dist;
                 V3 nrm;
-                if (!wall_dist(wall, q.x, q.r + s.interaction_distance, dist, nrm)) continue;
+                if (!wall_dist(w, q.x, q.r + s.interaction_distance, dist, nrm)) continue;
                 const auto key = std::make_tuple(2, q.id, w);
                 auto it = inter.find(key);
                 if (it == inter.end()) {
@@ -366,6 +543,9 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
     S.inst = *inst;
     S.species.assign(species, species + nspecies);
     S.walls.assign(walls, walls + nwalls);
+    S.wgeo.resize(nwalls);
+    for (int w = 0; w < nwalls; ++w)
+        if (walls[w].type != DEM_WALL_INFINITE) S.wgeo[w].build(walls[w]);
     for (int k = 0; k < 3; ++k) {
         S.L[k] = inst->periodic_max[k] - inst->periodic_min[k];
         S.half[k] = 0.5 * S.L[k];

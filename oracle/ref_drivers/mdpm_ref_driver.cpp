@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <sstream>
 #include <vector>
 
 #include "Boundaries/PeriodicBoundary.h"
@@ -32,11 +33,31 @@
 #include "Species/LinearViscoelasticFrictionSpecies.h"
 #include "Species/LinearViscoelasticSlidingFrictionSpecies.h"
 #include "Species/LinearViscoelasticSpecies.h"
+#include "Walls/AxisymmetricIntersectionOfWalls.h"
 #include "Walls/InfiniteWall.h"
+#include "Walls/IntersectionOfWalls.h"
 
 #include "../../include/dem_b200.h"
 
 namespace {
+
+// MindlinInteraction keeps its sliding spring without a getter; its public
+// write() prints it after the token "slidingSpring" (MindlinInteraction.cc:166-170).
+Vec3D mindlin_sliding_spring(const BaseInteraction* c)
+{
+    std::ostringstream os;
+    os.precision(17);
+    c->write(os);
+    std::istringstream is(os.str());
+    std::string tok;
+    while (is >> tok)
+        if (tok == "slidingSpring") {
+            Vec3D v;
+            is >> v.X >> v.Y >> v.Z;
+            return v;
+        }
+    return Vec3D(0, 0, 0);
+}
 
 void apply_parts(BaseSpecies* s, const dem_species_pair& p)
 {
@@ -120,14 +141,24 @@ public:
         setRotation(cfg->rotation != 0);
         for (int w = 0; w < nwalls; ++w) {
             const dem_wall& x = walls[w];
-            if (x.type != DEM_WALL_INFINITE) continue;
-            InfiniteWall wall;
-            wall.setSpecies(speciesHandler.getObject(x.species));
-            wall.setOrientation(Quaternion(x.orientation[0], x.orientation[1], x.orientation[2], x.orientation[3]));
-            wall.setPosition(Vec3D(x.position[0], x.position[1], x.position[2]));
-            wall.setVelocity(Vec3D(x.velocity[0], x.velocity[1], x.velocity[2]));
-            wall.setAngularVelocity(Vec3D(x.angular_velocity[0], x.angular_velocity[1], x.angular_velocity[2]));
-            wallHandler.copyAndAddObject(wall);
+            BaseWall* wall = nullptr;
+            if (x.type == DEM_WALL_INFINITE) {
+                wall = new InfiniteWall();
+            } else {
+                IntersectionOfWalls* iw = (x.type == DEM_WALL_AXISYMMETRIC) ? new AxisymmetricIntersectionOfWalls()
+                                                                           : new IntersectionOfWalls();
+                for (int f = 0; f < x.n_faces; ++f)
+                    iw->addObject(Vec3D(x.faces[f][0], x.faces[f][1], x.faces[f][2]),
+                                  Vec3D(x.faces[f][3], x.faces[f][4], x.faces[f][5]));
+                wall = iw;
+            }
+            wall->setSpecies(speciesHandler.getObject(x.species));
+            wall->setOrientation(Quaternion(x.orientation[0], x.orientation[1], x.orientation[2], x.orientation[3]));
+            wall->setPosition(Vec3D(x.position[0], x.position[1], x.position[2]));
+            wall->setVelocity(Vec3D(x.velocity[0], x.velocity[1], x.velocity[2]));
+            wall->setAngularVelocity(Vec3D(x.angular_velocity[0], x.angular_velocity[1], x.angular_velocity[2]));
+            wallHandler.copyAndAddObject(*wall);
+            delete wall;
         }
         for (int k = 0; k < 3; ++k) {
             if (!((inst->periodic_mask >> k) & 1u)) continue;
@@ -253,6 +284,7 @@ int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem
                 for (int k = 0; k < 9; ++k) s[k] = 0.0;
                 Vec3D sl(0, 0, 0), ro(0, 0, 0), to(0, 0, 0);
                 if (auto* fi = dynamic_cast<SlidingFrictionInteraction*>(c)) sl = fi->getSlidingSpring();
+                if (dynamic_cast<MindlinInteraction*>(c)) sl = mindlin_sliding_spring(c);
                 if (auto* fi = dynamic_cast<FrictionInteraction*>(c)) { ro = fi->getRollingSpring(); to = fi->getTorsionSpring(); }
                 if (auto* fi = dynamic_cast<MindlinRollingTorsionInteraction*>(c)) { ro = fi->getRollingSpring(); to = fi->getTorsionSpring(); }
                 s[0] = sl.X; s[1] = sl.Y; s[2] = sl.Z; s[3] = ro.X; s[4] = ro.Y; s[5] = ro.Z; s[6] = to.X; s[7] = to.Y; s[8] = to.Z;

@@ -91,3 +91,120 @@ def tangential_spring():
         t += g["time_step"]
         steps += 1
     return sc, steps, g["expected"]
+
+
+def _hertz_mindlin_table(nsp):
+    from mercurydpm_fork_b200.scenarios import hertz_mindlin_species
+    sp = hertz_mindlin_species(1e7, 1e7 / 2 * 1.3, 0.7, 0.4, 0.05, 0.02, sliding_dissipation=0.3,
+                               rolling_dissipation=0.2, torsion_dissipation=0.1)
+    return [sp] * (nsp * nsp)
+
+
+def _rot(q, v):
+    q0, q1, q2, q3 = q
+    Rm = np.array([[q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3, 2 * (q1 * q2 - q0 * q3), 2 * (q1 * q3 + q0 * q2)],
+                   [2 * (q1 * q2 + q0 * q3), q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3, 2 * (q2 * q3 - q0 * q1)],
+                   [2 * (q1 * q3 - q0 * q2), 2 * (q2 * q3 + q0 * q1), q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3]])
+    return v @ Rm.T
+
+
+def wall_probe(kind: str, n: int = 300, seed: int = 11, omega=(0.0, 0.0, 0.0)):
+    """Spheres (d = 1 mm, Hertz-Mindlin with rolling and torsion) scattered
+    without mutual overlap within 0.3-1.1 radii of an intersection wall, so
+    that face, edge and corner contacts all occur at the start:
+
+    * "heap_base": CalibrationHeap's floor disk (AxisymmetricIntersectionOfWalls,
+      axis z, addObject((-1,0,0),(R,0,0)) and addObject((0,0,-1),(0,0,0)),
+      Drivers/Calibration/CalibrationHeap.cpp:86-91), R = 6 mm;
+    * "ring_ridge": an axisymmetric ring of triangular cross-section (axis z;
+      r > 4 mm, a > 0, r + a < 5.5 mm): near its narrow tip a sphere is
+      within reach of all three faces, whose normals are coplanar in the
+      (r, a) plane, so the reference's corner point is not finite and its
+      corner branch falls through to the edge branch;
+    * "box_corner": an IntersectionOfWalls of three orthogonal faces (a solid
+      octant) at a seeded random orientation and position: face, edge and
+      corner contacts in 3D.
+    The wall rotates with angular velocity `omega` about its own position."""
+    from mercurydpm_fork_b200.engine import axisymmetric_wall, intersection_wall
+    from mercurydpm_fork_b200.scenarios import hertz_collision_time
+    rng = np.random.Generator(np.random.PCG64(seed))
+    d = 1e-3
+    r = 0.5 * d
+    R = 6e-3
+    q = None
+    if kind == "heap_base":
+        wall = axisymmetric_wall((0, 0, 1), [((-1, 0, 0), (R, 0, 0)), ((0, 0, -1), (0, 0, 0))], species=1,
+                                 angular_velocity=omega)
+
+        def local(m):
+            rr = np.sqrt(rng.uniform(0, (R + 2 * r) ** 2, m))
+            ph = rng.uniform(0, 2 * PI, m)
+            z = rng.uniform(-2 * r, 2 * r, m)
+            p = np.stack([rr * np.cos(ph), rr * np.sin(ph), z], 1)
+            dist = np.where(rr <= R, z, np.where(z <= 0, rr - R, np.hypot(rr - R, z)))
+            return p, dist
+    elif kind == "ring_ridge":
+        R1, R2 = 4e-3, 5.5e-3
+        wall = axisymmetric_wall((0, 0, 1), [((1, 0, 0), (R1, 0, 0)), ((0, 0, 1), (0, 0, 0)),
+                                             ((-1, 0, -1), (R2, 0, 0))], species=1, angular_velocity=omega)
+        tri = np.array([[R1, 0.0], [R2, 0.0], [R1, R2 - R1]])
+
+        def local(m):
+            rr = rng.uniform(R1 - 2 * r, R2 + 2 * r, m)
+            a = rng.uniform(-2 * r, R2 - R1 + 2 * r, m)
+            ph = rng.uniform(0, 2 * PI, m)
+            p = np.stack([rr * np.cos(ph), rr * np.sin(ph), a], 1)
+            q2 = np.stack([rr, a], 1)
+            dist = np.full(m, np.inf)
+            for k in range(3):
+                s0, s1 = tri[k], tri[(k + 1) % 3]
+                t = np.clip(((q2 - s0) @ (s1 - s0)) / ((s1 - s0) @ (s1 - s0)), 0, 1)
+                dist = np.minimum(dist, np.linalg.norm(q2 - (s0 + t[:, None] * (s1 - s0)), axis=1))
+            inside = (rr > R1) & (a > 0) & (rr + a < R2)
+            return p, np.where(inside, -dist, dist)
+    elif kind == "box_corner":
+        qv = rng.normal(size=4)
+        q = tuple(qv / np.linalg.norm(qv))
+        origin = np.array([1e-3, -2e-3, 0.5e-3])
+        wall = intersection_wall([((1, 0, 0), (0, 0, 0)), ((0, 1, 0), (0, 0, 0)), ((0, 0, 1), (0, 0, 0))],
+                                 position=origin, orientation=q, species=1, angular_velocity=omega)
+
+        def local(m):
+            p = rng.uniform(-2 * r, 14 * r, size=(m, 3))
+            out = np.maximum(-p, 0.0)
+            dist = np.where((p > 0).all(1), -p.min(1), np.sqrt((out ** 2).sum(1)))
+            return p, dist
+    else:
+        raise ValueError(kind)
+    pts = []
+    for _ in range(50):
+        p, dist = local(4000)
+        for x in p[(dist > 0.3 * r) & (dist < 1.1 * r)]:
+            if len(pts) >= n:
+                break
+            if not pts or np.min(np.sum((np.array(pts) - x) ** 2, 1)) > (2.05 * r) ** 2:
+                pts.append(x)
+        if len(pts) >= n:
+            break
+    pos = np.array(pts)
+    if q is not None:
+        pos = _rot(q, pos) + origin
+    m = len(pos)
+    radius = np.full(m, r)
+    density = 2000.0
+    inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
+    vel = rng.normal(0.0, 0.05, size=(m, 3))
+    lo, hi = pos.min(0) - 8 * r, pos.max(0) + 8 * r
+    inst = Instance(domain_min=tuple(lo), domain_max=tuple(hi), gravity=(0, 0, -9.81), n_species=2)
+    dt = 0.02 * hertz_collision_time(d, density, 1e7)
+    return Scenario(f"wall_probe_{kind}", dt, inst, _hertz_mindlin_table(2), np.array([density, density]), [wall],
+                    pos, vel, radius, inv_mass, inv_inertia, np.zeros(m, np.int32), np.arange(m, dtype=np.int32))
+
+
+def small_drum(n=600, seed=5):
+    """Rotating drum (R = 12 mm, length 12 mm, 5 rad/s), bidisperse 1:3,
+    Hertz-Mindlin with rolling and torsion, bed pre-compressed, the outer
+    spheres pressed onto the cylinder."""
+    return scenarios.rotating_drum(n=n, seed=seed, radius_d=12, length_d=12, site_spacing=0.995, touch_wall=3.0,
+                                   omega=5.0, mu_o=0.02, sliding_dissipation=0.3, rolling_dissipation=0.2,
+                                   torsion_dissipation=0.1, vstd=0.02)

@@ -237,6 +237,8 @@ def pair_set(c) -> set:
 def rel_err(a, b, scale=None):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
+    if a.size == 0 and b.size == 0:
+        return 0.0
     s = np.max(np.abs(b)) if scale is None else scale
     if s == 0:
         return float(np.max(np.abs(a - b)))

@@ -62,3 +62,33 @@ def test_oracle_matches_reference_periodic_chute(nsteps):
     assert (o["contacts"]["periodic"] == r["contacts"]["periodic"]).all()
     assert H.rel_err(o["force"], r["force"]) < 1e-12
     assert H.rel_err(o["position"], r["position"], 1e-3) < 1e-14
+
+
+WALL_CASES = {
+    "drum": lambda: cases.small_drum(),
+    "heap_base": lambda: cases.wall_probe("heap_base", omega=(0.5, 1.0, 3.0)),
+    "ring_ridge": lambda: cases.wall_probe("ring_ridge", omega=(0.5, 1.0, 3.0)),
+    "box_corner": lambda: cases.wall_probe("box_corner", omega=(0.5, 1.0, 3.0)),
+}
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(WALL_CASES))
+@pytest.mark.parametrize("nsteps", [0, 10, 100])
+def test_oracle_matches_reference_intersection_walls(name, nsteps):
+    """AxisymmetricIntersectionOfWalls / IntersectionOfWalls (faces, edges,
+    corners, the non-finite-corner fall-through), rotating walls and the
+    Hertz-Mindlin rolling-torsion law against the reference build."""
+    sc = WALL_CASES[name]()
+    o = H.run_oracle(sc, nsteps)
+    r = H.run_reference(sc, nsteps)
+    assert H.pair_set(o["contacts"]) == H.pair_set(r["contacts"])
+    if nsteps == 0:
+        assert int(o["contacts"]["is_wall"].sum()) > 80
+        np.testing.assert_array_equal(o["contacts"]["force"], r["contacts"]["force"])
+        np.testing.assert_array_equal(o["contacts"]["overlap"], r["contacts"]["overlap"])
+        np.testing.assert_array_equal(o["contacts"]["springs"], r["contacts"]["springs"])
+    assert H.rel_err(o["force"], r["force"]) < 1e-12
+    assert H.rel_err(o["torque"], r["torque"]) < 1e-12
+    assert H.rel_err(o["position"], r["position"], 1e-3) < 1e-13
+    assert H.rel_err(o["contacts"]["springs"], r["contacts"]["springs"]) < 1e-11

@@ -181,20 +181,27 @@ def run_ours(args):
             traffic = None
 
     # end to end through the public API with host buffers
-    pos = torch.from_numpy(np.ascontiguousarray(sc.position)).pin_memory().numpy()
-    vel = torch.from_numpy(np.ascontiguousarray(sc.velocity)).pin_memory().numpy()
+    # (pinned host memory in both directions; each step uploads the full input
+    # state and reads back the evolved state: position, velocity, angular
+    # velocity, orientation)
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+    inputs = [pinned(a) for a in (sc.position, sc.velocity, sc.radius, sc.inv_mass, sc.inv_inertia,
+                                  sc.species_index, sc.ids)]
+    outputs = dict(position=pinned(np.zeros((sc.n, 3))), velocity=pinned(np.zeros((sc.n, 3))),
+                   angular_velocity=pinned(np.zeros((sc.n, 3))), orientation=pinned(np.zeros((sc.n, 4))))
+    h2d = sum(a.nbytes for a in inputs)
+    d2h = sum(a.nbytes for a in outputs.values())
     e2e_ms = 0.0
     e2e_steps = max(1, min(args.steps, 3))
-    h2d = d2h = 0
     barrier()
     for _ in range(e2e_steps):
         t1 = time.perf_counter()
-        eng.upload(pos, vel, sc.radius, sc.inv_mass, sc.inv_inertia, sc.species_index, sc.ids)
+        eng.upload(*inputs)
         eng.step(STEPS_PER_CALL)
-        out = eng.download()
+        eng.download(out=outputs)
         e2e_ms += (time.perf_counter() - t1) * 1e3
-        h2d = sc.n * (4 * 32 + 16 + 4)
-        d2h = sc.n * (4 * 32 + 16 + 4)
     e2e_value = n_moving * e2e_steps * STEPS_PER_CALL / (e2e_ms / 1e3) * world
 
     cpu = None

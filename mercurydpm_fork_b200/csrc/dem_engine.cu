@@ -42,6 +42,8 @@ struct Handle {
     dem_species_pair* d_species = nullptr;
     dem_wall* d_walls = nullptr;
     WallGeom* d_wgeom = nullptr;
+    double* d_stage = nullptr;         // caller-layout particle staging (18 words per slot)
+    std::vector<long long> layout;     // sizes the device arrays were allocated for
     Control* d_ctl = nullptr;
     ContactRecord* d_records = nullptr;
     unsigned record_capacity = 0;
@@ -101,6 +103,8 @@ void free_particle_arrays(Handle* h)
     h->allocs.clear();
     h->d_records = nullptr;
     h->record_capacity = 0;
+    h->d_stage = nullptr;
+    h->layout.clear();
 }
 
 inline unsigned grid_for(long long n, int block) { return (unsigned)std::max<long long>(1, (n + block - 1) / block); }
@@ -488,8 +492,15 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     cap = ((cap + 31) / 32) * 32;
     if (cap > 128) return fail(h, DEM_ERR_BAD_INPUT, "max_neighbors above 128 is not supported");
 
-    // ---- (re)allocate
-    free_particle_arrays(h);
+    // ---- (re)allocate: a re-upload with the same sizes keeps the device arrays
+    // and the captured graphs (their kernel arguments stay valid)
+    const unsigned record_capacity =
+        (unsigned)std::min<long long>(2000000000ll, 8 * n + 1024 + (long long)n * std::min(wmax, 4));
+    const std::vector<long long> layout = {n, cap, wmax, ncells, (long long)h->inst.size(), (long long)h->species.size(),
+                                           (long long)h->walls.size(), (long long)record_capacity, h->ncomp};
+    const bool reuse = !h->layout.empty() && h->layout == layout;
+    if (!reuse) free_particle_arrays(h);
+    const DevPtrs kept = h->d;
     h->d = DevPtrs{};
     DevPtrs& d = h->d;
     d.n = (int)n;
@@ -509,6 +520,29 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     h->nblocks_scan = (int)grid_for(ncells, 1024);
     const size_t NC = d.ncap;
     int rc;
+    if (reuse) {
+        // graphs hold the kernel arguments by value: keep them only if nothing changed
+        const bool same = d.n == kept.n && d.ncap == kept.ncap && d.cap == kept.cap && d.nwords == kept.nwords &&
+                          d.ncomp == kept.ncomp && d.wmax == kept.wmax && d.ncells == kept.ncells &&
+                          d.rotation == kept.rotation && d.single_instance == kept.single_instance &&
+                          d.n_species_table == kept.n_species_table && d.zero_idist == kept.zero_idist &&
+                          d.dt == kept.dt && d.drag == kept.drag;
+        if (!same) free_graphs(h);
+        for (int b = 0; b < 2; ++b) {
+            d.pr[b] = kept.pr[b]; d.vm[b] = kept.vm[b]; d.wi[b] = kept.wi[b]; d.qo[b] = kept.qo[b];
+            d.info[b] = kept.info[b]; d.caller[b] = kept.caller[b]; d.nbr[b] = kept.nbr[b]; d.cnt[b] = kept.cnt[b];
+            d.hist[b] = kept.hist[b]; d.act[b] = kept.act[b]; d.whist[b] = kept.whist[b]; d.wact[b] = kept.wact[b];
+        }
+        d.force = kept.force; d.torque = kept.torque; d.key = kept.key; d.perm = kept.perm; d.newidx = kept.newidx;
+        d.cell_count = kept.cell_count; d.cell_start = kept.cell_start; d.cell_cursor = kept.cell_cursor;
+        d.block_sums = kept.block_sums; d.inst = kept.inst; d.species = kept.species; d.walls = kept.walls;
+        d.wgeom = kept.wgeom; d.n_walls = kept.n_walls; d.ctl = kept.ctl; d.records = kept.records;
+        for (int b = 0; b < 2; ++b) { // no history carries over from the previous simulation
+            CU(cudaMemsetAsync(d.cnt[b], 0, NC * sizeof(int), h->stream));
+            CU(cudaMemsetAsync(d.act[b], 0, (size_t)d.nwords * NC * sizeof(unsigned), h->stream));
+            CU(cudaMemsetAsync(d.wact[b], 0, NC * sizeof(unsigned), h->stream));
+        }
+    } else {
     for (int b = 0; b < 2; ++b) {
         if ((rc = dalloc(h, &d.pr[b], NC))) return rc;
         if ((rc = dalloc(h, &d.vm[b], NC))) return rc;
@@ -537,8 +571,9 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     if ((rc = dalloc(h, &h->d_walls, std::max<size_t>(1, h->walls.size())))) return rc;
     if ((rc = dalloc(h, &h->d_wgeom, std::max<size_t>(1, h->wgeom.size())))) return rc;
     if ((rc = dalloc(h, &h->d_ctl, 1))) return rc;
-    h->record_capacity = (unsigned)std::min<long long>(2000000000ll, 8 * n + 1024 + (long long)n * std::min(wmax, 4));
+    h->record_capacity = record_capacity;
     if ((rc = dalloc(h, &h->d_records, h->record_capacity))) return rc;
+    if ((rc = dalloc(h, &h->d_stage, 18 * NC))) return rc;
     d.inst = h->d_inst;
     d.species = h->d_species;
     d.walls = h->d_walls;
@@ -546,30 +581,28 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     d.n_walls = (int)h->walls.size();
     d.ctl = h->d_ctl;
     d.records = h->d_records;
-
-    // ---- host staging in caller order
-    std::vector<double4> pr(n), vm(n), wi(n), qo(n);
-    std::vector<int4> info(n);
-    std::vector<int> caller(n);
-    for (long long i = 0; i < n; ++i) {
-        pr[i] = make_double4(p->position[3 * i], p->position[3 * i + 1], p->position[3 * i + 2], p->radius[i]);
-        vm[i] = make_double4(p->velocity[3 * i], p->velocity[3 * i + 1], p->velocity[3 * i + 2], p->inv_mass[i]);
-        const double* w = p->angular_velocity;
-        wi[i] = make_double4(w ? w[3 * i] : 0.0, w ? w[3 * i + 1] : 0.0, w ? w[3 * i + 2] : 0.0,
-                             p->inv_inertia ? p->inv_inertia[i] : 0.0);
-        const double* q = p->orientation;
-        qo[i] = q ? make_double4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]) : make_double4(1.0, 0.0, 0.0, 0.0);
-        const int in = p->instance ? p->instance[i] : 0;
-        const int flags = (p->inv_mass[i] == 0.0 ? FLAG_FIXED : 0) | (level[i] << LEVEL_SHIFT);
-        info[i] = make_int4(p->id[i], p->species[i], in, flags);
-        caller[i] = (int)i;
+    h->layout = layout;
     }
-    CU(cudaMemcpyAsync(d.pr[0], pr.data(), n * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
-    CU(cudaMemcpyAsync(d.vm[0], vm.data(), n * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
-    CU(cudaMemcpyAsync(d.wi[0], wi.data(), n * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
-    CU(cudaMemcpyAsync(d.qo[0], qo.data(), n * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
-    CU(cudaMemcpyAsync(d.info[0], info.data(), n * sizeof(int4), cudaMemcpyHostToDevice, h->stream));
-    CU(cudaMemcpyAsync(d.caller[0], caller.data(), n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+
+    // ---- the caller's arrays go to the device staging area as they are; k_pack
+    // builds the state records there
+    const StagePtrs st = stage_ptrs(h->d_stage, NC);
+    auto put = [&](void* dst, const void* src, size_t bytes) -> int {
+        if (src && bytes) CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream));
+        return DEM_OK;
+    };
+    const size_t dn = (size_t)n * sizeof(double), in4 = (size_t)n * sizeof(int);
+    if ((rc = put(st.pos, p->position, 3 * dn)) || (rc = put(st.vel, p->velocity, 3 * dn)) ||
+        (rc = put(st.ang, p->angular_velocity, 3 * dn)) || (rc = put(st.ori, p->orientation, 4 * dn)) ||
+        (rc = put(st.rad, p->radius, dn)) || (rc = put(st.im, p->inv_mass, dn)) ||
+        (rc = put(st.ii, p->inv_inertia, dn)) || (rc = put(st.sp, p->species, in4)) || (rc = put(st.id, p->id, in4)) ||
+        (rc = put(st.inst, p->instance, in4)) || (rc = put(st.lvl, level.data(), in4)))
+        return rc;
+    if (n > 0)
+        k_pack<<<grid_for(n, 256), 256, 0, h->stream>>>(d, st, p->angular_velocity != nullptr,
+                                                        p->orientation != nullptr, p->inv_inertia != nullptr,
+                                                        p->instance != nullptr);
+    CU(cudaGetLastError());
     CU(cudaMemcpyAsync(h->d_inst, h->inst.data(), h->inst.size() * sizeof(InstanceDev), cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(h->d_species, h->species.data(), h->species.size() * sizeof(dem_species_pair),
                        cudaMemcpyHostToDevice, h->stream));
@@ -802,36 +835,21 @@ int dem_download_particles(dem_handle* hh, dem_particles_soa* p)
     int rc = read_control(h, &c);
     if (rc) return rc;
     const int n = h->d.n, b = c.cur;
-    std::vector<double4> pr(n), vm(n), wi(n), qo(n);
-    std::vector<int4> info(n);
-    std::vector<int> caller(n);
-    CU(cudaMemcpyAsync(pr.data(), h->d.pr[b], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaMemcpyAsync(vm.data(), h->d.vm[b], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaMemcpyAsync(wi.data(), h->d.wi[b], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaMemcpyAsync(qo.data(), h->d.qo[b], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaMemcpyAsync(info.data(), h->d.info[b], n * sizeof(int4), cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaMemcpyAsync(caller.data(), h->d.caller[b], n * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    const StagePtrs st = stage_ptrs(h->d_stage, (size_t)h->d.ncap);
+    if (n > 0) k_unpack<<<grid_for(n, 256), 256, 0, h->stream>>>(h->d, b, st);
+    CU(cudaGetLastError());
+    auto get = [&](void* dst, const void* src, size_t bytes) -> int {
+        if (dst && bytes) CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+        return DEM_OK;
+    };
+    const size_t dn = (size_t)n * sizeof(double), in4 = (size_t)n * sizeof(int);
+    if ((rc = get(p->position, st.pos, 3 * dn)) || (rc = get(p->velocity, st.vel, 3 * dn)) ||
+        (rc = get(p->angular_velocity, st.ang, 3 * dn)) || (rc = get(p->orientation, st.ori, 4 * dn)) ||
+        (rc = get(p->radius, st.rad, dn)) || (rc = get(p->inv_mass, st.im, dn)) ||
+        (rc = get(p->inv_inertia, st.ii, dn)) || (rc = get(p->species, st.sp, in4)) || (rc = get(p->id, st.id, in4)) ||
+        (rc = get(p->instance, st.inst, in4)))
+        return rc;
     CU(cudaStreamSynchronize(h->stream));
-    for (int s = 0; s < n; ++s) {
-        const int i = caller[s];
-        if (p->position) { p->position[3 * i] = pr[s].x; p->position[3 * i + 1] = pr[s].y; p->position[3 * i + 2] = pr[s].z; }
-        if (p->velocity) { p->velocity[3 * i] = vm[s].x; p->velocity[3 * i + 1] = vm[s].y; p->velocity[3 * i + 2] = vm[s].z; }
-        if (p->angular_velocity) {
-            p->angular_velocity[3 * i] = wi[s].x;
-            p->angular_velocity[3 * i + 1] = wi[s].y;
-            p->angular_velocity[3 * i + 2] = wi[s].z;
-        }
-        if (p->orientation) {
-            p->orientation[4 * i] = qo[s].x; p->orientation[4 * i + 1] = qo[s].y;
-            p->orientation[4 * i + 2] = qo[s].z; p->orientation[4 * i + 3] = qo[s].w;
-        }
-        if (p->radius) p->radius[i] = pr[s].w;
-        if (p->inv_mass) p->inv_mass[i] = vm[s].w;
-        if (p->inv_inertia) p->inv_inertia[i] = wi[s].w;
-        if (p->species) p->species[i] = info[s].y;
-        if (p->id) p->id[i] = info[s].x;
-        if (p->instance) p->instance[i] = info[s].z;
-    }
     return DEM_OK;
 }
 

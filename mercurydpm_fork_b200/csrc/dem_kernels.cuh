@@ -1119,4 +1119,71 @@ __global__ void __launch_bounds__(256) k_reduce_records(DevPtrs d, int instance,
     }
 }
 
+// ---------------------------------------------------------------------------
+// host <-> device particle exchange through a device staging area holding the
+// caller's structure-of-arrays layout (dem_particles_soa), so that uploads and
+// downloads are plain contiguous copies and the (un)permutation runs here
+// ---------------------------------------------------------------------------
+struct StagePtrs {
+    double *pos, *vel, *ang, *ori, *rad, *im, *ii;
+    int *sp, *id, *inst, *lvl;
+};
+
+// 18 words of 8 bytes per particle slot
+__host__ __device__ inline StagePtrs stage_ptrs(double* base, size_t nc)
+{
+    StagePtrs s;
+    s.pos = base;
+    s.vel = base + 3 * nc;
+    s.ang = base + 6 * nc;
+    s.ori = base + 9 * nc;
+    s.rad = base + 13 * nc;
+    s.im = base + 14 * nc;
+    s.ii = base + 15 * nc;
+    int* ib = reinterpret_cast<int*>(base + 16 * nc);
+    s.sp = ib;
+    s.id = ib + nc;
+    s.inst = ib + 2 * nc;
+    s.lvl = ib + 3 * nc;
+    return s;
+}
+
+// caller order -> state buffer 0 (identity permutation until the first rebuild)
+__global__ void __launch_bounds__(256) k_pack(DevPtrs d, StagePtrs s, int has_ang, int has_ori, int has_ii,
+                                              int has_inst)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const double im = s.im[i];
+    d.pr[0][i] = make_double4(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], s.rad[i]);
+    d.vm[0][i] = make_double4(s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2], im);
+    d.wi[0][i] = make_double4(has_ang ? s.ang[3 * i] : 0.0, has_ang ? s.ang[3 * i + 1] : 0.0,
+                              has_ang ? s.ang[3 * i + 2] : 0.0, has_ii ? s.ii[i] : 0.0);
+    d.qo[0][i] = has_ori ? make_double4(s.ori[4 * i], s.ori[4 * i + 1], s.ori[4 * i + 2], s.ori[4 * i + 3])
+                         : make_double4(1.0, 0.0, 0.0, 0.0);
+    const int flags = (im == 0.0 ? FLAG_FIXED : 0) | (s.lvl[i] << LEVEL_SHIFT);
+    d.info[0][i] = make_int4(s.id[i], s.sp[i], has_inst ? s.inst[i] : 0, flags);
+    d.caller[0][i] = i;
+}
+
+// state buffer b (engine order) -> caller order
+__global__ void __launch_bounds__(256) k_unpack(DevPtrs d, int b, StagePtrs s)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.n) return;
+    const int i = d.caller[b][k];
+    const double4 p = d.pr[b][k], v = d.vm[b][k], w = d.wi[b][k], q = d.qo[b][k];
+    const int4 f = d.info[b][k];
+    s.pos[3 * i] = p.x; s.pos[3 * i + 1] = p.y; s.pos[3 * i + 2] = p.z;
+    s.vel[3 * i] = v.x; s.vel[3 * i + 1] = v.y; s.vel[3 * i + 2] = v.z;
+    s.ang[3 * i] = w.x; s.ang[3 * i + 1] = w.y; s.ang[3 * i + 2] = w.z;
+    s.ori[4 * i] = q.x; s.ori[4 * i + 1] = q.y; s.ori[4 * i + 2] = q.z; s.ori[4 * i + 3] = q.w;
+    s.rad[i] = p.w;
+    s.im[i] = v.w;
+    s.ii[i] = w.w;
+    s.sp[i] = f.y;
+    s.id[i] = f.x;
+    s.inst[i] = f.z;
+}
+
 } // namespace dem

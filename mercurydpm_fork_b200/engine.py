@@ -221,14 +221,26 @@ class DemEngine:
     def step(self, n: int = 1):
         self._check(lib().dem_step(self._h, int(n)))
 
-    def download(self) -> dict:
+    def download(self, out: dict | None = None) -> dict:
+        """Particle state in the caller's order. `out` may supply some of the
+        arrays (e.g. in pinned memory); only the fields it names are read then."""
         n = self.n
-        out = dict(position=np.zeros((n, 3)), velocity=np.zeros((n, 3)), angular_velocity=np.zeros((n, 3)),
-                   orientation=np.zeros((n, 4)), radius=np.zeros(n), inv_mass=np.zeros(n), inv_inertia=np.zeros(n),
-                   species=np.zeros(n, np.int32), id=np.zeros(n, np.int32), instance=np.zeros(n, np.int32))
-        p = _abi.ParticlesSoA(n, _dp(out["position"]), _dp(out["velocity"]), _dp(out["angular_velocity"]),
-                              _dp(out["orientation"]), _dp(out["radius"]), _dp(out["inv_mass"]),
-                              _dp(out["inv_inertia"]), _ip(out["species"]), _ip(out["id"]), _ip(out["instance"]))
+        if out is None:
+            out = dict(position=np.zeros((n, 3)), velocity=np.zeros((n, 3)), angular_velocity=np.zeros((n, 3)),
+                       orientation=np.zeros((n, 4)), radius=np.zeros(n), inv_mass=np.zeros(n),
+                       inv_inertia=np.zeros(n), species=np.zeros(n, np.int32), id=np.zeros(n, np.int32),
+                       instance=np.zeros(n, np.int32))
+        shapes = dict(position=((n, 3), np.float64), velocity=((n, 3), np.float64),
+                      angular_velocity=((n, 3), np.float64), orientation=((n, 4), np.float64),
+                      radius=((n,), np.float64), inv_mass=((n,), np.float64), inv_inertia=((n,), np.float64),
+                      species=((n,), np.int32), id=((n,), np.int32), instance=((n,), np.int32))
+        for k, a in out.items():
+            if k not in shapes or a.shape != shapes[k][0] or a.dtype != shapes[k][1] or not a.flags.c_contiguous:
+                raise ValueError(f"download: bad output array {k}")
+        g = out.get
+        p = _abi.ParticlesSoA(n, _dp(g("position")), _dp(g("velocity")), _dp(g("angular_velocity")),
+                              _dp(g("orientation")), _dp(g("radius")), _dp(g("inv_mass")), _dp(g("inv_inertia")),
+                              _ip(g("species")), _ip(g("id")), _ip(g("instance")))
         self._check(lib().dem_download_particles(self._h, C.byref(p)))
         return out
 

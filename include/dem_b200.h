@@ -60,6 +60,7 @@ extern "C" {
 #define DEM_MAX_LEVELS      4
 #define DEM_MAX_WALL_FACES  8
 #define DEM_MAX_WALLS_PER_INSTANCE 32
+#define DEM_MAX_DELETION_PER_INSTANCE 2
 
 /* Parameters of one (mixed) species pair, as held by the reference's
  * Species<Normal,Friction,Adhesive> objects and the mixed-species triangle
@@ -192,6 +193,19 @@ typedef struct dem_globals {
     int64_t n_steps;
 } dem_globals;
 
+/* A DeletionBoundary (Kernel/Boundaries/DeletionBoundary.cc:109-126): a
+ * particle of the instance whose position x has distance - x . normal < 0
+ * after a drift is removed from the simulation. Removed particles keep their
+ * slot: they stop interacting and moving, are left out of every balance and
+ * coarse-graining sum, and dem_download_particles reports them with
+ * instance -1 (position and velocity are then meaningless). */
+typedef struct dem_deletion_boundary {
+    int32_t instance;
+    int32_t reserved;
+    double  normal[3];
+    double  distance;
+} dem_deletion_boundary;
+
 /* Gaussian coarse-graining grid (CG<XZ|XYZ|O, Gauss, StandardFields>,
  * Kernel/CG/CG.hcc:233-528, Kernel/CG/Fields/StandardFields.cc:184-250).
  * The fields of StandardFields per grid point, in this order (29 doubles):
@@ -229,6 +243,9 @@ int  dem_create(const dem_config *config, const dem_instance_desc *instances,
 int  dem_set_species(dem_handle *h, const dem_species_pair *table, int n_entries);
 /* WallHandler contents (before dem_upload_particles). */
 int  dem_set_walls(dem_handle *h, const dem_wall *walls, int n);
+/* DeletionBoundary objects of BoundaryHandler, at most
+ * DEM_MAX_DELETION_PER_INSTANCE per instance (before dem_upload_particles). */
+int  dem_set_deletion_boundaries(dem_handle *h, const dem_deletion_boundary *b, int n);
 /* ParticleHandler contents; triggers the first force evaluation on the next
  * dem_step (the one DPMBase::initialiseSolve performs, DPMBase.cc:4180). */
 int  dem_upload_particles(dem_handle *h, const dem_particles_soa *p);
@@ -252,6 +269,12 @@ int  dem_download_walls(dem_handle *h, dem_wall *walls, int n);
 int  dem_download_contacts(dem_handle *h, dem_contacts_soa *c, int64_t capacity,
                            int64_t *count);
 int  dem_reduce(dem_handle *h, int instance, dem_globals *out);
+/* dem_reduce for the instances first .. first+count-1 of a batch in one pass
+ * (the per-instance kinetic-energy traces and centres of mass of a batch of
+ * calibration runs). Particle sums run in a fixed order; the elastic energy
+ * and contact counts are accumulated with atomics, so their last bits may
+ * vary between runs. */
+int  dem_reduce_batch(dem_handle *h, int first, int count, dem_globals *out);
 /* The balances of dem_reduce, computed without allocating any device memory.
  * It has no counterpart in the reference. It is for callers that may not
  * allocate GPU memory at the point where they need the balances, e.g. a

@@ -36,6 +36,7 @@ DEM_WALL_AXISYMMETRIC = 1
 DEM_WALL_INTERSECTION = 2
 DEM_MAX_LEVELS = 4
 DEM_MAX_WALL_FACES = 8
+DEM_MAX_DELETION_PER_INSTANCE = 2
 
 DEM_CG_NFIELDS = 29
 DEM_CG_O = 0
@@ -84,6 +85,10 @@ class ContactsSoA(C.Structure):
     ]
 
 
+class DeletionBoundary(C.Structure):
+    _fields_ = [("instance", _i32), ("reserved", _i32), ("normal", _d * 3), ("distance", _d)]
+
+
 class InstanceDesc(C.Structure):
     _fields_ = [
         ("domain_min", _d * 3), ("domain_max", _d * 3), ("gravity", _d * 3), ("periodic_mask", _u32),
@@ -126,6 +131,8 @@ _SIGNATURES = {
     "dem_download_walls": (C.c_int, [C.c_void_p, C.POINTER(Wall), C.c_int]),
     "dem_download_contacts": (C.c_int, [C.c_void_p, C.POINTER(ContactsSoA), _i64, C.POINTER(_i64)]),
     "dem_reduce": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Globals)]),
+    "dem_reduce_batch": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(Globals)]),
+    "dem_set_deletion_boundaries": (C.c_int, [C.c_void_p, C.POINTER(DeletionBoundary), C.c_int]),
     "dem_reduce_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Globals)]),
     "dem_cg_eval": (C.c_int, [C.c_void_p, C.POINTER(CGGrid), _pd]),
     "dem_last_step_stats": (C.c_int, [C.c_void_p, _pd, C.POINTER(_i64), C.POINTER(_i64)]),

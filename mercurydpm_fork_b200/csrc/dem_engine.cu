@@ -31,6 +31,7 @@ struct Handle {
     std::vector<WallGeom> wgeom;       // per wall, for intersection walls
     std::vector<int> wall_caller;      // grouped index -> caller index
     std::vector<int> wall_grouped;     // caller index -> grouped index
+    std::vector<dem_deletion_boundary> deletions;
     std::string err;
     int device = 0;
     cudaStream_t stream = nullptr, stream2 = nullptr;
@@ -43,6 +44,7 @@ struct Handle {
     dem_wall* d_walls = nullptr;
     WallGeom* d_wgeom = nullptr;
     double* d_stage = nullptr;         // caller-layout particle staging (18 words per slot)
+    double* d_batch = nullptr;         // per-instance balance rows of dem_reduce_batch
     std::vector<long long> layout;     // sizes the device arrays were allocated for
     Control* d_ctl = nullptr;
     ContactRecord* d_records = nullptr;
@@ -104,6 +106,7 @@ void free_particle_arrays(Handle* h)
     h->d_records = nullptr;
     h->record_capacity = 0;
     h->d_stage = nullptr;
+    h->d_batch = nullptr;
     h->layout.clear();
 }
 
@@ -396,6 +399,27 @@ int dem_set_walls(dem_handle* hh, const dem_wall* walls, int n)
     return DEM_OK;
 }
 
+int dem_set_deletion_boundaries(dem_handle* hh, const dem_deletion_boundary* b, int n)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || n < 0 || (n > 0 && !b)) return fail(h, DEM_ERR_BAD_INPUT, "dem_set_deletion_boundaries: bad arguments");
+    if (h->uploaded) return fail(h, DEM_ERR_STATE, "dem_set_deletion_boundaries must come before dem_upload_particles");
+    std::vector<int> per(h->inst_desc.size(), 0);
+    for (int k = 0; k < n; ++k) {
+        if (b[k].instance < 0 || b[k].instance >= (int)h->inst_desc.size())
+            return fail(h, DEM_ERR_BAD_INPUT, "deletion boundary instance out of range");
+        if (++per[b[k].instance] > DEM_MAX_DELETION_PER_INSTANCE)
+            return fail(h, DEM_ERR_BAD_INPUT, "too many deletion boundaries in one instance");
+        bool finite = std::isfinite(b[k].distance);
+        for (int a = 0; a < 3; ++a) finite = finite && std::isfinite(b[k].normal[a]);
+        const double l2 = b[k].normal[0] * b[k].normal[0] + b[k].normal[1] * b[k].normal[1] +
+                          b[k].normal[2] * b[k].normal[2];
+        if (!finite || !(l2 > 0.0)) return fail(h, DEM_ERR_BAD_INPUT, "bad deletion boundary");
+    }
+    h->deletions.assign(b, b + n);
+    return DEM_OK;
+}
+
 int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
 {
     Handle* h = reinterpret_cast<Handle*>(hh);
@@ -467,6 +491,15 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         I.n_species = D.n_species;
         I.wall_begin = wbegin[in];
         I.wall_end = wend[in];
+        I.n_del = 0;
+        for (const auto& db : h->deletions)
+            if (db.instance == in) { // DeletionBoundary::set normalises (DeletionBoundary.cc:86-91)
+                const double sf = 1. / std::sqrt(db.normal[0] * db.normal[0] + db.normal[1] * db.normal[1] +
+                                                 db.normal[2] * db.normal[2]);
+                for (int a = 0; a < 3; ++a) I.del_n[I.n_del][a] = db.normal[a] * sf;
+                I.del_d[I.n_del] = db.distance * sf;
+                ++I.n_del;
+            }
         std::vector<int> lv;
         setup_instance_grid(D, radii[in], skin, dmax, I, lv, cell_base);
         for (size_t k = 0; k < members[in].size(); ++k) level[members[in][k]] = lv[k];
@@ -479,7 +512,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
                     return fail(h, DEM_ERR_BAD_INPUT, "periodic box too small for the particle size");
             }
     }
-    const long long ncells = cell_base;
+    const long long ncells = cell_base + 1; // + the graveyard of deleted particles
     // ---- neighbour capacity
     int cap = h->cfg.max_neighbors;
     if (cap <= 0) {
@@ -512,6 +545,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     d.ncells = (int)ncells;
     d.rotation = h->cfg.rotation;
     d.single_instance = ninst == 1;
+    d.n_instances = ninst;
     d.n_species_table = (int)h->species.size();
     d.zero_idist = 1;
     for (const auto& sp : h->species) d.zero_idist = d.zero_idist && sp.interaction_distance == 0.0;
@@ -537,6 +571,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         d.cell_count = kept.cell_count; d.cell_start = kept.cell_start; d.cell_cursor = kept.cell_cursor;
         d.block_sums = kept.block_sums; d.inst = kept.inst; d.species = kept.species; d.walls = kept.walls;
         d.wgeom = kept.wgeom; d.n_walls = kept.n_walls; d.ctl = kept.ctl; d.records = kept.records;
+        d.n_instances = kept.n_instances;
         for (int b = 0; b < 2; ++b) { // no history carries over from the previous simulation
             CU(cudaMemsetAsync(d.cnt[b], 0, NC * sizeof(int), h->stream));
             CU(cudaMemsetAsync(d.act[b], 0, (size_t)d.nwords * NC * sizeof(unsigned), h->stream));
@@ -581,6 +616,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     d.n_walls = (int)h->walls.size();
     d.ctl = h->d_ctl;
     d.records = h->d_records;
+    if ((rc = dalloc(h, &h->d_batch, h->inst.size() * (RED_SLOTS + 3)))) return rc;
     h->layout = layout;
     }
 
@@ -975,6 +1011,45 @@ int dem_reduce(dem_handle* hh, int instance, dem_globals* out)
     out->n_wall_contacts = (int64_t)llround(racc[2]);
     out->time = h->steps_total * h->cfg.time_step;
     out->n_steps = h->steps_total;
+    return DEM_OK;
+}
+
+int dem_reduce_batch(dem_handle* hh, int first, int count, dem_globals* out)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !out || count < 0) return DEM_ERR_BAD_INPUT;
+    if (!h->uploaded) return fail(h, DEM_ERR_STATE, "nothing uploaded");
+    if (h->initial_pending) return fail(h, DEM_ERR_STATE, "no force evaluation yet (call dem_step)");
+    if (first < 0 || first + count > (int)h->inst.size()) return fail(h, DEM_ERR_BAD_INPUT, "instance range out of range");
+    if (count == 0) return DEM_OK;
+    CU(cudaSetDevice(h->device));
+    const unsigned nr = h->records_valid ? h->n_records : 0;
+    const size_t row = RED_SLOTS + 3;
+    k_reduce_instances<<<count, 256, 0, h->stream>>>(h->d, first, h->d_batch);
+    if (nr) k_reduce_records_instances<<<grid_for(nr, 256), 256, 0, h->stream>>>(h->d, first, count, nr, h->d_batch);
+    CU(cudaGetLastError());
+    std::vector<double> r((size_t)count * row);
+    CU(cudaMemcpyAsync(r.data(), h->d_batch, r.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < count; ++k) {
+        const double* a = r.data() + (size_t)k * row;
+        dem_globals& g = out[k];
+        std::memset(&g, 0, sizeof(g));
+        g.kinetic_energy = a[0];
+        g.rotational_energy = a[1];
+        g.gravitational_energy = a[2];
+        g.mass = a[3];
+        for (int q = 0; q < 3; ++q) {
+            g.momentum[q] = a[4 + q];
+            g.centre_of_mass[q] = a[3] > 0 ? a[7 + q] / a[3] : 0.0;
+            g.angular_momentum[q] = a[10 + q];
+        }
+        g.elastic_energy = a[RED_SLOTS];
+        g.n_contacts = (int64_t)llround(a[RED_SLOTS + 1]);
+        g.n_wall_contacts = (int64_t)llround(a[RED_SLOTS + 2]);
+        g.time = h->steps_total * h->cfg.time_step;
+        g.n_steps = h->steps_total;
+    }
     return DEM_OK;
 }
 

@@ -31,6 +31,10 @@
 namespace dem {
 
 constexpr int FLAG_FIXED = 1;
+// deleted by a DeletionBoundary: also FLAG_FIXED, parked at DELETED_COORD,
+// sorted into the graveyard cell (the last cell) at the next rebuild
+constexpr int FLAG_DELETED = 2;
+constexpr double DELETED_COORD = 1e300;
 constexpr int LEVEL_SHIFT = 8;
 
 struct InstanceDev {
@@ -51,6 +55,10 @@ struct InstanceDev {
     double inv_cell[DEM_MAX_LEVELS][3];
     double level_rmax[DEM_MAX_LEVELS];
     double max_interaction_distance;
+    // DeletionBoundary planes: a particle is deleted when del_d - x . del_n < 0
+    int n_del;
+    double del_n[DEM_MAX_DELETION_PER_INSTANCE][3];
+    double del_d[DEM_MAX_DELETION_PER_INSTANCE];
 };
 
 // Contact record written at the last force evaluation of a dem_step call:
@@ -123,6 +131,7 @@ struct DevPtrs {
     dem_wall *walls;         // moved by k_control every step
     const WallGeom *wgeom;   // per wall; faces, edges and corners of intersection walls
     int n_walls;
+    int n_instances;
     Control *ctl;
     ContactRecord *records;
     // sizes

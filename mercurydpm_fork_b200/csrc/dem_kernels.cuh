@@ -95,6 +95,11 @@ __global__ void k_keys(DevPtrs d)
     const int c = d.ctl->cur;
     const double4 p = d.pr[c][i];
     const int4 inf = d.info[c][i];
+    if (inf.w & FLAG_DELETED) { // the graveyard: the last cell, never searched
+        d.key[i] = d.ncells - 1;
+        atomicAdd(&d.cell_count[d.ncells - 1], 1);
+        return;
+    }
     const InstanceDev& I = d.inst[inf.z];
     const int lvl = (inf.w >> LEVEL_SHIFT) & 0xff;
     const int cx = cell_coord(p.x, I.origin[0], I.inv_cell[lvl][0], I.dims[lvl][0]);
@@ -188,7 +193,7 @@ __global__ void k_cell_sort(DevPtrs d)
     const int c = d.ctl->cur;
     d.cell_count[cell] = 0;
     d.cell_cursor[cell] = 0;
-    if (e - b < 2) return;
+    if (e - b < 2 || cell == d.ncells - 1) return; // the graveyard is not ordered
     if (e - b > 512) { // pathological pile-up (e.g. particles far outside the grid)
         atomicOr(&d.ctl->status, 1u << DEM_ERR_DOMAIN);
         return;
@@ -290,6 +295,12 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
     const InstanceDev& I = d.inst[is.z];
     const V3 xs = xyz(ps);
     const bool fixed_s = (is.w & FLAG_FIXED) != 0;
+    if (is.w & FLAG_DELETED) {
+        d.cnt[ln][s] = 0;
+        for (int w = 0; w < d.nwords; ++w) d.act[nb][(size_t)w * d.ncap + s] = 0u;
+        d.wact[nb][s] = 0u;
+        return;
+    }
     const double extra = I.max_interaction_distance + d.ctl->skin;
     int count = 0;
     bool overflow = false;
@@ -459,6 +470,26 @@ __device__ __forceinline__ double spring_energy(const dem_species_pair& sp, cons
         return e;
     }
     return 0.0;
+}
+
+// DeletionBoundary::checkBoundaryAfterParticleMoved (DeletionBoundary.cc:109-126)
+// after a drift: a deleted particle is parked far away as a fixed particle
+// (no contact predicate can succeed against it) and a rebuild moves it to the
+// graveyard cell.
+__device__ __forceinline__ bool deletion_check(const InstanceDev& I, V3 x)
+{
+    for (int k = 0; k < I.n_del; ++k)
+        if (I.del_d[k] - (x.x * I.del_n[k][0] + x.y * I.del_n[k][1] + x.z * I.del_n[k][2]) < 0) return true;
+    return false;
+}
+
+__device__ __forceinline__ void park_deleted(Control* ctl, double4& p, double4& v, double4& w, int4& info)
+{
+    p = make_double4(DELETED_COORD, DELETED_COORD, DELETED_COORD, p.w);
+    v = make_double4(0.0, 0.0, 0.0, 0.0);
+    w = make_double4(0.0, 0.0, 0.0, 0.0);
+    info.w |= FLAG_DELETED | FLAG_FIXED;
+    ctl->force_rebuild = 1;
 }
 
 constexpr int FORCE_BLOCK = 128;  // threads (particles) per block, 4 warps
@@ -953,11 +984,16 @@ __global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
             wn = make_double4(w.x, w.y, w.z, ws.w);
             qs = make_double4(q.q0, q.q1, q.q2, q.q3);
         }
+        int4 isn = is;
+        if (MODE == 1 && !final_step && I.n_del && !(is.w & FLAG_DELETED) && deletion_check(I, xyz(pn))) {
+            park_deleted(ctl, pn, vn, wn, isn);
+            disp2 = 0.0;
+        }
         d.pr[nb][s] = pn;
         d.vm[nb][s] = vn;
         d.wi[nb][s] = wn;
         d.qo[nb][s] = qs;
-        d.info[nb][s] = is;
+        d.info[nb][s] = isn;
         d.caller[nb][s] = d.caller[c][s];
     }
     // maximum displacement of this step (for the skin test)
@@ -1021,9 +1057,18 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevPtrs d)
                 }
             }
         }
-        d.pr[c][s] = make_double4(x.x, x.y, x.z, ps.w);
-        d.vm[c][s] = make_double4(v.x, v.y, v.z, vs.w);
-        d.wi[c][s] = make_double4(w.x, w.y, w.z, ws.w);
+        double4 pn = make_double4(x.x, x.y, x.z, ps.w);
+        double4 vn = make_double4(v.x, v.y, v.z, vs.w);
+        double4 wn = make_double4(w.x, w.y, w.z, ws.w);
+        if (I.n_del && !(is.w & FLAG_DELETED) && deletion_check(I, x)) {
+            int4 isn = is;
+            park_deleted(ctl, pn, vn, wn, isn);
+            d.info[c][s] = isn;
+            disp2 = 0.0;
+        }
+        d.pr[c][s] = pn;
+        d.vm[c][s] = vn;
+        d.wi[c][s] = wn;
         d.qo[c][s] = make_double4(q.q0, q.q1, q.q2, q.q3);
     }
 #pragma unroll
@@ -1183,7 +1228,74 @@ __global__ void __launch_bounds__(256) k_unpack(DevPtrs d, int b, StagePtrs s)
     s.ii[i] = w.w;
     s.sp[i] = f.y;
     s.id[i] = f.x;
-    s.inst[i] = f.z;
+    s.inst[i] = (f.w & FLAG_DELETED) ? -1 : f.z;
+}
+
+// ---------------------------------------------------------------------------
+// balances of many instances at once: instances are contiguous in the sorted
+// order, so block k sums instance first+k over its slot range (from the cell
+// table of the last rebuild) in a fixed order; contact records add their
+// elastic energy and counts with atomics
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_reduce_instances(DevPtrs d, int first, double* out)
+{
+    __shared__ double sh[RED_SLOTS][8];
+    const int k = first + blockIdx.x;
+    const int c = d.ctl->cur;
+    const int cb = d.inst[k].cell_base[0];
+    const int ce = (k + 1 < d.n_instances) ? d.inst[k + 1].cell_base[0] : d.ncells - 1;
+    const int b = d.cell_start[cb], e = d.cell_start[ce];
+    double v[RED_SLOTS];
+#pragma unroll
+    for (int q = 0; q < RED_SLOTS; ++q) v[q] = 0.0;
+    const InstanceDev& I = d.inst[k];
+    for (int s = b + threadIdx.x; s < e; s += blockDim.x) {
+        const int4 is = d.info[c][s];
+        if (is.w & FLAG_FIXED) continue;
+        const double4 p = d.pr[c][s];
+        const double4 vm = d.vm[c][s];
+        const double4 w = d.wi[c][s];
+        const double m = 1.0 / vm.w;
+        const V3 vel = xyz(vm), om = xyz(w), x = xyz(p);
+        const double inertia = 1.0 / w.w;
+        const V3 g = v3(-I.gravity[0], -I.gravity[1], -I.gravity[2]);
+        v[0] += .5 * m * len2(vel);
+        v[1] += .5 * dot(om, om * inertia);
+        v[2] += m * dot(g, x);
+        v[3] += m;
+        v[4] += m * vel.x; v[5] += m * vel.y; v[6] += m * vel.z;
+        v[7] += m * x.x; v[8] += m * x.y; v[9] += m * x.z;
+        v[10] += inertia * om.x; v[11] += inertia * om.y; v[12] += inertia * om.z;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < RED_SLOTS; ++q) {
+        double x = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[q][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < RED_SLOTS) {
+        double x = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += sh[threadIdx.x][w];
+        out[(size_t)blockIdx.x * (RED_SLOTS + 3) + threadIdx.x] = x;
+    }
+    if (threadIdx.x >= RED_SLOTS && threadIdx.x < RED_SLOTS + 3)
+        out[(size_t)blockIdx.x * (RED_SLOTS + 3) + threadIdx.x] = 0.0;
+}
+
+__global__ void __launch_bounds__(256) k_reduce_records_instances(DevPtrs d, int first, int count,
+                                                                  unsigned n_records, double* out)
+{
+    const unsigned r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_records) return;
+    const ContactRecord& rec = d.records[r];
+    const int k = d.info[d.ctl->cur][rec.slot_p].z - first;
+    if (k < 0 || k >= count) return;
+    double* o = out + (size_t)k * (RED_SLOTS + 3) + RED_SLOTS;
+    atomicAdd(o, rec.elastic_energy);
+    atomicAdd(o + (rec.is_wall ? 2 : 1), 1.0);
 }
 
 } // namespace dem

@@ -82,6 +82,16 @@ class Instance:
         return d
 
 
+def deletion_boundary(normal, distance, instance=0) -> _abi.DeletionBoundary:
+    """DeletionBoundary::set(normal, distance): particles with
+    distance - x . normal < 0 are removed."""
+    b = _abi.DeletionBoundary()
+    b.instance = instance
+    b.normal[:] = list(map(float, normal))
+    b.distance = float(distance)
+    return b
+
+
 def species_pair(**kw) -> _abi.SpeciesPair:
     s = _abi.SpeciesPair()
     for k, v in kw.items():
@@ -145,7 +155,8 @@ def axisymmetric_wall(axis, faces, position=(0, 0, 0), species=0, instance=0, ve
 class DemEngine:
     def __init__(self, time_step: float, instances: list[Instance], species: list[_abi.SpeciesPair],
                  walls: list[_abi.Wall] | None = None, rotation: bool = True, background_drag: float = 0.0,
-                 max_neighbors: int = 0, skin: float = 0.0, use_graphs: bool = True, device: int = 0):
+                 max_neighbors: int = 0, skin: float = 0.0, use_graphs: bool = True, device: int = 0,
+                 deletions: list | None = None):
         self._h = C.c_void_p()
         cfg = _abi.Config()
         cfg.time_step = time_step
@@ -167,6 +178,9 @@ class DemEngine:
         wa = (_abi.Wall * max(1, len(walls)))(*walls)
         self._check(lib().dem_set_walls(self._h, wa, len(walls)))
         self._nwalls = len(walls)
+        dels = deletions or []
+        da = (_abi.DeletionBoundary * max(1, len(dels)))(*dels)
+        self._check(lib().dem_set_deletion_boundaries(self._h, da, len(dels)))
         self.n = 0
 
     # ------------------------------------------------------------------
@@ -277,6 +291,23 @@ class DemEngine:
                     momentum=np.array(g.momentum[:]), angular_momentum=np.array(g.angular_momentum[:]),
                     mass=g.mass, centre_of_mass=np.array(g.centre_of_mass[:]), n_contacts=g.n_contacts,
                     n_wall_contacts=g.n_wall_contacts, time=g.time, n_steps=g.n_steps)
+
+    def reduce_batch(self, first: int = 0, count: int | None = None) -> dict:
+        """dem_reduce_batch: the balances of instances first..first+count-1 as
+        arrays with one row per instance."""
+        count = self.n_instances - first if count is None else count
+        arr = (_abi.Globals * max(1, count))()
+        self._check(lib().dem_reduce_batch(self._h, first, count, arr))
+        g = arr[:count]
+        return dict(kinetic_energy=np.array([x.kinetic_energy for x in g]),
+                    rotational_energy=np.array([x.rotational_energy for x in g]),
+                    gravitational_energy=np.array([x.gravitational_energy for x in g]),
+                    elastic_energy=np.array([x.elastic_energy for x in g]),
+                    mass=np.array([x.mass for x in g]),
+                    momentum=np.array([x.momentum[:] for x in g]).reshape(count, 3),
+                    centre_of_mass=np.array([x.centre_of_mass[:] for x in g]).reshape(count, 3),
+                    n_contacts=np.array([x.n_contacts for x in g]),
+                    n_wall_contacts=np.array([x.n_wall_contacts for x in g]))
 
     def cg(self, coordinates: int, n, lo, hi, width: float, cutoff_factor: float = 3.0, instance: int = 0):
         g = _abi.CGGrid()

@@ -375,3 +375,74 @@ def rotating_drum(n: int = 1_000_000, seed: int = 3, ds: float = 1e-3, size_rati
                     info=dict(n=n, n_small=n_small, n_large=n_large, seed=seed, radius_d=radius_d,
                               length_d=length_d, omega=omega, shear_modulus=G,
                               solid_fraction_of_drum=float(np.sum(4 / 3 * PI * radius ** 3) / (PI * R * R * L))))
+
+
+@dataclass
+class Batch:
+    """Several independent simulations in one handle (dem_instance_desc per
+    member): species tables concatenated with per-instance offsets, walls and
+    particles tagged with their instance, particle ids offset so that they are
+    unique across the batch (the order within each member is kept, so every
+    member's lower-id rule is unchanged)."""
+    time_step: float
+    instances: list
+    species: list
+    walls: list
+    position: np.ndarray
+    velocity: np.ndarray
+    radius: np.ndarray
+    inv_mass: np.ndarray
+    inv_inertia: np.ndarray
+    species_index: np.ndarray
+    ids: np.ndarray
+    instance: np.ndarray
+    members: list
+    offsets: np.ndarray
+    deletions: list = field(default_factory=list)
+    rotation: bool = True
+
+    @property
+    def n(self) -> int:
+        return len(self.radius)
+
+    def engine(self, **kw):
+        from .engine import DemEngine
+        e = DemEngine(self.time_step, self.instances, self.species, self.walls, rotation=self.rotation,
+                      deletions=self.deletions, **kw)
+        e.upload(self.position, self.velocity, self.radius, self.inv_mass, self.inv_inertia, self.species_index,
+                 self.ids, instance=self.instance)
+        return e
+
+    def member_slice(self, k: int) -> slice:
+        return slice(int(self.offsets[k]), int(self.offsets[k + 1]))
+
+
+def batch(members: list, time_step: float | None = None, deletions: list | None = None) -> Batch:
+    """Combines Scenarios into one Batch; all members run with one time step
+    (the smallest of theirs unless given). `deletions` holds, per member, a
+    list of (normal, distance) DeletionBoundary planes."""
+    import copy
+    from .engine import Instance, deletion_boundary
+    dt = min(m.time_step for m in members) if time_step is None else time_step
+    instances, species, walls, dels = [], [], [], []
+    id_off = 0
+    offsets = [0]
+    for k, m in enumerate(members):
+        inst = copy.copy(m.instance)
+        inst.species_offset = len(species)
+        instances.append(inst)
+        species.extend(m.species)
+        for w in m.walls:
+            w2 = copy.copy(w)
+            w2.instance = k
+            walls.append(w2)
+        if deletions is not None:
+            for nrm, dist in deletions[k]:
+                dels.append(deletion_boundary(nrm, dist, instance=k))
+        offsets.append(offsets[-1] + m.n)
+    cat = lambda f: np.concatenate([getattr(m, f) for m in members])
+    ids = np.concatenate([m.ids.astype(np.int64) + sum(mm.n for mm in members[:k]) for k, m in enumerate(members)])
+    return Batch(dt, instances, species, walls, cat("position"), cat("velocity"), cat("radius"), cat("inv_mass"),
+                 cat("inv_inertia"), cat("species_index").astype(np.int32), ids.astype(np.int32),
+                 np.concatenate([np.full(m.n, k, np.int32) for k, m in enumerate(members)]), members,
+                 np.array(offsets), dels, rotation=all(m.rotation for m in members))

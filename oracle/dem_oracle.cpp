@@ -44,6 +44,7 @@ struct Particle {
     double r, invm, invI;
     int species, id;
     bool fixed;
+    bool deleted = false;
     V3 F, T;
 };
 
@@ -358,6 +359,7 @@ struct Sim {
         ++evals;
         for (auto& q : p) { q.F = zero3(); q.T = zero3(); }
         const int n = (int)p.size();
+        // removed particles (DeletionBoundary) take no part
         // candidate pairs: uniform grid over the box (exact FP64 predicate decides)
         double rmax = 0.0;
         for (auto& q : p) rmax = std::max(rmax, q.r);
@@ -370,7 +372,8 @@ struct Sim {
             const bool per = (inst.periodic_mask >> k) & 1u;
             lo[k] = per ? inst.periodic_min[k] : inst.domain_min[k];
             hi[k] = per ? inst.periodic_max[k] : inst.domain_max[k];
-            for (auto& q : p) { lo[k] = std::min(lo[k], (&q.x.x)[k]); hi[k] = std::max(hi[k], (&q.x.x)[k]); }
+            for (auto& q : p)
+                if (!q.deleted) { lo[k] = std::min(lo[k], (&q.x.x)[k]); hi[k] = std::max(hi[k], (&q.x.x)[k]); }
             dim[k] = std::max(1, (int)std::floor((hi[k] - lo[k]) / cs));
         }
         auto cell_of = [&](V3 x, int k) {
@@ -379,11 +382,13 @@ struct Sim {
         };
         std::vector<std::vector<int>> cells((size_t)dim[0] * dim[1] * dim[2]);
         for (int i = 0; i < n; ++i) {
+            if (p[i].deleted) continue;
             const V3 x = p[i].x;
             cells[((size_t)cell_of(x, 2) * dim[1] + cell_of(x, 1)) * dim[0] + cell_of(x, 0)].push_back(i);
         }
         std::vector<int> cand;
         for (int i = 0; i < n; ++i) {
+            if (p[i].deleted) continue;
             cand.clear();
             int c[3];
             for (int k = 0; k < 3; ++k) c[k] = cell_of(p[i].x, k);
@@ -507,6 +512,36 @@ struct Sim {
         }
     }
 
+    // DeletionBoundary::checkBoundaryAfterParticleMoved (DeletionBoundary.cc:109-126):
+    // the particle and its interactions leave the simulation
+    std::vector<dem_deletion_boundary> dels;
+    void delete_particles()
+    {
+        for (auto& q : p) {
+            if (q.deleted) continue;
+            bool gone = false;
+            for (const auto& b : dels) {
+                const double sf = 1. / std::sqrt(b.normal[0] * b.normal[0] + b.normal[1] * b.normal[1] +
+                                                 b.normal[2] * b.normal[2]); // DeletionBoundary::set
+                const double nx = b.normal[0] * sf, ny = b.normal[1] * sf, nz = b.normal[2] * sf;
+                if (b.distance * sf - (q.x.x * nx + q.x.y * ny + q.x.z * nz) < 0) gone = true;
+            }
+            if (!gone) continue;
+            q.deleted = true;
+            q.fixed = true;
+            q.invm = 0.0;
+            q.v = zero3();
+            q.w = zero3();
+            for (auto it = inter.begin(); it != inter.end();) {
+                const int kind = std::get<0>(it->first), a = std::get<1>(it->first), b = std::get<2>(it->first);
+                if (a == q.id || (kind != 2 && b == q.id))
+                    it = inter.erase(it);
+                else
+                    ++it;
+            }
+        }
+    }
+
     void erase_old(unsigned current)
     {
         for (auto it = inter.begin(); it != inter.end();) {
@@ -521,6 +556,7 @@ struct Sim {
 } // namespace
 
 static int g_report_handler = 0;
+static std::vector<dem_deletion_boundary> g_deletions;
 
 extern "C" {
 
@@ -529,6 +565,9 @@ extern "C" {
 // after the step (after step 0 this includes interactions of the initial
 // evaluation that step 0 did not touch: both carry time stamp 1).
 void oracle_set_contact_report(int mode) { g_report_handler = mode; }
+
+// DeletionBoundary planes of the next oracle_run (the instance field is ignored).
+void oracle_set_deletion(const dem_deletion_boundary* b, int n) { g_deletions.assign(b, b + n); }
 
 // Runs nsteps reference time steps from the given state (after the initial
 // force evaluation of DPMBase::initialiseSolve) and returns the final state
@@ -543,6 +582,7 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
     S.inst = *inst;
     S.species.assign(species, species + nspecies);
     S.walls.assign(walls, walls + nwalls);
+    S.dels = g_deletions;
     S.wgeo.resize(nwalls);
     for (int w = 0; w < nwalls; ++w)
         if (walls[w].type != DEM_WALL_INFINITE) S.wgeo[w].build(walls[w]);
@@ -600,6 +640,7 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
     for (int step = 0; step < nsteps; ++step) {
         S.integrate_before();
         S.wrap();
+        S.delete_particles();
         S.snapshot_periodic();
         S.compute_forces();
         S.periodic_handover();
@@ -619,6 +660,7 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
                 out->orientation[4 * i] = q.q.q0; out->orientation[4 * i + 1] = q.q.q1;
                 out->orientation[4 * i + 2] = q.q.q2; out->orientation[4 * i + 3] = q.q.q3;
             }
+            if (out->instance) out->instance[i] = q.deleted ? -1 : 0;
         }
     }
     for (int64_t i = 0; i < n; ++i) {

@@ -14,6 +14,7 @@
 #include <sstream>
 #include <vector>
 
+#include "Boundaries/DeletionBoundary.h"
 #include "Boundaries/PeriodicBoundary.h"
 #include "CG/CG.h"
 #include "CG/Coordinates/O.h"
@@ -40,6 +41,8 @@
 #include "../../include/dem_b200.h"
 
 namespace {
+
+std::vector<dem_deletion_boundary> g_deletions; // DeletionBoundary planes of the next run
 
 // MindlinInteraction keeps its sliding spring without a getter; its public
 // write() prints it after the token "slidingSpring" (MindlinInteraction.cc:166-170).
@@ -167,6 +170,11 @@ public:
             b.set(n, inst->periodic_min[k], inst->periodic_max[k]);
             boundaryHandler.copyAndAddObject(b);
         }
+        for (const auto& db : g_deletions) {
+            DeletionBoundary b;
+            b.set(Vec3D(db.normal[0], db.normal[1], db.normal[2]), db.distance);
+            boundaryHandler.copyAndAddObject(b);
+        }
         SphericalParticle p;
         for (int64_t i = 0; i < in->n; ++i) {
             p.setSpecies(speciesHandler.getObject(in->species[i]));
@@ -224,6 +232,13 @@ void setup(RefDriver& d, const dem_config* cfg, const dem_instance_desc* inst, c
 
 extern "C" {
 
+// DeletionBoundary planes for the following runs (instance field ignored).
+void mdpm_ref_set_deletion(const dem_deletion_boundary* b, int n) { g_deletions.assign(b, b + n); }
+
+} // extern "C"
+
+extern "C" {
+
 // Same contract as oracle_run (oracle/dem_oracle.cpp), with the species
 // densities the reference needs to derive the particle masses.
 int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
@@ -236,8 +251,16 @@ int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem
     d.initialiseSolve();
     for (int k = 0; k < nsteps; ++k) d.computeOneTimeStep();
     const int64_t n = in->n;
-    for (int64_t i = 0; i < n; ++i) {
-        const BaseParticle* p = d.particleHandler.getObject((unsigned)i);
+    // deleted particles leave the handler (and reorder it): rows are matched by
+    // id, which the tests set to the caller index; rows of deleted particles
+    // keep instance -1
+    if (out && out->instance)
+        for (int64_t i = 0; i < n; ++i) out->instance[i] = -1;
+    for (int64_t r = 0; r < (int64_t)d.particleHandler.getSize(); ++r) {
+        const BaseParticle* p = d.particleHandler.getObject((unsigned)r);
+        const int64_t i = (int64_t)p->getId();
+        if (i < 0 || i >= n) continue;
+        if (out && out->instance) out->instance[i] = 0;
         const Vec3D x = p->getPosition(), v = p->getVelocity(), w = p->getAngularVelocity();
         const Quaternion q = p->getOrientation();
         if (out && out->position) { out->position[3 * i] = x.X; out->position[3 * i + 1] = x.Y; out->position[3 * i + 2] = x.Z; }

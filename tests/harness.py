@@ -44,6 +44,8 @@ def oracle_lib():
                                    C.POINTER(_abi.ContactsSoA), C.c_int64, C.POINTER(C.c_int64)]
         lib.oracle_set_contact_report.restype = None
         lib.oracle_set_contact_report.argtypes = [C.c_int]
+        lib.oracle_set_deletion.restype = None
+        lib.oracle_set_deletion.argtypes = [C.POINTER(_abi.DeletionBoundary), C.c_int]
         _oracle = lib
     return _oracle
 
@@ -62,6 +64,8 @@ def ref_lib(variant="serial"):
                                               C.POINTER(_abi.ContactsSoA), C.c_int64, C.POINTER(C.c_int64), _pd]
         lib.mdpm_ref_time.restype = C.c_int
         lib.mdpm_ref_time.argtypes = common + [C.c_int, C.c_int, C.c_int, _pd]
+        lib.mdpm_ref_set_deletion.restype = None
+        lib.mdpm_ref_set_deletion.argtypes = [C.POINTER(_abi.DeletionBoundary), C.c_int]
         _ref[variant] = lib
     return _ref[variant]
 
@@ -100,15 +104,24 @@ class _Inputs:
                                                 _ip(self._cid[3]), _dp(self._cid[4]), None, None)
 
 
+def _deletions(planes):
+    """ctypes array of DeletionBoundary from [(normal, distance), ...]."""
+    from mercurydpm_fork_b200.engine import deletion_boundary
+    planes = planes or []
+    arr = (_abi.DeletionBoundary * max(1, len(planes)))(*[deletion_boundary(nn, dd) for nn, dd in planes])
+    return arr, len(planes)
+
+
 def _outputs(n, cap):
     o = dict(position=np.zeros((n, 3)), velocity=np.zeros((n, 3)), angular_velocity=np.zeros((n, 3)),
              orientation=np.zeros((n, 4)), inv_mass=np.zeros(n), inv_inertia=np.zeros(n),
-             force=np.zeros((n, 3)), torque=np.zeros((n, 3)))
+             force=np.zeros((n, 3)), torque=np.zeros((n, 3)), instance=np.zeros(n, np.int32))
     c = dict(id_p=np.zeros(cap, np.int32), id_i=np.zeros(cap, np.int32), is_wall=np.zeros(cap, np.int32),
              periodic=np.zeros(cap, np.int32), springs=np.zeros((cap, 9)), force=np.zeros((cap, 3)),
              overlap=np.zeros(cap))
     soa = _abi.ParticlesSoA(n, _dp(o["position"]), _dp(o["velocity"]), _dp(o["angular_velocity"]),
-                            _dp(o["orientation"]), None, _dp(o["inv_mass"]), _dp(o["inv_inertia"]), None, None, None)
+                            _dp(o["orientation"]), None, _dp(o["inv_mass"]), _dp(o["inv_inertia"]), None, None,
+                            _ip(o["instance"]))
     csoa = _abi.ContactsSoA(cap, _ip(c["id_p"]), _ip(c["id_i"]), _ip(c["is_wall"]), _ip(c["periodic"]),
                             _dp(c["springs"]), _dp(c["force"]), _dp(c["overlap"]))
     return o, c, soa, csoa
@@ -123,10 +136,14 @@ def sort_contacts(c):
     return {k: v[order] for k, v in c.items()}
 
 
-def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated") -> dict:
+def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated", deletions=None) -> dict:
     """report="evaluated": contacts of the last force evaluation (what the
-    engine records); "handler": every interaction the reference still holds."""
+    engine records); "handler": every interaction the reference still holds.
+    deletions: DeletionBoundary planes [(normal, distance), ...]; the output
+    "instance" is -1 for deleted particles."""
     oracle_lib().oracle_set_contact_report(1 if report == "handler" else 0)
+    darr, nd = _deletions(deletions)
+    oracle_lib().oracle_set_deletion(darr, nd)
     inp = _Inputs(sc, contacts)
     cap = 16 * sc.n + 64
     o, c, soa, csoa = _outputs(sc.n, cap)
@@ -140,7 +157,9 @@ def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated") -> dic
     return o
 
 
-def run_reference(sc, nsteps: int, variant: str = "serial") -> dict:
+def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None) -> dict:
+    darr, nd = _deletions(deletions)
+    ref_lib(variant).mdpm_ref_set_deletion(darr, nd)
     inp = _Inputs(sc)
     cap = 16 * sc.n + 64
     o, c, soa, csoa = _outputs(sc.n, cap)
@@ -168,6 +187,8 @@ def cg_grid(coordinates: int, n, lo, hi, width: float, cutoff_factor: float = 3.
 
 def reference_cg(sc, nsteps: int, grid: _abi.CGGrid, variant: str = "serial") -> np.ndarray:
     """The reference's CG<Coordinates, Gauss, StandardFields> after nsteps steps (29 fields per point)."""
+    darr, nd = _deletions(None)
+    ref_lib(variant).mdpm_ref_set_deletion(darr, nd)
     inp = _Inputs(sc)
     npts = 1
     for k, res in enumerate((grid.coordinates != _abi.DEM_CG_O, grid.coordinates == _abi.DEM_CG_XYZ,
@@ -205,6 +226,8 @@ class quiet_stdout:
 
 
 def time_reference(sc, warmup: int, nsteps: int, threads: int, variant: str = "omp") -> float:
+    darr, nd = _deletions(None)
+    ref_lib(variant).mdpm_ref_set_deletion(darr, nd)
     inp = _Inputs(sc)
     sec = C.c_double(0)
     with quiet_stdout():
@@ -215,7 +238,10 @@ def time_reference(sc, warmup: int, nsteps: int, threads: int, variant: str = "o
     return sec.value
 
 
-def run_gpu(sc, nsteps: int, contacts=None, **kw) -> dict:
+def run_gpu(sc, nsteps: int, contacts=None, deletions=None, **kw) -> dict:
+    if deletions:
+        from mercurydpm_fork_b200.engine import deletion_boundary
+        kw["deletions"] = [deletion_boundary(nn, dd) for nn, dd in deletions]
     e = sc.engine(**kw)
     if contacts is not None:
         e.upload_contacts(contacts["id_p"], contacts["id_i"], contacts["springs"], contacts.get("is_wall"),

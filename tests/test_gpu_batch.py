@@ -1,0 +1,118 @@
+"""Batched instances (one handle, many independent simulations) and
+DeletionBoundary, through the C ABI against the CPU oracle run on each member
+alone.
+
+Tolerances as in test_gpu_parity: pair sets bit-exact, per-contact forces
+bit-exact at the initial evaluation; positions 1e-13 of a diameter and forces
+1e-9 relative over short horizons; balances from dem_reduce_batch equal to
+dem_reduce's to 1e-12 relative (same sums, different order for the records).
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import cases
+import harness as H
+from mercurydpm_fork_b200 import scenarios
+
+pytestmark = pytest.mark.gpu
+
+
+def _members():
+    return [cases.compressed_box(n=300), cases.small_drum(n=400), cases.wall_probe("heap_base", omega=(0.5, 1, 3)),
+            cases.small_chute(n_flow=600)]
+
+
+def _falling_probe():
+    sc = cases.wall_probe("heap_base")
+    rr = np.hypot(sc.position[:, 0], sc.position[:, 1])
+    sc.velocity[rr > 6e-3, 2] = -1.0
+    return sc, [((0, 0, -1), 0.9e-3)]  # delete below z = -0.9 mm
+
+
+def _member_contacts(b, g, k):
+    """The batch's contacts of member k in the member's own numbering."""
+    c = g["contacts"]
+    lo, hi = b.offsets[k], b.offsets[k + 1]
+    wall_off = sum(len(m.walls) for m in b.members[:k])
+    sel = (c["id_p"] >= lo) & (c["id_p"] < hi)
+    out = {key: v[sel].copy() for key, v in c.items()}
+    out["id_p"] -= lo
+    w = out["is_wall"] != 0
+    out["id_i"] = np.where(w, out["id_i"] - wall_off, out["id_i"] - lo)
+    return H.sort_contacts(out)
+
+
+def _run_batch(b, nsteps):
+    e = b.engine()
+    e.step(nsteps)
+    out = e.download()
+    out["force"], out["torque"] = e.forces()
+    out["contacts"] = e.contacts()
+    out["batch"] = e.reduce_batch()
+    out["single"] = [e.reduce(k) for k in range(len(b.members))]
+    e.close()
+    return out
+
+
+@pytest.mark.parametrize("nsteps", [0, 30])
+def test_batch_members_match_oracle(gpu, nsteps):
+    members = _members()
+    b = scenarios.batch(members)
+    g = _run_batch(b, nsteps)
+    for k, m in enumerate(members):
+        mk = dataclasses.replace(m, time_step=b.time_step)
+        o = H.run_oracle(mk, nsteps)
+        sl = b.member_slice(k)
+        gc = _member_contacts(b, g, k)
+        assert H.pair_set(gc) == H.pair_set(o["contacts"]), k
+        if nsteps == 0:
+            np.testing.assert_array_equal(gc["force"], o["contacts"]["force"])
+        assert H.rel_err(g["position"][sl], o["position"], 1e-3) < 1e-13
+        assert H.rel_err(g["force"][sl], o["force"]) < 1e-9
+        assert H.rel_err(g["torque"][sl], o["torque"]) < 1e-9
+        assert (g["instance"][sl] == k).all()
+
+
+def test_reduce_batch_equals_reduce(gpu):
+    b = scenarios.batch(_members())
+    g = _run_batch(b, 20)
+    for k, s in enumerate(g["single"]):
+        for key in ("kinetic_energy", "rotational_energy", "gravitational_energy", "elastic_energy", "mass"):
+            assert abs(g["batch"][key][k] - s[key]) <= 1e-12 * max(abs(s[key]), 1e-300), (k, key)
+        np.testing.assert_allclose(g["batch"]["centre_of_mass"][k], s["centre_of_mass"], rtol=1e-12, atol=1e-18)
+        assert g["batch"]["n_contacts"][k] == s["n_contacts"]
+        assert g["batch"]["n_wall_contacts"][k] == s["n_wall_contacts"]
+
+
+@pytest.mark.parametrize("nsteps", [50, 200])
+def test_deletion_boundary_matches_oracle(gpu, nsteps):
+    sc, dels = _falling_probe()
+    g = H.run_gpu(sc, nsteps, deletions=dels)
+    o = H.run_oracle(sc, nsteps, deletions=dels)
+    gone = o["instance"] < 0
+    assert gone.sum() > 5
+    np.testing.assert_array_equal(g["instance"] < 0, gone)
+    assert H.pair_set(g["contacts"]) == H.pair_set(o["contacts"])
+    assert H.rel_err(g["position"][~gone], o["position"][~gone], 1e-3) < 1e-13
+    assert H.rel_err(g["force"][~gone], o["force"][~gone]) < 1e-9
+    assert g["globals"]["mass"] > 0
+
+
+def test_deletion_in_one_batch_member(gpu):
+    """A deletion plane of one member leaves the other members untouched."""
+    probe, dels = _falling_probe()
+    members = [cases.compressed_box(n=300), probe]
+    b = scenarios.batch(members, deletions=[[], dels])
+    e = b.engine()
+    e.step(120)
+    out = e.download()
+    e.close()
+    for k, m in enumerate(members):
+        mk = dataclasses.replace(m, time_step=b.time_step)
+        o = H.run_oracle(mk, 120, deletions=dels if k == 1 else None)
+        sl = b.member_slice(k)
+        gone = o["instance"] < 0
+        np.testing.assert_array_equal(out["instance"][sl] < 0, gone)
+        assert H.rel_err(out["position"][sl][~gone], o["position"][~gone], 1e-3) < 1e-13

@@ -116,3 +116,27 @@ def test_deletion_in_one_batch_member(gpu):
         gone = o["instance"] < 0
         np.testing.assert_array_equal(out["instance"][sl] < 0, gone)
         assert H.rel_err(out["position"][sl][~gone], o["position"][~gone], 1e-3) < 1e-13
+
+
+def test_heap_batch_matches_oracle_and_runs(gpu):
+    """Four calibration heaps in one handle against the oracle per member,
+    then the batched pipeline's outputs (AoR estimators, packing fraction,
+    kinetic-energy traces)."""
+    from mercurydpm_fork_b200 import calibration as cal
+    b, params, R = cal.heap_batch(4, seed=5, n_range=(300, 500), base_radius_d=8, column_radius_d=4, v0=0.5)
+    e = b.engine()
+    e.step(1200)
+    out = e.download()
+    out["contacts"] = e.contacts()
+    e.close()
+    for k, m in enumerate(b.members):
+        o = H.run_oracle(m, 1200, deletions=[((0, 0, -1), 0.0)])
+        sl = b.member_slice(k)
+        alive = o["instance"] >= 0
+        assert H.pair_set(_member_contacts(b, out, k)) == H.pair_set(o["contacts"])
+        np.testing.assert_array_equal(out["instance"][sl] >= 0, alive)
+        assert H.rel_err(out["position"][sl][alive], o["position"][alive], 1e-3) < 1e-12
+    res = cal.run_heaps(b, R, steps=2000, trace_every=500)
+    assert res["kinetic_energy"].shape == (4, 5)
+    assert np.isfinite(res["aor_reference"]).all()
+    assert (res["n_remaining"] > 0).all()

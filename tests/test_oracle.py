@@ -92,3 +92,21 @@ def test_oracle_matches_reference_intersection_walls(name, nsteps):
     assert H.rel_err(o["torque"], r["torque"]) < 1e-12
     assert H.rel_err(o["position"], r["position"], 1e-3) < 1e-13
     assert H.rel_err(o["contacts"]["springs"], r["contacts"]["springs"]) < 1e-11
+
+
+@needs_ref
+def test_oracle_matches_reference_heap():
+    """A CalibrationHeap instance: LinearViscoelasticFrictionSpecies (linear
+    rolling and torsion springs), lognormal radii, the floor disk and the
+    DeletionBoundary below it."""
+    from mercurydpm_fork_b200 import calibration as cal
+    p = cal.HeapParams(n=400, sigma=0.15, mu=0.5, mu_r=0.1, restitution=0.5, seed=3)
+    sc, dels, _ = cal.heap_scenario(p, base_radius_d=8, column_radius_d=4, v0=0.5)
+    o = H.run_oracle(sc, 1200, deletions=dels)
+    r = H.run_reference(sc, 1200, deletions=dels)
+    assert H.pair_set(o["contacts"]) == H.pair_set(r["contacts"])
+    assert len(o["contacts"]["id_p"]) > 20 and int(o["contacts"]["is_wall"].sum()) > 0
+    np.testing.assert_array_equal(o["instance"], r["instance"])
+    assert H.rel_err(o["force"], r["force"]) < 1e-12
+    assert H.rel_err(o["position"], r["position"], 1e-3) < 1e-13
+    assert H.rel_err(o["contacts"]["springs"], r["contacts"]["springs"]) < 1e-11

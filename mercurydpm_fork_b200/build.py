@@ -15,6 +15,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdem_b200.so")
+# the calibration surrogate (tensor-core MLP) is a library of its own; it is
+# built without --fmad=false (no reference arithmetic to reproduce)
+SURROGATE_LIB = os.path.join(HERE, "libdem_surrogate.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -26,6 +29,10 @@ def sources():
     return [os.path.join(CSRC, "dem_engine.cu")]
 
 
+def surrogate_sources():
+    return [os.path.join(CSRC, "surrogate.cu")]
+
+
 def headers():
     out = []
     for d in (CSRC, os.path.join(ROOT, "include")):
@@ -35,22 +42,27 @@ def headers():
     return out
 
 
-def needs_build() -> bool:
-    if not os.path.exists(LIB):
+def needs_build(lib: str = LIB, srcs=None) -> bool:
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
-    return any(os.path.getmtime(f) > t for f in sources() + headers() + [__file__])
+    t = os.path.getmtime(lib)
+    return any(os.path.getmtime(f) > t for f in (srcs or sources()) + headers() + [__file__])
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not needs_build():
-        return LIB
-    cmd = [NVCC, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), *sources(), "-o", LIB + ".tmp"]
+def _compile(lib: str, srcs, flags, verbose: bool):
+    cmd = [NVCC, *ARCH, *flags, "-I", os.path.join(ROOT, "include"), *srcs, "-o", lib + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
-    os.replace(LIB + ".tmp", LIB)
+    os.replace(lib + ".tmp", lib)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or needs_build(LIB, sources()):
+        _compile(LIB, sources(), FLAGS, verbose)
+    if force or needs_build(SURROGATE_LIB, surrogate_sources()):
+        _compile(SURROGATE_LIB, surrogate_sources(), [f for f in FLAGS if f != "--fmad=false"], verbose)
     return LIB
 
 

@@ -1,0 +1,86 @@
+"""The calibration surrogate on the GPU (tcgen05 BF16 GEMMs with FP32
+accumulation) against the CPU oracle with BF16 rounding at the same points.
+
+Tolerances: the oracle accumulates in FP64 and evaluates erf/exp in double;
+the GPU accumulates in FP32 and rounds the pre-activations it turns into BF16
+from FP32, so a few BF16 values differ by one unit (2^-8 relative). Outputs
+are compared to 1e-2 of their norm, gradients per parameter block to 3e-2 of
+the block's norm.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import mlp_oracle as M  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _net(seed=7, capacity=4096):
+    from mercurydpm_fork_b200.surrogate import Surrogate
+    s = Surrogate(capacity=capacity, seed=seed)
+    s.set_normalisation([0.45, 0.15, 0.6, 0.1], [0.2, 0.09, 0.17, 0.06], [30.0, 0.6, 0.05], [5.0, 0.02, 0.02])
+    return s
+
+
+def _data(n, seed=0):
+    rng = np.random.default_rng(seed)
+    x = np.column_stack([rng.uniform(0.1, 0.8, n), rng.uniform(0, 0.3, n), rng.uniform(0.3, 0.9, n),
+                         rng.uniform(0, 0.2, n)])
+    y = np.column_stack([20 + 25 * x[:, 0] + 10 * x[:, 1], 0.55 + 0.1 * x[:, 2] - 0.2 * x[:, 3],
+                         0.03 + 0.04 * x[:, 2] * x[:, 0]])
+    return x, y
+
+
+@pytest.mark.parametrize("n", [1, 77, 300, 1024])
+def test_forward_matches_oracle(gpu, n):
+    s = _net()
+    x, _ = _data(n)
+    y = s.predict(x)
+    yo, _ = M.forward(s.params().astype(np.float64), x, s.norm)
+    yo = yo * s.norm[3] + s.norm[2]
+    s.close()
+    assert np.linalg.norm(y - yo) <= 1e-2 * np.linalg.norm(yo)
+
+
+@pytest.mark.parametrize("n", [64, 300, 1024])
+def test_gradients_match_oracle(gpu, n):
+    s = _net()
+    x, t = _data(n, seed=n)
+    loss, g = s.gradients(x, t)
+    lo, go = M.loss_and_grad(s.params().astype(np.float64), x, t, s.norm)
+    s.close()
+    assert abs(loss - lo) <= 1e-2 * lo
+    o = 0
+    for name, shape in M.SHAPES:
+        k = int(np.prod(shape))
+        a, b = g[o:o + k], go[o:o + k]
+        assert np.linalg.norm(a - b) <= 3e-2 * np.linalg.norm(b) + 1e-12, name
+        o += k
+
+
+def test_training_reduces_loss(gpu):
+    s = _net()
+    x, y = _data(4096, seed=3)
+    s.fit_normalisation(x, y)
+    hist = s.fit(x, y, epochs=60, batch=1024, lr=1e-3)
+    xv, yv = _data(1024, seed=4)
+    pred = s.predict(xv)
+    s.close()
+    assert hist[-1] < 0.1 * hist[0]
+    rel = np.abs(pred - yv) / np.abs(yv).mean(0)
+    assert rel.mean() < 0.05
+
+
+def test_large_batch_inference_is_consistent(gpu):
+    s = _net(capacity=65536)
+    x, _ = _data(65536, seed=9)
+    y = s.predict(x)
+    y2 = np.concatenate([s.predict(x[a:a + 1000]) for a in range(0, 3000, 1000)])
+    s.close()
+    assert np.isfinite(y).all()
+    np.testing.assert_array_equal(y[:3000], y2)

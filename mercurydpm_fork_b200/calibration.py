@@ -192,3 +192,119 @@ def run_heaps(b: Batch, base_radius: float, steps: int = 40_000, trace_every: in
         if a == a:
             out["packing_fraction"][k] = packing_fraction(pos, rad, base_radius, h0, a)
     return out
+
+
+# ---------------------------------------------------------------------------
+# surrogate-guided calibration
+# ---------------------------------------------------------------------------
+PARAM_NAMES = ("sliding_friction", "rolling_friction", "restitution", "psd_sigma")
+RESPONSE_NAMES = ("angle_of_repose", "packing_fraction", "settle_time")
+PARAM_BOX = np.array([[0.1, 0.8], [0.0, 0.3], [0.3, 0.9], [0.0, 0.2]])
+
+
+def heap_responses(params: np.ndarray, n: int = 600, seed: int = 11, steps: int = 20_000, trace_every: int = 500,
+                   chunk: int = 1024, **kw) -> np.ndarray:
+    """Runs one heap per parameter row (sliding friction, rolling friction,
+    restitution, PSD width) in batches of `chunk` instances and returns the
+    responses [angle of repose (reference estimator, degrees), packing
+    fraction, settle time (s)] per row. All heaps share `n` and the packing
+    seed, so the responses are a deterministic function of the parameters.
+
+    packing fraction: solid volume left on the floor over the volume of the
+    cone of height 4 COM_z on the floor disk (the cone the reference's AoR
+    estimator assumes); settle time: the first trace time at which the
+    kinetic energy is below 1e-2 of the elastic energy (the reference's settle
+    test, CalibrationHeap.cpp:119-131), or the end of the run."""
+    params = np.asarray(params, np.float64).reshape(-1, 4)
+    out = np.zeros((len(params), 3))
+    for a in range(0, len(params), chunk):
+        rows = params[a:a + chunk]
+        members, dels, R = [], [], None
+        for p in rows:
+            hp = HeapParams(n=n, sigma=float(p[3]), mu=float(p[0]), mu_r=float(p[1]), restitution=float(p[2]),
+                            seed=seed)
+            sc, d, R = heap_scenario(hp, **kw)
+            members.append(sc)
+            dels.append(d)
+        b = batch(members, deletions=dels)
+        e = b.engine()
+        e.step(0)
+        settle = np.full(len(rows), steps * b.time_step)
+        done = 0
+        g = None
+        while done < steps:
+            e.step(trace_every)
+            done += trace_every
+            g = e.reduce_batch()
+            quiet = (g["kinetic_energy"] < 1e-2 * g["elastic_energy"]) & (settle >= steps * b.time_step)
+            settle[quiet] = done * b.time_step
+        e.close()
+        com_z = g["centre_of_mass"][:, 2]
+        h = np.maximum(4.0 * com_z, 1e-9)
+        solid = g["mass"] / 2000.0  # density of every heap species
+        out[a:a + len(rows), 0] = aor_com(com_z, R)
+        out[a:a + len(rows), 1] = solid / (PI * R * R * h / 3.0)
+        out[a:a + len(rows), 2] = settle
+    return out
+
+
+def response_error(resp: np.ndarray, target: np.ndarray) -> np.ndarray:
+    """Largest relative error over angle of repose and packing fraction (the
+    settle time is quantised by the trace interval and is reported, not
+    judged)."""
+    resp = np.atleast_2d(resp)
+    return np.max(np.abs(resp[:, :2] - target[:2]) / np.abs(target[:2]), axis=1)
+
+
+def sample_params(rng, n: int) -> np.ndarray:
+    return PARAM_BOX[:, 0] + rng.uniform(size=(n, 4)) * (PARAM_BOX[:, 1] - PARAM_BOX[:, 0])
+
+
+def calibrate(target: np.ndarray, dem, surrogate=None, rounds: int = 4, proposals: int = 256,
+              candidates: int = 65_536, tol: float = 0.02, seed: int = 0, data=None, retrain_epochs: int = 30):
+    """Searches parameters whose DEM response is within `tol` of `target`.
+
+    Each round proposes `proposals` parameter sets and judges them with
+    `dem(params) -> responses` (batched DEM). With a surrogate, the proposals
+    are the candidates (of `candidates` uniform samples) whose predicted
+    responses are closest to the target; DEM then also judges the surrogate:
+    if its median prediction error on the proposals exceeds `tol`, the next
+    round falls back to plain proposals, and every DEM result refines the
+    network. Without a surrogate every round is plain: uniform proposals
+    (plain batched DEM search). Returns the best parameters, their error and
+    the per-round history."""
+    rng = np.random.default_rng(seed)
+    best_err, best_p, best_r = np.inf, None, None
+    hist = []
+    xs = [] if data is None else [np.asarray(data[0])]
+    ys = [] if data is None else [np.asarray(data[1])]
+    trust = surrogate is not None
+    for r in range(rounds):
+        pred = None
+        if trust:
+            cand = sample_params(rng, candidates)
+            pc = surrogate.predict(cand)
+            order = np.argsort(response_error(pc, target))[:proposals]
+            props, pred, mode = cand[order], pc[order], "surrogate"
+        else:
+            props, mode = sample_params(rng, proposals), ("fallback" if surrogate is not None else "plain")
+        resp = dem(props)
+        err = response_error(resp, target)
+        k = int(np.argmin(err))
+        if err[k] < best_err:
+            best_err, best_p, best_r = float(err[k]), props[k], resp[k]
+        rec = dict(round=r, mode=mode, best_error=float(err[k]), median_error=float(np.median(err)))
+        if surrogate is not None:
+            if pred is None:
+                pred = surrogate.predict(props)
+            surr_err = float(np.median(np.max(np.abs(pred[:, :2] - resp[:, :2]) / np.abs(resp[:, :2]), axis=1)))
+            rec["surrogate_error"] = surr_err
+            trust = surr_err <= tol
+            xs.append(props)
+            ys.append(resp)
+            surrogate.fit(np.concatenate(xs), np.concatenate(ys), epochs=retrain_epochs)
+        hist.append(rec)
+        if best_err <= tol:
+            break
+    return dict(best_error=best_err, params=best_p, response=best_r, history=hist, rounds=len(hist),
+                dem_runs=len(hist) * proposals)

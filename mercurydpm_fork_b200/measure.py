@@ -1,0 +1,88 @@
+"""Throughput of the workloads other than the headline bench (bench.py):
+
+    python -m mercurydpm_fork_b200.measure drum        # 1M-sphere rotating drum, Hertz-Mindlin
+    python -m mercurydpm_fork_b200.measure heaps       # 1,024 batched calibration heaps
+    python -m mercurydpm_fork_b200.measure surrogate   # MLP inference / training on the tensor cores
+
+Each prints one JSON line. Device time comes from CUDA events (dem_step's own
+events for DEM; torch events around the calls for the surrogate).
+"""
+from __future__ import annotations
+
+import json
+import sys
+import time
+
+import numpy as np
+
+
+def _time_dem(e, n_moving, steps_per_call=200, calls=5, warmup=2):
+    e.step(0)
+    for _ in range(warmup):
+        e.step(steps_per_call)
+    ms, rebuilds = 0.0, 0
+    for _ in range(calls):
+        e.step(steps_per_call)
+        st = e.stats()
+        ms += st["ms"]
+        rebuilds += st["rebuilds"]
+    return dict(value=n_moving * steps_per_call * calls / (ms / 1e3), unit="particle-timesteps/s",
+                ms_per_time_step=ms / (steps_per_call * calls), rebuilds_per_1000_steps=1000.0 * rebuilds /
+                (steps_per_call * calls))
+
+
+def drum(n=1_000_000, radius_d=175.0, length_d=60.0):
+    from . import scenarios
+    sc = scenarios.rotating_drum(n=n, radius_d=radius_d, length_d=length_d, vstd=0.0)
+    e = sc.engine()
+    out = _time_dem(e, sc.n_moving)
+    out["counts"] = e.counts()
+    e.close()
+    out.update(workload="rotating_drum", n=sc.n, radius_d=radius_d, length_d=length_d,
+               solid_fraction_of_drum=sc.info["solid_fraction_of_drum"], dt=sc.time_step,
+               species="HertzianViscoelasticMindlinRollingTorsion")
+    return out
+
+
+def heaps(n_instances=1024, seed=1):
+    from . import calibration as cal
+    t0 = time.perf_counter()
+    b, params, R = cal.heap_batch(n_instances, seed=seed)
+    t1 = time.perf_counter()
+    e = b.engine()
+    out = _time_dem(e, b.n, steps_per_call=200, calls=5)
+    e.close()
+    out.update(workload="calibration_heaps", instances=n_instances, n_total=b.n, build_s=t1 - t0,
+               instance_timesteps_per_s=out["value"] / b.n * n_instances)
+    return out
+
+
+def surrogate(batch=65536, train_batch=1024, reps=20):
+    import torch
+    from .surrogate import Surrogate
+    s = Surrogate(capacity=batch, seed=0)
+    rng = np.random.default_rng(0)
+    x = rng.uniform(size=(batch, 4)).astype(np.float32)
+    y = rng.uniform(size=(batch, 3)).astype(np.float32)
+    s.predict(x)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        s.predict(x)
+    t_inf = (time.perf_counter() - t0) / reps
+    s.train_step(x[:train_batch], y[:train_batch])
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        s.train_step(x[:train_batch], y[:train_batch])
+    t_train = (time.perf_counter() - t0) / reps
+    s.close()
+    flop = 2 * (4 * 256 + 2 * 256 * 256 + 256 * 3)
+    return dict(workload="surrogate", inference_batch=batch, inference_ms=t_inf * 1e3,
+                inference_tflops=flop * batch / t_inf / 1e12, train_batch=train_batch, train_step_ms=t_train * 1e3,
+                note="host-to-host wall time per call (host copies included)")
+
+
+if __name__ == "__main__":
+    which = sys.argv[1] if len(sys.argv) > 1 else "drum"
+    fn = dict(drum=drum, heaps=heaps, surrogate=surrogate)[which]
+    print(json.dumps(fn()))

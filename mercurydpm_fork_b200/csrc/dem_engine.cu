@@ -13,6 +13,7 @@
 #include "dem_engine.cuh"
 #include "dem_walls.cuh"
 #include "dem_kernels.cuh"
+#include "dem_pipeline.cuh"
 
 using namespace dem;
 
@@ -62,6 +63,7 @@ struct Handle {
     cudaGraphExec_t graph1 = nullptr, graphK = nullptr;
     int ncomp = 3;
     int law_variant = 0;
+    int sm_count = 148;
 };
 
 int fail(Handle* h, int code, const std::string& msg)
@@ -125,36 +127,49 @@ void launch_rebuild(Handle* h, cudaStream_t s)
     k_gather<<<grid_for(d.n, 256), 256, 0, s>>>(d);
     k_build<<<grid_for(d.n, 128), 128, 0, s>>>(d);
     k_rb_finish<<<1, 32, 0, s>>>(d);
+    k_rev<<<grid_for(d.n, 256), 256, 0, s>>>(d);
 }
-constexpr int REBUILD_LAUNCHES = 9;
+constexpr int REBUILD_LAUNCHES = 10;
+constexpr int FORCE_LAUNCHES = 3;
 
 // Law variants the force kernel is instantiated for; the handle uses a
 // specialised one when every species pair shares the same law pair.
 enum LawVariant { LAW_GENERIC = 0, LAW_LINEAR_SLIDING, LAW_LINEAR_ROLLING, LAW_HERTZ_MINDLIN, LAW_HERTZ_MINDLIN_RT };
 
+// one force evaluation: detect -> contacts -> sum (+ integration for MODE 1)
+template <int MODE, int NLAW, int FLAW, int NCOMP>
+void launch_pipeline(Handle* h, cudaStream_t s)
+{
+    DevPtrs& d = h->d;
+    k_detect<MODE, NCOMP><<<grid_for(d.n, DETECT_BLOCK), DETECT_BLOCK, 0, s>>>(d);
+    const unsigned gc = (unsigned)std::max(1, std::min((d.item_cap + CONTACT_BLOCK - 1) / CONTACT_BLOCK,
+                                                       h->sm_count * 8));
+    k_contacts<MODE, NLAW, FLAW, NCOMP><<<gc, CONTACT_BLOCK, 0, s>>>(d);
+    k_sum<MODE><<<grid_for(d.n, SUM_BLOCK), SUM_BLOCK, 0, s>>>(d);
+}
+
 template <int MODE>
 void launch_force_mode(Handle* h, cudaStream_t s)
 {
     DevPtrs& d = h->d;
-    const unsigned g = grid_for(d.n, 128);
     switch (h->law_variant) {
     case LAW_LINEAR_SLIDING:
-        k_force<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_SLIDING, 3><<<g, 128, 0, s>>>(d);
+        launch_pipeline<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_SLIDING, 3>(h, s);
         break;
     case LAW_LINEAR_ROLLING:
-        k_force<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_ROLLING_TORSION, 9><<<g, 128, 0, s>>>(d);
+        launch_pipeline<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_ROLLING_TORSION, 9>(h, s);
         break;
     case LAW_HERTZ_MINDLIN:
-        k_force<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN, 3><<<g, 128, 0, s>>>(d);
+        launch_pipeline<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN, 3>(h, s);
         break;
     case LAW_HERTZ_MINDLIN_RT:
-        k_force<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN_ROLLING_TORSION, 9><<<g, 128, 0, s>>>(d);
+        launch_pipeline<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN_ROLLING_TORSION, 9>(h, s);
         break;
     default:
         if (d.ncomp == 3)
-            k_force<MODE, -1, -1, 3><<<g, 128, 0, s>>>(d);
+            launch_pipeline<MODE, -1, -1, 3>(h, s);
         else
-            k_force<MODE, -1, -1, 9><<<g, 128, 0, s>>>(d);
+            launch_pipeline<MODE, -1, -1, 9>(h, s);
     }
 }
 
@@ -317,6 +332,9 @@ int dem_create(const dem_config* config, const dem_instance_desc* instances, dem
         delete h;
         return DEM_ERR_CUDA;
     }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) == cudaSuccess && sms > 0)
+        h->sm_count = sms;
     *out = reinterpret_cast<dem_handle*>(h);
     return DEM_OK;
 }
@@ -572,6 +590,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         d.block_sums = kept.block_sums; d.inst = kept.inst; d.species = kept.species; d.walls = kept.walls;
         d.wgeom = kept.wgeom; d.n_walls = kept.n_walls; d.ctl = kept.ctl; d.records = kept.records;
         d.n_instances = kept.n_instances;
+        d.rev = kept.rev; d.slot = kept.slot; d.slotw = kept.slotw; d.items = kept.items; d.shares = kept.shares;
+        d.item_cap = kept.item_cap;
         for (int b = 0; b < 2; ++b) { // no history carries over from the previous simulation
             CU(cudaMemsetAsync(d.cnt[b], 0, NC * sizeof(int), h->stream));
             CU(cudaMemsetAsync(d.act[b], 0, (size_t)d.nwords * NC * sizeof(unsigned), h->stream));
@@ -592,6 +612,14 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         if ((rc = dalloc(h, &d.whist[b], (size_t)d.ncomp * wmax * NC))) return rc;
         if ((rc = dalloc(h, &d.wact[b], NC))) return rc;
     }
+    if ((rc = dalloc(h, &d.rev, (size_t)cap * NC))) return rc;
+    if ((rc = dalloc(h, &d.slot, (size_t)cap * NC))) return rc;
+    if ((rc = dalloc(h, &d.slotw, (size_t)wmax * NC))) return rc;
+    // contact items: at most min(cap, 16) pairs owned per particle plus 4 walls
+    d.item_cap = (int)std::min<long long>(2000000000ll, (long long)n * std::min(cap, 16) +
+                                                            (long long)n * std::min(wmax, 4) + 1024);
+    if ((rc = dalloc(h, &d.items, (size_t)d.item_cap))) return rc;
+    if ((rc = dalloc(h, &d.shares, (size_t)d.item_cap * SHARE))) return rc;
     if ((rc = dalloc(h, &d.force, 3 * NC))) return rc;
     if ((rc = dalloc(h, &d.torque, 3 * NC))) return rc;
     if ((rc = dalloc(h, &d.key, NC))) return rc;
@@ -792,7 +820,7 @@ int dem_step(dem_handle* hh, int nsteps)
             }
             launch_force(h, h->stream, 0);
             k_flip<<<1, 32, 0, h->stream>>>(h->d_ctl);
-            launches += 2;
+            launches += FORCE_LAUNCHES + 1;
             CU(cudaGetLastError());
             h->initial_pending = false;
         }
@@ -812,7 +840,7 @@ int dem_step(dem_handle* hh, int nsteps)
                     left -= GRAPH_STEPS;
                 }
                 while (left-- > 0) CU(cudaGraphLaunch(h->graph1, h->stream));
-                launches += 2ll * nsteps;
+                launches += (1ll + FORCE_LAUNCHES) * nsteps;
             } else {
                 for (int k = 0; k < nsteps; ++k) {
                     k_control<<<1, CONTROL_THREADS, 0, h->stream>>>(h->d_ctl, d.walls, d.n_walls, d.dt,
@@ -821,7 +849,7 @@ int dem_step(dem_handle* hh, int nsteps)
                     launch_force(h, h->stream, 1);
                 }
                 CU(cudaGetLastError());
-                launches += (2ll + REBUILD_LAUNCHES) * nsteps;
+                launches += (1ll + FORCE_LAUNCHES + REBUILD_LAUNCHES) * nsteps;
             }
             k_flip<<<1, 32, 0, h->stream>>>(h->d_ctl);
             launches += 1;

@@ -97,6 +97,8 @@ struct Control {
     unsigned int n_records;
     unsigned int record_capacity;
     unsigned int lost_history;
+    unsigned int n_items;  // contact items of the current evaluation
+    unsigned int pad2;
 };
 
 __host__ __device__ __forceinline__ size_t nbr_at(int cap, int i, int k) { return (size_t)i * cap + k; }
@@ -132,6 +134,13 @@ struct DevPtrs {
     const WallGeom *wgeom;   // per wall; faces, edges and corners of intersection walls
     int n_walls;
     int n_instances;
+    // compact contact list of one evaluation (dem_pipeline.cuh)
+    int *rev;                // reverse index of the neighbour lists, n * cap
+    int *slot;               // per entry: item index, or SLOT_NONE / SLOT_IS_I
+    int *slotw;              // per (particle, wall): item index or SLOT_NONE
+    int2 *items;             // (particle, entry or ITEM_WALL + wall)
+    double *shares;          // 12 doubles per item
+    int item_cap;
     Control *ctl;
     ContactRecord *records;
     // sizes

@@ -7,19 +7,20 @@
 //               that runs the rebuild body (MercuryBase::hGridNeedsRebuilding,
 //               MercuryBase.cc:496-535, turned into a Verlet-skin test).
 //   rebuild     k_keys -> scan -> k_scatter -> k_cell_sort -> k_gather ->
-//               k_build -> k_rb_finish: cell keys per HGrid level, counting
-//               sort, per-cell ordering by particle id, permutation gather of
-//               the state, neighbour lists with contact-history carry-over
-//               (replaces HGrid buckets + InteractionHandler lookup,
-//               Mercury3D.cc:224-416, InteractionHandler.cc:103-174).
-//   k_force     one thread per particle: every neighbour-list entry is tested
-//               with the reference's exact FP64 contact predicate
-//               (BaseParticle::getInteractionWith, BaseParticle.cc:688-710),
-//               the contact law runs with the entry's spring history, walls
-//               and body forces are added, and the particle is integrated
-//               (second half-kick of this step, then first half-kick and
-//               drift of the next one: BaseParticle.cc:718-776) into the
-//               other state buffer.
+//               k_build -> k_rb_finish -> k_rev: cell keys per HGrid level,
+//               counting sort, per-cell ordering by particle id, permutation
+//               gather of the state, neighbour lists with contact-history
+//               carry-over, their reverse index (replaces HGrid buckets +
+//               InteractionHandler lookup, Mercury3D.cc:224-416,
+//               InteractionHandler.cc:103-174).
+//   force       k_detect -> k_contacts -> k_sum (dem_pipeline.cuh): the exact
+//               FP64 contact predicate (BaseParticle::getInteractionWith,
+//               BaseParticle.cc:688-710) on the entries each particle owns,
+//               the contact law once per contact with its spring history,
+//               the ordered sums with body force and walls, and the
+//               integration (second half-kick of this step, then first
+//               half-kick and drift of the next one: BaseParticle.cc:718-776)
+//               into the other state buffer.
 #pragma once
 #include "dem_engine.cuh"
 #include "dem_laws.cuh"
@@ -490,519 +491,6 @@ __device__ __forceinline__ void park_deleted(Control* ctl, double4& p, double4& 
     w = make_double4(0.0, 0.0, 0.0, 0.0);
     info.w |= FLAG_DELETED | FLAG_FIXED;
     ctl->force_rebuild = 1;
-}
-
-constexpr int FORCE_BLOCK = 128;  // threads (particles) per block, 4 warps
-constexpr int FORCE_QUEUE = 112;  // contacts a warp buffers before evaluating them (>= 64 + 48)
-constexpr int FORCE_SPECIES_SMEM = 16; // species tables up to this size are staged in shared memory
-
-__device__ __forceinline__ const dem_species_pair& species_at(const DevPtrs& d, const dem_species_pair* sm, int i)
-{
-    return sm ? sm[i] : d.species[i];
-}
-
-// Data of one warp's particle that the other lanes need, broadcast by shuffle.
-struct OwnerData {
-    V3 x;
-    double r;
-    int id, species, instance;
-};
-
-__device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
-__device__ __forceinline__ V3 shfl_v3(V3 v, int src) { return V3{shfl_d(v.x, src), shfl_d(v.y, src), shfl_d(v.z, src)}; }
-
-// MODE 0: initial force evaluation, 1: time step. NLAW/FLAW: the contact
-// law pair when every species pair of the simulation uses the same one
-// (-1: dispatch per contact); NCOMP: spring history doubles per contact.
-//
-// Work layout: one lane owns one particle (state, sums, integration), but the
-// candidate contacts of a warp's 32 particles -- neighbour-list entries first,
-// then (particle, wall) pairs -- are processed warp-wide, 32 or 64 at a time:
-//  (1) every lane tests one or two candidates with the exact contact
-//      predicate; contacts are appended, in (particle, candidate) order, to a
-//      per-warp queue in shared memory;
-//  (2) every lane evaluates the contact law of one queued contact and leaves
-//      the owner's force and torque share in shared memory;
-//  (3) each owner adds its shares in queue order, which is the order of its
-//      neighbour list and then of its walls, with the body force added in
-//      between -- the order the sequential code uses, so the sums (and the
-//      results) do not depend on how the work is spread over the lanes.
-// The contact law appears once in the kernel; the integration tail that
-// follows needs few registers.
-template <int MODE, int NLAW, int FLAW, int NCOMP>
-__global__ void __launch_bounds__(FORCE_BLOCK, 4) k_force(DevPtrs d)
-{
-    constexpr int NW = FORCE_BLOCK / 32;
-    constexpr int WALL_ITEM = 128;                   // queue items >= this are wall contacts
-    __shared__ int q_ok[NW][FORCE_QUEUE];            // (owner lane << 8) | entry (or WALL_ITEM + wall)
-    __shared__ int q_t[NW][FORCE_QUEUE];             // partner slot (particle contacts)
-    __shared__ double q_f[NW][6][FORCE_QUEUE];       // owner's force (0-2) and torque (3-5) share
-    __shared__ int pre[NW][33];                      // exclusive prefix of the warp's entry counts
-    __shared__ unsigned int newbits[NW][4][32];      // active bits of the next history buffer
-    __shared__ unsigned int wnewbits[NW][32];        // wall-contact bits of the next buffer
-    // the warp's particle data live in shared memory during the contact
-    // phases (field-major, so lanes reading different owners hit different banks)
-    __shared__ double own_d[NW][11][32];             // x(3) v(3) w(3) r invMass
-    __shared__ int own_i[NW][4][32];                 // id species instance flags
-    __shared__ unsigned int own_a[NW][4][32];        // active bits of the current history
-    __shared__ unsigned int own_wa[NW][32];          // current wall-contact bits
-    __shared__ InstanceDev s_inst;                   // instance record (single-instance runs)
-    __shared__ dem_species_pair s_species[FORCE_SPECIES_SMEM];
-
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    const int wbase = s - lane;
-    Control* ctl = d.ctl;
-    const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
-    const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
-    const bool record = final_step && ctl->record;
-    // first time step after the initial evaluation: the reference's
-    // initialiseSolve and step 0 stamp contacts with the same time stamp
-    // (DPMBase.cc:4180-4259, :4315-4389); see the uses below
-    const bool first = (MODE == 1) && ctl->first_step;
-    const bool active = s < d.n;
-    if (d.single_instance) {
-        const int* src = reinterpret_cast<const int*>(&d.inst[0]);
-        int* dst = reinterpret_cast<int*>(&s_inst);
-        for (int w = threadIdx.x; w < (int)(sizeof(InstanceDev) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
-    }
-    if (d.n_species_table <= FORCE_SPECIES_SMEM) {
-        const int words = d.n_species_table * (int)(sizeof(dem_species_pair) / sizeof(int));
-        const int* src = reinterpret_cast<const int*>(d.species);
-        int* dst = reinterpret_cast<int*>(s_species);
-        for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
-    }
-    __syncthreads();
-    const InstanceDev* inst_sm = d.single_instance ? &s_inst : nullptr;
-    const dem_species_pair* sp_sm = d.n_species_table <= FORCE_SPECIES_SMEM ? s_species : nullptr;
-    const double dt = d.dt;
-    constexpr size_t hstride = 1; // spring components are contiguous
-    constexpr size_t wstride = 1;
-    const double* hin = d.hist[c];
-    double* hout = d.hist[nb];
-
-    // ---- prologue: stage this warp's particles --------------------------
-    int count = 0, nwalls = 0;
-    {
-        double4 p4 = make_double4(0, 0, 0, 1), v4 = make_double4(0, 0, 0, 0), w4 = make_double4(0, 0, 0, 0);
-        int4 i4 = make_int4(-1, 0, 0, FLAG_FIXED);
-        unsigned int a[4] = {0u, 0u, 0u, 0u};
-        unsigned int wa = 0u;
-        if (active) {
-            p4 = d.pr[c][s];
-            v4 = d.vm[c][s];
-            w4 = d.wi[c][s];
-            i4 = d.info[c][s];
-            count = d.cnt[l][s];
-#pragma unroll
-            for (int w = 0; w < 4; ++w)
-                if (w < d.nwords) a[w] = d.act[c][(size_t)w * d.ncap + s];
-            wa = d.wact[c][s];
-            const InstanceDev& I = *(inst_sm ? inst_sm : &d.inst[i4.z]);
-            nwalls = (i4.w & FLAG_FIXED) ? 0 : I.wall_end - I.wall_begin;
-        }
-        own_d[wid][0][lane] = p4.x; own_d[wid][1][lane] = p4.y; own_d[wid][2][lane] = p4.z;
-        own_d[wid][3][lane] = v4.x; own_d[wid][4][lane] = v4.y; own_d[wid][5][lane] = v4.z;
-        own_d[wid][6][lane] = w4.x; own_d[wid][7][lane] = w4.y; own_d[wid][8][lane] = w4.z;
-        own_d[wid][9][lane] = p4.w; own_d[wid][10][lane] = v4.w;
-        own_i[wid][0][lane] = i4.x; own_i[wid][1][lane] = i4.y; own_i[wid][2][lane] = i4.z;
-        own_i[wid][3][lane] = i4.w;
-#pragma unroll
-        for (int w = 0; w < 4; ++w) {
-            own_a[wid][w][lane] = a[w];
-            newbits[wid][w][lane] = 0u;
-        }
-        own_wa[wid][lane] = wa;
-        wnewbits[wid][lane] = 0u;
-    }
-    // warp prefix of the entry counts; the widest wall list of the warp
-    int incl = count;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    pre[wid][lane + 1] = incl;
-    if (lane == 0) pre[wid][0] = 0;
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    const int nwmax = __reduce_max_sync(0xffffffffu, nwalls);
-    const int total_w = 32 * nwmax;
-    __syncwarp();
-
-    V3 F = zero3(), T = zero3();
-    int qn = 0;
-    int phase = 0, base = 0; // phase 0: neighbour-list entries, 1: walls
-    for (;;) {
-        bool last;
-        if (phase == 0) {
-            // ---- (1a) two neighbour entries per lane: exact contact predicate ----
-            // (two independent gather chains per lane for memory-level parallelism)
-            int oo[2], kk[2], tt[2];
-            bool hit[2] = {false, false};
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int j = base + 32 * h + lane;
-                int lo = 0, hi = 31;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (pre[wid][mid] <= j) lo = mid; else hi = mid - 1;
-                }
-                oo[h] = lo;
-                kk[h] = j - pre[wid][lo];
-                tt[h] = (j < total) ? d.nbr[l][nbr_at(d.cap, wbase + lo, kk[h])] : -1;
-            }
-            double4 pt2[2];
-            int4 it2[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (tt[h] >= 0) {
-                    pt2[h] = d.pr[c][tt[h]];
-                    it2[h] = d.info[c][tt[h]];
-                }
-            }
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (tt[h] < 0) continue;
-                const int o = oo[h], k = kk[h];
-                const double4 pt = pt2[h];
-                const int4 it = it2[h];
-                const V3 xo = v3(own_d[wid][0][o], own_d[wid][1][o], own_d[wid][2][o]);
-                const double ro = own_d[wid][9][o];
-                const int ido = own_i[wid][0][o], spo = own_i[wid][1][o], ino = own_i[wid][2][o];
-                const InstanceDev& I = *(inst_sm ? inst_sm : &d.inst[ino]);
-                bool periodic;
-                const V3 xt = image_of(I, xo, xyz(pt), periodic);
-                // P is the lower id (DPMBase.cc:3129-3139); against a periodic
-                // ghost the real particle is P (ghosts carry higher ids)
-                const bool selfP = periodic || (ido < it.x);
-                const V3 branch = selfP ? xo - xt : xt - xo;
-                const double d2 = len2(branch);
-                const double rP = selfP ? ro : pt.w;
-                const double rI = selfP ? pt.w : ro;
-                double idist = 0.0; // x + 0.0 == x: skipping the lookup keeps the predicate exact
-                if (!d.zero_idist) {
-                    const int ns = I.n_species;
-                    idist = species_at(d, sp_sm, I.species_offset + (selfP ? spo * ns + it.y : it.y * ns + spo))
-                                .interaction_distance;
-                }
-                const double sum = rI + rP + idist;
-                hit[h] = !(d2 >= sum * sum); // BaseParticle.cc:695-697
-                if (!hit[h] && first) {
-                    const bool derived = periodic && (ido > it.x);
-                    if (((own_a[wid][k >> 5][o] >> (k & 31)) & 1u) && !derived) {
-                        // an interaction of the initial evaluation outlives step 0
-                        // (InteractionHandler::eraseOldInteractions, stamps <= 0 only)
-                        Springs keep;
-                        const size_t hb = hist_at(d.cap, NCOMP, wbase + o, k);
-                        load_springs(hin, hb, hstride, NCOMP, keep);
-                        store_springs(hout, hb, hstride, NCOMP, keep);
-                        atomicOr(&newbits[wid][k >> 5][o], 1u << (k & 31));
-                    }
-                }
-            }
-#pragma unroll
-            for (int h = 0; h < 2; ++h) { // append in entry order: first half, then second
-                const unsigned int cm = __ballot_sync(0xffffffffu, hit[h]);
-                if (hit[h]) {
-                    const int pos = qn + __popc(cm & ((1u << lane) - 1u));
-                    q_ok[wid][pos] = (oo[h] << 8) | kk[h];
-                    q_t[wid][pos] = tt[h];
-                }
-                qn += __popc(cm);
-            }
-            base += 64;
-            last = base >= total;
-        } else {
-            // ---- (1b) one (particle, wall) pair per lane ----
-            const int j = base + lane;
-            const int o = j / (nwmax > 0 ? nwmax : 1), wl = j - o * (nwmax > 0 ? nwmax : 1);
-            bool hit = false;
-            if (j < total_w) {
-                const int ino = own_i[wid][2][o], spo = own_i[wid][1][o];
-                const bool fixed_o = (own_i[wid][3][o] & FLAG_FIXED) != 0;
-                const InstanceDev& I = *(inst_sm ? inst_sm : &d.inst[ino]);
-                if (!fixed_o && wl < I.wall_end - I.wall_begin) {
-                    const dem_wall& wall = d.walls[I.wall_begin + wl];
-                    const dem_species_pair& sp = species_at(d, sp_sm, I.species_offset + spo * I.n_species + wall.species);
-                    const V3 xo = v3(own_d[wid][0][o], own_d[wid][1][o], own_d[wid][2][o]);
-                    double dist;
-                    V3 nrm;
-                    hit = wall_distance(wall, d.wgeom + I.wall_begin + wl, xo, own_d[wid][9][o] + sp.interaction_distance,
-                                        dist, nrm);
-                    if (!hit && first && ((own_wa[wid][o] >> wl) & 1u)) { // survives step 0, as for pairs
-                        Springs keep;
-                        const size_t hb = whist_at(d.wmax, NCOMP, wbase + o, wl);
-                        load_springs(d.whist[c], hb, wstride, NCOMP, keep);
-                        store_springs(d.whist[nb], hb, wstride, NCOMP, keep);
-                        atomicOr(&wnewbits[wid][o], 1u << wl);
-                    }
-                }
-            }
-            const unsigned int cm = __ballot_sync(0xffffffffu, hit);
-            if (hit) {
-                const int pos = qn + __popc(cm & ((1u << lane) - 1u));
-                q_ok[wid][pos] = (o << 8) | (WALL_ITEM + wl);
-            }
-            qn += __popc(cm);
-            base += 32;
-            last = base >= total_w;
-        }
-        __syncwarp();
-
-        if (qn > FORCE_QUEUE - 64 || last) {
-            // ---- (2) one queued contact per lane: contact law ----
-            for (int q0 = 0; q0 < qn; q0 += 32) {
-                const int q = q0 + lane;
-                if (q >= qn) continue;
-                const int okq = q_ok[wid][q];
-                const int oq = okq >> 8, kq = okq & 0xff;
-                const int so = wbase + oq;
-                const V3 xq = v3(own_d[wid][0][oq], own_d[wid][1][oq], own_d[wid][2][oq]);
-                const V3 vq = v3(own_d[wid][3][oq], own_d[wid][4][oq], own_d[wid][5][oq]);
-                const V3 wq = v3(own_d[wid][6][oq], own_d[wid][7][oq], own_d[wid][8][oq]);
-                const double rq = own_d[wid][9][oq];
-                const double mq = own_d[wid][10][oq];
-                const int idq = own_i[wid][0][oq], spq = own_i[wid][1][oq], inq = own_i[wid][2][oq];
-                const InstanceDev& I = *(inst_sm ? inst_sm : &d.inst[inq]);
-                const int ns = I.n_species;
-                ContactGeom g;
-                Springs spr;
-                spr.slide = zero3(); spr.roll = zero3(); spr.tors = zero3();
-                const dem_species_pair* spp;
-                bool selfP = true, periodic = false, derived = false, was_active = false;
-                int tq = 0, pid_i = 0;
-                const bool is_wall = kq >= WALL_ITEM;
-                double* hdst;
-                size_t hb, hs;
-                if (is_wall) {
-                    // DPMBase::computeForcesDueToWalls / BaseWall::getInteractionWith
-                    // (DPMBase.cc:3188-3215, BaseWall.cc:367-437)
-                    const int wl = kq - WALL_ITEM;
-                    const int wg = I.wall_begin + wl;
-                    const dem_wall& wall = d.walls[wg];
-                    spp = &species_at(d, sp_sm, I.species_offset + spq * ns + wall.species);
-                    double dist;
-                    V3 nrm;
-                    wall_distance(wall, d.wgeom + wg, xq, rq + spp->interaction_distance, dist, nrm);
-                    g.n = -nrm;
-                    g.distance = dist;
-                    g.overlap = rq - dist;
-                    g.c = xq - (rq - 0.5 * g.overlap) * g.n;
-                    g.xp = xq; g.vp = vq; g.wp = wq; g.inv_mass_p = mq; g.curv_p = 1.0 / rq;
-                    g.xi = v3(wall.position[0], wall.position[1], wall.position[2]);
-                    g.vi = v3(wall.velocity[0], wall.velocity[1], wall.velocity[2]);
-                    g.wi = v3(wall.angular_velocity[0], wall.angular_velocity[1], wall.angular_velocity[2]);
-                    g.inv_mass_i = 0.0;
-                    g.curv_i = 0.0;
-                    g.i_is_wall = true;
-                    hb = whist_at(d.wmax, NCOMP, so, wl);
-                    hs = wstride;
-                    hdst = d.whist[nb];
-                    was_active = (own_wa[wid][oq] >> wl) & 1u;
-                    if (was_active) load_springs(d.whist[c], hb, hs, NCOMP, spr);
-                    pid_i = wg;
-                } else {
-                    tq = q_t[wid][q];
-                    const double4 pt = d.pr[c][tq];
-                    const int4 it = d.info[c][tq];
-                    const double4 vt4 = d.vm[c][tq];
-                    const double4 wt4 = d.wi[c][tq];
-                    const V3 xt = image_of(I, xq, xyz(pt), periodic);
-                    selfP = periodic || (idq < it.x);
-                    const V3 branch = selfP ? xq - xt : xt - xq;
-                    const double d2 = len2(branch);
-                    spp = &species_at(d, sp_sm, I.species_offset + (selfP ? spq * ns + it.y : it.y * ns + spq));
-                    const double rP = selfP ? rq : pt.w;
-                    const double rI = selfP ? pt.w : rq;
-                    g.distance = sqrt(d2);
-                    g.n = branch / g.distance;
-                    g.overlap = rP + rI - g.distance;
-                    if (selfP) {
-                        g.xp = xq; g.vp = vq; g.wp = wq; g.inv_mass_p = mq;
-                        g.xi = xt; g.vi = xyz(vt4); g.wi = xyz(wt4); g.inv_mass_i = vt4.w;
-                    } else {
-                        g.xp = xt; g.vp = xyz(vt4); g.wp = xyz(wt4); g.inv_mass_p = vt4.w;
-                        g.xi = xq; g.vi = vq; g.wi = wq; g.inv_mass_i = mq;
-                    }
-                    g.c = g.xp - (rP - 0.5 * g.overlap) * g.n;
-                    g.curv_p = 1.0 / rP;
-                    g.curv_i = 1.0 / rI;
-                    g.i_is_wall = false;
-                    hb = hist_at(d.cap, NCOMP, so, kq);
-                    hs = hstride;
-                    hdst = hout;
-                    was_active = (own_a[wid][kq >> 5][oq] >> (kq & 31)) & 1u;
-                    // the higher-id side of a periodic pair restarts every step from the
-                    // reversed spring of the lower-id side (InteractionHandler.cc:316-368,
-                    // BaseInteraction::copySwitchPointer / reverseHistory)
-                    derived = periodic && (idq > it.x);
-                    if (derived) {
-                        const int tc = d.cnt[l][tq];
-                        for (int m = 0; m < tc; ++m) {
-                            if (d.nbr[l][nbr_at(d.cap, tq, m)] != so) continue;
-                            if ((d.act[c][(size_t)(m >> 5) * d.ncap + tq] >> (m & 31)) & 1u) {
-                                load_springs(hin, hist_at(d.cap, NCOMP, tq, m), hstride, NCOMP, spr);
-                                spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
-                            }
-                            break;
-                        }
-                    } else if (was_active) {
-                        load_springs(hin, hb, hstride, NCOMP, spr);
-                    }
-                    pid_i = it.x;
-                }
-                const Springs before = spr;
-                ContactOut out;
-                evaluate_contact<NLAW, FLAW>(*spp, g, spr, dt, out);
-                // step 0 keeps the lower-id side's old spring of a periodic pair
-                // that existed at the initial evaluation (equal stamps,
-                // InteractionHandler.cc:339-352)
-                const Springs& kept = (first && periodic && !derived && was_active) ? before : spr;
-                store_springs(hdst, hb, hs, NCOMP, kept);
-                if (is_wall)
-                    atomicOr(&wnewbits[wid][oq], 1u << (kq - WALL_ITEM));
-                else
-                    atomicOr(&newbits[wid][kq >> 5][oq], 1u << (kq & 31));
-                V3 fs, ts;
-                if (selfP) {
-                    fs = out.force;
-                    ts = out.torque - cross(xq - g.c, out.force);
-                } else {
-                    fs = -out.force;
-                    ts = -out.torque + cross(xq - g.c, out.force);
-                }
-                q_f[wid][0][q] = fs.x; q_f[wid][1][q] = fs.y; q_f[wid][2][q] = fs.z;
-                q_f[wid][3][q] = ts.x; q_f[wid][4][q] = ts.y; q_f[wid][5][q] = ts.z;
-                if (record && (is_wall || (periodic ? (idq < pid_i) : selfP))) {
-                    const double meff = 1.0 / (g.inv_mass_p + g.inv_mass_i);
-                    write_record(d, idq, pid_i, is_wall ? 1 : 0, periodic ? 1 : 0, so, is_wall ? pid_i : tq, g, out,
-                                 kept, spring_energy(*spp, kept, meff));
-                }
-            }
-            __syncwarp();
-            // ---- (3) each owner adds its shares in queue order ----
-            {
-                int lo = 0, hi = qn; // first queue slot whose owner is >= lane
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if ((q_ok[wid][mid] >> 8) < lane) lo = mid + 1; else hi = mid;
-                }
-                for (int q = lo; q < qn && (q_ok[wid][q] >> 8) == lane; ++q) {
-                    F += v3(q_f[wid][0][q], q_f[wid][1][q], q_f[wid][2][q]);
-                    T += v3(q_f[wid][3][q], q_f[wid][4][q], q_f[wid][5][q]);
-                }
-            }
-            __syncwarp();
-            qn = 0;
-        }
-        if (last) {
-            if (phase == 1) break;
-            // body force between the particle and the wall contacts, as in
-            // DPMBase::computeAllForces: computeExternalForces (DPMBase.cc:3168-3179)
-            if (active && !(own_i[wid][3][lane] & FLAG_FIXED)) {
-                const InstanceDev& I = *(inst_sm ? inst_sm : &d.inst[own_i[wid][2][lane]]);
-                const double m = 1.0 / own_d[wid][10][lane];
-                const V3 g3 = v3(I.gravity[0], I.gravity[1], I.gravity[2]);
-                const V3 vo = v3(own_d[wid][3][lane], own_d[wid][4][lane], own_d[wid][5][lane]);
-                F += g3 * m - d.drag * vo;
-            }
-            if (total_w == 0) break;
-            phase = 1;
-            base = 0;
-        }
-    }
-    __syncwarp();
-
-    double disp2 = 0.0;
-    if (active) {
-        for (int w = 0; w < d.nwords; ++w) d.act[nb][(size_t)w * d.ncap + s] = newbits[wid][w][lane];
-        d.wact[nb][s] = wnewbits[wid][lane];
-        if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z))) atomicOr(&ctl->status, 1u << DEM_ERR_NAN);
-        // own state again (L1 hits): keeping it live across the contact phases costs registers
-        const double4 ps = d.pr[c][s];
-        const double4 vs = d.vm[c][s];
-        const double4 ws = d.wi[c][s];
-        double4 qs = d.qo[c][s];
-        const int4 is = d.info[c][s];
-        const InstanceDev& I = *(inst_sm ? inst_sm : &d.inst[is.z]);
-
-        // ---- integration ----
-        double4 pn = ps, vn = vs, wn = ws;
-        if (final_step) {
-            d.force[3 * (size_t)s + 0] = F.x;
-            d.force[3 * (size_t)s + 1] = F.y;
-            d.force[3 * (size_t)s + 2] = F.z;
-            d.torque[3 * (size_t)s + 0] = T.x;
-            d.torque[3 * (size_t)s + 1] = T.y;
-            d.torque[3 * (size_t)s + 2] = T.z;
-        }
-        if (MODE == 1) {
-            V3 x = xyz(ps), v = xyz(vs), w = xyz(ws);
-            Q4 q{qs.x, qs.y, qs.z, qs.w};
-            if (vs.w != 0.0) {
-                const V3 a = ((F * vs.w) * 0.5) * dt;
-                v += a; // BaseParticle::integrateAfterForceComputation
-                V3 aw = zero3();
-                if (d.rotation) {
-                    const S33 Ib{ws.w, 0.0, 0.0, ws.w, 0.0, ws.w};
-                    aw = ((rotate_inverse_inertia(q, Ib) * T) * 0.5) * dt;
-                    w += aw;
-                }
-                if (!final_step) { // BaseParticle::integrateBeforeForceComputation of the next step
-                    v += a;
-                    const V3 disp = v * dt;
-                    x += disp;
-                    disp2 = len2(disp);
-                    if (d.rotation) {
-                        w += aw;
-                        q = quat_rotate(q, w * dt);
-                    }
-                }
-            } else if (!final_step) { // BaseInteractable::integrateBeforeForceComputation
-                const V3 disp = v * dt;
-                x += disp;
-                disp2 = len2(disp);
-                q = quat_rotate(q, w * dt);
-            }
-            if (!final_step && I.per_mask) { // PeriodicBoundary::checkBoundaryAfterParticlesMove
-                double* xc = &x.x;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    if ((I.per_mask >> k) & 1u) {
-                        const double dl = xc[k] - I.per_lo[k], dr = I.per_hi[k] - xc[k];
-                        if ((dl < dr ? dl : dr) < 0) {
-                            if (I.per_hi[k] - xc[k] > xc[k] - I.per_lo[k])
-                                xc[k] = xc[k] + I.per_L[k];
-                            else
-                                xc[k] = xc[k] - I.per_L[k];
-                        }
-                    }
-                }
-            }
-            pn = make_double4(x.x, x.y, x.z, ps.w);
-            vn = make_double4(v.x, v.y, v.z, vs.w);
-            wn = make_double4(w.x, w.y, w.z, ws.w);
-            qs = make_double4(q.q0, q.q1, q.q2, q.q3);
-        }
-        int4 isn = is;
-        if (MODE == 1 && !final_step && I.n_del && !(is.w & FLAG_DELETED) && deletion_check(I, xyz(pn))) {
-            park_deleted(ctl, pn, vn, wn, isn);
-            disp2 = 0.0;
-        }
-        d.pr[nb][s] = pn;
-        d.vm[nb][s] = vn;
-        d.wi[nb][s] = wn;
-        d.qo[nb][s] = qs;
-        d.info[nb][s] = isn;
-        d.caller[nb][s] = d.caller[c][s];
-    }
-    // maximum displacement of this step (for the skin test)
-    if (MODE == 1) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) disp2 = fmax(disp2, __shfl_xor_sync(0xffffffffu, disp2, o));
-        if (lane == 0 && disp2 > 0.0)
-            atomicMax(&ctl->step_disp2_bits, (unsigned long long)__double_as_longlong(disp2));
-    }
 }
 
 // First half-kick and drift from the stored forces: the

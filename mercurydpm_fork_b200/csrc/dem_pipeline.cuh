@@ -1,0 +1,454 @@
+// dem_pipeline.cuh -- one force evaluation as three kernels over a compact
+// contact list, each contact's law evaluated once:
+//
+//   k_detect   one thread per particle: the exact contact predicate
+//              (BaseParticle::getInteractionWith, BaseParticle.cc:688-710) on
+//              the neighbour entries the particle owns as P -- the lower id,
+//              or its own view of a periodic pair (DPMBase.cc:3124-3139) --
+//              and on its walls; contacts are appended to a compact item list
+//              (one atomic per block) and every entry gets its item index or a
+//              role mark; history bits of the next buffer are written here.
+//   k_contacts one thread per contact item: the contact law with the spring
+//              history (DPMBase::computeInternalForce, DPMBase.cc:3113-3162;
+//              walls: DPMBase.cc:3188-3215), the force/torque share of P and,
+//              for an ordinary pair, of I, into the item's 12 doubles.
+//   k_sum      one thread per particle: the shares in neighbour-list order
+//              (P entries from its own items, I entries from the partner's
+//              item, which k_contacts announces in I's entry through the
+//              reverse index), the body force
+//              (DPMBase.cc:3168-3179), then the wall shares -- the order the
+//              sequential code adds them -- then the integration tail.
+//
+// The entry and item orders do not change any sum: each particle adds its
+// shares in its own list order, so results are independent of the atomics.
+#pragma once
+#include "dem_kernels.cuh"
+
+namespace dem {
+
+constexpr int ITEM_WALL = 1 << 20;   // item entry field >= this: wall contact (ITEM_WALL + wall)
+constexpr int SLOT_NONE = -1;        // P entry without a contact this evaluation
+constexpr int SLOT_IS_I = -2;        // entry whose partner owns the pair, no contact this evaluation
+constexpr int SLOT_I_BASE = -3;      // SLOT_I_BASE - q: I's share of the partner's item q
+constexpr int SHARE = 12;            // doubles per item: P force, P torque, I force, I torque
+constexpr int DETECT_BLOCK = 128;
+constexpr int CONTACT_BLOCK = 128;
+constexpr int SUM_BLOCK = 128;
+
+// Reverse index of the neighbour lists (after a rebuild): rev[s][k] = m with
+// nbr[t][m] == s for t = nbr[s][k] (the lists are symmetric).
+__global__ void __launch_bounds__(256) k_rev(DevPtrs d)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!d.ctl->rebuild || s >= d.n) return;
+    const int l = d.ctl->lbuf;
+    const int cnt = d.cnt[l][s];
+    for (int k = 0; k < cnt && k < d.cap; ++k) {
+        const int t = d.nbr[l][nbr_at(d.cap, s, k)];
+        const int ct = min(d.cnt[l][t], d.cap);
+        int m = 0;
+        while (m < ct && d.nbr[l][nbr_at(d.cap, t, m)] != s) ++m;
+        if (m == ct) {
+            atomicOr(&d.ctl->status, 1u << DEM_ERR_CAPACITY); // an asymmetric pair: the partner's row overflowed
+            m = 0;
+        }
+        d.rev[nbr_at(d.cap, s, k)] = m;
+    }
+}
+
+// Exclusive block scan of one int per thread (DETECT_BLOCK threads); returns
+// this thread's offset and the block total through `total`.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    int before = 0;
+    total = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        if (w < wid) before += warp_sums[w];
+        total += warp_sums[w];
+    }
+    return before + x - v;
+}
+
+template <int MODE, int NCOMP>
+__global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
+{
+    __shared__ int warp_sums[DETECT_BLOCK / 32];
+    __shared__ int block_base;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    Control* ctl = d.ctl;
+    const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
+    const bool first = (MODE == 1) && ctl->first_step;
+    const bool active = s < d.n;
+    unsigned int hitbits[4] = {0u, 0u, 0u, 0u}, newbits[4] = {0u, 0u, 0u, 0u};
+    unsigned int whit = 0u, wnew = 0u;
+    int count = 0, nwalls = 0;
+    if (active) {
+        const double4 ps = d.pr[c][s];
+        const int4 is = d.info[c][s];
+        const InstanceDev& I = d.inst[is.z];
+        const V3 xs = xyz(ps);
+        unsigned int a[4] = {0u, 0u, 0u, 0u};
+        for (int w = 0; w < d.nwords; ++w) a[w] = d.act[c][(size_t)w * d.ncap + s];
+        count = min(d.cnt[l][s], d.cap);
+        const int ns = I.n_species;
+        constexpr int B = 4; // entries whose gathers are in flight together
+        for (int k0 = 0; k0 < count; k0 += B) {
+        int tb[B];
+        double4 ptb[B];
+        int4 itb[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) tb[j] = (k0 + j < count) ? d.nbr[l][nbr_at(d.cap, s, k0 + j)] : -1;
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+            if (tb[j] >= 0) {
+                ptb[j] = d.pr[c][tb[j]];
+                itb[j] = d.info[c][tb[j]];
+            }
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            const int k = k0 + j;
+            if (k >= count) break;
+            const size_t e = nbr_at(d.cap, s, k);
+            const double4 pt = ptb[j];
+            const int4 it = itb[j];
+            bool periodic;
+            const V3 xt = image_of(I, xs, xyz(pt), periodic);
+            if (!periodic && !(is.x < it.x)) { // the partner (lower id) owns this pair
+                d.slot[e] = SLOT_IS_I;
+                continue;
+            }
+            d.slot[e] = SLOT_NONE;
+            const V3 branch = xs - xt;
+            const double d2 = len2(branch);
+            double idist = 0.0; // x + 0.0 == x: skipping the lookup keeps the predicate exact
+            if (!d.zero_idist) idist = d.species[I.species_offset + is.y * ns + it.y].interaction_distance;
+            const double sum = pt.w + ps.w + idist; // rI + rP + distance (BaseParticle.cc:695-697)
+            const unsigned int bit = 1u << (k & 31);
+            if (!(d2 >= sum * sum)) {
+                hitbits[k >> 5] |= bit;
+                newbits[k >> 5] |= bit;
+            } else if (first && (a[k >> 5] & bit) && !(periodic && is.x > it.x)) {
+                // an interaction of the initial evaluation outlives step 0
+                // (InteractionHandler::eraseOldInteractions erases stamps <= 0 only)
+                for (int q = 0; q < NCOMP; ++q)
+                    d.hist[nb][hist_at(d.cap, NCOMP, s, k) + q] = d.hist[c][hist_at(d.cap, NCOMP, s, k) + q];
+                newbits[k >> 5] |= bit;
+            }
+        }
+        }
+        if (!(is.w & FLAG_FIXED)) {
+            const unsigned int wa = d.wact[c][s];
+            nwalls = I.wall_end - I.wall_begin;
+            for (int w = 0; w < nwalls; ++w) {
+                const int wg = I.wall_begin + w;
+                const dem_wall& wall = d.walls[wg];
+                const dem_species_pair& sp = d.species[I.species_offset + is.y * ns + wall.species];
+                double dist;
+                V3 nrm;
+                const unsigned int bit = 1u << w;
+                d.slotw[(size_t)s * d.wmax + w] = SLOT_NONE;
+                if (wall_distance(wall, d.wgeom + wg, xs, ps.w + sp.interaction_distance, dist, nrm)) {
+                    whit |= bit;
+                    wnew |= bit;
+                } else if (first && (wa & bit)) {
+                    for (int q = 0; q < NCOMP; ++q)
+                        d.whist[nb][whist_at(d.wmax, NCOMP, s, w) + q] = d.whist[c][whist_at(d.wmax, NCOMP, s, w) + q];
+                    wnew |= bit;
+                }
+            }
+        }
+        for (int w = 0; w < d.nwords; ++w) d.act[nb][(size_t)w * d.ncap + s] = newbits[w];
+        d.wact[nb][s] = wnew;
+    }
+    // ---- compact the contacts of the block into the item list ----
+    int nh = __popc(whit);
+#pragma unroll
+    for (int w = 0; w < 4; ++w) nh += __popc(hitbits[w]);
+    int total;
+    const int off = block_exclusive_scan(nh, warp_sums, total);
+    if (threadIdx.x == 0) block_base = total ? (int)atomicAdd(&ctl->n_items, (unsigned)total) : 0;
+    __syncthreads();
+    int q = block_base + off;
+    if (nh == 0) return;
+    if (q + nh > d.item_cap) {
+        atomicOr(&ctl->status, 1u << DEM_ERR_CAPACITY);
+        return;
+    }
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        unsigned int b = hitbits[w];
+        while (b) {
+            const int k = w * 32 + __ffs(b) - 1;
+            b &= b - 1;
+            d.items[q] = make_int2(s, k);
+            d.slot[nbr_at(d.cap, s, k)] = q;
+            ++q;
+        }
+    }
+    unsigned int b = whit;
+    while (b) {
+        const int w = __ffs(b) - 1;
+        b &= b - 1;
+        d.items[q] = make_int2(s, ITEM_WALL + w);
+        d.slotw[(size_t)s * d.wmax + w] = q;
+        ++q;
+    }
+}
+
+template <int MODE, int NLAW, int FLAW, int NCOMP>
+__global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
+{
+    Control* ctl = d.ctl;
+    const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
+    const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
+    const bool record = final_step && ctl->record;
+    const bool first = (MODE == 1) && ctl->first_step;
+    const int n_items = min((int)ctl->n_items, d.item_cap);
+    const double dt = d.dt;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += gridDim.x * blockDim.x) {
+        const int2 item = d.items[q];
+        const int s = item.x, kq = item.y;
+        const double4 ps = d.pr[c][s];
+        const double4 vs = d.vm[c][s];
+        const double4 ws = d.wi[c][s];
+        const int4 is = d.info[c][s];
+        const InstanceDev& I = d.inst[is.z];
+        const int ns = I.n_species;
+        const V3 xq = xyz(ps), vq = xyz(vs), wq = xyz(ws);
+        const double rq = ps.w, mq = vs.w;
+        ContactGeom g;
+        Springs spr;
+        spr.slide = zero3(); spr.roll = zero3(); spr.tors = zero3();
+        const dem_species_pair* spp;
+        bool periodic = false, was_active = false;
+        int tq = 0, pid_i = 0;
+        const bool is_wall = kq >= ITEM_WALL;
+        double* hdst;
+        size_t hb;
+        V3 xt = zero3();
+        if (is_wall) {
+            // DPMBase::computeForcesDueToWalls / BaseWall::getInteractionWith
+            // (DPMBase.cc:3188-3215, BaseWall.cc:367-437)
+            const int wl = kq - ITEM_WALL;
+            const int wg = I.wall_begin + wl;
+            const dem_wall& wall = d.walls[wg];
+            spp = &d.species[I.species_offset + is.y * ns + wall.species];
+            double dist;
+            V3 nrm;
+            wall_distance(wall, d.wgeom + wg, xq, rq + spp->interaction_distance, dist, nrm);
+            g.n = -nrm;
+            g.distance = dist;
+            g.overlap = rq - dist;
+            g.c = xq - (rq - 0.5 * g.overlap) * g.n;
+            g.xp = xq; g.vp = vq; g.wp = wq; g.inv_mass_p = mq; g.curv_p = 1.0 / rq;
+            g.xi = v3(wall.position[0], wall.position[1], wall.position[2]);
+            g.vi = v3(wall.velocity[0], wall.velocity[1], wall.velocity[2]);
+            g.wi = v3(wall.angular_velocity[0], wall.angular_velocity[1], wall.angular_velocity[2]);
+            g.inv_mass_i = 0.0;
+            g.curv_i = 0.0;
+            g.i_is_wall = true;
+            hb = whist_at(d.wmax, NCOMP, s, wl);
+            hdst = d.whist[nb];
+            was_active = (d.wact[c][s] >> wl) & 1u;
+            if (was_active) load_springs(d.whist[c], hb, 1, NCOMP, spr);
+            pid_i = wg;
+        } else {
+            const size_t e = nbr_at(d.cap, s, kq);
+            tq = d.nbr[l][e];
+            const double4 pt = d.pr[c][tq];
+            const int4 it = d.info[c][tq];
+            const double4 vt4 = d.vm[c][tq];
+            const double4 wt4 = d.wi[c][tq];
+            xt = image_of(I, xq, xyz(pt), periodic);
+            // this particle is P: the lower id, or the real particle against
+            // the partner's periodic ghost (DPMBase.cc:3129-3139)
+            const V3 branch = xq - xt;
+            const double d2 = len2(branch);
+            spp = &d.species[I.species_offset + is.y * ns + it.y];
+            g.distance = sqrt(d2);
+            g.n = branch / g.distance;
+            g.overlap = rq + pt.w - g.distance;
+            g.xp = xq; g.vp = vq; g.wp = wq; g.inv_mass_p = mq;
+            g.xi = xt; g.vi = xyz(vt4); g.wi = xyz(wt4); g.inv_mass_i = vt4.w;
+            g.c = g.xp - (rq - 0.5 * g.overlap) * g.n;
+            g.curv_p = 1.0 / rq;
+            g.curv_i = 1.0 / pt.w;
+            g.i_is_wall = false;
+            hb = hist_at(d.cap, NCOMP, s, kq);
+            hdst = d.hist[nb];
+            was_active = (d.act[c][(size_t)(kq >> 5) * d.ncap + s] >> (kq & 31)) & 1u;
+            // the higher-id side of a periodic pair restarts every step from the
+            // reversed spring of the lower-id side (InteractionHandler.cc:316-368,
+            // BaseInteraction::copySwitchPointer / reverseHistory)
+            const bool derived = periodic && (is.x > it.x);
+            if (derived) {
+                const int m = d.rev[e];
+                if ((d.act[c][(size_t)(m >> 5) * d.ncap + tq] >> (m & 31)) & 1u) {
+                    load_springs(d.hist[c], hist_at(d.cap, NCOMP, tq, m), 1, NCOMP, spr);
+                    spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
+                }
+            } else if (was_active) {
+                load_springs(d.hist[c], hb, 1, NCOMP, spr);
+            }
+            pid_i = it.x;
+        }
+        const Springs before = spr;
+        ContactOut out;
+        evaluate_contact<NLAW, FLAW>(*spp, g, spr, dt, out);
+        // step 0 keeps the lower-id side's old spring of a periodic pair that
+        // existed at the initial evaluation (equal stamps, InteractionHandler.cc:339-352)
+        const Springs& kept = (first && periodic && !(is.x > pid_i) && was_active) ? before : spr;
+        store_springs(hdst, hb, 1, NCOMP, kept);
+        double* sh = d.shares + (size_t)q * SHARE;
+        const V3 tp = out.torque - cross(xq - g.c, out.force);
+        sh[0] = out.force.x; sh[1] = out.force.y; sh[2] = out.force.z;
+        sh[3] = tp.x; sh[4] = tp.y; sh[5] = tp.z;
+        if (!is_wall && !periodic) { // I's share of an ordinary pair, announced in I's own entry
+            const V3 fi = -out.force;
+            const V3 ti = -out.torque + cross(xt - g.c, out.force);
+            sh[6] = fi.x; sh[7] = fi.y; sh[8] = fi.z;
+            sh[9] = ti.x; sh[10] = ti.y; sh[11] = ti.z;
+            d.slot[nbr_at(d.cap, tq, d.rev[nbr_at(d.cap, s, kq)])] = SLOT_I_BASE - q;
+        }
+        if (record && (is_wall || !periodic || is.x < pid_i)) {
+            const double meff = 1.0 / (g.inv_mass_p + g.inv_mass_i);
+            write_record(d, is.x, pid_i, is_wall ? 1 : 0, periodic ? 1 : 0, s, is_wall ? pid_i : tq, g, out, kept,
+                         spring_energy(*spp, kept, meff));
+        }
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(SUM_BLOCK) k_sum(DevPtrs d)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    Control* ctl = d.ctl;
+    const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
+    const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
+    const double dt = d.dt;
+    if (s == 0) ctl->n_items = 0u; // k_contacts is done: the next evaluation starts a new list
+    double disp2 = 0.0;
+    if (s < d.n) {
+        const double4 ps = d.pr[c][s];
+        const double4 vs = d.vm[c][s];
+        const double4 ws = d.wi[c][s];
+        double4 qs = d.qo[c][s];
+        const int4 is = d.info[c][s];
+        const InstanceDev& I = d.inst[is.z];
+        // ---- the shares in list order, the body force, the wall shares ----
+        V3 F = zero3(), T = zero3();
+        const int count = min(d.cnt[l][s], d.cap);
+        for (int k = 0; k < count; ++k) {
+            int q = d.slot[nbr_at(d.cap, s, k)];
+            int half = 0;
+            if (q <= SLOT_I_BASE) {
+                q = SLOT_I_BASE - q;
+                half = 6;
+            }
+            if (q < 0) continue;
+            const double* sh = d.shares + (size_t)q * SHARE + half;
+            F += v3(sh[0], sh[1], sh[2]);
+            T += v3(sh[3], sh[4], sh[5]);
+        }
+        if (!(is.w & FLAG_FIXED)) { // DPMBase::computeExternalForces (DPMBase.cc:3168-3179)
+            const double m = 1.0 / vs.w;
+            F += v3(I.gravity[0], I.gravity[1], I.gravity[2]) * m - d.drag * xyz(vs);
+            const int nw = I.wall_end - I.wall_begin;
+            for (int w = 0; w < nw; ++w) {
+                const int q = d.slotw[(size_t)s * d.wmax + w];
+                if (q < 0) continue;
+                const double* sh = d.shares + (size_t)q * SHARE;
+                F += v3(sh[0], sh[1], sh[2]);
+                T += v3(sh[3], sh[4], sh[5]);
+            }
+        }
+        if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z))) atomicOr(&ctl->status, 1u << DEM_ERR_NAN);
+
+        // ---- integration ----
+        double4 pn = ps, vn = vs, wn = ws;
+        if (final_step) {
+            d.force[3 * (size_t)s + 0] = F.x;
+            d.force[3 * (size_t)s + 1] = F.y;
+            d.force[3 * (size_t)s + 2] = F.z;
+            d.torque[3 * (size_t)s + 0] = T.x;
+            d.torque[3 * (size_t)s + 1] = T.y;
+            d.torque[3 * (size_t)s + 2] = T.z;
+        }
+        if (MODE == 1) {
+            V3 x = xyz(ps), v = xyz(vs), w = xyz(ws);
+            Q4 q{qs.x, qs.y, qs.z, qs.w};
+            if (vs.w != 0.0) {
+                const V3 a = ((F * vs.w) * 0.5) * dt;
+                v += a; // BaseParticle::integrateAfterForceComputation
+                V3 aw = zero3();
+                if (d.rotation) {
+                    const S33 Ib{ws.w, 0.0, 0.0, ws.w, 0.0, ws.w};
+                    aw = ((rotate_inverse_inertia(q, Ib) * T) * 0.5) * dt;
+                    w += aw;
+                }
+                if (!final_step) { // BaseParticle::integrateBeforeForceComputation of the next step
+                    v += a;
+                    const V3 disp = v * dt;
+                    x += disp;
+                    disp2 = len2(disp);
+                    if (d.rotation) {
+                        w += aw;
+                        q = quat_rotate(q, w * dt);
+                    }
+                }
+            } else if (!final_step) { // BaseInteractable::integrateBeforeForceComputation
+                const V3 disp = v * dt;
+                x += disp;
+                disp2 = len2(disp);
+                q = quat_rotate(q, w * dt);
+            }
+            if (!final_step && I.per_mask) { // PeriodicBoundary::checkBoundaryAfterParticlesMove
+                double* xc = &x.x;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if ((I.per_mask >> k) & 1u) {
+                        const double dl = xc[k] - I.per_lo[k], dr = I.per_hi[k] - xc[k];
+                        if ((dl < dr ? dl : dr) < 0) {
+                            if (I.per_hi[k] - xc[k] > xc[k] - I.per_lo[k])
+                                xc[k] = xc[k] + I.per_L[k];
+                            else
+                                xc[k] = xc[k] - I.per_L[k];
+                        }
+                    }
+                }
+            }
+            pn = make_double4(x.x, x.y, x.z, ps.w);
+            vn = make_double4(v.x, v.y, v.z, vs.w);
+            wn = make_double4(w.x, w.y, w.z, ws.w);
+            qs = make_double4(q.q0, q.q1, q.q2, q.q3);
+        }
+        int4 isn = is;
+        if (MODE == 1 && !final_step && I.n_del && !(is.w & FLAG_DELETED) && deletion_check(I, xyz(pn))) {
+            park_deleted(ctl, pn, vn, wn, isn);
+            disp2 = 0.0;
+        }
+        d.pr[nb][s] = pn;
+        d.vm[nb][s] = vn;
+        d.wi[nb][s] = wn;
+        d.qo[nb][s] = qs;
+        d.info[nb][s] = isn;
+        d.caller[nb][s] = d.caller[c][s];
+    }
+    if (MODE == 1) { // maximum displacement of this step (for the skin test)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) disp2 = fmax(disp2, __shfl_xor_sync(0xffffffffu, disp2, o));
+        if ((threadIdx.x & 31) == 0 && disp2 > 0.0)
+            atomicMax(&ctl->step_disp2_bits, (unsigned long long)__double_as_longlong(disp2));
+    }
+}
+
+} // namespace dem

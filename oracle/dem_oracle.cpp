@@ -49,8 +49,12 @@ struct Particle {
 };
 
 // Persistent interaction (InteractionHandler object). Key: (kind, P id, I id)
-// kind 0: particle pair (P, I real ids); 1: P real vs ghost of I (P's view);
-// 2: wall (P particle, I wall index).
+// kind 0: particle pair, P the lower id -- an ordinary pair, or the lower-id
+//         particle's view of a periodic pair: after removeDuplicatePeriodicParticles
+//         that view is the real-real interaction (InteractionHandler.cc:316-368),
+//         so a pair that stops or starts being periodic keeps its spring;
+// kind 1: the higher-id particle's view of a periodic pair (P real vs ghost of I);
+// kind 2: wall (P particle, I wall index).
 struct Inter {
     Springs s;
     unsigned stamp;
@@ -292,11 +296,22 @@ struct Sim {
         const dem_species_pair& s = sp(P.species, I.species);
         const double sum = I.r + P.r + s.interaction_distance;
         if (d2 >= sum * sum) return;
-        const auto key = std::make_tuple(ghost ? 1 : 0, P.id, I.id);
+        const auto key = std::make_tuple((ghost && P.id > I.id) ? 1 : 0, P.id, I.id);
         auto it = inter.find(key);
         if (it == inter.end()) {
             Inter n{};
             n.s = Springs{zero3(), zero3(), zero3()};
+            if (std::get<0>(key) == 1) {
+                // the ghost of the lower-id particle carries a copy of its
+                // interaction with the real pair, history reversed
+                // (BaseInteraction::copySwitchPointer, BaseInteraction.cc:340-356)
+                auto pb = before.find(std::make_tuple(0, I.id, P.id));
+                if (pb != before.end()) {
+                    n.s.slide = -pb->second.second.slide;
+                    n.s.roll = -pb->second.second.roll;
+                    n.s.tors = -pb->second.second.tors;
+                }
+            }
             it = inter.emplace(key, n).first;
         }
         Inter& c = it->second;
@@ -486,7 +501,7 @@ struct Sim {
     {
         before.clear();
         for (auto& kv : inter)
-            if (std::get<0>(kv.first) == 1 && std::get<1>(kv.first) < std::get<2>(kv.first))
+            if (std::get<0>(kv.first) == 0)
                 before[kv.first] = {kv.second.stamp, kv.second.s};
     }
 
@@ -499,9 +514,9 @@ struct Sim {
     void periodic_handover()
     {
         for (auto& kv : inter) {
-            if (std::get<0>(kv.first) != 1) continue;
+            // the lower-id view of a pair that is periodic in this evaluation
+            if (std::get<0>(kv.first) != 0 || !kv.second.periodic || kv.second.eval != evals) continue;
             const int a = std::get<1>(kv.first), b = std::get<2>(kv.first);
-            if (a > b) continue;
             auto pb = before.find(kv.first);
             if (pb != before.end() && pb->second.first == kv.second.stamp) kv.second.s = pb->second.second;
             auto other = inter.find(std::make_tuple(1, b, a));
@@ -623,7 +638,8 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
             if (wall) {
                 S.inter[std::make_tuple(2, contacts_in->id_p[r], contacts_in->id_i[r])] = c;
             } else if (per) {
-                S.inter[std::make_tuple(1, contacts_in->id_p[r], contacts_in->id_i[r])] = c;
+                c.periodic = true;
+                S.inter[std::make_tuple(0, contacts_in->id_p[r], contacts_in->id_i[r])] = c;
                 Inter o = c;
                 o.s.slide = -c.s.slide; o.s.roll = -c.s.roll; o.s.tors = -c.s.tors;
                 S.inter[std::make_tuple(1, contacts_in->id_i[r], contacts_in->id_p[r])] = o;
@@ -679,12 +695,12 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
         } else if (kv.second.eval != S.evals) {
             continue; // only contacts of the last force evaluation
         }
-        if (kind == 1 && a > b) continue; // the kept view of a periodic pair
+        if (kind == 1) continue; // the higher-id view of a periodic pair is not kept
         if (contacts_out && cnt < contacts_capacity) {
             contacts_out->id_p[cnt] = a;
             contacts_out->id_i[cnt] = b;
             if (contacts_out->is_wall) contacts_out->is_wall[cnt] = kind == 2;
-            if (contacts_out->periodic) contacts_out->periodic[cnt] = kind == 1;
+            if (contacts_out->periodic) contacts_out->periodic[cnt] = kind == 0 && kv.second.periodic;
             if (contacts_out->overlap) contacts_out->overlap[cnt] = kv.second.overlap;
             if (contacts_out->force) {
                 contacts_out->force[3 * cnt] = kv.second.force.x;

@@ -154,3 +154,17 @@ def test_reupload_same_and_other_size(gpu):
     e.close()
     np.testing.assert_array_equal(out2["position"], ref2["position"])
     np.testing.assert_array_equal(out2["velocity"], ref2["velocity"])
+
+
+def test_periodic_chute_long_horizon(gpu):
+    """300 steps of the periodic chute: pairs cross the periodic boundaries
+    and back, so a contact changes between a periodic pair (two views, each
+    particle P of its own) and an ordinary pair (one interaction, the lower
+    id is P); the spring must follow the reference's single interaction."""
+    sc = cases.small_chute()
+    g = H.run_gpu(sc, 300)
+    o = H.run_oracle(sc, 300)
+    _same_pairs(g, o)
+    assert H.rel_err(g["position"], o["position"], 1e-3) < 1e-11
+    assert H.rel_err(g["force"], o["force"]) < 1e-6
+    assert H.rel_err(g["contacts"]["springs"], o["contacts"]["springs"]) < 1e-6

@@ -110,3 +110,18 @@ def test_oracle_matches_reference_heap():
     assert H.rel_err(o["force"], r["force"]) < 1e-12
     assert H.rel_err(o["position"], r["position"], 1e-3) < 1e-13
     assert H.rel_err(o["contacts"]["springs"], r["contacts"]["springs"]) < 1e-11
+
+
+@needs_ref
+def test_oracle_matches_reference_periodic_transitions():
+    """300 steps of the periodic chute: contacts cross the periodic boundaries,
+    turning ordinary pairs into periodic ones and back. The reference keeps
+    one real-real interaction (the lower index's view,
+    InteractionHandler::removeObjectKeepingPeriodics) and gives the other
+    particle's ghost a reversed copy (BaseInteraction::copySwitchPointer)."""
+    sc = cases.small_chute()
+    o = H.run_oracle(sc, 300)
+    r = H.run_reference(sc, 300)
+    assert H.pair_set(o["contacts"]) == H.pair_set(r["contacts"])
+    assert H.rel_err(o["force"], r["force"]) < 1e-12
+    assert H.rel_err(o["position"], r["position"], 1e-3) < 1e-13

@@ -745,9 +745,9 @@ int dem_upload_contacts(dem_handle* hh, const dem_contacts_soa* cs)
     };
     auto set_entry = [&](int s, int t, const double* spr, double sign) -> bool {
         for (int k = 0; k < cnt[s]; ++k) {
-            if (nbr[nbr_at(d.cap, s, k)] != t) continue;
+            if (nbr[nbr_at(d.ncap, s, k)] != t) continue;
             for (int comp = 0; comp < d.ncomp; ++comp)
-                hist[hist_at(d.cap, d.ncomp, s, k) + comp] = sign * spr[comp];
+                hist[hist_at(d.ncap, d.ncomp, s, k) + comp] = sign * spr[comp];
             act[(size_t)(k >> 5) * NC + s] |= 1u << (k & 31);
             return true;
         }
@@ -766,7 +766,7 @@ int dem_upload_contacts(dem_handle* hh, const dem_contacts_soa* cs)
             const int w = h->wall_grouped[wc] - h->inst[in].wall_begin;
             if (w < 0 || w >= h->inst[in].wall_end - h->inst[in].wall_begin)
                 return fail(h, DEM_ERR_BAD_INPUT, "contact refers to a wall outside the particle's instance");
-            for (int comp = 0; comp < d.ncomp; ++comp) whist[whist_at(d.wmax, d.ncomp, sp, w) + comp] = spr[comp];
+            for (int comp = 0; comp < d.ncomp; ++comp) whist[whist_at(d.ncap, d.ncomp, sp, w) + comp] = spr[comp];
             wact[sp] |= 1u << w;
             continue;
         }

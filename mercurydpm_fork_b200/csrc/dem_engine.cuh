@@ -101,14 +101,17 @@ struct Control {
     unsigned int pad2;
 };
 
-__host__ __device__ __forceinline__ size_t nbr_at(int cap, int i, int k) { return (size_t)i * cap + k; }
-__host__ __device__ __forceinline__ size_t hist_at(int cap, int ncomp, int i, int k)
+// Entry-major layouts: entry k of every particle is contiguous, so threads
+// of consecutive particles touch consecutive words; the spring components of
+// one entry are contiguous (one sector for a contact's history).
+__host__ __device__ __forceinline__ size_t nbr_at(int ncap, int i, int k) { return (size_t)k * ncap + i; }
+__host__ __device__ __forceinline__ size_t hist_at(int ncap, int ncomp, int i, int k)
 {
-    return ((size_t)i * cap + k) * ncomp;
+    return ((size_t)k * ncap + i) * ncomp;
 }
-__host__ __device__ __forceinline__ size_t whist_at(int wmax, int ncomp, int i, int w)
+__host__ __device__ __forceinline__ size_t whist_at(int ncap, int ncomp, int i, int w)
 {
-    return ((size_t)i * wmax + w) * ncomp;
+    return ((size_t)w * ncap + i) * ncomp;
 }
 
 struct DevPtrs {

@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
                         const double cut = ps.w + pt.w + extra;
                         if (len2(br) < cut * cut) {
                             if (count < d.cap) {
-                                d.nbr[ln][nbr_at(d.cap, s, count)] = t;
+                                d.nbr[ln][nbr_at(d.ncap, s, count)] = t;
                             } else {
                                 overflow = true;
                             }
@@ -359,10 +359,10 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
             bits &= bits - 1;
             const int k = w * 32 + b;
             if (k >= ocnt) break;
-            const int tnew = d.newidx[d.nbr[lo_][nbr_at(d.cap, o, k)]];
+            const int tnew = d.newidx[d.nbr[lo_][nbr_at(d.ncap, o, k)]];
             int m = -1;
             for (int q = 0; q < count; ++q) {
-                if (d.nbr[ln][nbr_at(d.cap, s, q)] == tnew) {
+                if (d.nbr[ln][nbr_at(d.ncap, s, q)] == tnew) {
                     m = q;
                     break;
                 }
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
                 continue;
             }
             for (int comp = 0; comp < d.ncomp; ++comp)
-                d.hist[nb][hist_at(d.cap, d.ncomp, s, m) + comp] = d.hist[hc][hist_at(d.cap, d.ncomp, o, k) + comp];
+                d.hist[nb][hist_at(d.ncap, d.ncomp, s, m) + comp] = d.hist[hc][hist_at(d.ncap, d.ncomp, o, k) + comp];
             neww[m >> 5] |= 1u << (m & 31);
         }
     }
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
         const int w = __ffs(bits) - 1;
         bits &= bits - 1;
         for (int comp = 0; comp < d.ncomp; ++comp)
-            d.whist[nb][whist_at(d.wmax, d.ncomp, s, w) + comp] = d.whist[hc][whist_at(d.wmax, d.ncomp, o, w) + comp];
+            d.whist[nb][whist_at(d.ncap, d.ncomp, s, w) + comp] = d.whist[hc][whist_at(d.ncap, d.ncomp, o, w) + comp];
     }
 }
 

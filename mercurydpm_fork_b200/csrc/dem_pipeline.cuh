@@ -44,15 +44,15 @@ __global__ void __launch_bounds__(256) k_rev(DevPtrs d)
     const int l = d.ctl->lbuf;
     const int cnt = d.cnt[l][s];
     for (int k = 0; k < cnt && k < d.cap; ++k) {
-        const int t = d.nbr[l][nbr_at(d.cap, s, k)];
+        const int t = d.nbr[l][nbr_at(d.ncap, s, k)];
         const int ct = min(d.cnt[l][t], d.cap);
         int m = 0;
-        while (m < ct && d.nbr[l][nbr_at(d.cap, t, m)] != s) ++m;
+        while (m < ct && d.nbr[l][nbr_at(d.ncap, t, m)] != s) ++m;
         if (m == ct) {
             atomicOr(&d.ctl->status, 1u << DEM_ERR_CAPACITY); // an asymmetric pair: the partner's row overflowed
             m = 0;
         }
-        d.rev[nbr_at(d.cap, s, k)] = m;
+        d.rev[nbr_at(d.ncap, s, k)] = m;
     }
 }
 
@@ -101,25 +101,26 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         count = min(d.cnt[l][s], d.cap);
         const int ns = I.n_species;
         constexpr int B = 4; // entries whose gathers are in flight together
+        const int2* info2 = reinterpret_cast<const int2*>(d.info[c]); // (id, species) of each info record
         for (int k0 = 0; k0 < count; k0 += B) {
         int tb[B];
         double4 ptb[B];
-        int4 itb[B];
+        int2 itb[B];
 #pragma unroll
-        for (int j = 0; j < B; ++j) tb[j] = (k0 + j < count) ? d.nbr[l][nbr_at(d.cap, s, k0 + j)] : -1;
+        for (int j = 0; j < B; ++j) tb[j] = (k0 + j < count) ? d.nbr[l][nbr_at(d.ncap, s, k0 + j)] : -1;
 #pragma unroll
         for (int j = 0; j < B; ++j)
             if (tb[j] >= 0) {
                 ptb[j] = d.pr[c][tb[j]];
-                itb[j] = d.info[c][tb[j]];
+                itb[j] = info2[2 * (size_t)tb[j]];
             }
 #pragma unroll
         for (int j = 0; j < B; ++j) {
             const int k = k0 + j;
             if (k >= count) break;
-            const size_t e = nbr_at(d.cap, s, k);
+            const size_t e = nbr_at(d.ncap, s, k);
             const double4 pt = ptb[j];
-            const int4 it = itb[j];
+            const int2 it = itb[j];
             bool periodic;
             const V3 xt = image_of(I, xs, xyz(pt), periodic);
             if (!periodic && !(is.x < it.x)) { // the partner (lower id) owns this pair
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
                 // an interaction of the initial evaluation outlives step 0
                 // (InteractionHandler::eraseOldInteractions erases stamps <= 0 only)
                 for (int q = 0; q < NCOMP; ++q)
-                    d.hist[nb][hist_at(d.cap, NCOMP, s, k) + q] = d.hist[c][hist_at(d.cap, NCOMP, s, k) + q];
+                    d.hist[nb][hist_at(d.ncap, NCOMP, s, k) + q] = d.hist[c][hist_at(d.ncap, NCOMP, s, k) + q];
                 newbits[k >> 5] |= bit;
             }
         }
@@ -155,13 +156,13 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
                 double dist;
                 V3 nrm;
                 const unsigned int bit = 1u << w;
-                d.slotw[(size_t)s * d.wmax + w] = SLOT_NONE;
+                d.slotw[(size_t)w * d.ncap + s] = SLOT_NONE;
                 if (wall_distance(wall, d.wgeom + wg, xs, ps.w + sp.interaction_distance, dist, nrm)) {
                     whit |= bit;
                     wnew |= bit;
                 } else if (first && (wa & bit)) {
                     for (int q = 0; q < NCOMP; ++q)
-                        d.whist[nb][whist_at(d.wmax, NCOMP, s, w) + q] = d.whist[c][whist_at(d.wmax, NCOMP, s, w) + q];
+                        d.whist[nb][whist_at(d.ncap, NCOMP, s, w) + q] = d.whist[c][whist_at(d.ncap, NCOMP, s, w) + q];
                     wnew |= bit;
                 }
             }
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
             const int k = w * 32 + __ffs(b) - 1;
             b &= b - 1;
             d.items[q] = make_int2(s, k);
-            d.slot[nbr_at(d.cap, s, k)] = q;
+            d.slot[nbr_at(d.ncap, s, k)] = q;
             ++q;
         }
     }
@@ -199,7 +200,7 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         const int w = __ffs(b) - 1;
         b &= b - 1;
         d.items[q] = make_int2(s, ITEM_WALL + w);
-        d.slotw[(size_t)s * d.wmax + w] = q;
+        d.slotw[(size_t)w * d.ncap + s] = q;
         ++q;
     }
 }
@@ -256,13 +257,13 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             g.inv_mass_i = 0.0;
             g.curv_i = 0.0;
             g.i_is_wall = true;
-            hb = whist_at(d.wmax, NCOMP, s, wl);
+            hb = whist_at(d.ncap, NCOMP, s, wl);
             hdst = d.whist[nb];
             was_active = (d.wact[c][s] >> wl) & 1u;
             if (was_active) load_springs(d.whist[c], hb, 1, NCOMP, spr);
             pid_i = wg;
         } else {
-            const size_t e = nbr_at(d.cap, s, kq);
+            const size_t e = nbr_at(d.ncap, s, kq);
             tq = d.nbr[l][e];
             const double4 pt = d.pr[c][tq];
             const int4 it = d.info[c][tq];
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             g.curv_p = 1.0 / rq;
             g.curv_i = 1.0 / pt.w;
             g.i_is_wall = false;
-            hb = hist_at(d.cap, NCOMP, s, kq);
+            hb = hist_at(d.ncap, NCOMP, s, kq);
             hdst = d.hist[nb];
             was_active = (d.act[c][(size_t)(kq >> 5) * d.ncap + s] >> (kq & 31)) & 1u;
             // the higher-id side of a periodic pair restarts every step from the
@@ -293,7 +294,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             if (derived) {
                 const int m = d.rev[e];
                 if ((d.act[c][(size_t)(m >> 5) * d.ncap + tq] >> (m & 31)) & 1u) {
-                    load_springs(d.hist[c], hist_at(d.cap, NCOMP, tq, m), 1, NCOMP, spr);
+                    load_springs(d.hist[c], hist_at(d.ncap, NCOMP, tq, m), 1, NCOMP, spr);
                     spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
                 }
             } else if (was_active) {
@@ -317,7 +318,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             const V3 ti = -out.torque + cross(xt - g.c, out.force);
             sh[6] = fi.x; sh[7] = fi.y; sh[8] = fi.z;
             sh[9] = ti.x; sh[10] = ti.y; sh[11] = ti.z;
-            d.slot[nbr_at(d.cap, tq, d.rev[nbr_at(d.cap, s, kq)])] = SLOT_I_BASE - q;
+            d.slot[nbr_at(d.ncap, tq, d.rev[nbr_at(d.ncap, s, kq)])] = SLOT_I_BASE - q;
         }
         if (record && (is_wall || !periodic || is.x < pid_i)) {
             const double meff = 1.0 / (g.inv_mass_p + g.inv_mass_i);
@@ -347,24 +348,39 @@ __global__ void __launch_bounds__(SUM_BLOCK) k_sum(DevPtrs d)
         // ---- the shares in list order, the body force, the wall shares ----
         V3 F = zero3(), T = zero3();
         const int count = min(d.cnt[l][s], d.cap);
-        for (int k = 0; k < count; ++k) {
-            int q = d.slot[nbr_at(d.cap, s, k)];
-            int half = 0;
-            if (q <= SLOT_I_BASE) {
-                q = SLOT_I_BASE - q;
-                half = 6;
+        constexpr int B = 4; // slots read together, then their shares
+        for (int k0 = 0; k0 < count; k0 += B) {
+            int qs_[B];
+#pragma unroll
+            for (int j = 0; j < B; ++j) qs_[j] = (k0 + j < count) ? d.slot[nbr_at(d.ncap, s, k0 + j)] : SLOT_NONE;
+            double sh6[B][6];
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                int q = qs_[j];
+                int half = 0;
+                if (q <= SLOT_I_BASE) {
+                    q = SLOT_I_BASE - q;
+                    half = 6;
+                }
+                if (q >= 0) {
+                    const double* sh = d.shares + (size_t)q * SHARE + half;
+#pragma unroll
+                    for (int u = 0; u < 6; ++u) sh6[j][u] = sh[u];
+                }
             }
-            if (q < 0) continue;
-            const double* sh = d.shares + (size_t)q * SHARE + half;
-            F += v3(sh[0], sh[1], sh[2]);
-            T += v3(sh[3], sh[4], sh[5]);
+#pragma unroll
+            for (int j = 0; j < B; ++j) // in list order
+                if (qs_[j] >= 0 || qs_[j] <= SLOT_I_BASE) {
+                    F += v3(sh6[j][0], sh6[j][1], sh6[j][2]);
+                    T += v3(sh6[j][3], sh6[j][4], sh6[j][5]);
+                }
         }
         if (!(is.w & FLAG_FIXED)) { // DPMBase::computeExternalForces (DPMBase.cc:3168-3179)
             const double m = 1.0 / vs.w;
             F += v3(I.gravity[0], I.gravity[1], I.gravity[2]) * m - d.drag * xyz(vs);
             const int nw = I.wall_end - I.wall_begin;
             for (int w = 0; w < nw; ++w) {
-                const int q = d.slotw[(size_t)s * d.wmax + w];
+                const int q = d.slotw[(size_t)w * d.ncap + s];
                 if (q < 0) continue;
                 const double* sh = d.shares + (size_t)q * SHARE;
                 F += v3(sh[0], sh[1], sh[2]);

@@ -104,18 +104,20 @@ def measured_peak():
 
 
 def force_kernel_bytes(n, nwords, entries, contacts, wall_contacts, ncomp=3):
-    """Algorithmic bytes of one time-step force kernel launch (compulsory traffic).
+    """Algorithmic bytes of one time-step force evaluation (compulsory traffic
+    of k_detect + k_contacts + k_sum).
 
     per particle: read pr, vm, wi, qo (4 x 32 B) + info (16 B) + caller (4 B),
                   write the same 6 arrays to the other buffer (148 B),
                   active-bit words read + written (8 B x words), wall bits (8 B);
     per neighbour-list entry: its index (4 B);
-    per contact side (a particle pair has two sides, a wall contact one):
+    per contact (a particle pair once, a wall contact once):
                   spring history read + written (2 x 8 B x ncomp).
-    Neighbour state gathers are cache hits (sorted order) and not counted.
+    Neighbour state gathers are cache hits (sorted order) and not counted, nor
+    is the compact contact list the three kernels pass between them.
     """
     per_particle = (4 * 32 + 16 + 4) + (4 * 32 + 16 + 4) + 8 * nwords + 8
-    return n * per_particle + 4 * entries + (2 * contacts + wall_contacts) * 2 * 8 * ncomp
+    return n * per_particle + 4 * entries + (contacts + wall_contacts) * 2 * 8 * ncomp
 
 
 def run_ours(args):
@@ -216,7 +218,7 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": "particle-timesteps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "k_force<1> (force + integration)", "peak_source": peak_kind,
+                     "traffic": traffic, "kernel": "force evaluation: k_detect + k_contacts + k_sum (force + integration)", "peak_source": peak_kind,
                      "bytes_per_launch": fk_bytes, "launch_ms": fk_ms},
         "cpu_baseline": cpu,
         "gpu_launches": launches,

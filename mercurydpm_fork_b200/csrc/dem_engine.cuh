@@ -141,7 +141,7 @@ struct DevPtrs {
     int *rev;                // reverse index of the neighbour lists, n * cap
     int *slot;               // per entry: item index, or SLOT_NONE / SLOT_IS_I
     int *slotw;              // per (particle, wall): item index or SLOT_NONE
-    int2 *items;             // (particle, entry or ITEM_WALL + wall)
+    int4 *items;             // (particle, entry or ITEM_WALL + wall, partner slot, 0)
     double *shares;          // 12 doubles per item
     int item_cap;
     Control *ctl;

@@ -89,6 +89,9 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
     const bool first = (MODE == 1) && ctl->first_step;
     const bool active = s < d.n;
     unsigned int hitbits[4] = {0u, 0u, 0u, 0u}, newbits[4] = {0u, 0u, 0u, 0u};
+    constexpr int HIT_KEEP = 16; // partner slots of the first hits, kept for the item pass
+    int hit_t[HIT_KEEP];
+    int nkept = 0;
     unsigned int whit = 0u, wnew = 0u;
     int count = 0, nwalls = 0;
     if (active) {
@@ -136,6 +139,7 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
             const unsigned int bit = 1u << (k & 31);
             if (!(d2 >= sum * sum)) {
                 hitbits[k >> 5] |= bit;
+                if (nkept < HIT_KEEP) hit_t[nkept++] = tb[j];
                 newbits[k >> 5] |= bit;
             } else if (first && (a[k >> 5] & bit) && !(periodic && is.x > it.x)) {
                 // an interaction of the initial evaluation outlives step 0
@@ -184,13 +188,16 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         atomicOr(&ctl->status, 1u << DEM_ERR_CAPACITY);
         return;
     }
+    int nh_seen = 0;
 #pragma unroll
     for (int w = 0; w < 4; ++w) {
         unsigned int b = hitbits[w];
         while (b) {
             const int k = w * 32 + __ffs(b) - 1;
             b &= b - 1;
-            d.items[q] = make_int2(s, k);
+            const int t = (nh_seen < HIT_KEEP) ? hit_t[nh_seen] : d.nbr[l][nbr_at(d.ncap, s, k)];
+            ++nh_seen;
+            d.items[q] = make_int4(s, k, t, 0);
             d.slot[nbr_at(d.ncap, s, k)] = q;
             ++q;
         }
@@ -199,7 +206,7 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
     while (b) {
         const int w = __ffs(b) - 1;
         b &= b - 1;
-        d.items[q] = make_int2(s, ITEM_WALL + w);
+        d.items[q] = make_int4(s, ITEM_WALL + w, -1, 0);
         d.slotw[(size_t)w * d.ncap + s] = q;
         ++q;
     }
@@ -216,7 +223,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
     const int n_items = min((int)ctl->n_items, d.item_cap);
     const double dt = d.dt;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += gridDim.x * blockDim.x) {
-        const int2 item = d.items[q];
+        const int4 item = d.items[q];
         const int s = item.x, kq = item.y;
         const double4 ps = d.pr[c][s];
         const double4 vs = d.vm[c][s];
@@ -264,7 +271,10 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             pid_i = wg;
         } else {
             const size_t e = nbr_at(d.ncap, s, kq);
-            tq = d.nbr[l][e];
+            tq = item.z;
+            hb = hist_at(d.ncap, NCOMP, s, kq);
+            Springs own; // read before the active bit is known: one less dependent load
+            load_springs(d.hist[c], hb, 1, NCOMP, own);
             const double4 pt = d.pr[c][tq];
             const int4 it = d.info[c][tq];
             const double4 vt4 = d.vm[c][tq];
@@ -284,7 +294,6 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             g.curv_p = 1.0 / rq;
             g.curv_i = 1.0 / pt.w;
             g.i_is_wall = false;
-            hb = hist_at(d.ncap, NCOMP, s, kq);
             hdst = d.hist[nb];
             was_active = (d.act[c][(size_t)(kq >> 5) * d.ncap + s] >> (kq & 31)) & 1u;
             // the higher-id side of a periodic pair restarts every step from the
@@ -298,7 +307,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
                     spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
                 }
             } else if (was_active) {
-                load_springs(d.hist[c], hb, 1, NCOMP, spr);
+                spr = own;
             }
             pid_i = it.x;
         }

@@ -171,7 +171,7 @@ typedef struct dem_config {
     int32_t  device;               /* CUDA device ordinal                            */
     int32_t  max_neighbors;        /* neighbour-list capacity per particle (0: auto) */
     int32_t  use_graphs;           /* capture the step loop in CUDA graphs           */
-    double   skin;                 /* Verlet skin distance (0: auto)                 */
+    double   skin;                 /* Verlet skin distance (0: 0.4 x smallest radius)*/
     int32_t  n_instances;          /* >= 1                                           */
     int32_t  reserved;
 } dem_config;

@@ -483,7 +483,9 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     for (int in = 0; in < ninst; ++in) wmax = std::max(wmax, wend[in] - wbegin[in]);
     // ---- skin and levels
     double skin = h->cfg.skin;
-    if (!(skin > 0.0)) skin = (n > 0) ? 0.2 * rmin_all : 1e-3;
+    // auto: 0.4 of the smallest radius (measured on the 200k chute: 0.2 rebuilds
+    // every 9 steps and costs 7 % more per step; the evaluation grows only 3 %)
+    if (!(skin > 0.0)) skin = (n > 0) ? 0.4 * rmin_all : 1e-3;
     h->inst.assign(ninst, InstanceDev{});
     std::vector<int> level(n, 0);
     int cell_base = 0;

@@ -316,15 +316,30 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
             const int wz = ((I.per_mask >> 2) & 1u) ? wrap_cell(cz, dz) : cz;
             for (int cy = lo[1]; cy <= hi[1]; ++cy) {
                 const int wy = ((I.per_mask >> 1) & 1u) ? wrap_cell(cy, dy) : cy;
-                for (int cx = lo[0]; cx <= hi[0]; ++cx) {
-                    const int wx = (I.per_mask & 1u) ? wrap_cell(cx, dx) : cx;
-                    const int cell = I.cell_base[lvl] + (wz * dy + wy) * dx + wx;
-                    const int b = d.cell_start[cell], e = d.cell_start[cell + 1];
+                const int row = I.cell_base[lvl] + (wz * dy + wy) * dx;
+                // the x cells of a row are consecutive: their members form one
+                // slot range (two when a periodic row wraps)
+                int seg_lo[2], seg_hi[2], nseg = 1;
+                seg_lo[0] = lo[0];
+                seg_hi[0] = hi[0];
+                if (I.per_mask & 1u) {
+                    if (lo[0] < 0) {
+                        seg_lo[0] = lo[0] + dx; seg_hi[0] = dx - 1;
+                        seg_lo[1] = 0; seg_hi[1] = hi[0];
+                        nseg = 2;
+                    } else if (hi[0] >= dx) {
+                        seg_lo[0] = lo[0]; seg_hi[0] = dx - 1;
+                        seg_lo[1] = 0; seg_hi[1] = hi[0] - dx;
+                        nseg = 2;
+                    }
+                }
+                for (int g = 0; g < nseg; ++g) {
+                    const int b = d.cell_start[row + seg_lo[g]], e = d.cell_start[row + seg_hi[g] + 1];
                     for (int t = b; t < e; ++t) {
                         if (t == s) continue;
                         const int4 it = d.info[nb][t];
-                        if (fixed_s && (it.w & FLAG_FIXED)) continue; // DPMBase.cc:3116-3120
                         const double4 pt = d.pr[nb][t];
+                        if (fixed_s && (it.w & FLAG_FIXED)) continue; // DPMBase.cc:3116-3120
                         bool per;
                         const V3 xt = image_of(I, xs, xyz(pt), per);
                         const V3 br = xs - xt;

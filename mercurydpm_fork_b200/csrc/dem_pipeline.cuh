@@ -216,7 +216,7 @@ template <int MODE, int NLAW, int FLAW, int NCOMP>
 __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
 {
     Control* ctl = d.ctl;
-    const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
+    const int c = ctl->cur, nb = c ^ 1;
     const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
     const bool record = final_step && ctl->record;
     const bool first = (MODE == 1) && ctl->first_step;

@@ -54,6 +54,9 @@ int  dem_mlp_gradients(dem_mlp *h, const float *x, const float *t, int n, float 
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the batch; *loss is the
  * batch loss before the update. */
 int  dem_mlp_train_step(dem_mlp *h, const float *x, const float *t, int n, float lr, float *loss);
+/* Device time of the forward pass (inputs already on the device from the
+ * last call) for n rows, averaged over reps launches: *ms per pass. */
+int  dem_mlp_time_forward(dem_mlp *h, int n, int reps, float *ms);
 const char *dem_mlp_last_error(dem_mlp *h);
 void dem_mlp_destroy(dem_mlp *h);
 

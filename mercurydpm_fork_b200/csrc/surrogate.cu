@@ -183,21 +183,20 @@ int gemm(Mlp* h, const __nv_bfloat16* A, long long a_sm, long long a_sk, const _
 // ---------------------------------------------------------------------------
 namespace {
 
-int forward(Mlp* h, int n)
+// keep_z: store the pre-activations for a backward pass (training)
+int forward(Mlp* h, int n, bool keep_z = true)
 {
+    const int epi = keep_z ? EPI_BIAS_GELU : EPI_BIAS_GELU_H;
     int rc;
     const __nv_bfloat16* W = h->wb;
     const float* P = h->p;
     k_norm_inputs<<<grid1((long long)n * NI, 256), 256, 0, h->stream>>>(h->x, h->d_norm, n, h->xb);
     // z1 = x W1^T + b1, h1 = gelu(z1), ... (A rows = samples, B rows = output features)
-    if ((rc = gemm(h, h->xb, NI, 1, W + OFF_W1, NI, 1, n, NH, NI, EPI_BIAS_GELU, P + OFF_B1, nullptr, h->z1, h->h1,
-                   NH)))
+    if ((rc = gemm(h, h->xb, NI, 1, W + OFF_W1, NI, 1, n, NH, NI, epi, P + OFF_B1, nullptr, h->z1, h->h1, NH)))
         return rc;
-    if ((rc = gemm(h, h->h1, NH, 1, W + OFF_W2, NH, 1, n, NH, NH, EPI_BIAS_GELU, P + OFF_B2, nullptr, h->z2, h->h2,
-                   NH)))
+    if ((rc = gemm(h, h->h1, NH, 1, W + OFF_W2, NH, 1, n, NH, NH, epi, P + OFF_B2, nullptr, h->z2, h->h2, NH)))
         return rc;
-    if ((rc = gemm(h, h->h2, NH, 1, W + OFF_W3, NH, 1, n, NH, NH, EPI_BIAS_GELU, P + OFF_B3, nullptr, h->z3, h->h3,
-                   NH)))
+    if ((rc = gemm(h, h->h2, NH, 1, W + OFF_W3, NH, 1, n, NH, NH, epi, P + OFF_B3, nullptr, h->z3, h->h3, NH)))
         return rc;
     return gemm(h, h->h3, NH, 1, W + OFF_W4, NH, 1, n, NO, NH, EPI_BIAS_F32, P + OFF_B4, nullptr, h->y, nullptr, NO);
 }
@@ -365,7 +364,7 @@ int dem_mlp_forward(dem_mlp* h, const float* x, int n, float* y)
 {
     if (!h || !y) return DEM_MLP_ERR_BAD_INPUT;
     int rc;
-    if ((rc = load_batch(h, x, nullptr, n)) || (rc = forward(h, n))) return rc;
+    if ((rc = load_batch(h, x, nullptr, n)) || (rc = forward(h, n, false))) return rc;
     k_denorm_outputs<<<grid1((long long)n * NO, 256), 256, 0, h->stream>>>(h->y, h->d_norm, n, h->t);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(y, h->t, (size_t)n * NO * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
@@ -393,6 +392,27 @@ int dem_mlp_train_step(dem_mlp* h, const float* x, const float* t, int n, float 
     k_adam<<<grid1(NPARAM, 256), 256, 0, h->stream>>>(h->p, h->g, h->m, h->v, NPARAM, lr, bc1, bc2, h->wb);
     CK(cudaGetLastError());
     if (loss) CK(cudaMemcpyAsync(loss, h->loss, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    return check_device_status(h);
+}
+
+int dem_mlp_time_forward(dem_mlp* h, int n, int reps, float* ms)
+{
+    if (!h || !ms || n <= 0 || n > h->capacity || reps <= 0) return DEM_MLP_ERR_BAD_INPUT;
+    CK(cudaSetDevice(h->device));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int rc = forward(h, n, false); // warm-up
+    CK(cudaEventRecord(e0, h->stream));
+    for (int r = 0; r < reps && !rc; ++r) rc = forward(h, n, false);
+    CK(cudaEventRecord(e1, h->stream));
+    CK(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    *ms = t / reps;
     return check_device_status(h);
 }
 

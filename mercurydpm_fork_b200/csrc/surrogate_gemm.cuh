@@ -37,6 +37,7 @@ enum Epilogue : int {
     EPI_BIAS_GELU = 1,    // z = acc + bias[n]; out_f32 = z; out_bf16 = gelu(z)
     EPI_BIAS_F32 = 2,     // out_f32 = acc + bias[n]
     EPI_DGELU_BF16 = 3,   // out_bf16 = acc * gelu'(z[m, n]) with z = aux_f32
+    EPI_BIAS_GELU_H = 4,  // out_bf16 = gelu(acc + bias[n]) (inference: no pre-activation kept)
 };
 
 struct GemmArgs {
@@ -172,6 +173,28 @@ __device__ __forceinline__ void stage_tile(unsigned char* dst, const __nv_bfloat
     }
 }
 
+// The same staging for a row-contiguous matrix with 16-byte aligned rows:
+// one cp.async of 16 bytes per (row, 8-element k group), zero-filled past
+// the matrix edge, in flight together (cp.async.commit_group by the caller).
+__device__ __forceinline__ void stage_tile_async(unsigned char* dst, const __nv_bfloat16* src, long long s_row,
+                                                 int row0, int rows, int nrows, int k0, int K)
+{
+    const int items = rows * (GEMM_BK / 8);
+    for (int it = threadIdx.x; it < items; it += GEMM_THREADS) {
+        const int r = it >> 3, g = it & 7;
+        const int row = row0 + r;
+        const int kb = k0 + g * 8;
+        int bytes = 0;
+        const __nv_bfloat16* p = src;
+        if (row < nrows && kb < K) {
+            bytes = (K - kb >= 8) ? 16 : (K - kb) * 2;
+            p = src + (long long)row * s_row + kb;
+        }
+        const uint32_t d = smem_u32(dst + (r >> 3) * 1024 + g * 128 + (r & 7) * 16);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(p), "r"(bytes) : "memory");
+    }
+}
+
 } // namespace surrogate
 
 namespace surrogate {
@@ -218,13 +241,22 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_bf16(GemmArgs g)
     constexpr uint32_t idesc = umma_idesc_bf16(BN);
 
     const int nk = (g.K + GEMM_BK - 1) / GEMM_BK;
+    // row-contiguous operands with 16-byte rows are staged with cp.async, so
+    // the next chunk's copies run while this chunk's MMAs do
+    const bool a_async = g.a_sk == 1 && (g.a_sm & 7) == 0 && ((reinterpret_cast<uintptr_t>(g.A) & 15) == 0);
+    const bool b_async = g.b_sk == 1 && (g.b_sn & 7) == 0 && ((reinterpret_cast<uintptr_t>(g.B) & 15) == 0);
+    auto stage = [&](int c, int b) {
+        if (a_async) stage_tile_async(sA[b], g.A, g.a_sm, m0, GEMM_BM, g.M, c * GEMM_BK, g.K);
+        else stage_tile(sA[b], g.A, g.a_sm, g.a_sk, m0, GEMM_BM, g.M, c * GEMM_BK, g.K);
+        if (b_async) stage_tile_async(sB[b], g.B, g.b_sn, n0, BN, g.N, c * GEMM_BK, g.K);
+        else stage_tile(sB[b], g.B, g.b_sn, g.b_sk, n0, BN, g.N, c * GEMM_BK, g.K);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    stage(0, 0);
     for (int c = 0; c < nk; ++c) {
         const int b = c & 1;
-        if (c >= 2 && !mbar_wait(&bar[b], ((c >> 1) - 1) & 1)) failed = 1; // stage b's previous MMAs
-        __syncwarp();
-        stage_tile(sA[b], g.A, g.a_sm, g.a_sk, m0, GEMM_BM, g.M, c * GEMM_BK, g.K);
-        stage_tile(sB[b], g.B, g.b_sn, g.b_sk, n0, BN, g.N, c * GEMM_BK, g.K);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // generic writes -> async-proxy reads
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // generic/cp.async writes -> async-proxy reads
         __syncthreads();
         if (threadIdx.x == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -235,6 +267,12 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_bf16(GemmArgs g)
                 umma_bf16(tmem, ad, bd, idesc, (c > 0 || j > 0) ? 1u : 0u);
             }
             umma_commit(&bar[b]);
+        }
+        if (c + 1 < nk) {
+            const int b1 = (c + 1) & 1;
+            // the MMAs of chunk c - 1 read buffer b1: wait for them before overwriting it
+            if (c >= 1 && !mbar_wait(&bar[b1], ((c - 1) >> 1) & 1)) failed = 1;
+            stage(c + 1, b1);
         }
     }
     const int last = nk - 1;
@@ -267,6 +305,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_bf16(GemmArgs g)
                     g.out_bf16[base + n] = __float2bfloat16_rn(gelu_f(z));
                     break;
                 }
+                case EPI_BIAS_GELU_H:
+                    g.out_bf16[base + n] = __float2bfloat16_rn(gelu_f(a + g.bias[n]));
+                    break;
                 default: // EPI_DGELU_BF16
                     g.out_bf16[base + n] = __float2bfloat16_rn(a * gelu_grad_f(g.aux_f32[base + n]));
                 }

@@ -34,6 +34,7 @@ def lib() -> C.CDLL:
             "dem_mlp_forward": (C.c_int, [C.c_void_p, _pf, C.c_int, _pf]),
             "dem_mlp_gradients": (C.c_int, [C.c_void_p, _pf, _pf, C.c_int, _pf, _pf]),
             "dem_mlp_train_step": (C.c_int, [C.c_void_p, _pf, _pf, C.c_int, C.c_float, _pf]),
+            "dem_mlp_time_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _pf]),
             "dem_mlp_last_error": (C.c_char_p, [C.c_void_p]),
             "dem_mlp_destroy": (None, [C.c_void_p]),
         }
@@ -112,6 +113,12 @@ class Surrogate:
             self._check(lib().dem_mlp_forward(self._h, _p(xs), b - a, _p(ys)))
             out[a:b] = ys
         return out
+
+    def time_forward(self, n: int, reps: int = 20) -> float:
+        """Device milliseconds of one forward pass of n rows already on the device."""
+        ms = C.c_float(0)
+        self._check(lib().dem_mlp_time_forward(self._h, n, reps, C.byref(ms)))
+        return float(ms.value)
 
     def gradients(self, x, t):
         x, t = _f32(x, (-1, NI)), _f32(t, (-1, NO))

@@ -291,9 +291,61 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_bf16(GemmArgs g)
             tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 32), v);
             if (!row_ok) continue;
             const long long base = (long long)row * g.ldc;
+            const int nb0 = n0 + cc * 32;
+            if (cc * 32 + 32 <= BN && nb0 + 32 <= g.N && (g.ldc & 7) == 0) {
+                // a whole 32-column run of this row: 16-byte stores (the row's
+                // 64 or 128 bytes are contiguous)
+                float r[32];
+                if (g.epilogue == EPI_BIAS_GELU || g.epilogue == EPI_BIAS_F32 || g.epilogue == EPI_BIAS_GELU_H) {
+                    const float4* b4 = reinterpret_cast<const float4*>(g.bias + nb0);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const float4 bb = b4[i];
+                        r[4 * i] = v[4 * i] + bb.x;
+                        r[4 * i + 1] = v[4 * i + 1] + bb.y;
+                        r[4 * i + 2] = v[4 * i + 2] + bb.z;
+                        r[4 * i + 3] = v[4 * i + 3] + bb.w;
+                    }
+                } else if (g.epilogue == EPI_DGELU_BF16) {
+                    const float4* z4 = reinterpret_cast<const float4*>(g.aux_f32 + base + nb0);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const float4 zz = z4[i];
+                        r[4 * i] = v[4 * i] * gelu_grad_f(zz.x);
+                        r[4 * i + 1] = v[4 * i + 1] * gelu_grad_f(zz.y);
+                        r[4 * i + 2] = v[4 * i + 2] * gelu_grad_f(zz.z);
+                        r[4 * i + 3] = v[4 * i + 3] * gelu_grad_f(zz.w);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) r[i] = v[i];
+                }
+                if (g.epilogue == EPI_STORE_F32 || g.epilogue == EPI_BIAS_F32 || g.epilogue == EPI_BIAS_GELU) {
+                    float4* o4 = reinterpret_cast<float4*>(g.out_f32 + base + nb0);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) o4[i] = make_float4(r[4 * i], r[4 * i + 1], r[4 * i + 2], r[4 * i + 3]);
+                }
+                if (g.epilogue == EPI_BIAS_GELU || g.epilogue == EPI_BIAS_GELU_H || g.epilogue == EPI_DGELU_BF16) {
+                    const bool act = g.epilogue != EPI_DGELU_BF16;
+                    uint4* o4 = reinterpret_cast<uint4*>(g.out_bf16 + base + nb0);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        uint32_t w[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const float x0 = act ? gelu_f(r[8 * i + 2 * j]) : r[8 * i + 2 * j];
+                            const float x1 = act ? gelu_f(r[8 * i + 2 * j + 1]) : r[8 * i + 2 * j + 1];
+                            w[j] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x0)) |
+                                   ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x1)) << 16);
+                        }
+                        o4[i] = make_uint4(w[0], w[1], w[2], w[3]);
+                    }
+                }
+                continue;
+            }
 #pragma unroll
             for (int i = 0; i < 32; ++i) {
-                const int n = n0 + cc * 32 + i;
+                const int n = nb0 + i;
                 if (cc * 32 + i >= BN || n >= g.N) break;
                 const float a = v[i];
                 switch (g.epilogue) {

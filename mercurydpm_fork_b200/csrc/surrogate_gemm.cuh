@@ -5,14 +5,15 @@
 //   C[m, n] = sum_k A(m, k) B(n, k)      A(m, k) = A[m * a_sm + k * a_sk]
 //                                        B(n, k) = B[n * b_sn + k * b_sk]
 //
-// One CTA of 128 threads computes a 128 x BN tile (BN <= 256, a multiple of
+// One CTA of 256 threads computes a 128 x BN tile (BN <= 256, a multiple of
 // 16) over the whole K range: K is staged 64 at a time into shared memory in
 // the K-major canonical layout without swizzle (8 x 16-byte core matrices;
 // LBO = 128 B between the two K halves of an instruction, SBO = 1024 B
 // between 8-row groups), two stages deep; one elected thread issues four
 // K=16 tcgen05.mma per stage and commits them to the stage's mbarrier; the
 // accumulator lives in tensor memory (128 lanes x BN columns of FP32) and the
-// four warps read their 32 lanes back with tcgen05.ld for the fused epilogue.
+// eight warps read it back with tcgen05.ld (each lane quarter by two warps,
+// alternate 32-column runs) for the fused epilogue.
 // Operand staging uses plain loads, so any strides (transposes) are allowed:
 // the backward pass reads its operands transposed without extra copies.
 //
@@ -28,7 +29,7 @@ namespace surrogate {
 
 constexpr int GEMM_BM = 128;
 constexpr int GEMM_BK = 64;
-constexpr int GEMM_THREADS = 128;
+constexpr int GEMM_THREADS = 256; // 8 warps: warps w and w + 4 share TMEM lanes 32 (w % 4) ..
 constexpr int GEMM_MAX_BN = 256;
 constexpr unsigned long long WAIT_LIMIT = 1ull << 26; // try_wait polls before giving up
 
@@ -282,13 +283,15 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_bf16(GemmArgs g)
     if (failed) {
         if (threadIdx.x == 0) atomicExch(g.error, 1u);
     } else {
-        // ---- epilogue: thread = accumulator row (tensor-memory lane) ----
-        const int row = m0 + warp * 32 + lane;
+        // ---- epilogue: thread = accumulator row (tensor-memory lane); the two
+        // warps of a lane quarter take alternate 32-column runs ----
+        const int quarter = warp & 3, half = warp >> 2;
+        const int row = m0 + quarter * 32 + lane;
         const bool row_ok = row < g.M;
 #pragma unroll 1
-        for (int cc = 0; cc < (BN + 31) / 32; ++cc) { // a 16-wide tile reads 32 allocated columns
+        for (int cc = half; cc < (BN + 31) / 32; cc += 2) { // a 16-wide tile reads 32 allocated columns
             float v[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 32), v);
+            tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(cc * 32), v);
             if (!row_ok) continue;
             const long long base = (long long)row * g.ldc;
             const int nb0 = n0 + cc * 32;

@@ -14,6 +14,7 @@
 #include "dem_walls.cuh"
 #include "dem_kernels.cuh"
 #include "dem_pipeline.cuh"
+#include "dem_rebuild.cuh"
 
 using namespace dem;
 
@@ -50,7 +51,6 @@ struct Handle {
     Control* d_ctl = nullptr;
     ContactRecord* d_records = nullptr;
     unsigned record_capacity = 0;
-    int nblocks_scan = 0;
     bool uploaded = false;
     bool initial_pending = false;
     bool records_valid = false;
@@ -64,6 +64,7 @@ struct Handle {
     int ncomp = 3;
     int law_variant = 0;
     int sm_count = 148;
+    int rb_grid = 148;                 // blocks of the cooperative rebuild (all resident)
 };
 
 int fail(Handle* h, int code, const std::string& msg)
@@ -115,21 +116,23 @@ void free_particle_arrays(Handle* h)
 inline unsigned grid_for(long long n, int block) { return (unsigned)std::max<long long>(1, (n + block - 1) / block); }
 
 // ---- kernel launch sequences ------------------------------------------------
-void launch_rebuild(Handle* h, cudaStream_t s)
+// The rebuild kernel (dem_rebuild.cuh): a cooperative launch, so that its
+// grid barriers are safe; it returns at once unless the rebuild flag is set.
+cudaError_t launch_rebuild(Handle* h, cudaStream_t s)
 {
-    DevPtrs& d = h->d;
-    k_keys<<<grid_for(d.n, 256), 256, 0, s>>>(d);
-    k_scan_blocks<<<h->nblocks_scan, 1024, 0, s>>>(d);
-    k_scan_sums<<<1, 1024, 0, s>>>(d, h->nblocks_scan);
-    k_scan_add<<<grid_for(d.ncells, 256), 256, 0, s>>>(d);
-    k_scatter<<<grid_for(d.n, 256), 256, 0, s>>>(d);
-    k_cell_sort<<<grid_for(d.ncells, 128), 128, 0, s>>>(d);
-    k_gather<<<grid_for(d.n, 256), 256, 0, s>>>(d);
-    k_build<<<grid_for(d.n, 128), 128, 0, s>>>(d);
-    k_rb_finish<<<1, 32, 0, s>>>(d);
-    k_rev<<<grid_for(d.n, 256), 256, 0, s>>>(d);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)h->rb_grid);
+    cfg.blockDim = dim3(RB_BLOCK);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_rebuild, h->d, h->d.rb_barrier);
 }
-constexpr int REBUILD_LAUNCHES = 10;
+constexpr int REBUILD_LAUNCHES = 1;
 constexpr int FORCE_LAUNCHES = 3;
 
 // Law variants the force kernel is instantiated for; the handle uses a
@@ -181,37 +184,21 @@ void launch_force(Handle* h, cudaStream_t s, int mode)
         launch_force_mode<1>(h, s);
 }
 
-// Captures `steps` time steps: control -> (if rebuild) rebuild body -> force.
+// Captures `steps` time steps: control -> rebuild (returns at once unless
+// the skin test fired) -> force.
 int build_graph(Handle* h, int steps, cudaGraphExec_t* out)
 {
     cudaStream_t s = h->stream;
     CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < steps; ++k) {
-        cudaStreamCaptureStatus st;
-        cudaGraph_t g = nullptr;
-        CU(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr));
-        cudaGraphConditionalHandle handle;
-        CU(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
-        k_control<<<1, CONTROL_THREADS, 0, s>>>(h->d_ctl, h->d.walls, h->d.n_walls, h->d.dt, handle, 1);
-        const cudaGraphNode_t* deps = nullptr;
-        size_t ndeps = 0;
-        CU(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps));
-        // cudaGraphNodeParams has no default constructor; build it in zeroed storage
-        alignas(cudaGraphNodeParams) unsigned char storage[sizeof(cudaGraphNodeParams)];
-        std::memset(storage, 0, sizeof(storage));
-        cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(storage);
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = handle;
-        cp.conditional.type = cudaGraphCondTypeIf;
-        cp.conditional.size = 1;
-        cudaGraphNode_t cnode;
-        CU(cudaGraphAddNode(&cnode, g, deps, ndeps, &cp));
-        CU(cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies));
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        CU(cudaStreamBeginCaptureToGraph(h->stream2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        launch_rebuild(h, h->stream2);
-        cudaGraph_t body_out = nullptr;
-        CU(cudaStreamEndCapture(h->stream2, &body_out));
+        k_control<<<1, CONTROL_THREADS, 0, s>>>(h->d_ctl, h->d.walls, h->d.n_walls, h->d.dt);
+        const cudaError_t e = launch_rebuild(h, s);
+        if (e != cudaSuccess) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            return fail(h, DEM_ERR_CUDA, std::string("rebuild launch in capture: ") + cudaGetErrorString(e));
+        }
         launch_force(h, s, 1);
     }
     cudaGraph_t graph = nullptr;
@@ -237,6 +224,9 @@ int check_status(Handle* h, const Control& c)
         return fail(h, DEM_ERR_CAPACITY, "neighbour-list capacity exceeded (max_neighbors=" +
                                              std::to_string(h->d.cap) + "); raise dem_config.max_neighbors");
     if (st & (1u << DEM_ERR_NAN)) return fail(h, DEM_ERR_NAN, "non-finite force detected");
+    // a rebuild block gave up at a grid barrier: the arrival counter no longer
+    // sits on a multiple of the launch's barriers, so it starts again at zero
+    if (h->d.rb_barrier) cudaMemsetAsync(h->d.rb_barrier, 0, sizeof(unsigned long long), h->stream);
     return fail(h, DEM_ERR_TIMEOUT, "device wait timed out");
 }
 
@@ -335,6 +325,16 @@ int dem_create(const dem_config* config, const dem_instance_desc* instances, dem
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) == cudaSuccess && sms > 0)
         h->sm_count = sms;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebuild, RB_BLOCK, 0) != cudaSuccess || per_sm < 1) {
+        cudaStreamDestroy(h->stream);
+        cudaStreamDestroy(h->stream2);
+        cudaEventDestroy(h->ev0);
+        cudaEventDestroy(h->ev1);
+        delete h;
+        return DEM_ERR_CUDA;
+    }
+    h->rb_grid = h->sm_count * per_sm;
     *out = reinterpret_cast<dem_handle*>(h);
     return DEM_OK;
 }
@@ -571,7 +571,6 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     for (const auto& sp : h->species) d.zero_idist = d.zero_idist && sp.interaction_distance == 0.0;
     d.dt = h->cfg.time_step;
     d.drag = h->cfg.background_drag;
-    h->nblocks_scan = (int)grid_for(ncells, 1024);
     const size_t NC = d.ncap;
     int rc;
     if (reuse) {
@@ -589,9 +588,10 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         }
         d.force = kept.force; d.torque = kept.torque; d.key = kept.key; d.perm = kept.perm; d.newidx = kept.newidx;
         d.cell_count = kept.cell_count; d.cell_start = kept.cell_start; d.cell_cursor = kept.cell_cursor;
-        d.block_sums = kept.block_sums; d.inst = kept.inst; d.species = kept.species; d.walls = kept.walls;
+        d.block_sums = kept.block_sums; d.rb_barrier = kept.rb_barrier; d.inst = kept.inst; d.species = kept.species; d.walls = kept.walls;
         d.wgeom = kept.wgeom; d.n_walls = kept.n_walls; d.ctl = kept.ctl; d.records = kept.records;
         d.n_instances = kept.n_instances;
+        d.pf = kept.pf; d.rows = kept.rows;
         d.rev = kept.rev; d.slot = kept.slot; d.slotw = kept.slotw; d.items = kept.items; d.shares = kept.shares;
         d.item_cap = kept.item_cap;
         for (int b = 0; b < 2; ++b) { // no history carries over from the previous simulation
@@ -615,6 +615,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         if ((rc = dalloc(h, &d.wact[b], NC))) return rc;
     }
     if ((rc = dalloc(h, &d.rev, (size_t)cap * NC))) return rc;
+    if ((rc = dalloc(h, &d.rows, (size_t)cap * NC))) return rc;
+    if ((rc = dalloc(h, &d.pf, NC))) return rc;
     if ((rc = dalloc(h, &d.slot, (size_t)cap * NC))) return rc;
     if ((rc = dalloc(h, &d.slotw, (size_t)wmax * NC))) return rc;
     // contact items: at most min(cap, 16) pairs owned per particle plus 4 walls
@@ -630,7 +632,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     if ((rc = dalloc(h, &d.cell_count, (size_t)ncells + 1))) return rc;
     if ((rc = dalloc(h, &d.cell_start, (size_t)ncells + 1))) return rc;
     if ((rc = dalloc(h, &d.cell_cursor, (size_t)ncells + 1))) return rc;
-    if ((rc = dalloc(h, &d.block_sums, (size_t)h->nblocks_scan + 1))) return rc;
+    if ((rc = dalloc(h, &d.block_sums, (size_t)h->rb_grid + 1))) return rc;
+    if ((rc = dalloc(h, &d.rb_barrier, 1))) return rc;
     if ((rc = dalloc(h, &h->d_inst, h->inst.size()))) return rc;
     if ((rc = dalloc(h, &h->d_species, h->species.size()))) return rc;
     if ((rc = dalloc(h, &h->d_walls, std::max<size_t>(1, h->walls.size())))) return rc;
@@ -705,8 +708,7 @@ static int ensure_lists(Handle* h)
     c.rebuild = 1;
     c.force_rebuild = 0;
     CU(cudaMemcpyAsync(h->d_ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
-    launch_rebuild(h, h->stream);
-    CU(cudaGetLastError());
+    CU(launch_rebuild(h, h->stream));
     return read_control(h, &c);
 }
 
@@ -817,7 +819,7 @@ int dem_step(dem_handle* hh, int nsteps)
     if (d.n > 0) {
         if (h->initial_pending) {
             if (c0.rebuild) {
-                launch_rebuild(h, h->stream);
+                CU(launch_rebuild(h, h->stream));
                 launches += REBUILD_LAUNCHES;
             }
             launch_force(h, h->stream, 0);
@@ -842,12 +844,11 @@ int dem_step(dem_handle* hh, int nsteps)
                     left -= GRAPH_STEPS;
                 }
                 while (left-- > 0) CU(cudaGraphLaunch(h->graph1, h->stream));
-                launches += (1ll + FORCE_LAUNCHES) * nsteps;
+                launches += (1ll + REBUILD_LAUNCHES + FORCE_LAUNCHES) * nsteps;
             } else {
                 for (int k = 0; k < nsteps; ++k) {
-                    k_control<<<1, CONTROL_THREADS, 0, h->stream>>>(h->d_ctl, d.walls, d.n_walls, d.dt,
-                                                                     cudaGraphConditionalHandle{}, 0);
-                    launch_rebuild(h, h->stream);
+                    k_control<<<1, CONTROL_THREADS, 0, h->stream>>>(h->d_ctl, d.walls, d.n_walls, d.dt);
+                    CU(launch_rebuild(h, h->stream));
                     launch_force(h, h->stream, 1);
                 }
                 CU(cudaGetLastError());
@@ -865,7 +866,7 @@ int dem_step(dem_handle* hh, int nsteps)
     h->last_ms = ms;
     const long long rb = c.n_rebuilds - rebuilds0;
     h->last_rebuilds = rb;
-    h->last_launches = launches + (h->cfg.use_graphs ? rb * REBUILD_LAUNCHES : 0);
+    h->last_launches = launches;
     h->steps_total += nsteps;
     if (evaluates) {
         h->n_records = c.n_records;

@@ -130,6 +130,9 @@ struct DevPtrs {
     unsigned int *wact[2];
     // broad phase scratch
     int *key, *perm, *newidx, *cell_count, *cell_start, *cell_cursor, *block_sums;
+    unsigned long long *rb_barrier; // arrivals at the rebuild's grid barriers (only grows)
+    float4 *pf;              // (x, y, z, r) in FP32 of the gathered state: the list build's prefilter
+    int *rows;               // neighbour lists particle-major (rows[s * cap + k]), for the reverse index
     // tables
     const InstanceDev *inst;
     const dem_species_pair *species;

@@ -3,16 +3,16 @@
 // Per time step (captured in a CUDA graph):
 //   k_control   moves the walls (one thread per wall); one thread applies
 //               the pending state-buffer flip, adds the last step's maximum
-//               displacement to the skin budget and sets the graph condition
-//               that runs the rebuild body (MercuryBase::hGridNeedsRebuilding,
-//               MercuryBase.cc:496-535, turned into a Verlet-skin test).
-//   rebuild     k_keys -> scan -> k_scatter -> k_cell_sort -> k_gather ->
-//               k_build -> k_rb_finish -> k_rev: cell keys per HGrid level,
-//               counting sort, per-cell ordering by particle id, permutation
-//               gather of the state, neighbour lists with contact-history
-//               carry-over, their reverse index (replaces HGrid buckets +
-//               InteractionHandler lookup, Mercury3D.cc:224-416,
-//               InteractionHandler.cc:103-174).
+//               displacement to the skin budget and sets the rebuild flag
+//               (MercuryBase::hGridNeedsRebuilding, MercuryBase.cc:496-535,
+//               turned into a Verlet-skin test).
+//   k_rebuild   one cooperative kernel, launched every step and returning at
+//               once unless the flag is set (dem_rebuild.cuh): cell keys per
+//               HGrid level, counting sort, per-cell ordering by particle id,
+//               permutation gather of the state, neighbour lists with
+//               contact-history carry-over, their reverse index (replaces
+//               HGrid buckets + InteractionHandler lookup, Mercury3D.cc:224-416,
+//               InteractionHandler.cc:103-174). The per-item steps are below.
 //   force       k_detect -> k_contacts -> k_sum (dem_pipeline.cuh): the exact
 //               FP64 contact predicate (BaseParticle::getInteractionWith,
 //               BaseParticle.cc:688-710) on the entries each particle owns,
@@ -32,8 +32,7 @@ __device__ __forceinline__ V3 xyz(double4 a) { return V3{a.x, a.y, a.z}; }
 // ---------------------------------------------------------------------------
 // control
 // ---------------------------------------------------------------------------
-__global__ void k_control(Control* ctl, dem_wall* walls, int n_walls, double dt, cudaGraphConditionalHandle handle,
-                          int use_handle)
+__global__ void k_control(Control* ctl, dem_wall* walls, int n_walls, double dt)
 {
     // Walls move before the force evaluation of every step, after the particles
     // (DPMBase::integrateBeforeForceComputation, DPMBase.cc:3228-3261, through
@@ -63,7 +62,6 @@ __global__ void k_control(Control* ctl, dem_wall* walls, int n_walls, double dt,
     ctl->first_step = (ctl->steps_done == 0);
     ctl->steps_done += 1;
     ctl->pending_flip = 1; // the force kernel of this step writes the other buffer
-    if (use_handle) cudaGraphSetConditional(handle, rebuild ? 1u : 0u);
 }
 
 __global__ void k_flip(Control* ctl)
@@ -89,11 +87,11 @@ __device__ __forceinline__ int cell_coord(double x, double origin, double inv, i
     return (int)f;
 }
 
-__global__ void k_keys(DevPtrs d)
+// ---- the steps of a rebuild, one item each (run by k_rebuild, dem_rebuild.cuh) ----
+
+// Cell key of particle i (state buffer c) and its count.
+__device__ __forceinline__ void keys_one(const DevPtrs& d, int i, int c)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (!d.ctl->rebuild || i >= d.n) return;
-    const int c = d.ctl->cur;
     const double4 p = d.pr[c][i];
     const int4 inf = d.info[c][i];
     if (inf.w & FLAG_DELETED) { // the graveyard: the last cell, never searched
@@ -111,73 +109,9 @@ __global__ void k_keys(DevPtrs d)
     atomicAdd(&d.cell_count[key], 1);
 }
 
-// Exclusive scan of cell_count into cell_start, 1024 cells per block.
-__device__ __forceinline__ int block_inclusive_scan_1024(int v, int* warp_sums)
+// Slot of particle i in the counting sort.
+__device__ __forceinline__ void scatter_one(const DevPtrs& d, int i)
 {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += t;
-    }
-    if (lane == 31) warp_sums[wid] = v;
-    __syncthreads();
-    if (wid == 0) {
-        int w = warp_sums[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += t;
-        }
-        warp_sums[lane] = w;
-    }
-    __syncthreads();
-    if (wid > 0) v += warp_sums[wid - 1];
-    return v;
-}
-
-__global__ void __launch_bounds__(1024) k_scan_blocks(DevPtrs d)
-{
-    __shared__ int ws[32];
-    if (!d.ctl->rebuild) return;
-    const int i = blockIdx.x * 1024 + threadIdx.x;
-    const int v = (i < d.ncells) ? d.cell_count[i] : 0;
-    const int inc = block_inclusive_scan_1024(v, ws);
-    if (i < d.ncells) d.cell_start[i] = inc - v;
-    if (threadIdx.x == 1023) d.block_sums[blockIdx.x] = inc;
-}
-
-__global__ void __launch_bounds__(1024) k_scan_sums(DevPtrs d, int nblocks)
-{
-    __shared__ int ws[32];
-    __shared__ int carry;
-    if (!d.ctl->rebuild) return;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int base = 0; base < nblocks; base += 1024) {
-        const int i = base + threadIdx.x;
-        const int v = (i < nblocks) ? d.block_sums[i] : 0;
-        const int inc = block_inclusive_scan_1024(v, ws);
-        const int c0 = carry;
-        if (i < nblocks) d.block_sums[i] = c0 + inc - v;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = c0 + inc;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) d.cell_start[d.ncells] = carry;
-}
-
-__global__ void k_scan_add(DevPtrs d)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (!d.ctl->rebuild || i >= d.ncells) return;
-    d.cell_start[i] += d.block_sums[i >> 10];
-}
-
-__global__ void k_scatter(DevPtrs d)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (!d.ctl->rebuild || i >= d.n) return;
     const int key = d.key[i];
     const int slot = d.cell_start[key] + atomicAdd(&d.cell_cursor[key], 1);
     d.perm[slot] = i;
@@ -186,12 +120,9 @@ __global__ void k_scatter(DevPtrs d)
 // Orders the members of every cell by particle id, so the sorted order (and
 // with it every neighbour list and force sum) does not depend on the order in
 // which the atomics above were served. Resets the counters for the next rebuild.
-__global__ void k_cell_sort(DevPtrs d)
+__device__ __forceinline__ void cell_sort_one(const DevPtrs& d, int cell, int c)
 {
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (!d.ctl->rebuild || cell >= d.ncells) return;
     const int b = d.cell_start[cell], e = d.cell_start[cell + 1];
-    const int c = d.ctl->cur;
     d.cell_count[cell] = 0;
     d.cell_cursor[cell] = 0;
     if (e - b < 2 || cell == d.ncells - 1) return; // the graveyard is not ordered
@@ -211,13 +142,14 @@ __global__ void k_cell_sort(DevPtrs d)
     }
 }
 
-__global__ void k_gather(DevPtrs d)
+// State of slot s gathered from buffer c into the other buffer.
+__device__ __forceinline__ void gather_one(const DevPtrs& d, int s, int c)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (!d.ctl->rebuild || s >= d.n) return;
-    const int c = d.ctl->cur, nb = c ^ 1;
+    const int nb = c ^ 1;
     const int o = d.perm[s];
-    d.pr[nb][s] = d.pr[c][o];
+    const double4 p = d.pr[c][o];
+    d.pr[nb][s] = p;
+    d.pf[s] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
     d.vm[nb][s] = d.vm[c][o];
     d.wi[nb][s] = d.wi[c][o];
     d.qo[nb][s] = d.qo[c][o];
@@ -279,17 +211,64 @@ __device__ __forceinline__ void cell_range(const InstanceDev& I, int lvl, int k,
 
 __device__ __forceinline__ int wrap_cell(int c, int dim)
 {
+    if ((unsigned)c < (unsigned)dim) return c;
+    const int once = c < 0 ? c + dim : c - dim; // a range one period beyond the grid
+    if ((unsigned)once < (unsigned)dim) return once;
     c %= dim;
     return c < 0 ? c + dim : c;
 }
 
-__global__ void __launch_bounds__(128) k_build(DevPtrs d)
+// Sets bit m of a 4-word mask held in registers.
+__device__ __forceinline__ void set_bit4(unsigned int& w0, unsigned int& w1, unsigned int& w2, unsigned int& w3, int m)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (!d.ctl->rebuild || s >= d.n) return;
-    const int hc = d.ctl->cur;         // old state order and its history
+    const unsigned int bit = 1u << (m & 31);
+    const int w = m >> 5;
+    if (w == 0) w0 |= bit;
+    else if (w == 1) w1 |= bit;
+    else if (w == 2) w2 |= bit;
+    else w3 |= bit;
+}
+
+// Slot ranges of one (z, y) row of cells between x cells lo..hi: one range,
+// or two when a periodic row wraps (the second empty otherwise).
+__device__ __forceinline__ void row_ranges(const DevPtrs& d, const InstanceDev& I, int lvl, int row, int lo, int hi,
+                                           int& b0, int& e0, int& b1, int& e1)
+{
+    const int dx = I.dims[lvl][0];
+    int l0 = lo, h0 = hi, l1 = 0, h1 = -1;
+    if (I.per_mask & 1u) {
+        if (lo < 0) {
+            l0 = lo + dx; h0 = dx - 1;
+            l1 = 0; h1 = hi;
+        } else if (hi >= dx) {
+            l0 = lo; h0 = dx - 1;
+            l1 = 0; h1 = hi - dx;
+        }
+    }
+    b0 = d.cell_start[row + l0];
+    e0 = d.cell_start[row + h0 + 1];
+    if (h1 >= l1) {
+        b1 = d.cell_start[row + l1];
+        e1 = d.cell_start[row + h1 + 1];
+    } else {
+        b1 = e1 = 0;
+    }
+}
+
+// Neighbour list of one particle: every particle of the cells within reach
+// whose distance is below r_s + r_t + interaction distance + skin, in
+// cell-row order. The distance test runs in FP32 on the `pf` copy with a
+// margin that bounds its rounding (16 units of FP32 rounding on the cut and
+// on the magnitudes of the coordinates and the period), so the list is a
+// superset of the FP64 test's list; pairs whose periodic image is ambiguous
+// in FP32 take the FP64 test. Contacts themselves are always decided in FP64
+// by the force evaluation, so the superset changes no result. The next row's
+// slot ranges are read ahead and candidates are read BUILD_BATCH at a time.
+constexpr int BUILD_BATCH = 2;
+__device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int lo_)
+{
+    // hc: old state order and its history; lo_: old lists
     const int nb = hc ^ 1;             // gathered (new) state; new history
-    const int lo_ = d.ctl->lbuf;       // old lists
     const int ln = lo_ ^ 1;            // new lists
     const double4 ps = d.pr[nb][s];
     const int4 is = d.info[nb][s];
@@ -303,50 +282,90 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
         return;
     }
     const double extra = I.max_interaction_distance + d.ctl->skin;
+    const float4 fs = d.pf[s];
+    const float ms = fmaxf(fabsf(fs.x), fmaxf(fabsf(fs.y), fabsf(fs.z)));
+    const float extra_f = (float)extra;
+    const unsigned int pm = I.per_mask;
+    float Lf[3], hf[3], lmax = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        Lf[k] = (float)I.per_L[k];
+        hf[k] = (float)I.per_half[k];
+        if ((pm >> k) & 1u) lmax = fmaxf(lmax, fabsf(Lf[k]));
+    }
+    constexpr float U20 = 9.5367431640625e-07f; // 2^-20
     int count = 0;
     bool overflow = false;
     for (int lvl = 0; lvl < I.n_levels; ++lvl) {
         const double reach = ps.w + I.level_rmax[lvl] + extra;
-        int lo[3], hi[3];
-        cell_range(I, lvl, 0, xs.x, reach, lo[0], hi[0]);
-        cell_range(I, lvl, 1, xs.y, reach, lo[1], hi[1]);
-        cell_range(I, lvl, 2, xs.z, reach, lo[2], hi[2]);
+        int lox, hix, loy, hiy, loz, hiz;
+        cell_range(I, lvl, 0, xs.x, reach, lox, hix);
+        cell_range(I, lvl, 1, xs.y, reach, loy, hiy);
+        cell_range(I, lvl, 2, xs.z, reach, loz, hiz);
         const int dx = I.dims[lvl][0], dy = I.dims[lvl][1], dz = I.dims[lvl][2];
-        for (int cz = lo[2]; cz <= hi[2]; ++cz) {
-            const int wz = ((I.per_mask >> 2) & 1u) ? wrap_cell(cz, dz) : cz;
-            for (int cy = lo[1]; cy <= hi[1]; ++cy) {
-                const int wy = ((I.per_mask >> 1) & 1u) ? wrap_cell(cy, dy) : cy;
-                const int row = I.cell_base[lvl] + (wz * dy + wy) * dx;
-                // the x cells of a row are consecutive: their members form one
-                // slot range (two when a periodic row wraps)
-                int seg_lo[2], seg_hi[2], nseg = 1;
-                seg_lo[0] = lo[0];
-                seg_hi[0] = hi[0];
-                if (I.per_mask & 1u) {
-                    if (lo[0] < 0) {
-                        seg_lo[0] = lo[0] + dx; seg_hi[0] = dx - 1;
-                        seg_lo[1] = 0; seg_hi[1] = hi[0];
-                        nseg = 2;
-                    } else if (hi[0] >= dx) {
-                        seg_lo[0] = lo[0]; seg_hi[0] = dx - 1;
-                        seg_lo[1] = 0; seg_hi[1] = hi[0] - dx;
-                        nseg = 2;
-                    }
-                }
-                for (int g = 0; g < nseg; ++g) {
-                    const int b = d.cell_start[row + seg_lo[g]], e = d.cell_start[row + seg_hi[g] + 1];
-                    for (int t = b; t < e; ++t) {
+        const int ny = hiy - loy + 1, nz = hiz - loz + 1;
+        const int nrows = (ny > 0 && nz > 0) ? ny * nz : 0;
+        auto row_of = [&](int cz, int cy) {
+            const int wz = ((pm >> 2) & 1u) ? wrap_cell(cz, dz) : cz;
+            const int wy = ((pm >> 1) & 1u) ? wrap_cell(cy, dy) : cy;
+            return I.cell_base[lvl] + (wz * dy + wy) * dx;
+        };
+        int cz = loz, cy = loy;
+        int nb0 = 0, ne0 = 0, nb1 = 0, ne1 = 0;
+        if (nrows > 0) row_ranges(d, I, lvl, row_of(cz, cy), lox, hix, nb0, ne0, nb1, ne1);
+        for (int r = 0; r < nrows; ++r) {
+            const int b0 = nb0, e0 = ne0, b1 = nb1, e1 = ne1;
+            int ncy = cy + 1, ncz = cz;
+            if (ncy > hiy) {
+                ncy = loy;
+                ++ncz;
+            }
+            if (r + 1 < nrows) row_ranges(d, I, lvl, row_of(ncz, ncy), lox, hix, nb0, ne0, nb1, ne1);
+            cy = ncy;
+            cz = ncz;
+            for (int g = 0; g < 2; ++g) {
+                const int b = g ? b1 : b0, e = g ? e1 : e0;
+                for (int t0 = b; t0 < e; t0 += BUILD_BATCH) {
+                    float4 ftb[BUILD_BATCH];
+#pragma unroll
+                    for (int j = 0; j < BUILD_BATCH; ++j)
+                        if (t0 + j < e) ftb[j] = d.pf[t0 + j];
+#pragma unroll
+                    for (int j = 0; j < BUILD_BATCH; ++j) {
+                        const int t = t0 + j;
+                        if (t >= e) break;
                         if (t == s) continue;
-                        const int4 it = d.info[nb][t];
-                        const double4 pt = d.pr[nb][t];
-                        if (fixed_s && (it.w & FLAG_FIXED)) continue; // DPMBase.cc:3116-3120
-                        bool per;
-                        const V3 xt = image_of(I, xs, xyz(pt), per);
-                        const V3 br = xs - xt;
-                        const double cut = ps.w + pt.w + extra;
-                        if (len2(br) < cut * cut) {
+                        if (fixed_s && (d.info[nb][t].w & FLAG_FIXED)) continue; // DPMBase.cc:3116-3120
+                        const float4 ft = ftb[j];
+                        const float mt = fmaxf(fabsf(ft.x), fmaxf(fabsf(ft.y), fabsf(ft.z)));
+                        const float err = U20 * ((ms + mt) + lmax);
+                        float bq[3] = {fs.x - ft.x, fs.y - ft.y, fs.z - ft.z};
+                        bool ambiguous = false;
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            if ((pm >> k) & 1u) {
+                                ambiguous = ambiguous || fabsf(fabsf(bq[k]) - hf[k]) <= 4.0f * err;
+                                if (bq[k] > hf[k]) bq[k] = bq[k] - Lf[k];
+                                else if (bq[k] < -hf[k]) bq[k] = bq[k] + Lf[k];
+                            }
+                        }
+                        bool near;
+                        if (!ambiguous) {
+                            const float cut = (fs.w + ft.w) + extra_f;
+                            const float lim = cut * (1.0f + U20) + err;
+                            near = (bq[0] * bq[0] + bq[1] * bq[1] + bq[2] * bq[2]) < lim * lim;
+                        } else { // the FP64 test of the sequential scan
+                            const double4 pt = d.pr[nb][t];
+                            bool per;
+                            const V3 xt = image_of(I, xs, xyz(pt), per);
+                            const V3 br = xs - xt;
+                            const double cut = ps.w + pt.w + extra;
+                            near = len2(br) < cut * cut;
+                        }
+                        if (near) {
                             if (count < d.cap) {
                                 d.nbr[ln][nbr_at(d.ncap, s, count)] = t;
+                                d.rows[(size_t)s * d.cap + count] = t;
                             } else {
                                 overflow = true;
                             }
@@ -363,35 +382,63 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
     }
     d.cnt[ln][s] = count;
 
-    // carry contact history from the old list (old order) to the new one
+    // carry contact history from the old list (old order) to the new one, up
+    // to 4 contacts per pass over the new list
     const int o = d.perm[s];
     const int ocnt = d.cnt[lo_][o];
-    unsigned int neww[4] = {0u, 0u, 0u, 0u};
+    unsigned int n0 = 0u, n1 = 0u, n2 = 0u, n3 = 0u;
     for (int w = 0; w < d.nwords; ++w) {
         unsigned int bits = d.act[hc][(size_t)w * d.ncap + o];
         while (bits) {
-            const int b = __ffs(bits) - 1;
-            bits &= bits - 1;
-            const int k = w * 32 + b;
-            if (k >= ocnt) break;
-            const int tnew = d.newidx[d.nbr[lo_][nbr_at(d.ncap, o, k)]];
-            int m = -1;
-            for (int q = 0; q < count; ++q) {
-                if (d.nbr[ln][nbr_at(d.ncap, s, q)] == tnew) {
-                    m = q;
-                    break;
+            int kk[4], tn[4], m[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                kk[j] = -1;
+                if (bits) {
+                    const int k = w * 32 + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    if (k < ocnt) kk[j] = k; // bits past the old count are stale
                 }
             }
-            if (m < 0) {
-                atomicAdd(&d.ctl->lost_history, 1u);
-                continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) tn[j] = kk[j] >= 0 ? d.nbr[lo_][nbr_at(d.ncap, o, kk[j])] : -1;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                tn[j] = tn[j] >= 0 ? d.newidx[tn[j]] : -1;
+                m[j] = -1;
             }
-            for (int comp = 0; comp < d.ncomp; ++comp)
-                d.hist[nb][hist_at(d.ncap, d.ncomp, s, m) + comp] = d.hist[hc][hist_at(d.ncap, d.ncomp, o, k) + comp];
-            neww[m >> 5] |= 1u << (m & 31);
+            for (int q0 = 0; q0 < count; q0 += 4) {
+                int v[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) v[i] = (q0 + i < count) ? d.nbr[ln][nbr_at(d.ncap, s, q0 + i)] : -2;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (m[j] < 0 && tn[j] >= 0 && v[i] == tn[j]) m[j] = q0 + i;
+                bool done = true;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) done = done && (tn[j] < 0 || m[j] >= 0);
+                if (done) break;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (kk[j] < 0) continue;
+                if (m[j] < 0) {
+                    atomicAdd(&d.ctl->lost_history, 1u);
+                    continue;
+                }
+                for (int comp = 0; comp < d.ncomp; ++comp)
+                    d.hist[nb][hist_at(d.ncap, d.ncomp, s, m[j]) + comp] =
+                        d.hist[hc][hist_at(d.ncap, d.ncomp, o, kk[j]) + comp];
+                set_bit4(n0, n1, n2, n3, m[j]);
+            }
         }
     }
-    for (int w = 0; w < d.nwords; ++w) d.act[nb][(size_t)w * d.ncap + s] = neww[w];
+    const unsigned int nw[4] = {n0, n1, n2, n3};
+#pragma unroll
+    for (int w = 0; w < 4; ++w)
+        if (w < d.nwords) d.act[nb][(size_t)w * d.ncap + s] = nw[w];
     // wall history moves with the particle
     const unsigned int wbits = d.wact[hc][o];
     d.wact[nb][s] = wbits;
@@ -402,17 +449,6 @@ __global__ void __launch_bounds__(128) k_build(DevPtrs d)
         for (int comp = 0; comp < d.ncomp; ++comp)
             d.whist[nb][whist_at(d.ncap, d.ncomp, s, w) + comp] = d.whist[hc][whist_at(d.ncap, d.ncomp, o, w) + comp];
     }
-}
-
-__global__ void k_rb_finish(DevPtrs d)
-{
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Control* ctl = d.ctl;
-    if (!ctl->rebuild) return;
-    ctl->cur ^= 1;
-    ctl->lbuf ^= 1;
-    ctl->disp_acc = 0.0;
-    ctl->n_rebuilds += 1;
 }
 
 // ---------------------------------------------------------------------------

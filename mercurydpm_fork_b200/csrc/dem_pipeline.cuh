@@ -35,24 +35,58 @@ constexpr int DETECT_BLOCK = 128;
 constexpr int CONTACT_BLOCK = 128;
 constexpr int SUM_BLOCK = 128;
 
-// Reverse index of the neighbour lists (after a rebuild): rev[s][k] = m with
-// nbr[t][m] == s for t = nbr[s][k] (the lists are symmetric).
-__global__ void __launch_bounds__(256) k_rev(DevPtrs d)
+// Position of s in the particle-major row of t (the first 16 entries come
+// from `head`, read ahead by the caller); -1 if absent.
+__device__ __forceinline__ int find_in_row(const DevPtrs& d, int s, int t, int ct, const int4 (&head)[4])
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (!d.ctl->rebuild || s >= d.n) return;
-    const int l = d.ctl->lbuf;
-    const int cnt = d.cnt[l][s];
-    for (int k = 0; k < cnt && k < d.cap; ++k) {
-        const int t = d.nbr[l][nbr_at(d.ncap, s, k)];
-        const int ct = min(d.cnt[l][t], d.cap);
-        int m = 0;
-        while (m < ct && d.nbr[l][nbr_at(d.ncap, t, m)] != s) ++m;
-        if (m == ct) {
-            atomicOr(&d.ctl->status, 1u << DEM_ERR_CAPACITY); // an asymmetric pair: the partner's row overflowed
-            m = 0;
+    const int4* row = reinterpret_cast<const int4*>(d.rows + (size_t)t * d.cap); // cap is a multiple of 32
+    for (int m0 = 0; m0 < ct; m0 += 16) {
+        int4 v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = m0 == 0 ? head[j] : ((m0 + 4 * j < ct) ? row[(m0 >> 2) + j] : make_int4(-1, -1, -1, -1));
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int q = m0 + 4 * j;
+            if (q + 0 < ct && v[j].x == s) return q + 0;
+            if (q + 1 < ct && v[j].y == s) return q + 1;
+            if (q + 2 < ct && v[j].z == s) return q + 2;
+            if (q + 3 < ct && v[j].w == s) return q + 3;
         }
-        d.rev[nbr_at(d.ncap, s, k)] = m;
+    }
+    return -1;
+}
+
+// Reverse index of one particle's list (after a rebuild, lists buffer l):
+// rev[s][k] = m with nbr[t][m] == s for t = nbr[s][k] (the lists are
+// symmetric). Two entries at a time; the partners' rows are read from the
+// particle-major copy that build_one writes (the first 16 entries of both
+// rows in flight together). Run by k_rebuild.
+__device__ __forceinline__ void rev_one(const DevPtrs& d, int s, int l)
+{
+    const int cnt = min(d.cnt[l][s], d.cap);
+    for (int k0 = 0; k0 < cnt; k0 += 2) {
+        int t[2], ct[2];
+        int4 head[2][4];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) t[j] = (k0 + j < cnt) ? d.nbr[l][nbr_at(d.ncap, s, k0 + j)] : -1;
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+            if (t[j] >= 0) {
+                ct[j] = d.cnt[l][t[j]];
+                const int4* row = reinterpret_cast<const int4*>(d.rows + (size_t)t[j] * d.cap);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) head[j][q] = row[q]; // 16 <= cap entries: inside the row
+            }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            if (t[j] < 0) continue;
+            int m = find_in_row(d, s, t[j], min(ct[j], d.cap), head[j]);
+            if (m < 0) {
+                atomicOr(&d.ctl->status, 1u << DEM_ERR_CAPACITY); // an asymmetric pair: the partner's row overflowed
+                m = 0;
+            }
+            d.rev[nbr_at(d.ncap, s, k0 + j)] = m;
+        }
     }
 }
 
@@ -81,16 +115,18 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& 
 template <int MODE, int NCOMP>
 __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
 {
+    constexpr int HIT_KEEP = 16; // partner slots of the first hits, kept for the item pass
     __shared__ int warp_sums[DETECT_BLOCK / 32];
     __shared__ int block_base;
+    __shared__ int kept_t[HIT_KEEP][DETECT_BLOCK];
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     Control* ctl = d.ctl;
     const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
     const bool first = (MODE == 1) && ctl->first_step;
     const bool active = s < d.n;
-    unsigned int hitbits[4] = {0u, 0u, 0u, 0u}, newbits[4] = {0u, 0u, 0u, 0u};
-    constexpr int HIT_KEEP = 16; // partner slots of the first hits, kept for the item pass
-    int hit_t[HIT_KEEP];
+    // hit bits of the (at most 4) list words, in registers: each word is
+    // finished before the next starts, so no dynamically indexed array
+    unsigned int hit0 = 0u, hit1 = 0u, hit2 = 0u, hit3 = 0u;
     int nkept = 0;
     unsigned int whit = 0u, wnew = 0u;
     int count = 0, nwalls = 0;
@@ -99,56 +135,64 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         const int4 is = d.info[c][s];
         const InstanceDev& I = d.inst[is.z];
         const V3 xs = xyz(ps);
-        unsigned int a[4] = {0u, 0u, 0u, 0u};
-        for (int w = 0; w < d.nwords; ++w) a[w] = d.act[c][(size_t)w * d.ncap + s];
         count = min(d.cnt[l][s], d.cap);
         const int ns = I.n_species;
-        constexpr int B = 4; // entries whose gathers are in flight together
+        constexpr int B = 2; // entries whose gathers are in flight together (divides 32; 2 keeps 80 registers)
         const int2* info2 = reinterpret_cast<const int2*>(d.info[c]); // (id, species) of each info record
-        for (int k0 = 0; k0 < count; k0 += B) {
-        int tb[B];
-        double4 ptb[B];
-        int2 itb[B];
+        for (int w = 0; w < d.nwords; ++w) {
+            unsigned int hitw = 0u, neww = 0u;
+            const unsigned int aw = first ? d.act[c][(size_t)w * d.ncap + s] : 0u;
+            const int kend = min(count, 32 * w + 32);
+            for (int k0 = 32 * w; k0 < kend; k0 += B) {
+                int tb[B];
+                double4 ptb[B];
+                int2 itb[B];
 #pragma unroll
-        for (int j = 0; j < B; ++j) tb[j] = (k0 + j < count) ? d.nbr[l][nbr_at(d.ncap, s, k0 + j)] : -1;
+                for (int j = 0; j < B; ++j) tb[j] = (k0 + j < kend) ? d.nbr[l][nbr_at(d.ncap, s, k0 + j)] : -1;
 #pragma unroll
-        for (int j = 0; j < B; ++j)
-            if (tb[j] >= 0) {
-                ptb[j] = d.pr[c][tb[j]];
-                itb[j] = info2[2 * (size_t)tb[j]];
-            }
+                for (int j = 0; j < B; ++j)
+                    if (tb[j] >= 0) {
+                        ptb[j] = d.pr[c][tb[j]];
+                        itb[j] = info2[2 * (size_t)tb[j]];
+                    }
 #pragma unroll
-        for (int j = 0; j < B; ++j) {
-            const int k = k0 + j;
-            if (k >= count) break;
-            const size_t e = nbr_at(d.ncap, s, k);
-            const double4 pt = ptb[j];
-            const int2 it = itb[j];
-            bool periodic;
-            const V3 xt = image_of(I, xs, xyz(pt), periodic);
-            if (!periodic && !(is.x < it.x)) { // the partner (lower id) owns this pair
-                d.slot[e] = SLOT_IS_I;
-                continue;
+                for (int j = 0; j < B; ++j) {
+                    const int k = k0 + j;
+                    if (k >= kend) break;
+                    const size_t e = nbr_at(d.ncap, s, k);
+                    const double4 pt = ptb[j];
+                    const int2 it = itb[j];
+                    bool periodic;
+                    const V3 xt = image_of(I, xs, xyz(pt), periodic);
+                    if (!periodic && !(is.x < it.x)) { // the partner (lower id) owns this pair
+                        d.slot[e] = SLOT_IS_I;
+                        continue;
+                    }
+                    d.slot[e] = SLOT_NONE;
+                    const V3 branch = xs - xt;
+                    const double d2 = len2(branch);
+                    double idist = 0.0; // x + 0.0 == x: skipping the lookup keeps the predicate exact
+                    if (!d.zero_idist) idist = d.species[I.species_offset + is.y * ns + it.y].interaction_distance;
+                    const double sum = pt.w + ps.w + idist; // rI + rP + distance (BaseParticle.cc:695-697)
+                    const unsigned int bit = 1u << (k & 31);
+                    if (!(d2 >= sum * sum)) {
+                        hitw |= bit;
+                        if (nkept < HIT_KEEP) kept_t[nkept++][threadIdx.x] = tb[j];
+                        neww |= bit;
+                    } else if (first && (aw & bit) && !(periodic && is.x > it.x)) {
+                        // an interaction of the initial evaluation outlives step 0
+                        // (InteractionHandler::eraseOldInteractions erases stamps <= 0 only)
+                        for (int q = 0; q < NCOMP; ++q)
+                            d.hist[nb][hist_at(d.ncap, NCOMP, s, k) + q] = d.hist[c][hist_at(d.ncap, NCOMP, s, k) + q];
+                        neww |= bit;
+                    }
+                }
             }
-            d.slot[e] = SLOT_NONE;
-            const V3 branch = xs - xt;
-            const double d2 = len2(branch);
-            double idist = 0.0; // x + 0.0 == x: skipping the lookup keeps the predicate exact
-            if (!d.zero_idist) idist = d.species[I.species_offset + is.y * ns + it.y].interaction_distance;
-            const double sum = pt.w + ps.w + idist; // rI + rP + distance (BaseParticle.cc:695-697)
-            const unsigned int bit = 1u << (k & 31);
-            if (!(d2 >= sum * sum)) {
-                hitbits[k >> 5] |= bit;
-                if (nkept < HIT_KEEP) hit_t[nkept++] = tb[j];
-                newbits[k >> 5] |= bit;
-            } else if (first && (a[k >> 5] & bit) && !(periodic && is.x > it.x)) {
-                // an interaction of the initial evaluation outlives step 0
-                // (InteractionHandler::eraseOldInteractions erases stamps <= 0 only)
-                for (int q = 0; q < NCOMP; ++q)
-                    d.hist[nb][hist_at(d.ncap, NCOMP, s, k) + q] = d.hist[c][hist_at(d.ncap, NCOMP, s, k) + q];
-                newbits[k >> 5] |= bit;
-            }
-        }
+            d.act[nb][(size_t)w * d.ncap + s] = neww;
+            if (w == 0) hit0 = hitw;
+            else if (w == 1) hit1 = hitw;
+            else if (w == 2) hit2 = hitw;
+            else hit3 = hitw;
         }
         if (!(is.w & FLAG_FIXED)) {
             const unsigned int wa = d.wact[c][s];
@@ -171,13 +215,13 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
                 }
             }
         }
-        for (int w = 0; w < d.nwords; ++w) d.act[nb][(size_t)w * d.ncap + s] = newbits[w];
         d.wact[nb][s] = wnew;
     }
     // ---- compact the contacts of the block into the item list ----
+    const unsigned int hits[4] = {hit0, hit1, hit2, hit3};
     int nh = __popc(whit);
 #pragma unroll
-    for (int w = 0; w < 4; ++w) nh += __popc(hitbits[w]);
+    for (int w = 0; w < 4; ++w) nh += __popc(hits[w]);
     int total;
     const int off = block_exclusive_scan(nh, warp_sums, total);
     if (threadIdx.x == 0) block_base = total ? (int)atomicAdd(&ctl->n_items, (unsigned)total) : 0;
@@ -191,11 +235,11 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
     int nh_seen = 0;
 #pragma unroll
     for (int w = 0; w < 4; ++w) {
-        unsigned int b = hitbits[w];
+        unsigned int b = hits[w];
         while (b) {
             const int k = w * 32 + __ffs(b) - 1;
             b &= b - 1;
-            const int t = (nh_seen < HIT_KEEP) ? hit_t[nh_seen] : d.nbr[l][nbr_at(d.ncap, s, k)];
+            const int t = (nh_seen < HIT_KEEP) ? kept_t[nh_seen][threadIdx.x] : d.nbr[l][nbr_at(d.ncap, s, k)];
             ++nh_seen;
             d.items[q] = make_int4(s, k, t, 0);
             d.slot[nbr_at(d.ncap, s, k)] = q;
@@ -311,12 +355,14 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             }
             pid_i = it.x;
         }
-        const Springs before = spr;
         ContactOut out;
         evaluate_contact<NLAW, FLAW>(*spp, g, spr, dt, out);
         // step 0 keeps the lower-id side's old spring of a periodic pair that
-        // existed at the initial evaluation (equal stamps, InteractionHandler.cc:339-352)
-        const Springs& kept = (first && periodic && !(is.x > pid_i) && was_active) ? before : spr;
+        // existed at the initial evaluation (equal stamps, InteractionHandler.cc:339-352);
+        // that side is not derived and was active, so its old spring is its own
+        // stored one, read again here instead of kept in registers
+        Springs kept = spr;
+        if (first && periodic && !(is.x > pid_i) && was_active) load_springs(d.hist[c], hb, 1, NCOMP, kept);
         store_springs(hdst, hb, 1, NCOMP, kept);
         double* sh = d.shares + (size_t)q * SHARE;
         const V3 tp = out.torque - cross(xq - g.c, out.force);
@@ -338,7 +384,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(SUM_BLOCK) k_sum(DevPtrs d)
+__global__ void __launch_bounds__(SUM_BLOCK, 5) k_sum(DevPtrs d)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     Control* ctl = d.ctl;

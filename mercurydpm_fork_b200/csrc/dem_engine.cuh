@@ -158,7 +158,7 @@ struct DevPtrs {
     int wmax;         // max walls per instance
     int ncells;
     int rotation;
-    int single_instance;   // one instance: its record is staged in shared memory
+    int single_instance;   // one instance: k_contacts stages its record in shared memory
     int n_species_table;   // entries of the species table
     int zero_idist;        // every species pair has interaction distance 0
     double dt;

@@ -285,7 +285,7 @@ def run_profile_target(args):
     force kernel (dem_time_force_kernel). Prints the kernel-launch plan."""
     from mercurydpm_fork_b200 import DemEngine
     sc = workload()
-    # direct launches: ncu cannot profile kernel nodes of graphs with conditional nodes
+    # direct launches: every kernel of a time step is its own launch in ncu's list
     eng = DemEngine(sc.time_step, [sc.instance], sc.species, sc.walls, rotation=True, use_graphs=False)
     eng.upload(sc.position, sc.velocity, sc.radius, sc.inv_mass, sc.inv_inertia, sc.species_index, sc.ids)
     eng.step(args.profile_steps)

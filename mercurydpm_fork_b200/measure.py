@@ -1,8 +1,10 @@
 """Throughput of the workloads other than the headline bench (bench.py):
 
-    python -m mercurydpm_fork_b200.measure drum        # 1M-sphere rotating drum, Hertz-Mindlin
+    python -m mercurydpm_fork_b200.measure drum        # 1M-sphere rotating drum, Hertz-Mindlin (loose start)
+    python -m mercurydpm_fork_b200.measure drum_dense  # the same drum started as a touching lattice bed
     python -m mercurydpm_fork_b200.measure heaps       # 1,024 batched calibration heaps
     python -m mercurydpm_fork_b200.measure surrogate   # MLP inference / training on the tensor cores
+    python -m mercurydpm_fork_b200.measure calibration # calibrations per hour at 2 % response error
 
 Each prints one JSON line. Device time comes from CUDA events (dem_step's own
 events for DEM; torch events around the calls for the surrogate).
@@ -31,17 +33,25 @@ def _time_dem(e, n_moving, steps_per_call=200, calls=5, warmup=2):
                 (steps_per_call * calls))
 
 
-def drum(n=1_000_000, radius_d=175.0, length_d=60.0):
+def drum(n=1_000_000, radius_d=175.0, length_d=60.0, site_spacing=1.02, workload="rotating_drum"):
     from . import scenarios
-    sc = scenarios.rotating_drum(n=n, radius_d=radius_d, length_d=length_d, vstd=0.0)
+    sc = scenarios.rotating_drum(n=n, radius_d=radius_d, length_d=length_d, vstd=0.0, site_spacing=site_spacing)
     e = sc.engine()
     out = _time_dem(e, sc.n_moving)
     out["counts"] = e.counts()
     e.close()
-    out.update(workload="rotating_drum", n=sc.n, radius_d=radius_d, length_d=length_d,
+    out.update(workload=workload, site_spacing_d=site_spacing, n=sc.n, radius_d=radius_d, length_d=length_d,
                solid_fraction_of_drum=sc.info["solid_fraction_of_drum"], dt=sc.time_step,
                species="HertzianViscoelasticMindlinRollingTorsion")
     return out
+
+
+def drum_dense():
+    """The drum with its bed started as a lattice whose neighbours overlap by
+    0.1 % of a diameter: every sphere is in contact from the first step, as in
+    a settled bed (the loose start of `drum` spends the timed steps in free
+    fall)."""
+    return drum(site_spacing=0.999, workload="rotating_drum_dense_bed")
 
 
 def heaps(n_instances=1024, seed=1):
@@ -85,7 +95,46 @@ def surrogate(batch=65536, train_batch=1024, reps=20):
                 note="inference_ms / train_step_ms: host-to-host per call; inference_device_ms: CUDA events")
 
 
+def calibration(n_train=2048, n_targets=8, tol=0.02, rounds=4, proposals=256, seed=3):
+    """Calibrations per hour at `tol` response error: training heaps from
+    batched DEM, the surrogate trained on them, then one calibration per
+    held-out target (parameters drawn from the same box, their responses from
+    DEM), timed host to host. Every heap is the 600-sphere heap of
+    `calibration.heap_responses` (20,000 steps)."""
+    from . import calibration as cal
+    from .surrogate import Surrogate
+    rng = np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    x = cal.sample_params(rng, n_train)
+    y = cal.heap_responses(x)
+    t_data = time.perf_counter() - t0
+    s = Surrogate(capacity=65536, seed=0)
+    s.fit_normalisation(x, y)
+    t0 = time.perf_counter()
+    s.fit(x, y, epochs=200, batch=1024)
+    t_train = time.perf_counter() - t0
+    pt = cal.sample_params(rng, n_targets)
+    targets = cal.heap_responses(pt)
+    times, errors, n_rounds = [], [], []
+    for k in range(n_targets):
+        t0 = time.perf_counter()
+        res = cal.calibrate(targets[k], cal.heap_responses, surrogate=s, rounds=rounds, proposals=proposals,
+                            candidates=65_536, tol=tol, seed=k, data=(x, y))
+        times.append(time.perf_counter() - t0)
+        errors.append(res["best_error"])
+        n_rounds.append(res["rounds"])
+    s.close()
+    ok = [e <= tol for e in errors]
+    mean_t = float(np.mean(times))
+    return dict(workload="calibration", value=3600.0 / mean_t, unit="calibrations/hour", tol=tol,
+                succeeded=int(sum(ok)), targets=n_targets, mean_seconds=mean_t, rounds=n_rounds,
+                best_errors=[round(e, 5) for e in errors], proposals_per_round=proposals,
+                training_runs=n_train, training_data_s=t_data, training_s=t_train,
+                per_hour_with_training_amortised_over_100=3600.0 / (mean_t + (t_data + t_train) / 100.0),
+                heap="600 spheres, 20,000 steps, lognormal PSD, rough floor disk (calibration.heap_responses)")
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "drum"
-    fn = dict(drum=drum, heaps=heaps, surrogate=surrogate)[which]
+    fn = dict(drum=drum, drum_dense=drum_dense, heaps=heaps, surrogate=surrogate, calibration=calibration)[which]
     print(json.dumps(fn()))

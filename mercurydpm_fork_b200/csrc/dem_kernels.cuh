@@ -148,12 +148,14 @@ __device__ __forceinline__ void gather_one(const DevPtrs& d, int s, int c)
     const int nb = c ^ 1;
     const int o = d.perm[s];
     const double4 p = d.pr[c][o];
+    const int4 inf = d.info[c][o];
     d.pr[nb][s] = p;
-    d.pf[s] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
+    const double* g = d.inst[inf.z].origin; // relative to the grid origin: small magnitudes in FP32
+    d.pf[s] = make_float4((float)(p.x - g[0]), (float)(p.y - g[1]), (float)(p.z - g[2]), (float)p.w);
     d.vm[nb][s] = d.vm[c][o];
     d.wi[nb][s] = d.wi[c][o];
     d.qo[nb][s] = d.qo[c][o];
-    d.info[nb][s] = d.info[c][o];
+    d.info[nb][s] = inf;
     d.caller[nb][s] = d.caller[c][o];
     d.newidx[o] = s;
 }
@@ -257,11 +259,13 @@ __device__ __forceinline__ void row_ranges(const DevPtrs& d, const InstanceDev& 
 
 // Neighbour list of one particle: every particle of the cells within reach
 // whose distance is below r_s + r_t + interaction distance + skin, in
-// cell-row order. The distance test runs in FP32 on the `pf` copy with a
-// margin that bounds its rounding (16 units of FP32 rounding on the cut and
-// on the magnitudes of the coordinates and the period), so the list is a
-// superset of the FP64 test's list; pairs whose periodic image is ambiguous
-// in FP32 take the FP64 test. Contacts themselves are always decided in FP64
+// cell-row order. The distance test runs in FP32 on the `pf` copy
+// (coordinates relative to the grid origin) with a margin that bounds its
+// rounding (16 units of FP32 rounding on the cut and on the magnitudes of the
+// coordinates and the period), so the list is a superset of the FP64 test's
+// list; pairs whose periodic image is ambiguous in FP32, or whose margin
+// exceeds 1/16 of the cut (coordinates very large against the particles),
+// take the FP64 test. Contacts themselves are always decided in FP64
 // by the force evaluation, so the superset changes no result. The next row's
 // slot ranges are read ahead and candidates are read BUILD_BATCH at a time.
 constexpr int BUILD_BATCH = 2;
@@ -350,8 +354,8 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
                             }
                         }
                         bool near;
-                        if (!ambiguous) {
-                            const float cut = (fs.w + ft.w) + extra_f;
+                        const float cut = (fs.w + ft.w) + extra_f;
+                        if (!ambiguous && err <= 0.0625f * cut) {
                             const float lim = cut * (1.0f + U20) + err;
                             near = (bq[0] * bq[0] + bq[1] * bq[1] + bq[2] * bq[2]) < lim * lim;
                         } else { // the FP64 test of the sequential scan

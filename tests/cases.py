@@ -39,6 +39,20 @@ def small_chute(n_flow=3000, seed=7):
     return sc
 
 
+def offset_chute(offset=1000.0):
+    """small_chute moved `offset` metres along every axis (domain, periodic
+    bounds and particles): coordinates are a million particle diameters from
+    the origin, where FP32 keeps about 0.1 mm of resolution."""
+    import dataclasses
+    sc = small_chute()
+    inst = sc.instance
+    shift = lambda t: tuple(float(v) + offset for v in t)
+    sc.instance = dataclasses.replace(inst, domain_min=shift(inst.domain_min), domain_max=shift(inst.domain_max),
+                                      periodic_min=shift(inst.periodic_min), periodic_max=shift(inst.periodic_max))
+    sc.position = sc.position + offset
+    return sc
+
+
 def cubic_packing(n=5, distance=0.99):
     """Drivers/UnitTests/CG3DPackingUnitTest.cpp: n^3 spheres (r = 0.5) on a
     cubic lattice of spacing 0.99 in a triply periodic box; every contact

@@ -243,6 +243,12 @@ int  dem_create(const dem_config *config, const dem_instance_desc *instances,
 int  dem_set_species(dem_handle *h, const dem_species_pair *table, int n_entries);
 /* WallHandler contents (before dem_upload_particles). */
 int  dem_set_walls(dem_handle *h, const dem_wall *walls, int n);
+/* PeriodicBoundary objects of one instance's BoundaryHandler
+ * (PeriodicBoundary::set, Kernel/Boundaries/PeriodicBoundary.cc:84-108): the
+ * directions in mask (bit k = axis k) become periodic between lo[k] and
+ * hi[k], the others take the instance's domain. The same fields as
+ * dem_instance_desc's periodic_*; before dem_upload_particles. */
+int  dem_set_periodic(dem_handle *h, int instance, const double lo[3], const double hi[3], uint32_t mask);
 /* DeletionBoundary objects of BoundaryHandler, at most
  * DEM_MAX_DELETION_PER_INSTANCE per instance (before dem_upload_particles). */
 int  dem_set_deletion_boundaries(dem_handle *h, const dem_deletion_boundary *b, int n);
@@ -275,6 +281,14 @@ int  dem_reduce(dem_handle *h, int instance, dem_globals *out);
  * and contact counts are accumulated with atomics, so their last bits may
  * vary between runs. */
 int  dem_reduce_batch(dem_handle *h, int first, int count, dem_globals *out);
+/* The batch form of the API: n_instances independent simulations in one
+ * handle (dem_create with config->n_instances = n_instances; particles name
+ * their instance in dem_particles_soa.instance, which is the instance-offset
+ * table of the batch), and a run of nsteps followed by the balances of every
+ * instance (out: n_instances entries). */
+int  dem_batch_create(const dem_config *config, int n_instances, const dem_instance_desc *instances,
+                      dem_handle **out);
+int  dem_batch_run(dem_handle *h, int nsteps, dem_globals *out);
 /* The balances of dem_reduce, computed without allocating any device memory.
  * It has no counterpart in the reference. It is for callers that may not
  * allocate GPU memory at the point where they need the balances, e.g. a

@@ -123,6 +123,7 @@ _SIGNATURES = {
     "dem_create": (C.c_int, [C.POINTER(Config), C.POINTER(InstanceDesc), C.POINTER(C.c_void_p)]),
     "dem_set_species": (C.c_int, [C.c_void_p, C.POINTER(SpeciesPair), C.c_int]),
     "dem_set_walls": (C.c_int, [C.c_void_p, C.POINTER(Wall), C.c_int]),
+    "dem_set_periodic": (C.c_int, [C.c_void_p, C.c_int, _pd, _pd, C.c_uint32]),
     "dem_upload_particles": (C.c_int, [C.c_void_p, C.POINTER(ParticlesSoA)]),
     "dem_upload_contacts": (C.c_int, [C.c_void_p, C.POINTER(ContactsSoA)]),
     "dem_step": (C.c_int, [C.c_void_p, C.c_int]),
@@ -132,6 +133,8 @@ _SIGNATURES = {
     "dem_download_contacts": (C.c_int, [C.c_void_p, C.POINTER(ContactsSoA), _i64, C.POINTER(_i64)]),
     "dem_reduce": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Globals)]),
     "dem_reduce_batch": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(Globals)]),
+    "dem_batch_create": (C.c_int, [C.POINTER(Config), C.c_int, C.POINTER(InstanceDesc), C.POINTER(C.c_void_p)]),
+    "dem_batch_run": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Globals)]),
     "dem_set_deletion_boundaries": (C.c_int, [C.c_void_p, C.POINTER(DeletionBoundary), C.c_int]),
     "dem_reduce_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Globals)]),
     "dem_cg_eval": (C.c_int, [C.c_void_p, C.POINTER(CGGrid), _pd]),

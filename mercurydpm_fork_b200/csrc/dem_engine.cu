@@ -371,6 +371,32 @@ int dem_set_species(dem_handle* hh, const dem_species_pair* table, int n_entries
     return DEM_OK;
 }
 
+int dem_set_periodic(dem_handle* hh, int instance, const double lo[3], const double hi[3], uint32_t mask)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || mask > 7u || ((mask != 0u) && (!lo || !hi))) return fail(h, DEM_ERR_BAD_INPUT, "dem_set_periodic: bad arguments");
+    if (instance < 0 || instance >= (int)h->inst_desc.size())
+        return fail(h, DEM_ERR_BAD_INPUT, "dem_set_periodic: instance out of range");
+    if (h->uploaded) return fail(h, DEM_ERR_STATE, "dem_set_periodic must come before dem_upload_particles");
+    dem_instance_desc in = h->inst_desc[instance];
+    for (int k = 0; k < 3; ++k) {
+        if ((mask >> k) & 1u) {
+            if (!(std::isfinite(lo[k]) && std::isfinite(hi[k]) && hi[k] > lo[k]))
+                return fail(h, DEM_ERR_BAD_INPUT, "dem_set_periodic: empty periodic interval");
+            in.periodic_min[k] = lo[k];
+            in.periodic_max[k] = hi[k];
+        } else {
+            if (!(in.domain_max[k] > in.domain_min[k]))
+                return fail(h, DEM_ERR_BAD_INPUT, "dem_set_periodic: a non-periodic direction needs a domain");
+            in.periodic_min[k] = 0.0;
+            in.periodic_max[k] = 0.0;
+        }
+    }
+    in.periodic_mask = mask;
+    h->inst_desc[instance] = in;
+    return DEM_OK;
+}
+
 int dem_set_walls(dem_handle* hh, const dem_wall* walls, int n)
 {
     Handle* h = reinterpret_cast<Handle*>(hh);
@@ -1278,3 +1304,20 @@ int dem_cg_eval(dem_handle* hh, const dem_cg_grid* grid, double* fields_out);
 } // extern "C"
 
 #include "dem_cg.cuh"
+
+int dem_batch_create(const dem_config* config, int n_instances, const dem_instance_desc* instances, dem_handle** out)
+{
+    if (!config || n_instances < 1) return DEM_ERR_BAD_INPUT;
+    dem_config c = *config;
+    c.n_instances = n_instances;
+    return dem_create(&c, instances, out);
+}
+
+int dem_batch_run(dem_handle* hh, int nsteps, dem_globals* out)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !out) return fail(h, DEM_ERR_BAD_INPUT, "dem_batch_run: bad arguments");
+    int rc = dem_step(hh, nsteps);
+    if (rc) return rc;
+    return dem_reduce_batch(hh, 0, (int)h->inst.size(), out);
+}

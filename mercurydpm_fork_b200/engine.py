@@ -156,7 +156,7 @@ class DemEngine:
     def __init__(self, time_step: float, instances: list[Instance], species: list[_abi.SpeciesPair],
                  walls: list[_abi.Wall] | None = None, rotation: bool = True, background_drag: float = 0.0,
                  max_neighbors: int = 0, skin: float = 0.0, use_graphs: bool = True, device: int = 0,
-                 deletions: list | None = None):
+                 deletions: list | None = None, batch_api: bool = False):
         self._h = C.c_void_p()
         cfg = _abi.Config()
         cfg.time_step = time_step
@@ -168,9 +168,12 @@ class DemEngine:
         cfg.skin = skin
         cfg.n_instances = len(instances)
         arr = (_abi.InstanceDesc * len(instances))(*[i.to_c() for i in instances])
-        rc = lib().dem_create(C.byref(cfg), arr, C.byref(self._h))
+        if batch_api:
+            rc = lib().dem_batch_create(C.byref(cfg), len(instances), arr, C.byref(self._h))
+        else:
+            rc = lib().dem_create(C.byref(cfg), arr, C.byref(self._h))
         if rc:
-            raise DemError(rc, "dem_create failed")
+            raise DemError(rc, "dem_batch_create failed" if batch_api else "dem_create failed")
         self.n_instances = len(instances)
         sp = (_abi.SpeciesPair * len(species))(*species)
         self._check(lib().dem_set_species(self._h, sp, len(species)))
@@ -292,12 +295,28 @@ class DemEngine:
                     mass=g.mass, centre_of_mass=np.array(g.centre_of_mass[:]), n_contacts=g.n_contacts,
                     n_wall_contacts=g.n_wall_contacts, time=g.time, n_steps=g.n_steps)
 
+    def set_periodic(self, instance: int, lo, hi, mask: int):
+        """dem_set_periodic (before upload)."""
+        a = (C.c_double * 3)(*map(float, lo))
+        b = (C.c_double * 3)(*map(float, hi))
+        self._check(lib().dem_set_periodic(self._h, instance, a, b, mask))
+
+    def batch_run(self, nsteps: int) -> dict:
+        """dem_batch_run: nsteps, then the balances of every instance (as reduce_batch)."""
+        arr = (_abi.Globals * max(1, self.n_instances))()
+        self._check(lib().dem_batch_run(self._h, nsteps, arr))
+        return self._globals_rows(arr, self.n_instances)
+
     def reduce_batch(self, first: int = 0, count: int | None = None) -> dict:
         """dem_reduce_batch: the balances of instances first..first+count-1 as
         arrays with one row per instance."""
         count = self.n_instances - first if count is None else count
         arr = (_abi.Globals * max(1, count))()
         self._check(lib().dem_reduce_batch(self._h, first, count, arr))
+        return self._globals_rows(arr, count)
+
+    @staticmethod
+    def _globals_rows(arr, count: int) -> dict:
         g = arr[:count]
         return dict(kinetic_energy=np.array([x.kinetic_energy for x in g]),
                     rotational_energy=np.array([x.rotational_energy for x in g]),

@@ -140,3 +140,41 @@ def test_heap_batch_matches_oracle_and_runs(gpu):
     assert res["kinetic_energy"].shape == (4, 5)
     assert np.isfinite(res["aor_reference"]).all()
     assert (res["n_remaining"] > 0).all()
+
+
+def test_batch_api_equals_step_and_reduce_batch(gpu):
+    """dem_batch_create + dem_batch_run against dem_create + dem_step +
+    dem_reduce_batch on the same batch: the same run, the same balances."""
+    b = scenarios.batch(_members())
+    e1 = b.engine(batch_api=True)
+    g1 = e1.batch_run(30)
+    x1 = e1.download()["position"]
+    e1.close()
+    e2 = b.engine()
+    e2.step(30)
+    g2 = e2.reduce_batch()
+    x2 = e2.download()["position"]
+    e2.close()
+    np.testing.assert_array_equal(x1, x2)
+    for key in ("kinetic_energy", "rotational_energy", "gravitational_energy", "mass", "n_contacts", "n_wall_contacts"):
+        np.testing.assert_array_equal(g1[key], g2[key])
+    np.testing.assert_allclose(g1["elastic_energy"], g2["elastic_energy"], rtol=1e-12)  # atomics: last bits
+
+
+def test_set_periodic_equals_instance_description(gpu):
+    """dem_set_periodic before the upload gives the run that periodic bounds
+    in the instance description give."""
+    from mercurydpm_fork_b200.engine import DemEngine
+    sc = cases.small_chute(n_flow=600)
+    inst = sc.instance
+    plain = dataclasses.replace(inst, periodic_mask=0, periodic_min=(0.0, 0.0, 0.0), periodic_max=(0.0, 0.0, 0.0))
+    e1 = DemEngine(sc.time_step, [plain], sc.species, sc.walls, rotation=sc.rotation)
+    e1.set_periodic(0, inst.periodic_min, inst.periodic_max, inst.periodic_mask)
+    e1.upload(sc.position, sc.velocity, sc.radius, sc.inv_mass, sc.inv_inertia, sc.species_index, sc.ids)
+    e1.step(20)
+    e2 = sc.engine()
+    e2.step(20)
+    np.testing.assert_array_equal(e1.download()["position"], e2.download()["position"])
+    np.testing.assert_array_equal(e1.forces()[0], e2.forces()[0])
+    e1.close()
+    e2.close()

@@ -5,6 +5,7 @@
     python -m mercurydpm_fork_b200.measure heaps       # 1,024 batched calibration heaps
     python -m mercurydpm_fork_b200.measure surrogate   # MLP inference / training on the tensor cores
     python -m mercurydpm_fork_b200.measure calibration # calibrations per hour at 2 % response error
+    python -m mercurydpm_fork_b200.measure cg          # Gaussian CG of the 200k chute (XZ 100 x 1 x 50)
 
 Each prints one JSON line. Device time comes from CUDA events (dem_step's own
 events for DEM; torch events around the calls for the surrogate).
@@ -134,7 +135,41 @@ def calibration(n_train=2048, n_targets=8, tol=0.02, rounds=4, proposals=256, se
                 heap="600 spheres, 20,000 steps, lognormal PSD, rough floor disk (calibration.heap_responses)")
 
 
+def cg(reps=10, steps_between=1000):
+    """Gaussian coarse-graining of the 200k periodic chute on an XZ grid of
+    100 x 1 x 50 points, width one small diameter, cutoff 3 widths (the
+    chute config's CG), evaluated after a flowing phase: ms per evaluation
+    host to host (fields copied back), and its share of a 1,000-step
+    interval."""
+    from . import scenarios
+    from ._abi import DEM_CG_XZ
+    sc = scenarios.periodic_chute(n_flow=200_000, seed=2, packing="layers", spacing_factor=1.0)
+    e = sc.engine()
+    e.step(0)
+    e.step(200)
+    d_small = 1e-3
+    x = e.download()["position"]
+    inst = sc.instance
+    lo = (inst.periodic_min[0], inst.periodic_min[1], float(inst.domain_min[2]))
+    hi = (inst.periodic_max[0], inst.periodic_max[1], float(x[:, 2].max()) + d_small)
+    n = (100, 1, 50)
+    e.cg(DEM_CG_XZ, n, lo, hi, d_small)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        f = e.cg(DEM_CG_XZ, n, lo, hi, d_small)
+    cg_ms = (time.perf_counter() - t0) / reps * 1e3
+    e.step(steps_between)
+    step_ms = e.stats()["ms"]
+    cnt = e.counts()
+    e.close()
+    return dict(workload="cg_chute_xz", value=cg_ms, unit="ms per CG evaluation (host to host)", points=list(n),
+                fields=int(f.shape[1]), width=d_small, cutoff_widths=3.0, particles=sc.n, contacts=cnt["contacts"],
+                steps_between=steps_between, step_loop_ms=step_ms,
+                cg_share_of_interval=cg_ms / (cg_ms + step_ms))
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "drum"
-    fn = dict(drum=drum, drum_dense=drum_dense, heaps=heaps, surrogate=surrogate, calibration=calibration)[which]
+    fn = dict(drum=drum, drum_dense=drum_dense, heaps=heaps, surrogate=surrogate, calibration=calibration,
+              cg=cg)[which]
     print(json.dumps(fn()))

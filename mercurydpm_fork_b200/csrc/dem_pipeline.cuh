@@ -329,6 +329,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
         double* hdst;
         size_t hb;
         V3 xt = zero3();
+        int rv = 0; // I's entry for this pair (reverse index), read with the other gathers
         if (is_wall) {
             // DPMBase::computeForcesDueToWalls / BaseWall::getInteractionWith
             // (DPMBase.cc:3188-3215, BaseWall.cc:367-437)
@@ -358,6 +359,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
         } else {
             const size_t e = nbr_at(d.ncap, s, kq);
             tq = item.z;
+            rv = d.rev[e];
             hb = hist_at(d.ncap, NCOMP, s, kq);
             Springs own; // read before the active bit is known: one less dependent load
             load_springs(d.hist[c], hb, 1, NCOMP, own);
@@ -387,7 +389,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             // BaseInteraction::copySwitchPointer / reverseHistory)
             const bool derived = periodic && (is.x > it.x);
             if (derived) {
-                const int m = d.rev[e];
+                const int m = rv;
                 if ((d.act[c][(size_t)(m >> 5) * d.ncap + tq] >> (m & 31)) & 1u) {
                     load_springs(d.hist[c], hist_at(d.ncap, NCOMP, tq, m), 1, NCOMP, spr);
                     spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
@@ -406,16 +408,19 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
         Springs kept = spr;
         if (first && periodic && !(is.x > pid_i) && was_active) load_springs(d.hist[c], hb, 1, NCOMP, kept);
         store_springs(hdst, hb, 1, NCOMP, kept);
-        double* sh = d.shares + (size_t)q * SHARE;
+        // shares as 16-byte stores (96-byte items: every item and half is 16-byte aligned)
+        double2* sh = reinterpret_cast<double2*>(d.shares + (size_t)q * SHARE);
         const V3 tp = out.torque - cross(xq - g.c, out.force);
-        sh[0] = out.force.x; sh[1] = out.force.y; sh[2] = out.force.z;
-        sh[3] = tp.x; sh[4] = tp.y; sh[5] = tp.z;
+        sh[0] = make_double2(out.force.x, out.force.y);
+        sh[1] = make_double2(out.force.z, tp.x);
+        sh[2] = make_double2(tp.y, tp.z);
         if (!is_wall && !periodic) { // I's share of an ordinary pair, announced in I's own entry
             const V3 fi = -out.force;
             const V3 ti = -out.torque + cross(xt - g.c, out.force);
-            sh[6] = fi.x; sh[7] = fi.y; sh[8] = fi.z;
-            sh[9] = ti.x; sh[10] = ti.y; sh[11] = ti.z;
-            d.slot[nbr_at(d.ncap, tq, d.rev[nbr_at(d.ncap, s, kq)])] = SLOT_I_BASE - q;
+            sh[3] = make_double2(fi.x, fi.y);
+            sh[4] = make_double2(fi.z, ti.x);
+            sh[5] = make_double2(ti.y, ti.z);
+            d.slot[nbr_at(d.ncap, tq, rv)] = SLOT_I_BASE - q;
         }
         if (record && (is_wall || !periodic || is.x < pid_i)) {
             const double meff = 1.0 / (g.inv_mass_p + g.inv_mass_i);
@@ -460,9 +465,10 @@ __global__ void __launch_bounds__(SUM_BLOCK, 5) k_sum(DevPtrs d)
                     half = 6;
                 }
                 if (q >= 0) {
-                    const double* sh = d.shares + (size_t)q * SHARE + half;
-#pragma unroll
-                    for (int u = 0; u < 6; ++u) sh6[j][u] = sh[u];
+                    const double2* sh = reinterpret_cast<const double2*>(d.shares + (size_t)q * SHARE + half);
+                    const double2 a = sh[0], b = sh[1], e2 = sh[2];
+                    sh6[j][0] = a.x; sh6[j][1] = a.y; sh6[j][2] = b.x;
+                    sh6[j][3] = b.y; sh6[j][4] = e2.x; sh6[j][5] = e2.y;
                 }
             }
 #pragma unroll
@@ -479,9 +485,10 @@ __global__ void __launch_bounds__(SUM_BLOCK, 5) k_sum(DevPtrs d)
             for (int w = 0; w < nw; ++w) {
                 const int q = d.slotw[(size_t)w * d.ncap + s];
                 if (q < 0) continue;
-                const double* sh = d.shares + (size_t)q * SHARE;
-                F += v3(sh[0], sh[1], sh[2]);
-                T += v3(sh[3], sh[4], sh[5]);
+                const double2* sh = reinterpret_cast<const double2*>(d.shares + (size_t)q * SHARE);
+                const double2 a = sh[0], b = sh[1], e2 = sh[2];
+                F += v3(a.x, a.y, b.x);
+                T += v3(b.y, e2.x, e2.y);
             }
         }
         if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z))) atomicOr(&ctl->status, 1u << DEM_ERR_NAN);

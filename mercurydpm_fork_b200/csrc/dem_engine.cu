@@ -635,9 +635,9 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         if ((rc = dalloc(h, &d.caller[b], NC))) return rc;
         if ((rc = dalloc(h, &d.nbr[b], (size_t)cap * NC))) return rc;
         if ((rc = dalloc(h, &d.cnt[b], NC))) return rc;
-        if ((rc = dalloc(h, &d.hist[b], (size_t)d.ncomp * cap * NC))) return rc;
+        if ((rc = dalloc(h, &d.hist[b], (size_t)hist_stride(d.ncomp) * cap * NC))) return rc;
         if ((rc = dalloc(h, &d.act[b], (size_t)d.nwords * NC))) return rc;
-        if ((rc = dalloc(h, &d.whist[b], (size_t)d.ncomp * wmax * NC))) return rc;
+        if ((rc = dalloc(h, &d.whist[b], (size_t)hist_stride(d.ncomp) * wmax * NC))) return rc;
         if ((rc = dalloc(h, &d.wact[b], NC))) return rc;
     }
     if ((rc = dalloc(h, &d.rev, (size_t)cap * NC))) return rc;
@@ -755,7 +755,7 @@ int dem_upload_contacts(dem_handle* hh, const dem_contacts_soa* cs)
     std::vector<double4> pr(n);
     std::vector<int> cnt(n), nbr((size_t)d.cap * NC);
     std::vector<unsigned> act((size_t)d.nwords * NC), wact(NC);
-    std::vector<double> hist((size_t)d.ncomp * d.cap * NC), whist((size_t)d.ncomp * d.wmax * NC);
+    std::vector<double> hist((size_t)hist_stride(d.ncomp) * d.cap * NC), whist((size_t)hist_stride(d.ncomp) * d.wmax * NC);
     CU(cudaMemcpyAsync(info.data(), d.info[cur], n * sizeof(int4), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaMemcpyAsync(pr.data(), d.pr[cur], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaMemcpyAsync(cnt.data(), d.cnt[l], n * sizeof(int), cudaMemcpyDeviceToHost, h->stream));

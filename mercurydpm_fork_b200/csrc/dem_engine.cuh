@@ -105,13 +105,16 @@ struct Control {
 // of consecutive particles touch consecutive words; the spring components of
 // one entry are contiguous (one sector for a contact's history).
 __host__ __device__ __forceinline__ size_t nbr_at(int ncap, int i, int k) { return (size_t)k * ncap + i; }
+// A spring record holds ncomp doubles padded to an even count (3 -> 4,
+// 9 -> 10), so every record starts on 16 bytes and moves as 16-byte vectors.
+__host__ __device__ __forceinline__ int hist_stride(int ncomp) { return ncomp + (ncomp & 1); }
 __host__ __device__ __forceinline__ size_t hist_at(int ncap, int ncomp, int i, int k)
 {
-    return ((size_t)k * ncap + i) * ncomp;
+    return ((size_t)k * ncap + i) * hist_stride(ncomp);
 }
 __host__ __device__ __forceinline__ size_t whist_at(int ncap, int ncomp, int i, int w)
 {
-    return ((size_t)w * ncap + i) * ncomp;
+    return ((size_t)w * ncap + i) * hist_stride(ncomp);
 }
 
 struct DevPtrs {

@@ -458,30 +458,35 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
 // ---------------------------------------------------------------------------
 // force + integration
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void load_springs(const double* h, size_t base, size_t stride, int ncomp, Springs& s)
+// One spring record (hist_at / whist_at: 16-byte aligned, padded to an even
+// count) as 16-byte vectors.
+__device__ __forceinline__ void load_springs(const double* h, size_t base, int ncomp, Springs& s)
 {
-    s.slide = v3(h[base], h[base + stride], h[base + 2 * stride]);
+    const double2* p = reinterpret_cast<const double2*>(h + base);
+    const double2 a = p[0], b = p[1];
+    s.slide = v3(a.x, a.y, b.x);
     if (ncomp > 3) {
-        s.roll = v3(h[base + 3 * stride], h[base + 4 * stride], h[base + 5 * stride]);
-        s.tors = v3(h[base + 6 * stride], h[base + 7 * stride], h[base + 8 * stride]);
+        const double2 c = p[2], e = p[3], f = p[4];
+        s.roll = v3(b.y, c.x, c.y);
+        s.tors = v3(e.x, e.y, f.x);
     } else {
         s.roll = zero3();
         s.tors = zero3();
     }
 }
 
-__device__ __forceinline__ void store_springs(double* h, size_t base, size_t stride, int ncomp, const Springs& s)
+__device__ __forceinline__ void store_springs(double* h, size_t base, int ncomp, const Springs& s)
 {
-    h[base] = s.slide.x;
-    h[base + stride] = s.slide.y;
-    h[base + 2 * stride] = s.slide.z;
+    double2* p = reinterpret_cast<double2*>(h + base);
     if (ncomp > 3) {
-        h[base + 3 * stride] = s.roll.x;
-        h[base + 4 * stride] = s.roll.y;
-        h[base + 5 * stride] = s.roll.z;
-        h[base + 6 * stride] = s.tors.x;
-        h[base + 7 * stride] = s.tors.y;
-        h[base + 8 * stride] = s.tors.z;
+        p[0] = make_double2(s.slide.x, s.slide.y);
+        p[1] = make_double2(s.slide.z, s.roll.x);
+        p[2] = make_double2(s.roll.y, s.roll.z);
+        p[3] = make_double2(s.tors.x, s.tors.y);
+        p[4] = make_double2(s.tors.z, 0.0);
+    } else {
+        p[0] = make_double2(s.slide.x, s.slide.y);
+        p[1] = make_double2(s.slide.z, 0.0);
     }
 }
 

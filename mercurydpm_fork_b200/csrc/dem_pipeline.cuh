@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             hb = whist_at(d.ncap, NCOMP, s, wl);
             hdst = d.whist[nb];
             was_active = (d.wact[c][s] >> wl) & 1u;
-            if (was_active) load_springs(d.whist[c], hb, 1, NCOMP, spr);
+            if (was_active) load_springs(d.whist[c], hb, NCOMP, spr);
             pid_i = wg;
         } else {
             const size_t e = nbr_at(d.ncap, s, kq);
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             rv = d.rev[e];
             hb = hist_at(d.ncap, NCOMP, s, kq);
             Springs own; // read before the active bit is known: one less dependent load
-            load_springs(d.hist[c], hb, 1, NCOMP, own);
+            load_springs(d.hist[c], hb, NCOMP, own);
             const double4 pt = d.pr[c][tq];
             const int4 it = d.info[c][tq];
             const double4 vt4 = d.vm[c][tq];
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
             if (derived) {
                 const int m = rv;
                 if ((d.act[c][(size_t)(m >> 5) * d.ncap + tq] >> (m & 31)) & 1u) {
-                    load_springs(d.hist[c], hist_at(d.ncap, NCOMP, tq, m), 1, NCOMP, spr);
+                    load_springs(d.hist[c], hist_at(d.ncap, NCOMP, tq, m), NCOMP, spr);
                     spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
                 }
             } else if (was_active) {
@@ -406,8 +406,8 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
         // that side is not derived and was active, so its old spring is its own
         // stored one, read again here instead of kept in registers
         Springs kept = spr;
-        if (first && periodic && !(is.x > pid_i) && was_active) load_springs(d.hist[c], hb, 1, NCOMP, kept);
-        store_springs(hdst, hb, 1, NCOMP, kept);
+        if (first && periodic && !(is.x > pid_i) && was_active) load_springs(d.hist[c], hb, NCOMP, kept);
+        store_springs(hdst, hb, NCOMP, kept);
         // shares as 16-byte stores (96-byte items: every item and half is 16-byte aligned)
         double2* sh = reinterpret_cast<double2*>(d.shares + (size_t)q * SHARE);
         const V3 tp = out.torque - cross(xq - g.c, out.force);

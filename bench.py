@@ -36,7 +36,13 @@ WORKLOAD = dict(workload="periodic_chute_200k", packing="close-packed layers (LL
                 n_flowing=200_000, size_ratio=2, hgrid_levels=2,
                 periodic="xy", domain_small_diameters=[100, 50], angle_deg=24, species="LinearViscoelasticSlidingFriction",
                 restitution=0.88, friction=0.5, dt="tc/50", time_steps_per_bench_step=STEPS_PER_CALL,
+                verlet_skin="0.8 x smallest radius (engine default 0.4)",
                 l2="working set >= L2; 256 MiB L2 flush before every timed dem_step call")
+# Verlet skin of the neighbour lists for this workload, in smallest radii:
+# the flowing chute moves fast enough that halving the rebuilds (skin 0.8)
+# outweighs the longer lists (measured 119 vs 122 us per time step); dense,
+# slow beds (drum, heaps) are faster with the engine's default 0.4.
+SKIN_OVER_RMIN = 0.8
 
 
 def rank_info():
@@ -130,7 +136,8 @@ def run_ours(args):
     from mercurydpm_fork_b200 import DemEngine, _abi
     sc = workload()
     n_moving = sc.n_moving
-    eng = DemEngine(sc.time_step, [sc.instance], sc.species, sc.walls, rotation=True, device=local)
+    eng = DemEngine(sc.time_step, [sc.instance], sc.species, sc.walls, rotation=True, device=local,
+                    skin=SKIN_OVER_RMIN * float(np.min(sc.radius)))
     eng.upload(sc.position, sc.velocity, sc.radius, sc.inv_mass, sc.inv_inertia, sc.species_index, sc.ids)
     eng.step(0)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
@@ -286,7 +293,8 @@ def run_profile_target(args):
     from mercurydpm_fork_b200 import DemEngine
     sc = workload()
     # direct launches: every kernel of a time step is its own launch in ncu's list
-    eng = DemEngine(sc.time_step, [sc.instance], sc.species, sc.walls, rotation=True, use_graphs=False)
+    eng = DemEngine(sc.time_step, [sc.instance], sc.species, sc.walls, rotation=True, use_graphs=False,
+                    skin=SKIN_OVER_RMIN * float(np.min(sc.radius)))
     eng.upload(sc.position, sc.velocity, sc.radius, sc.inv_mass, sc.inv_inertia, sc.species_index, sc.ids)
     eng.step(args.profile_steps)
     st = eng.stats()

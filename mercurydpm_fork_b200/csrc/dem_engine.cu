@@ -234,19 +234,26 @@ int check_status(Handle* h, const Control& c)
 // MercuryBase.cc:204-306, restated as dense per-level grids): radii are
 // grouped in geometric bands of ratio 2 starting at the smallest radius; a
 // level's cell edge is at least 2 r_max(level) + interaction distance + skin.
-void setup_instance_grid(const dem_instance_desc& in, const std::vector<double>& radii, double skin, double dmax,
+void setup_instance_grid(const dem_instance_desc& in, const double* radii, size_t count, double skin, double dmax,
                          InstanceDev& I, std::vector<int>& level_of, int& cell_base)
 {
     double rmin = 1e300, rmax = 0.0;
-    for (double r : radii) { rmin = std::min(rmin, r); rmax = std::max(rmax, r); }
-    if (radii.empty()) { rmin = rmax = 1.0; }
+    for (size_t i = 0; i < count; ++i) { rmin = std::min(rmin, radii[i]); rmax = std::max(rmax, radii[i]); }
+    const bool empty = count == 0;
+    if (empty) { rmin = rmax = 1.0; }
     int nl = 1;
     while (nl < DEM_MAX_LEVELS && rmax >= rmin * std::pow(2.0, nl)) ++nl;
     std::vector<double> lrmax(nl, 0.0);
     std::vector<int> used(nl, 0);
-    level_of.resize(radii.size());
-    for (size_t i = 0; i < radii.size(); ++i) {
-        int l = (int)std::floor(std::log2(radii[i] / rmin));
+    level_of.resize(count);
+    for (size_t i = 0; i < count; ++i) {
+        // floor(log2(r / rmin)) is the binary exponent of r / rmin >= 1 (a
+        // normal number): exact, and far cheaper than log2 for millions of
+        // particles
+        const double x = radii[i] / rmin;
+        uint64_t bits;
+        std::memcpy(&bits, &x, sizeof(bits));
+        int l = (int)((bits >> 52) & 0x7ffu) - 1023;
         l = std::max(0, std::min(nl - 1, l));
         level_of[i] = l;
         lrmax[l] = std::max(lrmax[l], radii[i]);
@@ -257,7 +264,7 @@ void setup_instance_grid(const dem_instance_desc& in, const std::vector<double>&
     int nu = 0;
     std::vector<double> lr;
     for (int l = 0; l < nl; ++l)
-        if (used[l] || radii.empty()) { remap[l] = nu++; lr.push_back(lrmax[l] > 0 ? lrmax[l] : rmax); }
+        if (used[l] || empty) { remap[l] = nu++; lr.push_back(lrmax[l] > 0 ? lrmax[l] : rmax); }
     for (auto& l : level_of) l = remap[l];
     I.n_levels = nu;
     for (int l = 0; l < nu; ++l) {
@@ -477,6 +484,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     // ---- validate and collect per-instance radii
     std::vector<std::vector<double>> radii(ninst);
     std::vector<std::vector<long long>> members(ninst);
+    const bool one = ninst == 1; // one instance: members are 0..n-1, radii the caller's array itself
     double rmin_all = 1e300;
     for (long long i = 0; i < n; ++i) {
         const int in = p->instance ? p->instance[i] : 0;
@@ -489,8 +497,10 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         for (int k = 0; k < 3; ++k)
             if (!std::isfinite(p->position[3 * i + k]) || !std::isfinite(p->velocity[3 * i + k]))
                 return fail(h, DEM_ERR_BAD_INPUT, "non-finite particle state");
-        radii[in].push_back(r);
-        members[in].push_back(i);
+        if (!one) {
+            radii[in].push_back(r);
+            members[in].push_back(i);
+        }
         rmin_all = std::min(rmin_all, r);
     }
     // ---- walls per instance
@@ -513,7 +523,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     // every 9 steps and costs 7 % more per step; the evaluation grows only 3 %)
     if (!(skin > 0.0)) skin = (n > 0) ? 0.4 * rmin_all : 1e-3;
     h->inst.assign(ninst, InstanceDev{});
-    std::vector<int> level(n, 0);
+    std::vector<int> level(one ? 0 : n, 0);
+    double rmax_all = 0.0;
     int cell_base = 0;
     for (int in = 0; in < ninst; ++in) {
         const auto& D = h->inst_desc[in];
@@ -547,24 +558,27 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
                 ++I.n_del;
             }
         std::vector<int> lv;
-        setup_instance_grid(D, radii[in], skin, dmax, I, lv, cell_base);
-        for (size_t k = 0; k < members[in].size(); ++k) level[members[in][k]] = lv[k];
+        const double* rad = one ? p->radius : radii[in].data();
+        const size_t nrad = one ? (size_t)n : radii[in].size();
+        setup_instance_grid(D, rad, nrad, skin, dmax, I, lv, cell_base);
+        if (one)
+            level.swap(lv);
+        else
+            for (size_t k = 0; k < members[in].size(); ++k) level[members[in][k]] = lv[k];
         // a periodic dimension must be longer than twice the largest reach
+        double rm = 0.0;
+        if (nrad > 0)
+            for (int l = 0; l < I.n_levels; ++l) rm = std::max(rm, I.level_rmax[l]);
+        rmax_all = std::max(rmax_all, rm);
         for (int k = 0; k < 3; ++k)
-            if ((D.periodic_mask >> k) & 1u) {
-                double rm = 0.0;
-                for (double r : radii[in]) rm = std::max(rm, r);
-                if (I.per_L[k] <= 2.0 * (2.0 * rm + dmax + skin))
-                    return fail(h, DEM_ERR_BAD_INPUT, "periodic box too small for the particle size");
-            }
+            if (((D.periodic_mask >> k) & 1u) && I.per_L[k] <= 2.0 * (2.0 * rm + dmax + skin))
+                return fail(h, DEM_ERR_BAD_INPUT, "periodic box too small for the particle size");
     }
     const long long ncells = cell_base + 1; // + the graveyard of deleted particles
     // ---- neighbour capacity
     int cap = h->cfg.max_neighbors;
     if (cap <= 0) {
         // auto: 48 for monodisperse-like packings, more when radii spread
-        double rmax_all = 0.0;
-        for (int in = 0; in < ninst; ++in) for (double r : radii[in]) rmax_all = std::max(rmax_all, r);
         const double ratio = (n > 0) ? rmax_all / rmin_all : 1.0;
         cap = ratio < 1.5 ? 48 : (ratio < 2.5 ? 96 : 128);
     }

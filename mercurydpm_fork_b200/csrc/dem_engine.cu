@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -486,7 +487,27 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     std::vector<std::vector<long long>> members(ninst);
     const bool one = ninst == 1; // one instance: members are 0..n-1, radii the caller's array itself
     double rmin_all = 1e300;
-    for (long long i = 0; i < n; ++i) {
+    // one instance: branch-free checks over whole arrays first (fast for
+    // millions of particles); the loop below runs only to name a failure
+    bool checked = false;
+    if (one) {
+        const int nsp = h->inst_desc[0].n_species;
+        int bad = 0;
+        double rmin = 1e300;
+        for (long long i = 0; i < n; ++i) {
+            const double r = p->radius[i];
+            bad |= !(r > 0.0) | !(r <= DBL_MAX) | (p->species[i] < 0) | (p->species[i] >= nsp) | !(p->inv_mass[i] >= 0.0);
+            if (p->instance) bad |= p->instance[i] != 0;
+            rmin = r < rmin ? r : rmin;
+        }
+        for (long long i = 0; i < 3 * n; ++i)
+            bad |= !(std::fabs(p->position[i]) <= DBL_MAX) | !(std::fabs(p->velocity[i]) <= DBL_MAX);
+        if (!bad) {
+            checked = true;
+            rmin_all = n > 0 ? rmin : rmin_all;
+        }
+    }
+    for (long long i = 0; i < n && !checked; ++i) {
         const int in = p->instance ? p->instance[i] : 0;
         if (in < 0 || in >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "particle instance out of range");
         const double r = p->radius[i];

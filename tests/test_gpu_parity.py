@@ -184,3 +184,32 @@ def test_periodic_chute_long_horizon(gpu):
     assert H.rel_err(g["position"], o["position"], 1e-3) < 1e-11
     assert H.rel_err(g["force"], o["force"]) < 1e-6
     assert H.rel_err(g["contacts"]["springs"], o["contacts"]["springs"]) < 1e-6
+
+
+def test_upload_rejects_bad_particles(gpu):
+    """dem_upload_particles refuses non-finite states, non-positive radii,
+    species out of range and negative inverse masses (DEM_ERR_BAD_INPUT with
+    a message naming the problem), and accepts the repaired arrays."""
+    from mercurydpm_fork_b200 import DemError, _abi
+    sc = cases.compressed_box(n=200)
+    from mercurydpm_fork_b200.engine import DemEngine
+    e = DemEngine(sc.time_step, [sc.instance], sc.species, sc.walls, rotation=sc.rotation)
+    base = dict(position=sc.position, velocity=sc.velocity, radius=sc.radius, inv_mass=sc.inv_mass,
+                inv_inertia=sc.inv_inertia, species=sc.species_index, ids=sc.ids)
+    bad_cases = []
+    x = sc.position.copy(); x[17, 1] = np.nan; bad_cases.append(("position", x, "non-finite"))
+    v = sc.velocity.copy(); v[3, 2] = np.inf; bad_cases.append(("velocity", v, "non-finite"))
+    r = sc.radius.copy(); r[5] = -r[5]; bad_cases.append(("radius", r, "radius"))
+    s = sc.species_index.copy(); s[9] = 7; bad_cases.append(("species", s, "species"))
+    m = sc.inv_mass.copy(); m[11] = -1.0; bad_cases.append(("inv_mass", m, "inverse mass"))
+    for key, arr, word in bad_cases:
+        kw = dict(base)
+        kw[key] = arr
+        with pytest.raises(DemError) as ex:
+            e.upload(kw["position"], kw["velocity"], kw["radius"], kw["inv_mass"], kw["inv_inertia"], kw["species"],
+                     kw["ids"])
+        assert ex.value.code == _abi.DEM_ERR_BAD_INPUT
+        assert word in str(ex.value), (key, str(ex.value))
+    e.upload(**base)
+    e.step(1)
+    e.close()

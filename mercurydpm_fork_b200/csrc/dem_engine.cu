@@ -146,8 +146,9 @@ void launch_pipeline(Handle* h, cudaStream_t s)
 {
     DevPtrs& d = h->d;
     k_detect<MODE, NCOMP><<<grid_for(d.n, DETECT_BLOCK), DETECT_BLOCK, 0, s>>>(d);
+    // one resident wave (4 blocks of 128 per SM at 128 registers), grid-stride over the items
     const unsigned gc = (unsigned)std::max(1, std::min((d.item_cap + CONTACT_BLOCK - 1) / CONTACT_BLOCK,
-                                                       h->sm_count * 8));
+                                                       h->sm_count * 4));
     k_contacts<MODE, NLAW, FLAW, NCOMP><<<gc, CONTACT_BLOCK, 0, s>>>(d);
     k_sum<MODE><<<grid_for(d.n, SUM_BLOCK), SUM_BLOCK, 0, s>>>(d);
 }

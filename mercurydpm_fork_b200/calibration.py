@@ -308,3 +308,62 @@ def calibrate(target: np.ndarray, dem, surrogate=None, rounds: int = 4, proposal
             break
     return dict(best_error=best_err, params=best_p, response=best_r, history=hist, rounds=len(hist),
                 dem_runs=len(hist) * proposals)
+
+
+def calibrate_batch(targets: np.ndarray, dem, surrogate, rounds: int = 4, proposals: int = 256,
+                    candidates: int = 65_536, tol: float = 0.02, seed: int = 0, data=None,
+                    retrain_epochs: int = 30) -> list:
+    """calibrate() for many targets at once: every round, each target still
+    above `tol` proposes `proposals` parameter sets (the surrogate's closest
+    candidates, or uniform ones while the surrogate is not trusted for that
+    target) and one call of `dem` judges all of them together, so a round of
+    many calibrations is one batched DEM run. The surrogate is refined once
+    per round on every new DEM result. Returns one result per target, as
+    calibrate() does."""
+    targets = np.atleast_2d(np.asarray(targets, np.float64))
+    nt = len(targets)
+    rng = np.random.default_rng(seed)
+    best_err = np.full(nt, np.inf)
+    best_p, best_r = [None] * nt, [None] * nt
+    hist = [[] for _ in range(nt)]
+    trust = np.full(nt, surrogate is not None)
+    xs = [] if data is None else [np.asarray(data[0])]
+    ys = [] if data is None else [np.asarray(data[1])]
+    for r in range(rounds):
+        active = [k for k in range(nt) if best_err[k] > tol]
+        if not active:
+            break
+        props, preds, modes = [], [], []
+        for k in active:
+            if trust[k]:
+                cand = sample_params(rng, candidates)
+                pc = surrogate.predict(cand)
+                order = np.argsort(response_error(pc, targets[k]))[:proposals]
+                props.append(cand[order])
+                preds.append(pc[order])
+                modes.append("surrogate")
+            else:
+                pk = sample_params(rng, proposals)
+                props.append(pk)
+                preds.append(surrogate.predict(pk) if surrogate is not None else None)
+                modes.append("fallback" if surrogate is not None else "plain")
+        resp = dem(np.concatenate(props))
+        for j, k in enumerate(active):
+            rk = resp[j * proposals:(j + 1) * proposals]
+            err = response_error(rk, targets[k])
+            i = int(np.argmin(err))
+            if err[i] < best_err[k]:
+                best_err[k], best_p[k], best_r[k] = float(err[i]), props[j][i], rk[i]
+            rec = dict(round=r, mode=modes[j], best_error=float(err[i]), median_error=float(np.median(err)))
+            if surrogate is not None:
+                pe = np.max(np.abs(preds[j][:, :2] - rk[:, :2]) / np.abs(rk[:, :2]), axis=1)
+                rec["surrogate_error"] = float(np.median(pe))
+                trust[k] = rec["surrogate_error"] <= tol
+            hist[k].append(rec)
+        if surrogate is not None and any(best_err[k] > tol for k in range(nt)) and r + 1 < rounds:
+            # refine only when another round follows: the next round is the one that uses it
+            xs.append(np.concatenate(props))
+            ys.append(resp)
+            surrogate.fit(np.concatenate(xs), np.concatenate(ys), epochs=retrain_epochs)
+    return [dict(best_error=float(best_err[k]), params=best_p[k], response=best_r[k], history=hist[k],
+                 rounds=len(hist[k]), dem_runs=len(hist[k]) * proposals) for k in range(nt)]

@@ -111,6 +111,14 @@ def test_surrogate_guided_calibration_beats_plain_search(gpu):
                           data=(X[:512], Y[:512]), retrain_epochs=1)
         b = cal.calibrate(target, dem, surrogate=None, rounds=1, proposals=64, seed=k, tol=0.0)
         gains.append((a["history"][0]["median_error"], b["history"][0]["median_error"]))
+    # both targets at once: one batched DEM run judges both targets' proposals
+    rb = cal.calibrate_batch(Y[512:514], dem, s, rounds=1, proposals=64, candidates=65536, seed=5, tol=0.0,
+                             data=(X[:512], Y[:512]), retrain_epochs=1)
+    assert len(rb) == 2
+    for k, r in enumerate(rb):
+        assert r["rounds"] == 1 and r["dem_runs"] == 64
+        assert abs(cal.response_error(r["response"], Y[512 + k])[0] - r["best_error"]) < 1e-12
+        assert r["history"][0]["median_error"] < 0.5 * gains[k][1], (r["history"], gains)
     s.close()
     for surr, plain in gains:
         assert surr < 0.5 * plain, gains

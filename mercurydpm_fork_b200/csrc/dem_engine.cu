@@ -66,6 +66,7 @@ struct Handle {
     int law_variant = 0;
     int sm_count = 148;
     int rb_grid = 148;                 // blocks of the cooperative rebuild (all resident)
+    std::vector<int> level_buf;        // HGrid level of every particle (one-instance uploads)
 };
 
 int fail(Handle* h, int code, const std::string& msg)
@@ -267,7 +268,8 @@ void setup_instance_grid(const dem_instance_desc& in, const double* radii, size_
     std::vector<double> lr;
     for (int l = 0; l < nl; ++l)
         if (used[l] || empty) { remap[l] = nu++; lr.push_back(lrmax[l] > 0 ? lrmax[l] : rmax); }
-    for (auto& l : level_of) l = remap[l];
+    if (nu != nl) // some level is empty: renumber (usually every level is used)
+        for (size_t i = 0; i < count; ++i) level_of[i] = remap[level_of[i]];
     I.n_levels = nu;
     for (int l = 0; l < nu; ++l) {
         const double cs = 2.0 * lr[l] + dmax + skin;
@@ -545,7 +547,10 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     // every 9 steps and costs 7 % more per step; the evaluation grows only 3 %)
     if (!(skin > 0.0)) skin = (n > 0) ? 0.4 * rmin_all : 1e-3;
     h->inst.assign(ninst, InstanceDev{});
-    std::vector<int> level(one ? 0 : n, 0);
+    // levels of all particles; one instance fills the handle's buffer, which
+    // keeps its size between uploads (no allocation or zeroing per upload)
+    std::vector<int> level_multi(one ? 0 : n, 0);
+    std::vector<int>& level = one ? h->level_buf : level_multi;
     double rmax_all = 0.0;
     int cell_base = 0;
     for (int in = 0; in < ninst; ++in) {
@@ -579,13 +584,12 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
                 I.del_d[I.n_del] = db.distance * sf;
                 ++I.n_del;
             }
-        std::vector<int> lv;
+        std::vector<int> lv_multi;
+        std::vector<int>& lv = one ? h->level_buf : lv_multi;
         const double* rad = one ? p->radius : radii[in].data();
         const size_t nrad = one ? (size_t)n : radii[in].size();
         setup_instance_grid(D, rad, nrad, skin, dmax, I, lv, cell_base);
-        if (one)
-            level.swap(lv);
-        else
+        if (!one)
             for (size_t k = 0; k < members[in].size(); ++k) level[members[in][k]] = lv[k];
         // a periodic dimension must be longer than twice the largest reach
         double rm = 0.0;

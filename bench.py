@@ -45,6 +45,22 @@ WORKLOAD = dict(workload="periodic_chute_200k", packing="close-packed layers (LL
 SKIN_OVER_RMIN = 0.8
 
 
+def max_over_ranks(ms: float, device: str) -> float:
+    """The largest of the ranks' times (every rank must call it, in the same
+    order); the time itself when there is one rank."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: float, world: int, max_ms: float) -> float:
+    """Whole-job throughput: every rank's units over the slowest rank's time."""
+    return units_per_rank * world / (max_ms / 1e3)
+
+
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
@@ -165,12 +181,9 @@ def run_ours(args):
             rebuilds += st["rebuilds"]
     barrier()
     wall = time.perf_counter() - t0
-    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(total_ms, f"cuda:{local}")
     steps_total = args.steps * STEPS_PER_CALL
-    value = n_moving * steps_total * world / (max_ms / 1e3)
+    value = job_rate(n_moving * steps_total, world, max_ms)
 
     # roofline of the dominant kernel (time-step force + integration)
     info = eng.stats()
@@ -211,7 +224,7 @@ def run_ours(args):
         eng.step(STEPS_PER_CALL)
         eng.download(out=outputs)
         e2e_ms += (time.perf_counter() - t1) * 1e3
-    e2e_value = n_moving * e2e_steps * STEPS_PER_CALL / (e2e_ms / 1e3) * world
+    e2e_value = job_rate(n_moving * e2e_steps * STEPS_PER_CALL, world, max_over_ranks(e2e_ms, f"cuda:{local}"))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -321,6 +321,12 @@ int  dem_get_counts(dem_handle *h, int64_t *list_entries, int64_t *contacts,
  * of one launch in milliseconds (CUDA events on the handle's stream). The
  * simulation state is unchanged. */
 int  dem_time_force_kernel(dem_handle *h, int reps, double *ms_per_launch);
+/* Self-test of the bounded device waits (no reference counterpart): launches,
+ * like the rebuild, one cooperative grid whose blocks meet at a barrier that
+ * can never complete, so that every wait gives up after `polls` polls and
+ * reports DEM_ERR_TIMEOUT; *status receives the status word the kernel wrote
+ * (1 << DEM_ERR_TIMEOUT expected). The handle stays usable afterwards. */
+int  dem_selftest_wait_expiry(dem_handle *h, int64_t polls, uint32_t *status);
 const char *dem_last_error(dem_handle *h);
 void dem_destroy(dem_handle *h);
 

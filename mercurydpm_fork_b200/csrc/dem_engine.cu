@@ -1361,3 +1361,30 @@ int dem_batch_run(dem_handle* hh, int nsteps, dem_globals* out)
     if (rc) return rc;
     return dem_reduce_batch(hh, 0, (int)h->inst.size(), out);
 }
+
+int dem_selftest_wait_expiry(dem_handle* hh, int64_t polls, uint32_t* status)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !status || polls < 1 || polls > (1ll << 24)) return fail(h, DEM_ERR_BAD_INPUT, "dem_selftest_wait_expiry: bad arguments");
+    CU(cudaSetDevice(h->device));
+    unsigned long long* ctr = nullptr;
+    unsigned int* st = nullptr;
+    CU(cudaMallocAsync(reinterpret_cast<void**>(&ctr), sizeof(unsigned long long) + 16, h->stream));
+    st = reinterpret_cast<unsigned int*>(ctr + 1);
+    CU(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) + 16, h->stream));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)h->rb_grid);
+    cfg.blockDim = dim3(RB_BLOCK);
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const long long limit = polls;
+    CU(cudaLaunchKernelEx(&cfg, k_barrier_expiry, ctr, st, limit));
+    CU(cudaMemcpyAsync(status, st, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaFreeAsync(ctr, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return DEM_OK;
+}

@@ -49,30 +49,52 @@ struct GridBarrier {
     unsigned int passed;
 };
 
+// Thread 0 of the block waits until the counter reaches target, at most
+// `limit` polls; false (and DEM_ERR_TIMEOUT in *status) if it gave up.
+__device__ __forceinline__ bool wait_counter(const unsigned long long* ctr, unsigned long long target,
+                                             unsigned int* status, long long limit)
+{
+    long long polls = 0;
+    while (ld_acquire_u64(ctr) < target) {
+        if (++polls > limit) {
+            atomicOr(status, 1u << DEM_ERR_TIMEOUT);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    return true;
+}
+
 // All blocks of the launch meet; false if this block gave up waiting.
 __device__ __forceinline__ bool grid_barrier(GridBarrier& g, Control* ctl)
 {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        ok = 1;
         ++g.passed;
         __threadfence();
         atomicAdd(g.ctr, 1ull);
         const unsigned long long target = g.base + (unsigned long long)g.passed * gridDim.x;
-        long long polls = 0;
-        while (ld_acquire_u64(g.ctr) < target) {
-            if (++polls > RB_POLL_LIMIT) {
-                atomicOr(&ctl->status, 1u << DEM_ERR_TIMEOUT);
-                ok = 0;
-                break;
-            }
-            __nanosleep(64);
-        }
+        ok = wait_counter(g.ctr, target, &ctl->status, RB_POLL_LIMIT) ? 1 : 0;
         __threadfence();
     }
     __syncthreads();
     return ok != 0;
+}
+
+// Self-test of the bounded wait: every block arrives at a barrier whose
+// target one block more than the grid would have to reach, so every wait
+// runs out after `limit` polls, sets DEM_ERR_TIMEOUT in *status and returns.
+// Its counter is its own (reset by the caller before the launch).
+__global__ void __launch_bounds__(RB_BLOCK) k_barrier_expiry(unsigned long long* ctr, unsigned int* status,
+                                                             long long limit)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(ctr, 1ull);
+        wait_counter(ctr, (unsigned long long)gridDim.x + 1ull, status, limit);
+    }
+    __syncthreads();
 }
 
 // Sum of one int per thread over the block (RB_BLOCK threads).

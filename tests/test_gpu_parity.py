@@ -213,3 +213,21 @@ def test_upload_rejects_bad_particles(gpu):
     e.upload(**base)
     e.step(1)
     e.close()
+
+
+def test_bounded_wait_expires_and_reports(gpu):
+    """The rebuild's grid-barrier wait is bounded: a barrier that can never
+    complete (one arrival short) makes every block give up after its poll
+    limit and report DEM_ERR_TIMEOUT in the status word, without a trap; the
+    engine keeps working afterwards."""
+    import ctypes as C
+    from mercurydpm_fork_b200 import _abi
+    from mercurydpm_fork_b200.engine import lib
+    sc = cases.compressed_box(n=200)
+    e = sc.engine()
+    st = C.c_uint32(0)
+    assert lib().dem_selftest_wait_expiry(e._h, 1 << 14, C.byref(st)) == 0
+    assert st.value == (1 << _abi.DEM_ERR_TIMEOUT)
+    e.step(5)
+    assert np.isfinite(e.download()["position"]).all()
+    e.close()

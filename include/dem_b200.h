@@ -274,6 +274,15 @@ int  dem_download_walls(dem_handle *h, dem_wall *walls, int n);
  * (rows beyond capacity are not written). */
 int  dem_download_contacts(dem_handle *h, dem_contacts_soa *c, int64_t capacity,
                            int64_t *count);
+/* Contact point, unit normal (from I towards P; a wall's normal points into
+ * the particle) and friction force (the tangential part of the contact force
+ * as the law computed it) of the same contacts, in the order
+ * dem_download_contacts reports them: what BaseInteraction::getContactPoint /
+ * getNormal / getTangentialForce give the .fstat output
+ * (BaseInteraction::writeToFStat, BaseInteraction.cc:487-530). Any of the
+ * three arrays (3 doubles per contact) may be null. */
+int  dem_download_contact_geometry(dem_handle *h, double *contact_point, double *normal, double *tangential_force,
+                                   int64_t capacity, int64_t *count);
 int  dem_reduce(dem_handle *h, int instance, dem_globals *out);
 /* dem_reduce for the instances first .. first+count-1 of a batch in one pass
  * (the per-instance kinetic-energy traces and centres of mass of a batch of

@@ -143,6 +143,7 @@ _SIGNATURES = {
     "dem_get_counts": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_time_force_kernel": (C.c_int, [C.c_void_p, C.c_int, _pd]),
     "dem_selftest_wait_expiry": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_uint32)]),
+    "dem_download_contact_geometry": (C.c_int, [C.c_void_p, _pd, _pd, _pd, C.c_int64, C.POINTER(C.c_int64)]),
     "dem_last_error": (C.c_char_p, [C.c_void_p]),
     "dem_destroy": (None, [C.c_void_p]),
 }

@@ -1028,17 +1028,18 @@ int dem_download_walls(dem_handle* hh, dem_wall* walls, int n)
     return DEM_OK;
 }
 
-int dem_download_contacts(dem_handle* hh, dem_contacts_soa* cs, int64_t capacity, int64_t* count)
+// The contact records of the last evaluation in the order the contact
+// downloads report them: particle pairs first, then wall contacts, each by
+// (id of P, id of I or the caller's wall index).
+static int sorted_records(Handle* h, std::vector<ContactRecord>& rec)
 {
-    Handle* h = reinterpret_cast<Handle*>(hh);
-    if (!h || !count || capacity < 0) return fail(h, DEM_ERR_BAD_INPUT, "dem_download_contacts: bad arguments");
     if (!h->uploaded || h->initial_pending) return fail(h, DEM_ERR_STATE, "no force evaluation yet (call dem_step)");
     if (!h->records_valid)
         return fail(h, DEM_ERR_CAPACITY, "contact records of the last evaluation overflowed; the buffer has grown, "
                                          "the next dem_step records all contacts");
     CU(cudaSetDevice(h->device));
     const unsigned nr = h->n_records;
-    std::vector<ContactRecord> rec(nr);
+    rec.resize(nr);
     if (nr) CU(cudaMemcpyAsync(rec.data(), h->d_records, nr * sizeof(ContactRecord), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     for (auto& x : rec)
@@ -1048,6 +1049,36 @@ int dem_download_contacts(dem_handle* hh, dem_contacts_soa* cs, int64_t capacity
         if (a.id_p != b.id_p) return a.id_p < b.id_p;
         return a.id_i < b.id_i;
     });
+    return DEM_OK;
+}
+
+int dem_download_contact_geometry(dem_handle* hh, double* contact_point, double* normal, double* tangential_force,
+                                  int64_t capacity, int64_t* count)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !count || capacity < 0) return fail(h, DEM_ERR_BAD_INPUT, "dem_download_contact_geometry: bad arguments");
+    std::vector<ContactRecord> rec;
+    int rc = sorted_records(h, rec);
+    if (rc) return rc;
+    *count = (int64_t)rec.size();
+    const int64_t m = std::min<int64_t>(capacity, (int64_t)rec.size());
+    for (int64_t r = 0; r < m; ++r)
+        for (int k = 0; k < 3; ++k) {
+            if (contact_point) contact_point[3 * r + k] = rec[r].contact_point[k];
+            if (normal) normal[3 * r + k] = rec[r].normal[k];
+            if (tangential_force) tangential_force[3 * r + k] = rec[r].tangential[k];
+        }
+    return DEM_OK;
+}
+
+int dem_download_contacts(dem_handle* hh, dem_contacts_soa* cs, int64_t capacity, int64_t* count)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !count || capacity < 0) return fail(h, DEM_ERR_BAD_INPUT, "dem_download_contacts: bad arguments");
+    std::vector<ContactRecord> rec;
+    int rc = sorted_records(h, rec);
+    if (rc) return rc;
+    const unsigned nr = (unsigned)rec.size();
     *count = nr;
     if (!cs) return DEM_OK;
     const int64_t m = std::min<int64_t>(capacity, nr);

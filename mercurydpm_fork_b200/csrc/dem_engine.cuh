@@ -73,6 +73,7 @@ struct ContactRecord {
     double contact_point[3];
     double branch[3];           // x_P - x_I (image position for periodic pairs); wall: 0
     double normal[3];           // unit normal of the contact (from I towards P)
+    double tangential[3];       // the friction force (part of force)
     double springs[9];
 };
 

@@ -510,6 +510,7 @@ __device__ __forceinline__ void write_record(const DevPtrs& d, int id_p, int id_
     const V3 br = is_wall ? zero3() : g.xp - g.xi;
     r.branch[0] = br.x; r.branch[1] = br.y; r.branch[2] = br.z;
     r.normal[0] = g.n.x; r.normal[1] = g.n.y; r.normal[2] = g.n.z;
+    r.tangential[0] = out.tangential.x; r.tangential[1] = out.tangential.y; r.tangential[2] = out.tangential.z;
     r.springs[0] = s.slide.x; r.springs[1] = s.slide.y; r.springs[2] = s.slide.z;
     r.springs[3] = s.roll.x; r.springs[4] = s.roll.y; r.springs[5] = s.roll.z;
     r.springs[6] = s.tors.x; r.springs[7] = s.tors.y; r.springs[8] = s.tors.z;

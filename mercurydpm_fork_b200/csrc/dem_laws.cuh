@@ -38,6 +38,7 @@ struct ContactGeom {
 struct ContactOut {
     V3 force;            // force on P
     V3 torque;           // interaction torque (rolling/torsion), on P
+    V3 tangential;       // the friction force (getTangentialForce), part of force
     double abs_normal_force;
     double normal_stiffness_energy; // elastic energy of this contact (for balances)
 };
@@ -66,6 +67,7 @@ __device__ __host__ __forceinline__ void evaluate_contact(const dem_species_pair
     double abs_fn = 0.0;
     V3 force = zero3();
     V3 torque = zero3();
+    V3 tangential = zero3();
     double kt0 = 0.0; // Mindlin tangential stiffness of this step
     out.normal_stiffness_energy = 0.0;
 
@@ -113,6 +115,7 @@ __device__ __host__ __forceinline__ void evaluate_contact(const dem_species_pair
                         force += ft;
                         s.slide = -(ft + sp.sliding_dissipation * vt) / sp.sliding_stiffness;
                     }
+                    tangential = ft;
                 } else {
                     const double vt2 = len2(vt);
                     V3 ft;
@@ -121,6 +124,7 @@ __device__ __host__ __forceinline__ void evaluate_contact(const dem_species_pair
                     else
                         ft = -(sp.sliding_mu * abs_fn / sqrt(vt2)) * vt;
                     force += ft;
+                    tangential = ft;
                 }
             }
             if (fl == DEM_FRICTION_ROLLING_TORSION) {
@@ -181,6 +185,7 @@ __device__ __host__ __forceinline__ void evaluate_contact(const dem_species_pair
                     force += ft;
                     s.slide = -(ft / (2.0 / 3.0 * kt0));
                 }
+                tangential = ft;
             }
             if (fl == DEM_FRICTION_MINDLIN_ROLLING_TORSION) {
                 if (sp.rolling_mu != 0.0) {
@@ -219,6 +224,7 @@ __device__ __host__ __forceinline__ void evaluate_contact(const dem_species_pair
     }
     out.force = force;
     out.torque = torque;
+    out.tangential = tangential;
     out.abs_normal_force = abs_fn;
 }
 

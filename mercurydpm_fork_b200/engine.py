@@ -286,6 +286,17 @@ class DemEngine:
         self._check(lib().dem_download_contacts(self._h, C.byref(c), m, C.byref(cnt)))
         return out
 
+    def contact_geometry(self) -> dict:
+        """dem_download_contact_geometry: contact points, unit normals and
+        friction forces of the contacts of contacts(), in the same order."""
+        cnt = C.c_int64(0)
+        self._check(lib().dem_download_contact_geometry(self._h, None, None, None, 0, C.byref(cnt)))
+        m = cnt.value
+        out = dict(contact_point=np.zeros((m, 3)), normal=np.zeros((m, 3)), tangential_force=np.zeros((m, 3)))
+        self._check(lib().dem_download_contact_geometry(self._h, _dp(out["contact_point"]), _dp(out["normal"]),
+                                                        _dp(out["tangential_force"]), m, C.byref(cnt)))
+        return out
+
     def reduce(self, instance: int = 0) -> dict:
         g = _abi.Globals()
         self._check(lib().dem_reduce(self._h, instance, C.byref(g)))

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <fstream>
 #include <sstream>
 #include <vector>
 
@@ -120,6 +121,17 @@ ParticleSpecies* make_species(const dem_species_pair& p)
 
 class RefDriver : public Mercury3D {
 public:
+    // The reference's own writers of the .ene, .fstat and .data outputs
+    // (DPMBase::writeEneHeader / writeEneTimeStep, writeFstatHeader,
+    // outputXBallsData) into the given streams.
+    void write_outputs(std::ostream& ene, std::ostream& fstat, std::ostream& data) const
+    {
+        writeEneHeader(ene);
+        writeEneTimeStep(ene);
+        writeFstatHeader(fstat);
+        outputXBallsData(data);
+    }
+
     const dem_config* cfg = nullptr;
     const dem_instance_desc* inst = nullptr;
     const dem_species_pair* species = nullptr;
@@ -385,6 +397,26 @@ int mdpm_ref_cg(const dem_config* cfg, const dem_instance_desc* inst, const dem_
         reference_cg<CGCoordinates::XZ>(d, grid, fields_out);
     else
         reference_cg<CGCoordinates::XYZ>(d, grid, fields_out);
+    return 0;
+}
+
+// The reference's .ene, .fstat and .data outputs after `nsteps` time steps,
+// written to prefix.ene / prefix.fstat / prefix.data with the precision of
+// the reference's file streams (10, DPMBase.cc:211-213).
+int mdpm_ref_write_outputs(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
+                           const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in,
+                           int nsteps, const char* prefix)
+{
+    RefDriver d;
+    setup(d, cfg, inst, species, density, walls, nwalls, in, 1);
+    d.initialiseSolve();
+    for (int k = 0; k < nsteps; ++k) d.computeOneTimeStep();
+    const std::string pre(prefix);
+    std::ofstream ene(pre + ".ene"), fstat(pre + ".fstat"), data(pre + ".data");
+    ene.precision(10);
+    fstat.precision(10);
+    data.precision(10);
+    d.write_outputs(ene, fstat, data);
     return 0;
 }
 

@@ -174,6 +174,21 @@ def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None) -> d
     return o
 
 
+def reference_outputs(sc, nsteps: int, prefix: str, variant: str = "serial"):
+    """The reference writes its own prefix.ene / .fstat / .data after nsteps."""
+    darr, nd = _deletions(None)
+    lib = ref_lib(variant)
+    lib.mdpm_ref_set_deletion(darr, nd)
+    inp = _Inputs(sc)
+    fn = lib.mdpm_ref_write_outputs
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(_abi.Config), C.POINTER(_abi.InstanceDesc), C.POINTER(_abi.SpeciesPair), _pd,
+                   C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA), C.c_int, C.c_char_p]
+    rc = fn(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density), inp.walls, inp.nwalls,
+            C.byref(inp.soa), nsteps, prefix.encode())
+    assert rc == 0
+
+
 def cg_grid(coordinates: int, n, lo, hi, width: float, cutoff_factor: float = 3.0) -> _abi.CGGrid:
     g = _abi.CGGrid()
     g.coordinates = coordinates

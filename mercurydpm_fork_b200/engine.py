@@ -353,6 +353,23 @@ class DemEngine:
         self._check(lib().dem_cg_eval(self._h, C.byref(g), _dp(out)))
         return out
 
+    def cg_time_average(self, coordinates: int, n, lo, hi, width: float, steps_between: int, evaluations: int,
+                        cutoff_factor: float = 3.0, instance: int = 0):
+        """TimeAveragedCG<Coordinates, Gauss, StandardFields>
+        (Kernel/CG/TimeAveragedCG.hcc:80-107): CG evaluated at the current
+        state and after every further `steps_between` time steps,
+        `evaluations` times in all (advancing the simulation), and averaged.
+        The reference sums the raw fields of every evaluation, then divides
+        by the averaged volume and by the number of evaluations; this is the
+        mean of the volume-averaged fields of each evaluation."""
+        total = None
+        for k in range(int(evaluations)):
+            if k:
+                self.step(steps_between)
+            f = self.cg(coordinates, n, lo, hi, width, cutoff_factor, instance)
+            total = f if total is None else total + f
+        return total / float(evaluations)
+
     def counts(self) -> dict:
         e, c, w = C.c_int64(0), C.c_int64(0), C.c_int64(0)
         self._check(lib().dem_get_counts(self._h, C.byref(e), C.byref(c), C.byref(w)))

@@ -80,3 +80,21 @@ def test_cg_box_xyz_matches_reference(gpu):
     e.close()
     ref = H.reference_cg(sc, 300, H.cg_grid(*args))
     _close(out, ref, tol=1e-8)  # 300 steps of chaotic divergence at the 1e-12 level
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_cg_time_average_matches_reference(gpu):
+    """TimeAveragedCG<XZ> on the chute: evaluations after 5, 10 and 15 steps
+    averaged, against the mean of the reference's CG at the same states (the
+    reference's time average sums the raw fields and divides by the volume
+    and the number of evaluations, TimeAveragedCG.hcc:80-107)."""
+    sc = cases.small_chute()
+    args = (_abi.DEM_CG_XZ, (20, 1, 10), (0.0, 0.0, 0.0), (0.02, 0.01, 0.02), 1e-3)
+    e = sc.engine()
+    e.step(5)
+    out = e.cg_time_average(*args, steps_between=5, evaluations=3)
+    e.close()
+    ref = sum(H.reference_cg(sc, k, H.cg_grid(*args)) for k in (5, 10, 15)) / 3.0
+    assert np.abs(ref[:, 11]).max() > 0
+    _close(out, ref)

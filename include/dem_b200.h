@@ -56,8 +56,11 @@ extern "C" {
 #define DEM_WALL_INFINITE        0 /* InfiniteWall.cc:151-175                       */
 #define DEM_WALL_AXISYMMETRIC    1 /* AxisymmetricIntersectionOfWalls.cc:93-124     */
 #define DEM_WALL_INTERSECTION    2 /* IntersectionOfWalls.cc:532-547, 567-712       */
+#define DEM_WALL_TRIANGLE        3 /* TriangleWall.cc:57-104, 218-262 (+ the triangle-wall
+                                      correction, DPMBase.cc:3443-3486, BaseWall.cc:375-409) */
 
 #define DEM_MAX_LEVELS      4
+#define DEM_MAX_TRIANGLE_CONTACTS 8
 #define DEM_MAX_WALL_FACES  8
 #define DEM_MAX_WALLS_PER_INSTANCE 32
 #define DEM_MAX_DELETION_PER_INSTANCE 2
@@ -97,6 +100,16 @@ typedef struct dem_species_pair {
  *    (IntersectionOfWalls: the frame given by position and orientation;
  *    axisymmetric: (r, 0, a) about the axis through position). The engine
  *    derives the faces' quaternions, edges and corners as the reference does.
+ *  - DEM_WALL_TRIANGLE: faces[0..2][0..2] = the vertices A, B, C in lab
+ *    coordinates and position = the wall's position, as
+ *    TriangleWall::setVertices(A, B, C, position) takes them (setVertices(A, B, C)
+ *    is position = (A + B + C) / 3); the engine keeps A - position, B - position,
+ *    C - position (vertexInLabFrame_) and rotates them with the orientation.
+ *    n_faces is 3. group is BaseObject::groupId: triangles of one group > 0
+ *    keep only the contact of larger overlap when their contacts are not both
+ *    face contacts (BaseWall::getInteractionWith); a particle with two or more
+ *    triangle contacts gets them weighted by overlap (DPMBase::computeAllForces).
+ *    At most DEM_MAX_TRIANGLE_CONTACTS triangle contacts per particle.
  * Walls move every time step as BaseInteractable::integrateBeforeForceComputation
  * does without prescribed motion: position += velocity dt, orientation
  * rotated by angular_velocity dt. Wall indices in contacts are indices into
@@ -106,6 +119,8 @@ typedef struct dem_wall {
     int32_t species;               /* species index of the wall                      */
     int32_t instance;              /* owning instance (0 for a single simulation)    */
     int32_t n_faces;               /* intersection walls: number of faces            */
+    int32_t group;                 /* triangle walls: group id (0: none)             */
+    int32_t reserved;
     double  position[3];
     double  orientation[4];        /* quaternion q0..q3                              */
     double  velocity[3];

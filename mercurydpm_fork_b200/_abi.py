@@ -34,6 +34,8 @@ DEM_FRICTION_MINDLIN_ROLLING_TORSION = 4
 DEM_WALL_INFINITE = 0
 DEM_WALL_AXISYMMETRIC = 1
 DEM_WALL_INTERSECTION = 2
+DEM_WALL_TRIANGLE = 3
+DEM_MAX_TRIANGLE_CONTACTS = 8
 DEM_MAX_LEVELS = 4
 DEM_MAX_WALL_FACES = 8
 DEM_MAX_DELETION_PER_INSTANCE = 2
@@ -64,8 +66,8 @@ class SpeciesPair(C.Structure):
 
 class Wall(C.Structure):
     _fields_ = [
-        ("type", _i32), ("species", _i32), ("instance", _i32), ("n_faces", _i32),
-        ("position", _d * 3), ("orientation", _d * 4), ("velocity", _d * 3), ("angular_velocity", _d * 3),
+        ("type", _i32), ("species", _i32), ("instance", _i32), ("n_faces", _i32), ("group", _i32),
+        ("reserved", _i32), ("position", _d * 3), ("orientation", _d * 4), ("velocity", _d * 3), ("angular_velocity", _d * 3),
         ("faces", (_d * 6) * DEM_MAX_WALL_FACES),
     ]
 

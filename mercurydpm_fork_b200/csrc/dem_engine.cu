@@ -151,8 +151,13 @@ void launch_pipeline(Handle* h, cudaStream_t s)
     const unsigned gc = (unsigned)std::max(1, std::min((d.item_cap + CONTACT_BLOCK - 1) / CONTACT_BLOCK,
                                                        h->sm_count * 4));
     k_contacts<MODE, NLAW, FLAW, NCOMP><<<gc, CONTACT_BLOCK, 0, s>>>(d);
+    if (d.has_tri) { // at most one triangle item per particle
+        const unsigned gt = (unsigned)std::max(1, std::min((d.n + TRI_BLOCK - 1) / TRI_BLOCK, h->sm_count * 4));
+        k_tri<MODE, NLAW, FLAW, NCOMP><<<gt, TRI_BLOCK, 0, s>>>(d);
+    }
     k_sum<MODE><<<grid_for(d.n, SUM_BLOCK), SUM_BLOCK, 0, s>>>(d);
 }
+int force_launches(const Handle* h) { return FORCE_LAUNCHES + (h->d.has_tri ? 1 : 0); }
 
 template <int MODE>
 void launch_force_mode(Handle* h, cudaStream_t s)
@@ -194,7 +199,7 @@ int build_graph(Handle* h, int steps, cudaGraphExec_t* out)
     cudaStream_t s = h->stream;
     CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < steps; ++k) {
-        k_control<<<1, CONTROL_THREADS, 0, s>>>(h->d_ctl, h->d.walls, h->d.n_walls, h->d.dt);
+        k_control<<<1, CONTROL_THREADS, 0, s>>>(h->d_ctl, h->d.walls, h->d_wgeom, h->d.n_walls, h->d.dt);
         const cudaError_t e = launch_rebuild(h, s);
         if (e != cudaSuccess) {
             cudaGraph_t g = nullptr;
@@ -423,8 +428,11 @@ int dem_set_walls(dem_handle* hh, const dem_wall* walls, int n)
         const dem_wall& x = walls[order[k]];
         if (x.instance < 0 || x.instance >= (int)h->inst_desc.size())
             return fail(h, DEM_ERR_BAD_INPUT, "wall instance out of range");
-        if (x.type != DEM_WALL_INFINITE && x.type != DEM_WALL_AXISYMMETRIC && x.type != DEM_WALL_INTERSECTION)
+        if (x.type != DEM_WALL_INFINITE && x.type != DEM_WALL_AXISYMMETRIC && x.type != DEM_WALL_INTERSECTION &&
+            x.type != DEM_WALL_TRIANGLE)
             return fail(h, DEM_ERR_BAD_INPUT, "unknown wall type");
+        if (x.type == DEM_WALL_TRIANGLE && (x.n_faces != 3 || x.group < 0))
+            return fail(h, DEM_ERR_BAD_INPUT, "a triangle wall has n_faces 3 and a group >= 0");
         if (x.n_faces < 0 || x.n_faces > DEM_MAX_WALL_FACES) return fail(h, DEM_ERR_BAD_INPUT, "too many wall faces");
         if (x.species < 0 || x.species >= h->inst_desc[x.instance].n_species)
             return fail(h, DEM_ERR_BAD_INPUT, "wall species out of range");
@@ -434,7 +442,14 @@ int dem_set_walls(dem_handle* hh, const dem_wall* walls, int n)
                      std::isfinite(x.angular_velocity[a]);
         for (int a = 0; a < 4; ++a) finite = finite && std::isfinite(x.orientation[a]);
         if (!finite) return fail(h, DEM_ERR_BAD_INPUT, "non-finite wall state");
-        if (x.type != DEM_WALL_INFINITE) {
+        if (x.type == DEM_WALL_TRIANGLE) {
+            for (int f = 0; f < 3; ++f)
+                for (int a = 0; a < 3; ++a) finite = finite && std::isfinite(x.faces[f][a]);
+            if (!finite) return fail(h, DEM_ERR_BAD_INPUT, "non-finite triangle vertex");
+            const V3 e0 = row3(x.faces[1]) - row3(x.faces[0]), e1 = row3(x.faces[2]) - row3(x.faces[1]);
+            if (!(len2(cross(e0, e1)) > 0.0)) return fail(h, DEM_ERR_BAD_INPUT, "degenerate triangle wall");
+            build_wall_geom(x, g[k]);
+        } else if (x.type != DEM_WALL_INFINITE) {
             for (int f = 0; f < x.n_faces; ++f) {
                 const double l2 = x.faces[f][0] * x.faces[f][0] + x.faces[f][1] * x.faces[f][1] +
                                   x.faces[f][2] * x.faces[f][2];
@@ -635,6 +650,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     d.n_species_table = (int)h->species.size();
     d.zero_idist = 1;
     for (const auto& sp : h->species) d.zero_idist = d.zero_idist && sp.interaction_distance == 0.0;
+    d.has_tri = 0;
+    for (const auto& w : h->walls) d.has_tri = d.has_tri || w.type == DEM_WALL_TRIANGLE;
     d.dt = h->cfg.time_step;
     d.drag = h->cfg.background_drag;
     const size_t NC = d.ncap;
@@ -645,7 +662,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
                           d.ncomp == kept.ncomp && d.wmax == kept.wmax && d.ncells == kept.ncells &&
                           d.rotation == kept.rotation && d.single_instance == kept.single_instance &&
                           d.n_species_table == kept.n_species_table && d.zero_idist == kept.zero_idist &&
-                          d.dt == kept.dt && d.drag == kept.drag;
+                          d.dt == kept.dt && d.drag == kept.drag && d.has_tri == kept.has_tri;
         if (!same) free_graphs(h);
         for (int b = 0; b < 2; ++b) {
             d.pr[b] = kept.pr[b]; d.vm[b] = kept.vm[b]; d.wi[b] = kept.wi[b]; d.qo[b] = kept.qo[b];
@@ -660,6 +677,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         d.pf = kept.pf; d.rows = kept.rows;
         d.rev = kept.rev; d.slot = kept.slot; d.slotw = kept.slotw; d.items = kept.items; d.shares = kept.shares;
         d.item_cap = kept.item_cap;
+        d.tri_list = kept.tri_list;
         for (int b = 0; b < 2; ++b) { // no history carries over from the previous simulation
             CU(cudaMemsetAsync(d.cnt[b], 0, NC * sizeof(int), h->stream));
             CU(cudaMemsetAsync(d.act[b], 0, (size_t)d.nwords * NC * sizeof(unsigned), h->stream));
@@ -690,6 +708,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
                                                             (long long)n * std::min(wmax, 4) + 1024);
     if ((rc = dalloc(h, &d.items, (size_t)d.item_cap))) return rc;
     if ((rc = dalloc(h, &d.shares, (size_t)d.item_cap * SHARE))) return rc;
+    if ((rc = dalloc(h, &d.tri_list, NC))) return rc;
     if ((rc = dalloc(h, &d.force, 3 * NC))) return rc;
     if ((rc = dalloc(h, &d.torque, 3 * NC))) return rc;
     if ((rc = dalloc(h, &d.key, NC))) return rc;
@@ -890,7 +909,7 @@ int dem_step(dem_handle* hh, int nsteps)
             }
             launch_force(h, h->stream, 0);
             k_flip<<<1, 32, 0, h->stream>>>(h->d_ctl);
-            launches += FORCE_LAUNCHES + 1;
+            launches += force_launches(h) + 1;
             CU(cudaGetLastError());
             h->initial_pending = false;
         }
@@ -910,15 +929,15 @@ int dem_step(dem_handle* hh, int nsteps)
                     left -= GRAPH_STEPS;
                 }
                 while (left-- > 0) CU(cudaGraphLaunch(h->graph1, h->stream));
-                launches += (1ll + REBUILD_LAUNCHES + FORCE_LAUNCHES) * nsteps;
+                launches += (1ll + REBUILD_LAUNCHES + force_launches(h)) * nsteps;
             } else {
                 for (int k = 0; k < nsteps; ++k) {
-                    k_control<<<1, CONTROL_THREADS, 0, h->stream>>>(h->d_ctl, d.walls, d.n_walls, d.dt);
+                    k_control<<<1, CONTROL_THREADS, 0, h->stream>>>(h->d_ctl, d.walls, h->d_wgeom, d.n_walls, d.dt);
                     CU(launch_rebuild(h, h->stream));
                     launch_force(h, h->stream, 1);
                 }
                 CU(cudaGetLastError());
-                launches += (1ll + FORCE_LAUNCHES + REBUILD_LAUNCHES) * nsteps;
+                launches += (1ll + force_launches(h) + REBUILD_LAUNCHES) * nsteps;
             }
             k_flip<<<1, 32, 0, h->stream>>>(h->d_ctl);
             launches += 1;

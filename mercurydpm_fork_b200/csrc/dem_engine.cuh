@@ -99,7 +99,7 @@ struct Control {
     unsigned int record_capacity;
     unsigned int lost_history;
     unsigned int n_items;  // contact items of the current evaluation
-    unsigned int pad2;
+    unsigned int n_tri;    // triangle-wall items of the current evaluation (tri_list)
 };
 
 // Entry-major layouts: entry k of every particle is contiguous, so threads
@@ -148,7 +148,9 @@ struct DevPtrs {
     int *rev;                // reverse index of the neighbour lists, n * cap
     int *slot;               // per entry: item index, or SLOT_NONE / SLOT_IS_I
     int *slotw;              // per (particle, wall): item index or SLOT_NONE
-    int4 *items;             // (particle, entry or ITEM_WALL + wall, partner slot, 0)
+    int4 *items;             // (particle, entry or ITEM_WALL + wall, partner slot, 0);
+                             // (particle, ITEM_TRI, triangle-wall hit bits, 0)
+    int *tri_list;           // item index of each triangle-wall item (n_tri of them)
     double *shares;          // 12 doubles per item
     int item_cap;
     Control *ctl;
@@ -165,6 +167,7 @@ struct DevPtrs {
     int single_instance;   // one instance: k_contacts stages its record in shared memory
     int n_species_table;   // entries of the species table
     int zero_idist;        // every species pair has interaction distance 0
+    int has_tri;           // some wall is a triangle wall (k_tri runs)
     double dt;
     double drag;
 };

@@ -32,18 +32,21 @@ __device__ __forceinline__ V3 xyz(double4 a) { return V3{a.x, a.y, a.z}; }
 // ---------------------------------------------------------------------------
 // control
 // ---------------------------------------------------------------------------
-__global__ void k_control(Control* ctl, dem_wall* walls, int n_walls, double dt)
+__global__ void k_control(Control* ctl, dem_wall* walls, WallGeom* wgeom, int n_walls, double dt)
 {
     // Walls move before the force evaluation of every step, after the particles
     // (DPMBase::integrateBeforeForceComputation, DPMBase.cc:3228-3261, through
     // BaseInteractable::integrateBeforeForceComputation, BaseInteractable.cc:538-600:
     // move(v dt), then rotate(omega dt) = Quaternion::updateAngularDisplacement).
+    // A triangle wall then recomputes its vertices and normals
+    // (TriangleWall::move / rotate -> updateVertexAndNormal).
     for (int k = threadIdx.x; k < n_walls; k += blockDim.x) {
         dem_wall& w = walls[k];
         for (int a = 0; a < 3; ++a) w.position[a] += w.velocity[a] * dt;
         const Q4 q = quat_rotate(Q4{w.orientation[0], w.orientation[1], w.orientation[2], w.orientation[3]},
                                  v3(w.angular_velocity[0] * dt, w.angular_velocity[1] * dt, w.angular_velocity[2] * dt));
         w.orientation[0] = q.q0; w.orientation[1] = q.q1; w.orientation[2] = q.q2; w.orientation[3] = q.q3;
+        if (w.type == DEM_WALL_TRIANGLE) triangle_geometry(w, wgeom[k]);
     }
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (ctl->pending_flip) {
@@ -443,14 +446,15 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
 #pragma unroll
     for (int w = 0; w < 4; ++w)
         if (w < d.nwords) d.act[nb][(size_t)w * d.ncap + s] = nw[w];
-    // wall history moves with the particle
+    // wall history moves with the particle (with the pad word: a triangle
+    // contact's creation key, k_tri)
     const unsigned int wbits = d.wact[hc][o];
     d.wact[nb][s] = wbits;
     unsigned int bits = wbits;
     while (bits) {
         const int w = __ffs(bits) - 1;
         bits &= bits - 1;
-        for (int comp = 0; comp < d.ncomp; ++comp)
+        for (int comp = 0; comp < hist_stride(d.ncomp); ++comp)
             d.whist[nb][whist_at(d.ncap, d.ncomp, s, w) + comp] = d.whist[hc][whist_at(d.ncap, d.ncomp, o, w) + comp];
     }
 }

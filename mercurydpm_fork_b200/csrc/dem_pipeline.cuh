@@ -12,6 +12,9 @@
 //              history (DPMBase::computeInternalForce, DPMBase.cc:3113-3162;
 //              walls: DPMBase.cc:3188-3215), the force/torque share of P and,
 //              for an ordinary pair, of I, into the item's 12 doubles.
+//   k_tri      (only with triangle walls) one thread per particle with
+//              triangle-wall candidates: the reference's wall loop for them
+//              with group merging and overlap weighting, into one item.
 //   k_sum      one thread per particle: the shares in neighbour-list order
 //              (P entries from its own items, I entries from the partner's
 //              item, which k_contacts announces in I's entry through the
@@ -27,6 +30,7 @@
 namespace dem {
 
 constexpr int ITEM_WALL = 1 << 20;   // item entry field >= this: wall contact (ITEM_WALL + wall)
+constexpr int ITEM_TRI = ITEM_WALL + (1 << 10); // all triangle-wall contacts of a particle (k_tri)
 constexpr int SLOT_NONE = -1;        // P entry without a contact this evaluation
 constexpr int SLOT_IS_I = -2;        // entry whose partner owns the pair, no contact this evaluation
 constexpr int SLOT_I_BASE = -3;      // SLOT_I_BASE - q: I's share of the partner's item q
@@ -167,7 +171,7 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
     // finished before the next starts, so no dynamically indexed array
     unsigned int hit0 = 0u, hit1 = 0u, hit2 = 0u, hit3 = 0u;
     int nkept = 0;
-    unsigned int whit = 0u, wnew = 0u;
+    unsigned int whit = 0u, wnew = 0u, thit = 0u;
     int count = 0, nwalls = 0;
     if (active) {
         const double4 ps = d.pr[c][s];
@@ -244,11 +248,22 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
                 V3 nrm;
                 const unsigned int bit = 1u << w;
                 d.slotw[(size_t)w * d.ncap + s] = SLOT_NONE;
-                if (wall_distance(wall, d.wgeom + wg, xs, ps.w + sp.interaction_distance, dist, nrm)) {
-                    whit |= bit;
+                const double R = ps.w + sp.interaction_distance;
+                bool hit;
+                if (wall.type == DEM_WALL_TRIANGLE) {
+                    // the face-plane test that opens TriangleWall::getDistanceAndNormal;
+                    // k_tri finishes it and settles the history bits of these walls
+                    const WallGeom& tg = d.wgeom[wg];
+                    hit = fabs(dot(xs - row3(tg.tv[0]), row3(tg.tfn))) < R;
+                    if (hit) thit |= bit;
+                } else {
+                    hit = wall_distance(wall, d.wgeom + wg, xs, R, dist, nrm);
+                    if (hit) whit |= bit;
+                }
+                if (hit) {
                     wnew |= bit;
                 } else if (first && (wa & bit)) {
-                    for (int q = 0; q < NCOMP; ++q)
+                    for (int q = 0; q < hist_stride(NCOMP); ++q) // with a triangle contact's creation key
                         d.whist[nb][whist_at(d.ncap, NCOMP, s, w) + q] = d.whist[c][whist_at(d.ncap, NCOMP, s, w) + q];
                     wnew |= bit;
                 }
@@ -258,7 +273,7 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
     }
     // ---- compact the contacts of the block into the item list ----
     const unsigned int hits[4] = {hit0, hit1, hit2, hit3};
-    int nh = __popc(whit);
+    int nh = __popc(whit) + (thit ? 1 : 0);
 #pragma unroll
     for (int w = 0; w < 4; ++w) nh += __popc(hits[w]);
     int total;
@@ -293,6 +308,11 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         d.slotw[(size_t)w * d.ncap + s] = q;
         ++q;
     }
+    if (thit) { // its net share is summed at the first triangle wall's place
+        d.items[q] = make_int4(s, ITEM_TRI, (int)thit, 0);
+        d.slotw[(size_t)(__ffs(thit) - 1) * d.ncap + s] = q;
+        d.tri_list[atomicAdd(&ctl->n_tri, 1u)] = q;
+    }
 }
 
 template <int MODE, int NLAW, int FLAW, int NCOMP>
@@ -311,6 +331,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += gridDim.x * blockDim.x) {
         const int4 item = d.items[q];
         const int s = item.x, kq = item.y;
+        if (kq == ITEM_TRI) continue; // k_tri
         const double4 ps = d.pr[c][s];
         const double4 vs = d.vm[c][s];
         const double4 ws = d.wi[c][s];
@@ -430,6 +451,193 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
     }
 }
 
+// All triangle-wall contacts of one particle, in wall order, as the
+// reference's sequential wall loop makes them with the triangle-wall
+// correction on (its default build; DPMBase::computeForcesDueToWalls,
+// DPMBase.cc:3188-3215):
+//  * BaseWall::getInteractionWith (BaseWall.cc:375-409): a triangle of group
+//    g > 0 meets every contact already made this step with a triangle of the
+//    same group; unless both are face contacts, the larger overlap wins -- a
+//    larger new overlap takes the earlier contact over (its force is taken
+//    back, it moves to the new triangle with its spring), a smaller one drops
+//    the new contact; otherwise the contact with this triangle from the last
+//    step (InteractionHandler::getInteraction) or a new one is used.
+//  * DPMBase::computeAllForces (DPMBase.cc:3443-3486): with two or more
+//    triangle contacts, each force and torque is taken back and applied again
+//    weighted by overlap / (sum of overlaps), at the contact point moved by
+//    the same weight.
+// The particle's net force and torque from these steps go into the item's P
+// share; the springs of the contacts left go to their triangles' history rows.
+// The contacts are visited in the particle's interaction-list order, which
+// is creation order (BaseInteractable::addInteraction appends,
+// removeInteraction erases in place): each triangle contact carries a
+// creation key (the time step it was made x 16 + its rank within that
+// step) in the pad word of its history row.
+constexpr int TRI_BLOCK = 64;
+template <int MODE, int NLAW, int FLAW, int NCOMP>
+__global__ void __launch_bounds__(TRI_BLOCK) k_tri(DevPtrs d)
+{
+    constexpr int MAXT = DEM_MAX_TRIANGLE_CONTACTS;
+    static_assert(NCOMP % 2 == 1, "the pad word of a history row holds the creation key");
+    Control* ctl = d.ctl;
+    const int c = ctl->cur, nb = c ^ 1;
+    const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
+    const bool record = final_step && ctl->record;
+    const bool first = (MODE == 1) && ctl->first_step;
+    const int n_tri = min((int)ctl->n_tri, d.n);
+    const double dt = d.dt;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_tri; t += gridDim.x * blockDim.x) {
+        const int q = d.tri_list[t];
+        const int4 item = d.items[q];
+        const int s = item.x;
+        const unsigned int mask = (unsigned int)item.z;
+        const double4 ps = d.pr[c][s];
+        const double4 vs = d.vm[c][s];
+        const double4 ws = d.wi[c][s];
+        const int4 is = d.info[c][s];
+        const InstanceDev& I = d.inst[is.z];
+        const int ns = I.n_species;
+        const V3 xq = xyz(ps), vq = xyz(vs), wq = xyz(ws);
+        const double rq = ps.w, mq = vs.w;
+        const unsigned int was = d.wact[c][s];
+        int ew[MAXT], esw[MAXT], ord[MAXT]; // ord: entries in interaction-list order
+        double eov[MAXT], eel[MAXT], ek[MAXT];
+        const double step_key = 16.0 * (double)ctl->steps_done;
+        int made = 0; // contacts made this step
+        V3 en[MAXT], ec[MAXT], ef[MAXT], et[MAXT], etan[MAXT];
+        Springs es[MAXT];
+        int ne = 0;
+        unsigned int taken = 0u; // triangles whose last-step contact went into an entry
+        V3 F = zero3(), T = zero3();
+        for (unsigned int b = mask; b; b &= b - 1) {
+            const int w = __ffs(b) - 1;
+            const int wg = I.wall_begin + w;
+            const dem_wall& wall = d.walls[wg];
+            const dem_species_pair* spw = &d.species[I.species_offset + is.y * ns + wall.species];
+            double dist;
+            V3 nrm;
+            if (!triangle_distance(d.wgeom[wg], xq, rq + spw->interaction_distance, dist, nrm)) continue;
+            const double overlap = rq - dist;
+            int k = -1;
+            bool dropped = false;
+            if (wall.group > 0) {
+                const bool face = triangle_face_contact(d.wgeom[wg], nrm);
+                for (int o = 0; o < ne; ++o) {
+                    const int e = ord[o];
+                    const int eg = I.wall_begin + ew[e];
+                    if (d.walls[eg].group != wall.group) continue;
+                    if (face && triangle_face_contact(d.wgeom[eg], en[e])) continue;
+                    if (overlap > eov[e]) { // take e's force back; e moves to this triangle
+                        F += -ef[e];
+                        T += -et[e] + cross(xq - ec[e], ef[e]);
+                        ew[e] = w;
+                        k = e;
+                    } else {
+                        dropped = true;
+                        break;
+                    }
+                }
+            }
+            if (dropped) continue;
+            if (k < 0) {
+                if (ne == MAXT) {
+                    atomicOr(&ctl->status, 1u << DEM_ERR_CAPACITY);
+                    continue;
+                }
+                k = ne;
+                ew[k] = w;
+                esw[k] = wall.species;
+                es[k].slide = zero3(); es[k].roll = zero3(); es[k].tors = zero3();
+                if ((was >> w) & 1u) { // the contact with this triangle from the last step
+                    const size_t hb = whist_at(d.ncap, NCOMP, s, w);
+                    load_springs(d.whist[c], hb, NCOMP, es[k]);
+                    ek[k] = d.whist[c][hb + NCOMP];
+                    taken |= 1u << w;
+                } else {
+                    ek[k] = step_key + (double)(made++);
+                }
+                int o = ne++; // insert by creation key
+                while (o > 0 && ek[ord[o - 1]] > ek[k]) {
+                    ord[o] = ord[o - 1];
+                    --o;
+                }
+                ord[o] = k;
+            }
+            ContactGeom g;
+            g.n = -nrm;
+            g.distance = dist;
+            g.overlap = overlap;
+            g.c = xq - (rq - 0.5 * g.overlap) * g.n;
+            g.xp = xq; g.vp = vq; g.wp = wq; g.inv_mass_p = mq; g.curv_p = 1.0 / rq;
+            g.xi = v3(wall.position[0], wall.position[1], wall.position[2]);
+            g.vi = v3(wall.velocity[0], wall.velocity[1], wall.velocity[2]);
+            g.wi = v3(wall.angular_velocity[0], wall.angular_velocity[1], wall.angular_velocity[2]);
+            g.inv_mass_i = 0.0;
+            g.curv_i = 0.0;
+            g.i_is_wall = true;
+            ContactOut out;
+            evaluate_contact<NLAW, FLAW>(d.species[I.species_offset + is.y * ns + esw[k]], g, es[k], dt, out);
+            en[k] = g.n; eov[k] = g.overlap; ec[k] = g.c;
+            ef[k] = out.force; et[k] = out.torque; etan[k] = out.tangential; eel[k] = out.normal_stiffness_energy;
+            F += ef[k];
+            T += et[k] - cross(xq - ec[k], ef[k]);
+        }
+        if (ne > 1) {
+            double osum = 0.0;
+            for (int o = 0; o < ne; ++o) osum += eov[ord[o]];
+            for (int o = 0; o < ne; ++o) {
+                const int e = ord[o];
+                F += -ef[e];
+                T += -et[e] + cross(xq - ec[e], ef[e]);
+                const double wgt = eov[e] / osum;
+                ec[e] = xq - (rq - 0.5 * eov[e]) * wgt * en[e];
+                ef[e] = ef[e] * wgt;
+                et[e] = et[e] * wgt;
+                F += ef[e];
+                T += et[e] - cross(xq - ec[e], ef[e]);
+            }
+        }
+        double2* sh = reinterpret_cast<double2*>(d.shares + (size_t)q * SHARE);
+        sh[0] = make_double2(F.x, F.y);
+        sh[1] = make_double2(F.z, T.x);
+        sh[2] = make_double2(T.y, T.z);
+        // history: each triangle keeps the first contact (in order) now attached
+        // to it; at the first step after the initial evaluation a contact of that
+        // evaluation that no entry took outlives the step (as k_detect carries them)
+        unsigned int kept_bits = 0u;
+        for (int o = 0; o < ne; ++o) {
+            const int e = ord[o];
+            const unsigned int bit = 1u << ew[e];
+            if (kept_bits & bit) continue;
+            kept_bits |= bit;
+            const size_t hb = whist_at(d.ncap, NCOMP, s, ew[e]);
+            store_springs(d.whist[nb], hb, NCOMP, es[e]);
+            d.whist[nb][hb + NCOMP] = ek[e];
+        }
+        if (first) {
+            for (unsigned int b = mask & was & ~taken & ~kept_bits; b; b &= b - 1) {
+                const int w = __ffs(b) - 1;
+                const size_t hb = whist_at(d.ncap, NCOMP, s, w);
+                for (int q2 = 0; q2 < hist_stride(NCOMP); ++q2) d.whist[nb][hb + q2] = d.whist[c][hb + q2];
+                kept_bits |= 1u << w;
+            }
+        }
+        d.wact[nb][s] = (d.wact[nb][s] & ~mask) | kept_bits;
+        if (record) {
+            for (int e = 0; e < ne; ++e) {
+                const int wg = I.wall_begin + ew[e];
+                ContactGeom g;
+                g.n = en[e]; g.overlap = eov[e]; g.c = ec[e]; g.xp = xq; g.xi = zero3();
+                ContactOut out;
+                out.force = ef[e]; out.torque = et[e]; out.tangential = etan[e];
+                out.abs_normal_force = 0.0; out.normal_stiffness_energy = eel[e];
+                const dem_species_pair& sp = d.species[I.species_offset + is.y * ns + esw[e]];
+                write_record(d, is.x, wg, 1, 0, s, wg, g, out, es[e], spring_energy(sp, es[e], 1.0 / mq));
+            }
+        }
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(SUM_BLOCK, 5) k_sum(DevPtrs d)
 {
@@ -438,7 +646,10 @@ __global__ void __launch_bounds__(SUM_BLOCK, 5) k_sum(DevPtrs d)
     const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
     const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
     const double dt = d.dt;
-    if (s == 0) ctl->n_items = 0u; // k_contacts is done: the next evaluation starts a new list
+    if (s == 0) { // k_contacts and k_tri are done: the next evaluation starts new lists
+        ctl->n_items = 0u;
+        ctl->n_tri = 0u;
+    }
     double disp2 = 0.0;
     if (s < d.n) {
         const double4 ps = d.pr[c][s];

@@ -34,6 +34,13 @@ struct WallGeom {
     double A[WALL_PAIRS][3];          // a point on the edge of faces (m, n)
     double AB[WALL_PAIRS][3];         // unit direction of that edge
     double C[WALL_TRIPLES][3];        // the corner of faces (l, m, n)
+    // triangle walls
+    double tvl[3][3];                 // vertices relative to the position (vertexInLabFrame_)
+    double tv[3][3];                  // vertices in the lab frame (vertex_)
+    double te[3][3];                  // unit edges v1-v0, v2-v1, v0-v2 (edge_)
+    double ten[3][3];                 // unit in-plane edge normals (edgeNormal_)
+    double tel[3];                    // edge lengths (edgeLength_)
+    double tfn[3];                    // unit face normal (faceNormal_)
 };
 
 __host__ __device__ __forceinline__ Q4 wall_q(const dem_wall& w)
@@ -178,6 +185,95 @@ __host__ __device__ __forceinline__ bool intersection_distance(const WallGeom& g
     return true;
 }
 
+// TriangleWall::updateVertexAndNormal (TriangleWall.cc:218-249) from the
+// wall's current position and orientation; Vec3D::normalise divides by the
+// square root of the squared length (Vector.cc:124-132).
+__host__ __device__ inline void triangle_geometry(const dem_wall& w, WallGeom& g)
+{
+    const Q4 q = wall_q(w);
+    const V3 wp = v3(w.position[0], w.position[1], w.position[2]);
+    V3 v[3];
+    for (int i = 0; i < 3; ++i) v[i] = quat_to_lab(q, row3(g.tvl[i])) + wp;
+    V3 e[3] = {v[1] - v[0], v[2] - v[1], v[0] - v[2]};
+    V3 fn = cross(e[0], e[1]);
+    fn = fn / sqrt(len2(fn));
+    for (int i = 0; i < 3; ++i) {
+        V3 en = cross(e[i], fn);
+        const double l = sqrt(len2(e[i]));
+        e[i] = e[i] / l;
+        en = en / sqrt(len2(en));
+        g.tv[i][0] = v[i].x; g.tv[i][1] = v[i].y; g.tv[i][2] = v[i].z;
+        g.te[i][0] = e[i].x; g.te[i][1] = e[i].y; g.te[i][2] = e[i].z;
+        g.ten[i][0] = en.x; g.ten[i][1] = en.y; g.ten[i][2] = en.z;
+        g.tel[i] = l;
+    }
+    g.tfn[0] = fn.x; g.tfn[1] = fn.y; g.tfn[2] = fn.z;
+}
+
+// TriangleWall::isInsideTriangle (TriangleWall.cc:251-262): the three
+// area ratios are tested as written there, `1 > s > 0`, which C++ evaluates
+// as (1 > s) > 0, i.e. s < 1.
+__host__ __device__ __forceinline__ bool triangle_inside(const WallGeom& g, V3 p)
+{
+    const V3 v0 = row3(g.tv[0]), v1 = row3(g.tv[1]), v2 = row3(g.tv[2]);
+    const V3 b0 = p - v0, b1 = p - v1, b2 = p - v2;
+    const double s = sqrt(len2(cross(v1 - v0, v2 - v1)));
+    const double s0 = sqrt(len2(cross(b0, b1))) / s;
+    const double s1 = sqrt(len2(cross(b1, b2))) / s;
+    const double s2 = sqrt(len2(cross(b2, b0))) / s;
+    return s0 < 1 && s1 < 1 && s2 < 1;
+}
+
+// TriangleWall::getDistanceAndNormal (TriangleWall.cc:57-104): face contact
+// if the particle projects inside the triangle, else the edge of largest
+// in-plane distance or one of its vertices. R is the wall interaction radius.
+__host__ __device__ __forceinline__ bool triangle_distance(const WallGeom& g, V3 x, double R, double& dist,
+                                                           V3& normal)
+{
+    const V3 fn = row3(g.tfn);
+    const double sd = dot(x - row3(g.tv[0]), fn);
+    dist = fabs(sd);
+    if (dist >= R) return false;
+    // selected by value, not by a local array index (which would live on the stack)
+    const V3 b0 = x - row3(g.tv[0]), b1 = x - row3(g.tv[1]), b2 = x - row3(g.tv[2]);
+    const double e0 = dot(b0, row3(g.ten[0])), e1 = dot(b1, row3(g.ten[1])), e2 = dot(b2, row3(g.ten[2]));
+    const int id = (e1 > e2) ? (e0 > e1 ? 0 : 1) : (e0 > e2 ? 0 : 2);
+    const double eid = (id == 0) ? e0 : (id == 1) ? e1 : e2;
+    if (eid > R) return false;
+    const V3 proj = x - sd * fn;
+    if (eid <= 0 && triangle_inside(g, proj)) {
+        normal = (sd >= 0) ? -fn : fn;
+        return true;
+    }
+    const V3 bid = (id == 0) ? b0 : (id == 1) ? b1 : b2;
+    const V3 e = row3(g.te[id]);
+    const double along = dot(bid, e);
+    if (along < 0) {
+        dist = sqrt(len2(bid));
+        if (dist > R) return false;
+        normal = bid / -dist;
+    } else if (along > g.tel[id]) {
+        const V3 bnext = (id == 0) ? b1 : (id == 1) ? b2 : b0; // vertex (id + 1) % 3
+        dist = sqrt(len2(bnext));
+        if (dist > R) return false;
+        normal = bnext / -dist;
+    } else {
+        normal = e * along - bid;
+        dist = sqrt(len2(normal));
+        if (dist > R) return false;
+        normal = normal / dist;
+    }
+    return true;
+}
+
+// TriangleWall::isFaceContact (TriangleWall.h:151-153): exact comparison
+// with the face normal or its negative.
+__host__ __device__ __forceinline__ bool triangle_face_contact(const WallGeom& g, V3 n)
+{
+    const V3 fn = row3(g.tfn);
+    return (n.x == fn.x && n.y == fn.y && n.z == fn.z) || (n.x == -fn.x && n.y == -fn.y && n.z == -fn.z);
+}
+
 // BaseWall::getDistanceNormalOverlap for the supported wall types: signed
 // distance of x from the wall and the wall's outward normal at the contact;
 // false when x is not within R of the wall.
@@ -204,7 +300,7 @@ __host__ __device__ __forceinline__ bool wall_distance(const dem_wall& w, const 
         normal = nrz.z * axis + nrz.x * radial;
         return true;
     }
-    // DEM_WALL_INTERSECTION
+    // DEM_WALL_INTERSECTION (triangle walls: triangle_distance, called by k_tri only)
     const V3 pb = quat_to_body(q, x - wp);
     V3 nb;
     if (!intersection_distance(*geom, w.n_faces, pb, R, dist, nb)) return false;
@@ -256,6 +352,15 @@ __host__ inline V3 cross_ref(V3 a, V3 b)
 __host__ inline void build_wall_geom(const dem_wall& w, WallGeom& g)
 {
     std::memset(&g, 0, sizeof(g));
+    if (w.type == DEM_WALL_TRIANGLE) { // TriangleWall::setVertices(A, B, C, position)
+        const V3 wp = v3(w.position[0], w.position[1], w.position[2]);
+        for (int i = 0; i < 3; ++i) {
+            const V3 r = row3(w.faces[i]) - wp;
+            g.tvl[i][0] = r.x; g.tvl[i][1] = r.y; g.tvl[i][2] = r.z;
+        }
+        triangle_geometry(w, g);
+        return;
+    }
     for (int n = 0; n < w.n_faces; ++n) {
         V3 nrm = row3(w.faces[n]);
         nrm = nrm / sqrt(len2(nrm)); // addObject normalises, setNormal normalises again

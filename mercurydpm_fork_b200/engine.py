@@ -142,6 +142,30 @@ def intersection_wall(faces, position=(0, 0, 0), orientation=(1, 0, 0, 0), speci
     return w
 
 
+def triangle_wall(a, b, c, species=0, instance=0, group=0, position=None, orientation=(1, 0, 0, 0),
+                  velocity=(0, 0, 0), angular_velocity=(0, 0, 0)) -> _abi.Wall:
+    """TriangleWall with vertices a, b, c (lab frame): setVertices(a, b, c),
+    whose position is (a + b + c) / 3 computed as Vec3D does, or
+    setVertices(a, b, c, position); `group` is the wall's group id
+    (WallHandler::readTriangleWall gives every triangle of a mesh one)."""
+    a, b, c = (tuple(map(float, v)) for v in (a, b, c))
+    if position is None:
+        position = tuple((a[k] + b[k] + c[k]) / 3 for k in range(3))
+    w = _abi.Wall()
+    w.type = _abi.DEM_WALL_TRIANGLE
+    w.species = species
+    w.instance = instance
+    w.n_faces = 3
+    w.group = group
+    w.position[:] = list(map(float, position))
+    w.orientation[:] = list(map(float, orientation))
+    w.velocity[:] = list(map(float, velocity))
+    w.angular_velocity[:] = list(map(float, angular_velocity))
+    for k, v in enumerate((a, b, c)):
+        w.faces[k][:] = list(v) + [0.0, 0.0, 0.0]
+    return w
+
+
 def axisymmetric_wall(axis, faces, position=(0, 0, 0), species=0, instance=0, velocity=(0, 0, 0),
                       angular_velocity=(0, 0, 0)) -> _abi.Wall:
     """AxisymmetricIntersectionOfWalls with setAxis(axis), setPosition(position)

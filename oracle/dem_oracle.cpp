@@ -592,6 +592,8 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
                int nsteps, dem_particles_soa* out, double* force, double* torque, dem_contacts_soa* contacts_out,
                int64_t contacts_capacity, int64_t* contacts_count)
 {
+    for (int w = 0; w < nwalls; ++w) // triangle walls are checked against the reference build itself
+        if (walls[w].type == DEM_WALL_TRIANGLE) return -2;
     Sim S;
     S.cfg = *cfg;
     S.inst = *inst;

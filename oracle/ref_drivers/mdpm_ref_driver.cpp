@@ -38,6 +38,7 @@
 #include "Walls/AxisymmetricIntersectionOfWalls.h"
 #include "Walls/InfiniteWall.h"
 #include "Walls/IntersectionOfWalls.h"
+#include "Walls/TriangleWall.h"
 
 #include "../../include/dem_b200.h"
 
@@ -159,6 +160,14 @@ public:
             BaseWall* wall = nullptr;
             if (x.type == DEM_WALL_INFINITE) {
                 wall = new InfiniteWall();
+            } else if (x.type == DEM_WALL_TRIANGLE) {
+                TriangleWall* tw = new TriangleWall();
+                tw->setVertices(Vec3D(x.faces[0][0], x.faces[0][1], x.faces[0][2]),
+                                Vec3D(x.faces[1][0], x.faces[1][1], x.faces[1][2]),
+                                Vec3D(x.faces[2][0], x.faces[2][1], x.faces[2][2]),
+                                Vec3D(x.position[0], x.position[1], x.position[2]));
+                tw->setGroupId((unsigned)x.group);
+                wall = tw;
             } else {
                 IntersectionOfWalls* iw = (x.type == DEM_WALL_AXISYMMETRIC) ? new AxisymmetricIntersectionOfWalls()
                                                                            : new IntersectionOfWalls();

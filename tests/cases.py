@@ -222,3 +222,93 @@ def small_drum(n=600, seed=5):
     return scenarios.rotating_drum(n=n, seed=seed, radius_d=12, length_d=12, site_spacing=0.995, touch_wall=3.0,
                                    omega=5.0, mu_o=0.02, sliding_dissipation=0.3, rolling_dissipation=0.2,
                                    torsion_dissipation=0.1, vstd=0.02)
+
+
+def point_triangle_distance(p, a, b, c):
+    """Distance from each point of p (m x 3) to the triangle abc: the plane
+    distance where the projection lies inside, else the distance to the
+    nearest edge segment."""
+    p = np.atleast_2d(p)
+    n = np.cross(b - a, c - a)
+    n = n / np.linalg.norm(n)
+    sd = (p - a) @ n
+    proj = p - sd[:, None] * n
+    inside = np.ones(len(p), bool)
+    for u, v in ((a, b), (b, c), (c, a)):
+        inside &= (np.cross(v - u, proj - u) @ n) >= 0
+    seg = np.full(len(p), np.inf)
+    for u, v in ((a, b), (b, c), (c, a)):
+        t = np.clip(((p - u) @ (v - u)) / ((v - u) @ (v - u)), 0.0, 1.0)
+        seg = np.minimum(seg, np.linalg.norm(p - (u + t[:, None] * (v - u)), axis=1))
+    return np.where(inside, np.abs(sd), seg)
+
+
+def triangle_mesh_triangles():
+    """A triangulated height field z = h(x) over x in [-4, 4] mm, y in [-3, 3] mm:
+    two valleys (x = -2, 2 mm) and a ridge (x = 0), nodes every 2 mm in x and
+    3 mm in y, 16 triangles; both diagonals directions occur."""
+    xs = np.array([-4e-3, -2e-3, 0.0, 2e-3, 4e-3])
+    hs = np.array([2e-3, 0.0, 1.2e-3, 0.0, 2e-3])
+    ys = np.array([-3e-3, 0.0, 3e-3])
+    tris = []
+    for i in range(4):
+        for j in range(2):
+            p00 = np.array([xs[i], ys[j], hs[i]])
+            p10 = np.array([xs[i + 1], ys[j], hs[i + 1]])
+            p01 = np.array([xs[i], ys[j + 1], hs[i]])
+            p11 = np.array([xs[i + 1], ys[j + 1], hs[i + 1]])
+            if (i + j) % 2 == 0:
+                tris += [(p00, p10, p11), (p00, p11, p01)]
+            else:
+                tris += [(p00, p10, p01), (p10, p11, p01)]
+    return tris
+
+
+def triangle_mesh(group: int = 1, n: int = 300, seed: int = 13, velocity=(0.0, 0.0, 0.0), dropped: bool = False):
+    """Spheres (d = 0.5 mm, Hertz-Mindlin with rolling and torsion) scattered
+    without mutual overlap within 0.3-1.1 radii of the triangulated surface of
+    triangle_mesh_triangles() (TriangleWall::setVertices(A, B, C) each, one
+    group id for all), so that face, edge and vertex contacts, particles on
+    shared edges and in the valleys (two face contacts) all occur; gravity
+    pulls them into the surface. `velocity` moves every triangle. With
+    `dropped`, the spheres start 0.02-0.2 radii clear of the surface moving
+    towards it at 1 m/s under 500 m/s^2 of gravity, so that every triangle
+    contact is made during the run and most of them last."""
+    from mercurydpm_fork_b200.engine import triangle_wall
+    from mercurydpm_fork_b200.scenarios import hertz_collision_time
+    rng = np.random.Generator(np.random.PCG64(seed))
+    d = 0.5e-3
+    r = 0.5 * d
+    tris = triangle_mesh_triangles()
+    walls = [triangle_wall(a, b, c, species=1, group=group, velocity=velocity) for a, b, c in tris]
+    pts = []
+    for _ in range(50):
+        x = rng.uniform(-4e-3, 4e-3, 4000)
+        h = np.interp(x, [-4e-3, -2e-3, 0.0, 2e-3, 4e-3], [2e-3, 0.0, 1.2e-3, 0.0, 2e-3])
+        lift = (1.0, 2.6) if dropped else (0.1, 1.6)
+        p = np.stack([x, rng.uniform(-3e-3, 3e-3, 4000), h + rng.uniform(lift[0] * r, lift[1] * r, 4000)], 1)
+        dist = np.min([point_triangle_distance(p, a, b, c) for a, b, c in tris], axis=0)
+        # above the surface: the height field at x, linearly interpolated
+        above = p[:, 2] > np.interp(p[:, 0], [-4e-3, -2e-3, 0.0, 2e-3, 4e-3], [2e-3, 0.0, 1.2e-3, 0.0, 2e-3])
+        band = (dist > 1.02 * r) & (dist < 1.2 * r) if dropped else (dist > 0.3 * r) & (dist < 1.1 * r)
+        for x in p[above & band]:
+            if len(pts) >= n:
+                break
+            if not pts or np.min(np.sum((np.array(pts) - x) ** 2, 1)) > (2.05 * r) ** 2:
+                pts.append(x)
+        if len(pts) >= n:
+            break
+    pos = np.array(pts)
+    m = len(pos)
+    radius = np.full(m, r)
+    density = 2000.0
+    inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
+    vel = rng.normal(0.0, 0.05, size=(m, 3))
+    if dropped:
+        vel[:, 2] -= 1.0
+    lo, hi = pos.min(0) - 8 * r, pos.max(0) + 8 * r
+    inst = Instance(domain_min=tuple(lo), domain_max=tuple(hi), gravity=(0, 0, -500.0 if dropped else -9.81),
+                    n_species=2)
+    dt = 0.02 * hertz_collision_time(d, density, 1e7)
+    return Scenario(f"triangle_mesh_g{group}{'_dropped' if dropped else ''}", dt, inst, _hertz_mindlin_table(2), np.array([density, density]), walls,
+                    pos, vel, radius, inv_mass, inv_inertia, np.zeros(m, np.int32), np.arange(m, dtype=np.int32))

@@ -1,0 +1,99 @@
+"""TriangleWall with the reference's triangle-wall correction (its default
+build): TriangleWall::getDistanceAndNormal (TriangleWall.cc:57-104), group
+merging (BaseWall.cc:375-409) and overlap weighting (DPMBase.cc:3443-3486),
+checked against the reference build itself (oracle/_ref, serial, correction
+on). The CPU oracle restatement does not cover triangle walls.
+
+CPU: the reference's initial contacts with an ungrouped triangulated surface
+are exactly the (particle, triangle) pairs within one radius by an
+independent point-triangle distance, so the scenario exercises face, edge
+and vertex contacts.
+
+GPU: at the uploaded state the contact set and every per-contact force,
+overlap and spring are bit-exact against the reference; over 20-100 steps
+(contacts made, merged, weighted, handed between triangles) positions agree
+to 1e-13 of a diameter and forces, torques and springs to 1e-9 relative.
+Grouped triangles run from a state without triangle contacts (spheres
+dropped onto the mesh): in the reference's first time step the contacts of
+the initial evaluation carry the current time stamp (both use
+numberOfTimeSteps + 1 = 1), so its group rule also compares against
+contacts of triangles not yet visited in that step; the engine applies the
+rule of every later step there.
+"""
+import numpy as np
+import pytest
+
+import cases
+import harness as H
+
+needs_reference = pytest.mark.skipif(not H.reference_available("serial"), reason="reference build absent")
+
+
+@needs_reference
+def test_reference_triangle_contacts_match_point_triangle_distance():
+    sc = cases.triangle_mesh(group=0)
+    r = H.run_reference(sc, 0)
+    c = r["contacts"]
+    walls = {(int(p), int(w)) for p, w, iw in zip(c["id_p"], c["id_i"], c["is_wall"]) if iw}
+    tris = cases.triangle_mesh_triangles()
+    expect = set()
+    for w, (a, b, cc) in enumerate(tris):
+        dist = cases.point_triangle_distance(sc.position, a, b, cc)
+        for p in np.nonzero(dist < sc.radius)[0]:
+            expect.add((int(sc.ids[p]), w))
+    assert walls == expect
+    per_particle = np.bincount([p for p, _ in walls])
+    assert per_particle.max() >= 2  # particles on shared edges and in the valleys
+    assert len(walls) > 150
+
+
+def _triangle_pairs(c):
+    return sum(1 for iw in c["is_wall"] if iw)
+
+
+@pytest.mark.gpu
+@needs_reference
+@pytest.mark.parametrize("group", [0, 1])
+def test_triangle_walls_initial_evaluation_bit_exact(gpu, group):
+    sc = cases.triangle_mesh(group=group)
+    g = H.run_gpu(sc, 0)
+    r = H.run_reference(sc, 0)
+    assert H.pair_set(g["contacts"]) == H.pair_set(r["contacts"])
+    assert _triangle_pairs(g["contacts"]) > 100
+    for k in ("force", "overlap", "springs"):
+        np.testing.assert_array_equal(g["contacts"][k], r["contacts"][k])
+    assert H.rel_err(g["force"], r["force"]) < 1e-14
+    assert H.rel_err(g["torque"], r["torque"]) < 1e-14
+
+
+@pytest.mark.gpu
+@needs_reference
+@pytest.mark.parametrize("group,dropped", [(0, False), (0, True), (1, True)])
+@pytest.mark.parametrize("nsteps", [20, 100])
+def test_triangle_walls_short_horizon(gpu, group, dropped, nsteps):
+    sc = cases.triangle_mesh(group=group, dropped=dropped)
+    g = H.run_gpu(sc, nsteps)
+    r = H.run_reference(sc, nsteps)
+    assert H.pair_set(g["contacts"]) == H.pair_set(r["contacts"])
+    # touching spheres mostly rebound within 100 steps; dropped ones are pressed on
+    assert _triangle_pairs(g["contacts"]) > {(False, 20): 100, (False, 100): 0, (True, 20): 25, (True, 100): 80}[
+        (dropped, nsteps)]
+    assert H.rel_err(g["position"], r["position"], 1e-3) < 1e-13
+    assert H.rel_err(g["velocity"], r["velocity"]) < 1e-9
+    assert H.rel_err(g["angular_velocity"], r["angular_velocity"]) < 1e-9
+    assert H.rel_err(g["force"], r["force"]) < 1e-9
+    assert H.rel_err(g["torque"], r["torque"]) < 1e-9
+    assert H.rel_err(g["contacts"]["springs"], r["contacts"]["springs"]) < 1e-9
+
+
+@pytest.mark.gpu
+@needs_reference
+def test_moving_triangle_walls_match_reference(gpu):
+    """Triangles translating every step: vertices and normals recomputed
+    after each move (TriangleWall::move -> updateVertexAndNormal)."""
+    sc = cases.triangle_mesh(group=1, velocity=(0.01, -0.02, 0.005), dropped=True)
+    g = H.run_gpu(sc, 50)
+    r = H.run_reference(sc, 50)
+    assert H.pair_set(g["contacts"]) == H.pair_set(r["contacts"])
+    assert H.rel_err(g["position"], r["position"], 1e-3) < 1e-13
+    assert H.rel_err(g["force"], r["force"]) < 1e-9

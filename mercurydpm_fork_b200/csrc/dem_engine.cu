@@ -630,8 +630,10 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     // and the captured graphs (their kernel arguments stay valid)
     const unsigned record_capacity =
         (unsigned)std::min<long long>(2000000000ll, 8 * n + 1024 + (long long)n * std::min(wmax, 4));
+    long long any_tri = 0;
+    for (const auto& w : h->walls) any_tri = any_tri || w.type == DEM_WALL_TRIANGLE;
     const std::vector<long long> layout = {n, cap, wmax, ncells, (long long)h->inst.size(), (long long)h->species.size(),
-                                           (long long)h->walls.size(), (long long)record_capacity, h->ncomp};
+                                           (long long)h->walls.size(), (long long)record_capacity, h->ncomp, any_tri};
     const bool reuse = !h->layout.empty() && h->layout == layout;
     if (!reuse) free_particle_arrays(h);
     const DevPtrs kept = h->d;
@@ -678,6 +680,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         d.rev = kept.rev; d.slot = kept.slot; d.slotw = kept.slotw; d.items = kept.items; d.shares = kept.shares;
         d.item_cap = kept.item_cap;
         d.tri_list = kept.tri_list;
+        d.tri_first = kept.tri_first;
+        d.tri_first_n = kept.tri_first_n;
         for (int b = 0; b < 2; ++b) { // no history carries over from the previous simulation
             CU(cudaMemsetAsync(d.cnt[b], 0, NC * sizeof(int), h->stream));
             CU(cudaMemsetAsync(d.act[b], 0, (size_t)d.nwords * NC * sizeof(unsigned), h->stream));
@@ -709,6 +713,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     if ((rc = dalloc(h, &d.items, (size_t)d.item_cap))) return rc;
     if ((rc = dalloc(h, &d.shares, (size_t)d.item_cap * SHARE))) return rc;
     if ((rc = dalloc(h, &d.tri_list, NC))) return rc;
+    if ((rc = dalloc(h, &d.tri_first_n, NC))) return rc;
+    if ((rc = dalloc(h, &d.tri_first, any_tri ? NC * DEM_MAX_TRIANGLE_CONTACTS * TRI_REC : 1))) return rc;
     if ((rc = dalloc(h, &d.force, 3 * NC))) return rc;
     if ((rc = dalloc(h, &d.torque, 3 * NC))) return rc;
     if ((rc = dalloc(h, &d.key, NC))) return rc;
@@ -774,6 +780,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     c.record = 1;
     c.record_capacity = h->record_capacity;
     CU(cudaMemcpyAsync(h->d_ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemsetAsync(d.tri_first_n, 0, NC * sizeof(int), h->stream)); // filled by the initial evaluation
     CU(cudaStreamSynchronize(h->stream));
     h->uploaded = true;
     h->initial_pending = true;

@@ -151,6 +151,9 @@ struct DevPtrs {
     int4 *items;             // (particle, entry or ITEM_WALL + wall, partner slot, 0);
                              // (particle, ITEM_TRI, triangle-wall hit bits, 0)
     int *tri_list;           // item index of each triangle-wall item (n_tri of them)
+    double *tri_first;       // triangle contacts of the initial evaluation, TRI_REC doubles each,
+                             // DEM_MAX_TRIANGLE_CONTACTS per particle in caller order (k_tri)
+    int *tri_first_n;        // their number per particle (caller order)
     double *shares;          // 12 doubles per item
     int item_cap;
     Control *ctl;

@@ -31,6 +31,10 @@ namespace dem {
 
 constexpr int ITEM_WALL = 1 << 20;   // item entry field >= this: wall contact (ITEM_WALL + wall)
 constexpr int ITEM_TRI = ITEM_WALL + (1 << 10); // all triangle-wall contacts of a particle (k_tri)
+// One triangle contact of the initial evaluation (k_tri): wall, creation key,
+// overlap, normal, force, torque, contact point, species, normal elastic
+// energy, springs.
+constexpr int TRI_REC = 26;
 constexpr int SLOT_NONE = -1;        // P entry without a contact this evaluation
 constexpr int SLOT_IS_I = -2;        // entry whose partner owns the pair, no contact this evaluation
 constexpr int SLOT_I_BASE = -3;      // SLOT_I_BASE - q: I's share of the partner's item q
@@ -473,6 +477,12 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
 // removeInteraction erases in place): each triangle contact carries a
 // creation key (the time step it was made x 16 + its rank within that
 // step) in the pad word of its history row.
+// The first time step shares its time stamp with the initial evaluation
+// (both numberOfTimeSteps + 1 = 1), so there every contact of the initial
+// evaluation counts as made this step: the group rule compares against all
+// of them from the start, a triangle takes its own contact over from that
+// list, and the weighting includes those not touched again. The initial
+// evaluation keeps its contacts' state in tri_first for this.
 constexpr int TRI_BLOCK = 64;
 template <int MODE, int NLAW, int FLAW, int NCOMP>
 __global__ void __launch_bounds__(TRI_BLOCK) k_tri(DevPtrs d)
@@ -507,8 +517,26 @@ __global__ void __launch_bounds__(TRI_BLOCK) k_tri(DevPtrs d)
         V3 en[MAXT], ec[MAXT], ef[MAXT], et[MAXT], etan[MAXT];
         Springs es[MAXT];
         int ne = 0;
-        unsigned int taken = 0u; // triangles whose last-step contact went into an entry
         V3 F = zero3(), T = zero3();
+        const int ci = d.caller[c][s];
+        if (first) { // the initial evaluation's contacts, in list order
+            const int n0 = min(d.tri_first_n[ci], MAXT);
+            const double* rec = d.tri_first + (size_t)ci * MAXT * TRI_REC;
+            for (int o = 0; o < n0; ++o, rec += TRI_REC) {
+                ew[o] = (int)rec[0]; ek[o] = rec[1]; eov[o] = rec[2];
+                en[o] = v3(rec[3], rec[4], rec[5]);
+                ef[o] = v3(rec[6], rec[7], rec[8]);
+                et[o] = v3(rec[9], rec[10], rec[11]);
+                ec[o] = v3(rec[12], rec[13], rec[14]);
+                esw[o] = (int)rec[15]; eel[o] = rec[16];
+                es[o].slide = v3(rec[17], rec[18], rec[19]);
+                es[o].roll = v3(rec[20], rec[21], rec[22]);
+                es[o].tors = v3(rec[23], rec[24], rec[25]);
+                etan[o] = zero3();
+                ord[o] = o;
+            }
+            ne = n0;
+        }
         for (unsigned int b = mask; b; b &= b - 1) {
             const int w = __ffs(b) - 1;
             const int wg = I.wall_begin + w;
@@ -539,6 +567,12 @@ __global__ void __launch_bounds__(TRI_BLOCK) k_tri(DevPtrs d)
                 }
             }
             if (dropped) continue;
+            if (k < 0 && first) // InteractionHandler::getExistingInteraction: first in list order
+                for (int o = 0; o < ne; ++o)
+                    if (ew[ord[o]] == w) {
+                        k = ord[o];
+                        break;
+                    }
             if (k < 0) {
                 if (ne == MAXT) {
                     atomicOr(&ctl->status, 1u << DEM_ERR_CAPACITY);
@@ -548,11 +582,10 @@ __global__ void __launch_bounds__(TRI_BLOCK) k_tri(DevPtrs d)
                 ew[k] = w;
                 esw[k] = wall.species;
                 es[k].slide = zero3(); es[k].roll = zero3(); es[k].tors = zero3();
-                if ((was >> w) & 1u) { // the contact with this triangle from the last step
+                if (!first && ((was >> w) & 1u)) { // the contact with this triangle from the last step
                     const size_t hb = whist_at(d.ncap, NCOMP, s, w);
                     load_springs(d.whist[c], hb, NCOMP, es[k]);
                     ek[k] = d.whist[c][hb + NCOMP];
-                    taken |= 1u << w;
                 } else {
                     ek[k] = step_key + (double)(made++);
                 }
@@ -614,15 +647,23 @@ __global__ void __launch_bounds__(TRI_BLOCK) k_tri(DevPtrs d)
             store_springs(d.whist[nb], hb, NCOMP, es[e]);
             d.whist[nb][hb + NCOMP] = ek[e];
         }
-        if (first) {
-            for (unsigned int b = mask & was & ~taken & ~kept_bits; b; b &= b - 1) {
-                const int w = __ffs(b) - 1;
-                const size_t hb = whist_at(d.ncap, NCOMP, s, w);
-                for (int q2 = 0; q2 < hist_stride(NCOMP); ++q2) d.whist[nb][hb + q2] = d.whist[c][hb + q2];
-                kept_bits |= 1u << w;
-            }
-        }
         d.wact[nb][s] = (d.wact[nb][s] & ~mask) | kept_bits;
+        if (MODE == 0) { // kept for the first time step
+            double* rec = d.tri_first + (size_t)ci * MAXT * TRI_REC;
+            for (int o = 0; o < ne; ++o, rec += TRI_REC) {
+                const int e = ord[o];
+                rec[0] = (double)ew[e]; rec[1] = ek[e]; rec[2] = eov[e];
+                rec[3] = en[e].x; rec[4] = en[e].y; rec[5] = en[e].z;
+                rec[6] = ef[e].x; rec[7] = ef[e].y; rec[8] = ef[e].z;
+                rec[9] = et[e].x; rec[10] = et[e].y; rec[11] = et[e].z;
+                rec[12] = ec[e].x; rec[13] = ec[e].y; rec[14] = ec[e].z;
+                rec[15] = (double)esw[e]; rec[16] = eel[e];
+                rec[17] = es[e].slide.x; rec[18] = es[e].slide.y; rec[19] = es[e].slide.z;
+                rec[20] = es[e].roll.x; rec[21] = es[e].roll.y; rec[22] = es[e].roll.z;
+                rec[23] = es[e].tors.x; rec[24] = es[e].tors.y; rec[25] = es[e].tors.z;
+            }
+            d.tri_first_n[ci] = ne;
+        }
         if (record) {
             for (int e = 0; e < ne; ++e) {
                 const int wg = I.wall_begin + ew[e];

@@ -13,12 +13,10 @@ GPU: at the uploaded state the contact set and every per-contact force,
 overlap and spring are bit-exact against the reference; over 20-100 steps
 (contacts made, merged, weighted, handed between triangles) positions agree
 to 1e-13 of a diameter and forces, torques and springs to 1e-9 relative.
-Grouped triangles run from a state without triangle contacts (spheres
-dropped onto the mesh): in the reference's first time step the contacts of
-the initial evaluation carry the current time stamp (both use
-numberOfTimeSteps + 1 = 1), so its group rule also compares against
-contacts of triangles not yet visited in that step; the engine applies the
-rule of every later step there.
+Both start states occur: spheres touching the mesh at the upload, where the
+reference's first time step shares its time stamp with the initial
+evaluation (both numberOfTimeSteps + 1 = 1) and its group rule sees every
+contact of that evaluation, and spheres dropped onto the mesh.
 """
 import numpy as np
 import pytest
@@ -68,7 +66,7 @@ def test_triangle_walls_initial_evaluation_bit_exact(gpu, group):
 
 @pytest.mark.gpu
 @needs_reference
-@pytest.mark.parametrize("group,dropped", [(0, False), (0, True), (1, True)])
+@pytest.mark.parametrize("group,dropped", [(0, False), (0, True), (1, False), (1, True)])
 @pytest.mark.parametrize("nsteps", [20, 100])
 def test_triangle_walls_short_horizon(gpu, group, dropped, nsteps):
     sc = cases.triangle_mesh(group=group, dropped=dropped)
@@ -76,7 +74,7 @@ def test_triangle_walls_short_horizon(gpu, group, dropped, nsteps):
     r = H.run_reference(sc, nsteps)
     assert H.pair_set(g["contacts"]) == H.pair_set(r["contacts"])
     # touching spheres mostly rebound within 100 steps; dropped ones are pressed on
-    assert _triangle_pairs(g["contacts"]) > {(False, 20): 100, (False, 100): 0, (True, 20): 25, (True, 100): 80}[
+    assert _triangle_pairs(g["contacts"]) > {(False, 20): 60, (False, 100): 0, (True, 20): 25, (True, 100): 80}[
         (dropped, nsteps)]
     assert H.rel_err(g["position"], r["position"], 1e-3) < 1e-13
     assert H.rel_err(g["velocity"], r["velocity"]) < 1e-9

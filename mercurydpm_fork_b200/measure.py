@@ -6,6 +6,7 @@
     python -m mercurydpm_fork_b200.measure surrogate   # MLP inference / training on the tensor cores
     python -m mercurydpm_fork_b200.measure calibration # calibrations per hour at 2 % response error
     python -m mercurydpm_fork_b200.measure cg          # Gaussian CG of the 200k chute (XZ 100 x 1 x 50)
+    python -m mercurydpm_fork_b200.measure triangles   # 200k spheres settling on a 32-triangle mesh floor
 
 Each prints one JSON line. Device time comes from CUDA events (dem_step's own
 events for DEM; torch events around the calls for the surrogate).
@@ -166,8 +167,26 @@ def cg(reps=10, steps_between=1000):
                 cg_share_of_interval=cg_ms / (cg_ms + step_ms))
 
 
+def triangles(n=200_000, settle_steps=40_000):
+    """The triangle_floor scenario after `settle_steps` steps (the bed has
+    landed on the mesh), then timed; counts of triangle contacts reported."""
+    from . import scenarios
+    sc = scenarios.triangle_floor(n=n)
+    e = sc.engine()
+    e.step(settle_steps)
+    out = _time_dem(e, sc.n_moving)
+    c = e.contacts()
+    out["counts"] = e.counts()
+    out["triangle_contacts"] = int(np.count_nonzero(c["is_wall"]))
+    e.close()
+    out.update(workload="triangle_floor", n=sc.n, triangles=sc.info["triangles"], group=sc.info["group"],
+               layers=sc.info["layers"], settle_steps=settle_steps, dt=sc.time_step,
+               species="LinearViscoelasticSlidingFriction")
+    return out
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "drum"
     fn = dict(drum=drum, drum_dense=drum_dense, heaps=heaps, surrogate=surrogate, calibration=calibration,
-              cg=cg)[which]
+              cg=cg, triangles=triangles)[which]
     print(json.dumps(fn()))

@@ -446,3 +446,45 @@ def batch(members: list, time_step: float | None = None, deletions: list | None 
                  cat("inv_inertia"), cat("species_index").astype(np.int32), ids.astype(np.int32),
                  np.concatenate([np.full(m.n, k, np.int32) for k, m in enumerate(members)]), members,
                  np.array(offsets), dels, rotation=all(m.rotation for m in members))
+
+
+def triangle_floor(n: int = 200_000, seed: int = 4, d: float = 1e-3, density: float = 2000.0, tc: float = 1e-4,
+                   eps: float = 0.8, mu: float = 0.5, l_d: float = 100.0, spacing: float = 1.05,
+                   amplitude_d: float = 3.0, group: int = 1, vstd: float = 0.01) -> Scenario:
+    """Spheres (d = 1 mm, linear viscoelastic + sliding friction) on a simple-
+    cubic lattice (spacing 1.05 d) falling onto a triangulated floor: a height
+    field over the periodic square [0, L]^2 (L = 100 d, periodic in x and y)
+    with 5 x 5 nodes, heights amplitude x a seeded pattern, 32 TriangleWalls of
+    one group (as a mesh read by WallHandler::readTriangleWall gets)."""
+    from .engine import triangle_wall
+    rng = np.random.Generator(np.random.PCG64(seed))
+    r = 0.5 * d
+    L = l_d * d
+    nodes = np.linspace(0.0, L, 5)
+    hz = rng.uniform(0.0, amplitude_d * d, size=(5, 5))
+    hz[-1, :] = hz[0, :]  # the floor is periodic
+    hz[:, -1] = hz[:, 0]
+    walls = []
+    for i in range(4):
+        for j in range(4):
+            p = [np.array([nodes[i + a], nodes[j + b], hz[i + a, j + b]]) for a, b in ((0, 0), (1, 0), (0, 1), (1, 1))]
+            if (i + j) % 2 == 0:
+                walls += [triangle_wall(p[0], p[1], p[3], group=group), triangle_wall(p[0], p[3], p[2], group=group)]
+            else:
+                walls += [triangle_wall(p[0], p[1], p[2], group=group), triangle_wall(p[1], p[3], p[2], group=group)]
+    nx = int(L / (spacing * d))
+    nz = -(-n // (nx * nx))
+    i = np.arange(n)
+    ix, iy, iz = i % nx, (i // nx) % nx, i // (nx * nx)
+    z0 = hz.max() + d
+    pos = np.stack([(ix + 0.5) * spacing * d, (iy + 0.5) * spacing * d, z0 + iz * spacing * d], 1)
+    vel = rng.normal(0.0, vstd, size=(n, 3))
+    radius = np.full(n, r)
+    inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
+    sp = linear_sliding_species(tc, eps, 1.0 / inv_mass[0], mu)
+    top = z0 + nz * spacing * d + 10 * d
+    inst = Instance(domain_min=(0, 0, -d), domain_max=(L, L, top), gravity=(0, 0, -9.81), n_species=1,
+                    periodic_mask=0b011, periodic_min=(0, 0, 0), periodic_max=(L, L, 0))
+    return Scenario("triangle_floor", tc / 50, inst, [sp], np.array([density]), walls, pos, vel, radius, inv_mass,
+                    inv_inertia, np.zeros(n, np.int32), np.arange(n, dtype=np.int32),
+                    info=dict(n=n, d=d, seed=seed, l_d=l_d, layers=nz, triangles=len(walls), group=group))

@@ -454,8 +454,9 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
     while (bits) {
         const int w = __ffs(bits) - 1;
         bits &= bits - 1;
-        for (int comp = 0; comp < hist_stride(d.ncomp); ++comp)
+        for (int comp = 0; comp < d.ncomp; ++comp)
             d.whist[nb][whist_at(d.ncap, d.ncomp, s, w) + comp] = d.whist[hc][whist_at(d.ncap, d.ncomp, o, w) + comp];
+        if (d.has_tri) d.whist[nb][whist_at(d.ncap, d.ncomp, s, w) + d.ncomp] = d.whist[hc][whist_at(d.ncap, d.ncomp, o, w) + d.ncomp];
     }
 }
 

@@ -450,12 +450,15 @@ def batch(members: list, time_step: float | None = None, deletions: list | None 
 
 def triangle_floor(n: int = 200_000, seed: int = 4, d: float = 1e-3, density: float = 2000.0, tc: float = 1e-4,
                    eps: float = 0.8, mu: float = 0.5, l_d: float = 100.0, spacing: float = 1.05,
-                   amplitude_d: float = 3.0, group: int = 1, vstd: float = 0.01) -> Scenario:
+                   amplitude_d: float = 3.0, group: int = 1, vstd: float = 0.01, drop_d: float = 1.0,
+                   v0: float = 0.0) -> Scenario:
     """Spheres (d = 1 mm, linear viscoelastic + sliding friction) on a simple-
     cubic lattice (spacing 1.05 d) falling onto a triangulated floor: a height
     field over the periodic square [0, L]^2 (L = 100 d, periodic in x and y)
     with 5 x 5 nodes, heights amplitude x a seeded pattern, 32 TriangleWalls of
-    one group (as a mesh read by WallHandler::readTriangleWall gets)."""
+    one group (as a mesh read by WallHandler::readTriangleWall gets). The
+    lowest layer starts drop_d diameters above the highest floor node, every
+    sphere moving down at v0."""
     from .engine import triangle_wall
     rng = np.random.Generator(np.random.PCG64(seed))
     r = 0.5 * d
@@ -476,9 +479,10 @@ def triangle_floor(n: int = 200_000, seed: int = 4, d: float = 1e-3, density: fl
     nz = -(-n // (nx * nx))
     i = np.arange(n)
     ix, iy, iz = i % nx, (i // nx) % nx, i // (nx * nx)
-    z0 = hz.max() + d
+    z0 = hz.max() + r + drop_d * d
     pos = np.stack([(ix + 0.5) * spacing * d, (iy + 0.5) * spacing * d, z0 + iz * spacing * d], 1)
     vel = rng.normal(0.0, vstd, size=(n, 3))
+    vel[:, 2] -= v0
     radius = np.full(n, r)
     inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
     sp = linear_sliding_species(tc, eps, 1.0 / inv_mass[0], mu)

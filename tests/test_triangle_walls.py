@@ -95,3 +95,19 @@ def test_moving_triangle_walls_match_reference(gpu):
     assert H.pair_set(g["contacts"]) == H.pair_set(r["contacts"])
     assert H.rel_err(g["position"], r["position"], 1e-3) < 1e-13
     assert H.rel_err(g["force"], r["force"]) < 1e-9
+
+
+@pytest.mark.gpu
+@needs_reference
+def test_periodic_triangle_floor_matches_reference(gpu):
+    """Grouped triangles spanning a periodic square (x and y), spheres
+    arriving at 1 m/s: contacts near the periodic seams, list rebuilds."""
+    from mercurydpm_fork_b200 import scenarios
+    sc = scenarios.triangle_floor(n=1500, l_d=20.0, amplitude_d=0.3, drop_d=0.05, v0=1.0)
+    g = H.run_gpu(sc, 200)
+    r = H.run_reference(sc, 200)
+    assert H.pair_set(g["contacts"]) == H.pair_set(r["contacts"])
+    assert _triangle_pairs(g["contacts"]) > 100
+    assert H.rel_err(g["position"], r["position"], 1e-3) < 1e-13
+    assert H.rel_err(g["force"], r["force"]) < 1e-9
+    assert H.rel_err(g["contacts"]["springs"], r["contacts"]["springs"]) < 1e-9

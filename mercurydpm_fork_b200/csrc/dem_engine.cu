@@ -590,6 +590,9 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         I.n_species = D.n_species;
         I.wall_begin = wbegin[in];
         I.wall_end = wend[in];
+        I.tri_mask = 0u;
+        for (int w = wbegin[in]; w < wend[in]; ++w)
+            if (h->walls[w].type == DEM_WALL_TRIANGLE) I.tri_mask |= 1u << (w - wbegin[in]);
         I.n_del = 0;
         for (const auto& db : h->deletions)
             if (db.instance == in) { // DeletionBoundary::set normalises (DeletionBoundary.cc:86-91)
@@ -680,6 +683,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         d.rev = kept.rev; d.slot = kept.slot; d.slotw = kept.slotw; d.items = kept.items; d.shares = kept.shares;
         d.item_cap = kept.item_cap;
         d.tri_list = kept.tri_list;
+        d.slott = kept.slott;
         d.tri_first = kept.tri_first;
         d.tri_first_n = kept.tri_first_n;
         for (int b = 0; b < 2; ++b) { // no history carries over from the previous simulation
@@ -713,6 +717,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     if ((rc = dalloc(h, &d.items, (size_t)d.item_cap))) return rc;
     if ((rc = dalloc(h, &d.shares, (size_t)d.item_cap * SHARE))) return rc;
     if ((rc = dalloc(h, &d.tri_list, NC))) return rc;
+    if ((rc = dalloc(h, &d.slott, NC))) return rc;
     if ((rc = dalloc(h, &d.tri_first_n, NC))) return rc;
     if ((rc = dalloc(h, &d.tri_first, any_tri ? NC * DEM_MAX_TRIANGLE_CONTACTS * TRI_REC : 1))) return rc;
     if ((rc = dalloc(h, &d.force, 3 * NC))) return rc;

@@ -57,6 +57,7 @@ struct InstanceDev {
     double max_interaction_distance;
     // DeletionBoundary planes: a particle is deleted when del_d - x . del_n < 0
     int n_del;
+    uint32_t tri_mask;     // walls (bit w = wall_begin + w) that are triangle walls
     double del_n[DEM_MAX_DELETION_PER_INSTANCE][3];
     double del_d[DEM_MAX_DELETION_PER_INSTANCE];
 };
@@ -151,6 +152,7 @@ struct DevPtrs {
     int4 *items;             // (particle, entry or ITEM_WALL + wall, partner slot, 0);
                              // (particle, ITEM_TRI, triangle-wall hit bits, 0)
     int *tri_list;           // item index of each triangle-wall item (n_tri of them)
+    int *slott;              // per particle: its triangle-wall item or SLOT_NONE
     double *tri_first;       // triangle contacts of the initial evaluation, TRI_REC doubles each,
                              // DEM_MAX_TRIANGLE_CONTACTS per particle in caller order (k_tri)
     int *tri_first_n;        // their number per particle (caller order)

@@ -46,7 +46,10 @@ __global__ void k_control(Control* ctl, dem_wall* walls, WallGeom* wgeom, int n_
         const Q4 q = quat_rotate(Q4{w.orientation[0], w.orientation[1], w.orientation[2], w.orientation[3]},
                                  v3(w.angular_velocity[0] * dt, w.angular_velocity[1] * dt, w.angular_velocity[2] * dt));
         w.orientation[0] = q.q0; w.orientation[1] = q.q1; w.orientation[2] = q.q2; w.orientation[3] = q.q3;
-        if (w.type == DEM_WALL_TRIANGLE) triangle_geometry(w, wgeom[k]);
+        const bool still = w.velocity[0] == 0.0 && w.velocity[1] == 0.0 && w.velocity[2] == 0.0 &&
+                           w.angular_velocity[0] == 0.0 && w.angular_velocity[1] == 0.0 &&
+                           w.angular_velocity[2] == 0.0; // nothing moved: the geometry stands
+        if (w.type == DEM_WALL_TRIANGLE && !still) triangle_geometry(w, wgeom[k]);
     }
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (ctl->pending_flip) {

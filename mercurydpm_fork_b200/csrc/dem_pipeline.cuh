@@ -244,24 +244,30 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         if (!(is.w & FLAG_FIXED)) {
             const unsigned int wa = d.wact[c][s];
             nwalls = I.wall_end - I.wall_begin;
+            if (I.tri_mask) d.slott[s] = SLOT_NONE;
             for (int w = 0; w < nwalls; ++w) {
                 const int wg = I.wall_begin + w;
-                const dem_wall& wall = d.walls[wg];
-                const dem_species_pair& sp = d.species[I.species_offset + is.y * ns + wall.species];
-                double dist;
-                V3 nrm;
                 const unsigned int bit = 1u << w;
-                d.slotw[(size_t)w * d.ncap + s] = SLOT_NONE;
-                const double R = ps.w + sp.interaction_distance;
                 bool hit;
-                if (wall.type == DEM_WALL_TRIANGLE) {
-                    // the face-plane test that opens TriangleWall::getDistanceAndNormal;
-                    // k_tri finishes it and settles the history bits of these walls
+                if (I.tri_mask & bit) {
+                    // within R of the vertices' bounding box (the region the reference
+                    // searches, Mercury3D::computeWallForces with TriangleWall::isLocal)
+                    // and the face-plane test that opens TriangleWall::getDistanceAndNormal,
+                    // R with the instance's largest interaction distance; k_tri finishes
+                    // it and settles the history bits of these walls
                     const WallGeom& tg = d.wgeom[wg];
-                    hit = fabs(dot(xs - row3(tg.tv[0]), row3(tg.tfn))) < R;
+                    const double R = ps.w + I.max_interaction_distance;
+                    hit = xs.x > tg.tlo[0] - R && xs.x < tg.thi[0] + R && xs.y > tg.tlo[1] - R &&
+                          xs.y < tg.thi[1] + R && xs.z > tg.tlo[2] - R && xs.z < tg.thi[2] + R &&
+                          fabs(dot(xs - row3(tg.tv[0]), row3(tg.tfn))) < R;
                     if (hit) thit |= bit;
                 } else {
-                    hit = wall_distance(wall, d.wgeom + wg, xs, R, dist, nrm);
+                    const dem_wall& wall = d.walls[wg];
+                    const dem_species_pair& sp = d.species[I.species_offset + is.y * ns + wall.species];
+                    double dist;
+                    V3 nrm;
+                    d.slotw[(size_t)w * d.ncap + s] = SLOT_NONE;
+                    hit = wall_distance(wall, d.wgeom + wg, xs, ps.w + sp.interaction_distance, dist, nrm);
                     if (hit) whit |= bit;
                 }
                 if (hit) {
@@ -312,9 +318,9 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         d.slotw[(size_t)w * d.ncap + s] = q;
         ++q;
     }
-    if (thit) { // its net share is summed at the first triangle wall's place
+    if (thit) { // its net share is summed after the other walls' shares
         d.items[q] = make_int4(s, ITEM_TRI, (int)thit, 0);
-        d.slotw[(size_t)(__ffs(thit) - 1) * d.ncap + s] = q;
+        d.slott[s] = q;
         d.tri_list[atomicAdd(&ctl->n_tri, 1u)] = q;
     }
 }
@@ -735,12 +741,22 @@ __global__ void __launch_bounds__(SUM_BLOCK, 5) k_sum(DevPtrs d)
             F += v3(I.gravity[0], I.gravity[1], I.gravity[2]) * m - d.drag * xyz(vs);
             const int nw = I.wall_end - I.wall_begin;
             for (int w = 0; w < nw; ++w) {
+                if ((I.tri_mask >> w) & 1u) continue;
                 const int q = d.slotw[(size_t)w * d.ncap + s];
                 if (q < 0) continue;
                 const double2* sh = reinterpret_cast<const double2*>(d.shares + (size_t)q * SHARE);
                 const double2 a = sh[0], b = sh[1], e2 = sh[2];
                 F += v3(a.x, a.y, b.x);
                 T += v3(b.y, e2.x, e2.y);
+            }
+            if (I.tri_mask) { // the net share of all triangle contacts (k_tri)
+                const int q = d.slott[s];
+                if (q >= 0) {
+                    const double2* sh = reinterpret_cast<const double2*>(d.shares + (size_t)q * SHARE);
+                    const double2 a = sh[0], b = sh[1], e2 = sh[2];
+                    F += v3(a.x, a.y, b.x);
+                    T += v3(b.y, e2.x, e2.y);
+                }
             }
         }
         if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z))) atomicOr(&ctl->status, 1u << DEM_ERR_NAN);

@@ -41,6 +41,7 @@ struct WallGeom {
     double ten[3][3];                 // unit in-plane edge normals (edgeNormal_)
     double tel[3];                    // edge lengths (edgeLength_)
     double tfn[3];                    // unit face normal (faceNormal_)
+    double tlo[3], thi[3];            // bounding box of the vertices (vertexMin_, vertexMax_)
 };
 
 __host__ __device__ __forceinline__ Q4 wall_q(const dem_wall& w)
@@ -208,6 +209,10 @@ __host__ __device__ inline void triangle_geometry(const dem_wall& w, WallGeom& g
         g.tel[i] = l;
     }
     g.tfn[0] = fn.x; g.tfn[1] = fn.y; g.tfn[2] = fn.z;
+    for (int k = 0; k < 3; ++k) {
+        g.tlo[k] = fmin(fmin(g.tv[0][k], g.tv[1][k]), g.tv[2][k]);
+        g.thi[k] = fmax(fmax(g.tv[0][k], g.tv[1][k]), g.tv[2][k]);
+    }
 }
 
 // TriangleWall::isInsideTriangle (TriangleWall.cc:251-262): the three

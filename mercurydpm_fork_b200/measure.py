@@ -167,11 +167,12 @@ def cg(reps=10, steps_between=1000):
                 cg_share_of_interval=cg_ms / (cg_ms + step_ms))
 
 
-def triangles(n=200_000, settle_steps=40_000):
+def triangles(n=200_000, settle_steps=40_000, drop_d=1.0, v0=0.0):
     """The triangle_floor scenario after `settle_steps` steps (the bed has
     landed on the mesh), then timed; counts of triangle contacts reported."""
     from . import scenarios
-    sc = scenarios.triangle_floor(n=n)
+    sc = scenarios.triangle_floor(n=int(n), drop_d=float(drop_d), v0=float(v0))
+    settle_steps = int(settle_steps)
     e = sc.engine()
     e.step(settle_steps)
     out = _time_dem(e, sc.n_moving)
@@ -187,6 +188,7 @@ def triangles(n=200_000, settle_steps=40_000):
 
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "drum"
+    kwargs = dict(a.split("=", 1) for a in sys.argv[2:])  # e.g. triangles n=20000 settle_steps=2000
     fn = dict(drum=drum, drum_dense=drum_dense, heaps=heaps, surrogate=surrogate, calibration=calibration,
               cg=cg, triangles=triangles)[which]
-    print(json.dumps(fn()))
+    print(json.dumps(fn(**kwargs)))

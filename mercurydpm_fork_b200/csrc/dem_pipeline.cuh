@@ -244,12 +244,12 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         if (!(is.w & FLAG_FIXED)) {
             const unsigned int wa = d.wact[c][s];
             nwalls = I.wall_end - I.wall_begin;
-            if (I.tri_mask) d.slott[s] = SLOT_NONE;
+            if (d.has_tri && I.tri_mask) d.slott[s] = SLOT_NONE;
             for (int w = 0; w < nwalls; ++w) {
                 const int wg = I.wall_begin + w;
                 const unsigned int bit = 1u << w;
                 bool hit;
-                if (I.tri_mask & bit) {
+                if (d.has_tri && (I.tri_mask & bit)) {
                     // within R of the vertices' bounding box (the region the reference
                     // searches, Mercury3D::computeWallForces with TriangleWall::isLocal)
                     // and the face-plane test that opens TriangleWall::getDistanceAndNormal,
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += gridDim.x * blockDim.x) {
         const int4 item = d.items[q];
         const int s = item.x, kq = item.y;
-        if (kq == ITEM_TRI) continue; // k_tri
+        if (d.has_tri && kq == ITEM_TRI) continue; // k_tri
         const double4 ps = d.pr[c][s];
         const double4 vs = d.vm[c][s];
         const double4 ws = d.wi[c][s];
@@ -741,7 +741,7 @@ __global__ void __launch_bounds__(SUM_BLOCK, 5) k_sum(DevPtrs d)
             F += v3(I.gravity[0], I.gravity[1], I.gravity[2]) * m - d.drag * xyz(vs);
             const int nw = I.wall_end - I.wall_begin;
             for (int w = 0; w < nw; ++w) {
-                if ((I.tri_mask >> w) & 1u) continue;
+                if (d.has_tri && ((I.tri_mask >> w) & 1u)) continue;
                 const int q = d.slotw[(size_t)w * d.ncap + s];
                 if (q < 0) continue;
                 const double2* sh = reinterpret_cast<const double2*>(d.shares + (size_t)q * SHARE);
@@ -749,7 +749,7 @@ __global__ void __launch_bounds__(SUM_BLOCK, 5) k_sum(DevPtrs d)
                 F += v3(a.x, a.y, b.x);
                 T += v3(b.y, e2.x, e2.y);
             }
-            if (I.tri_mask) { // the net share of all triangle contacts (k_tri)
+            if (d.has_tri && I.tri_mask) { // the net share of all triangle contacts (k_tri)
                 const int q = d.slott[s];
                 if (q >= 0) {
                     const double2* sh = reinterpret_cast<const double2*>(d.shares + (size_t)q * SHARE);

@@ -591,8 +591,21 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         I.wall_begin = wbegin[in];
         I.wall_end = wend[in];
         I.tri_mask = 0u;
-        for (int w = wbegin[in]; w < wend[in]; ++w)
-            if (h->walls[w].type == DEM_WALL_TRIANGLE) I.tri_mask |= 1u << (w - wbegin[in]);
+        I.tri_static = 1;
+        for (int k = 0; k < 3; ++k) {
+            I.tri_lo[k] = DBL_MAX;
+            I.tri_hi[k] = -DBL_MAX;
+        }
+        for (int w = wbegin[in]; w < wend[in]; ++w) {
+            const dem_wall& x = h->walls[w];
+            if (x.type != DEM_WALL_TRIANGLE) continue;
+            I.tri_mask |= 1u << (w - wbegin[in]);
+            for (int k = 0; k < 3; ++k) {
+                I.tri_static = I.tri_static && x.velocity[k] == 0.0 && x.angular_velocity[k] == 0.0;
+                I.tri_lo[k] = std::min(I.tri_lo[k], h->wgeom[w].tlo[k]);
+                I.tri_hi[k] = std::max(I.tri_hi[k], h->wgeom[w].thi[k]);
+            }
+        }
         I.n_del = 0;
         for (const auto& db : h->deletions)
             if (db.instance == in) { // DeletionBoundary::set normalises (DeletionBoundary.cc:86-91)

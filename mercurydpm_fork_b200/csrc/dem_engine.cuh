@@ -58,6 +58,8 @@ struct InstanceDev {
     // DeletionBoundary planes: a particle is deleted when del_d - x . del_n < 0
     int n_del;
     uint32_t tri_mask;     // walls (bit w = wall_begin + w) that are triangle walls
+    int tri_static;        // every triangle wall of the instance stands still: tri_lo/hi hold
+    double tri_lo[3], tri_hi[3]; // the bounding box of all their vertices
     double del_n[DEM_MAX_DELETION_PER_INSTANCE][3];
     double del_d[DEM_MAX_DELETION_PER_INSTANCE];
 };

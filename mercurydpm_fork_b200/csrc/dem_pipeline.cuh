@@ -244,7 +244,14 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         if (!(is.w & FLAG_FIXED)) {
             const unsigned int wa = d.wact[c][s];
             nwalls = I.wall_end - I.wall_begin;
-            if (d.has_tri && I.tri_mask) d.slott[s] = SLOT_NONE;
+            bool near_tri = false; // within reach of the instance's triangles (all of them, if they move)
+            if (d.has_tri && I.tri_mask) {
+                d.slott[s] = SLOT_NONE;
+                const double R = ps.w + I.max_interaction_distance;
+                near_tri = !I.tri_static ||
+                           (xs.x > I.tri_lo[0] - R && xs.x < I.tri_hi[0] + R && xs.y > I.tri_lo[1] - R &&
+                            xs.y < I.tri_hi[1] + R && xs.z > I.tri_lo[2] - R && xs.z < I.tri_hi[2] + R);
+            }
             for (int w = 0; w < nwalls; ++w) {
                 const int wg = I.wall_begin + w;
                 const unsigned int bit = 1u << w;
@@ -255,12 +262,15 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
                     // and the face-plane test that opens TriangleWall::getDistanceAndNormal,
                     // R with the instance's largest interaction distance; k_tri finishes
                     // it and settles the history bits of these walls
-                    const WallGeom& tg = d.wgeom[wg];
-                    const double R = ps.w + I.max_interaction_distance;
-                    hit = xs.x > tg.tlo[0] - R && xs.x < tg.thi[0] + R && xs.y > tg.tlo[1] - R &&
-                          xs.y < tg.thi[1] + R && xs.z > tg.tlo[2] - R && xs.z < tg.thi[2] + R &&
-                          fabs(dot(xs - row3(tg.tv[0]), row3(tg.tfn))) < R;
-                    if (hit) thit |= bit;
+                    hit = false;
+                    if (near_tri) {
+                        const WallGeom& tg = d.wgeom[wg];
+                        const double R = ps.w + I.max_interaction_distance;
+                        hit = xs.x > tg.tlo[0] - R && xs.x < tg.thi[0] + R && xs.y > tg.tlo[1] - R &&
+                              xs.y < tg.thi[1] + R && xs.z > tg.tlo[2] - R && xs.z < tg.thi[2] + R &&
+                              fabs(dot(xs - row3(tg.tv[0]), row3(tg.tfn))) < R;
+                        if (hit) thit |= bit;
+                    }
                 } else {
                     const dem_wall& wall = d.walls[wg];
                     const dem_species_pair& sp = d.species[I.species_offset + is.y * ns + wall.species];

@@ -324,7 +324,9 @@ int  dem_batch_run(dem_handle *h, int nsteps, dem_globals *out);
  * process exits) and therefore accepts at most 2,097,152 particles and
  * 2,097,152 contact records (DEM_ERR_CAPACITY above that). The first call on
  * a device looks up the array's device address; make that first call before
- * any stream capture. All calls share the array: calls that overlap on the
+ * any stream capture. The address is kept for the life of the process, so a
+ * cudaDeviceReset of that device (which also invalidates every handle on it)
+ * ends this entry point's use in the process. All calls share the array: calls that overlap on the
  * GPU (several handles on concurrent streams of one device) race. Results are
  * the same sums, in the same order, as dem_reduce. */
 int  dem_reduce_noalloc(dem_handle *h, int instance, dem_globals *out);

@@ -13,8 +13,12 @@
 # variant into oracle/_ref/libmdpm_ref_{serial,omp}.so (extern "C" entry points
 # used by tests/ and by bench.py's reference arm).
 #
-# Usage:  make -f oracle/ref.mk -j8 REF=/root/reference
-REF ?= /root/reference
+# Usage:  make -f oracle/ref.mk -j8 REF=<reference checkout>
+#         (or with the checkout in $MERCURYDPM_REF)
+REF ?= $(MERCURYDPM_REF)
+ifeq ($(strip $(REF)),)
+$(error give the reference checkout: REF=<path> or MERCURYDPM_REF=<path>)
+endif
 OUT := oracle/_ref
 K   := $(REF)/Kernel
 

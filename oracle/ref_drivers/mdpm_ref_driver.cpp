@@ -133,6 +133,19 @@ public:
         outputXBallsData(data);
     }
 
+    // DPMBase::solve with the .ene file as the only output, a line every
+    // save_count time steps (DPMBase::writeEneTimeStep, DPMBase.cc:2100-2123),
+    // to name.ene. The soft stop stays off: it would replace the host
+    // process's SIGINT / SIGTERM handlers.
+    void solve_writing_ene(const std::string& name, unsigned save_count)
+    {
+        setName(name);
+        eneFile.setFileType(FileType::ONE_FILE);
+        eneFile.setSaveCount(save_count);
+        disableSoftStop();
+        solve();
+    }
+
     const dem_config* cfg = nullptr;
     const dem_instance_desc* inst = nullptr;
     const dem_species_pair* species = nullptr;
@@ -444,6 +457,42 @@ int mdpm_ref_time(const dem_config* cfg, const dem_instance_desc* inst, const de
     for (int k = 0; k < nsteps; ++k) d.computeOneTimeStep();
     const auto t1 = std::chrono::steady_clock::now();
     *seconds = std::chrono::duration<double>(t1 - t0).count();
+    return 0;
+}
+
+// The reference's own run of `nsteps` time steps through DPMBase::solve(),
+// writing its .ene file (prefix.ene) every `save_count` steps and at the end.
+// timeMax sits half a step short of nsteps * dt, so that the solve loop
+// (while time < timeMax) takes exactly nsteps steps.
+int mdpm_ref_solve_ene(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
+                       const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in,
+                       int nsteps, int save_count, int threads, const char* prefix)
+{
+    RefDriver d;
+    setup(d, cfg, inst, species, density, walls, nwalls, in, threads);
+    d.setTimeMax((nsteps - 0.5) * cfg->time_step);
+    d.solve_writing_ene(prefix, (unsigned)save_count);
+    return 0;
+}
+
+// mdpm_ref_time, also reporting the interactions the handler holds (particle
+// pairs and wall contacts) when the timed window starts and when it ends, so
+// that a caller can show which phase of the run the window sampled.
+int mdpm_ref_time_window(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
+                         const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in,
+                         int warmup, int nsteps, int threads, double* seconds, int64_t* interactions_start,
+                         int64_t* interactions_end)
+{
+    RefDriver d;
+    setup(d, cfg, inst, species, density, walls, nwalls, in, threads);
+    d.initialiseSolve();
+    for (int k = 0; k < warmup; ++k) d.computeOneTimeStep();
+    *interactions_start = (int64_t)d.interactionHandler.getNumberOfObjects();
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int k = 0; k < nsteps; ++k) d.computeOneTimeStep();
+    const auto t1 = std::chrono::steady_clock::now();
+    *seconds = std::chrono::duration<double>(t1 - t0).count();
+    *interactions_end = (int64_t)d.interactionHandler.getNumberOfObjects();
     return 0;
 }
 

@@ -6,6 +6,16 @@ tests never read the reference at run time).
   Drivers/UnitTests/TangentialSpringUnitTest.cpp asserts (final position,
   velocity and angular velocity of the rolling sphere, tolerance 1e-7), plus
   the set-up numbers of that test.
+* settling_box_ene.json: the .ene file the reference writes (its own
+  DPMBase::solve and writeEneTimeStep, a line every 500 steps) for the
+  5,000-sphere settling box over 20,000 steps (scenarios.settling_box), from
+  its serial build and from its OpenMP build on 8 threads. The two builds
+  differ only in the order of floating-point sums; their difference is the
+  chaos envelope the GPU run is held to. Needs the reference build
+  (oracle/_ref, `make -f oracle/ref.mk`).
+
+Usage: python tests/golden/make_golden.py [REFERENCE_CHECKOUT] [fixture ...]
+(the checkout defaults to $MERCURYDPM_REF).
 """
 from __future__ import annotations
 
@@ -14,8 +24,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = sys.argv[1] if len(sys.argv) > 1 and os.path.isdir(sys.argv[1]) else os.environ.get("MERCURYDPM_REF", "")
 
 
 def vec(s):
@@ -41,8 +52,35 @@ def tangential_spring():
     return out
 
 
+ENE_STEPS = 20_000
+ENE_SAVE = 500
+
+
+def settling_box_ene():
+    import tempfile
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.dirname(HERE))
+    import harness as H
+    from mercurydpm_fork_b200 import scenarios
+    sc = scenarios.settling_box()
+    with tempfile.TemporaryDirectory() as tmp:
+        serial = H.reference_ene(sc, ENE_STEPS, ENE_SAVE, os.path.join(tmp, "serial"), "serial")
+        omp = H.reference_ene(sc, ENE_STEPS, ENE_SAVE, os.path.join(tmp, "omp"), "omp", threads=8)
+    return {"scenario": "scenarios.settling_box() (5,000 spheres, 20 x 20 x 40 d box, dt = tc/50 = 2e-6 s)",
+            "steps": ENE_STEPS, "save_count": ENE_SAVE,
+            "columns": ["time", "gravitational", "kinetic", "rotational", "elastic", "com_x", "com_y", "com_z",
+                        "interactions"],
+            "serial": serial.tolist(), "omp8": omp.tolist()}
+
+
+FIXTURES = {"tangential_spring": tangential_spring, "settling_box_ene": settling_box_ene}
+
 if __name__ == "__main__":
-    data = tangential_spring()
-    with open(os.path.join(HERE, "tangential_spring.json"), "w") as f:
-        json.dump(data, f, indent=1)
-    print(json.dumps(data, indent=1))
+    if not REF:
+        sys.exit("give the reference checkout as the first argument or in $MERCURYDPM_REF")
+    names = [a for a in sys.argv[1:] if a in FIXTURES] or list(FIXTURES)
+    for name in names:
+        data = FIXTURES[name]()
+        with open(os.path.join(HERE, name + ".json"), "w") as f:
+            json.dump(data, f, indent=1)
+        print(name, "written")

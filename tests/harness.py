@@ -128,7 +128,15 @@ def _outputs(n, cap):
 
 
 def _trim(c, m):
+    assert m <= len(c["id_p"]), f"{m} contacts exceed the {len(c['id_p'])} rows allocated"
     return {k: v[:m] for k, v in c.items()}
+
+
+def _contact_rows(n: int) -> int:
+    """Contact rows allocated for a run of n particles: 16 per particle for
+    small cases (dense packings of several sizes), 4 per particle above
+    100,000 (the large workloads have under 2 contacts per particle)."""
+    return 16 * n + 64 if n <= 100_000 else 4 * n + 4096
 
 
 def sort_contacts(c):
@@ -145,7 +153,7 @@ def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated", deleti
     darr, nd = _deletions(deletions)
     oracle_lib().oracle_set_deletion(darr, nd)
     inp = _Inputs(sc, contacts)
-    cap = 16 * sc.n + 64
+    cap = _contact_rows(sc.n)
     o, c, soa, csoa = _outputs(sc.n, cap)
     cnt = C.c_int64(0)
     rc = oracle_lib().oracle_run(C.byref(inp.cfg), C.byref(inp.inst), inp.species, len(sc.species), inp.walls,
@@ -161,7 +169,7 @@ def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None) -> d
     darr, nd = _deletions(deletions)
     ref_lib(variant).mdpm_ref_set_deletion(darr, nd)
     inp = _Inputs(sc)
-    cap = 16 * sc.n + 64
+    cap = _contact_rows(sc.n)
     o, c, soa, csoa = _outputs(sc.n, cap)
     cnt = C.c_int64(0)
     ene = np.zeros(4)
@@ -240,17 +248,66 @@ class quiet_stdout:
         return False
 
 
-def time_reference(sc, warmup: int, nsteps: int, threads: int, variant: str = "omp") -> float:
+def reference_ene(sc, nsteps: int, save_count: int, prefix: str, variant: str = "serial", threads: int = 1):
+    """The reference's DPMBase::solve() over nsteps time steps with its own
+    .ene writer (a line every save_count steps and one at the end); returns
+    the parsed rows (time, gravitational, kinetic, rotational, elastic
+    energy, centre of mass x y z, interactions), one per distinct time."""
     darr, nd = _deletions(None)
-    ref_lib(variant).mdpm_ref_set_deletion(darr, nd)
+    lib = ref_lib(variant)
+    lib.mdpm_ref_set_deletion(darr, nd)
+    fn = lib.mdpm_ref_solve_ene
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(_abi.Config), C.POINTER(_abi.InstanceDesc), C.POINTER(_abi.SpeciesPair), _pd,
+                   C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA), C.c_int, C.c_int, C.c_int, C.c_char_p]
+    inp = _Inputs(sc)
+    with quiet_stdout():
+        rc = fn(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density), inp.walls, inp.nwalls,
+                C.byref(inp.soa), nsteps, save_count, threads, prefix.encode())
+    assert rc == 0
+    return parse_ene(open(prefix + ".ene").read())
+
+
+def parse_ene(text: str) -> np.ndarray:
+    """Rows of a .ene file (header lines skipped, repeated times dropped)."""
+    rows, seen = [], set()
+    for ln in text.splitlines():
+        parts = ln.split()
+        try:
+            vals = [float(x) for x in parts]
+        except ValueError:
+            continue
+        if len(vals) != 9 or vals[0] in seen:
+            continue
+        seen.add(vals[0])
+        rows.append(vals)
+    return np.array(rows)
+
+
+def time_reference(sc, warmup: int, nsteps: int, threads: int, variant: str = "omp") -> float:
+    return time_reference_window(sc, warmup, nsteps, threads, variant)["seconds"]
+
+
+def time_reference_window(sc, warmup: int, nsteps: int, threads: int, variant: str = "omp") -> dict:
+    """The reference's wall time of time steps warmup+1 .. warmup+nsteps
+    (std::chrono around computeOneTimeStep, set-up excluded) and the number
+    of interactions its handler holds at the start and end of that window."""
+    darr, nd = _deletions(None)
+    lib = ref_lib(variant)
+    lib.mdpm_ref_set_deletion(darr, nd)
+    fn = lib.mdpm_ref_time_window
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(_abi.Config), C.POINTER(_abi.InstanceDesc), C.POINTER(_abi.SpeciesPair), _pd,
+                   C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA), C.c_int, C.c_int, C.c_int, _pd,
+                   C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     inp = _Inputs(sc)
     sec = C.c_double(0)
+    a, b = C.c_int64(0), C.c_int64(0)
     with quiet_stdout():
-        rc = ref_lib(variant).mdpm_ref_time(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density),
-                                            inp.walls, inp.nwalls, C.byref(inp.soa), warmup, nsteps, threads,
-                                            C.byref(sec))
+        rc = fn(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density), inp.walls, inp.nwalls,
+                C.byref(inp.soa), warmup, nsteps, threads, C.byref(sec), C.byref(a), C.byref(b))
     assert rc == 0
-    return sec.value
+    return dict(seconds=sec.value, interactions_start=a.value, interactions_end=b.value)
 
 
 def run_gpu(sc, nsteps: int, contacts=None, deletions=None, **kw) -> dict:

@@ -293,13 +293,35 @@ def hertz_collision_time(d: float, density: float, E: float, v: float = 1.0) -> 
     return 2.214 * ((density / E) ** 2 / v) ** 0.2 * d
 
 
+def _press_onto_cylinder(position, radius, R, band, overlap, tolerance):
+    """Moves spheres whose surface lies within `band` of a cylinder of radius
+    R about x radially outwards until they overlap it by `overlap`, outermost
+    first, keeping a move only if the sphere then overlaps no other sphere by
+    more than `tolerance` (in place)."""
+    from scipy.spatial import cKDTree
+    rho = np.hypot(position[:, 1], position[:, 2])
+    cand = np.nonzero(rho + radius > R - band)[0]
+    cand = cand[np.argsort(-(rho[cand] + radius[cand]))]
+    tree = cKDTree(position)
+    reach = 2.0 * radius.max() + band
+    for i in cand:
+        new = position[i].copy()
+        new[1:] *= (R - radius[i] + overlap) / rho[i]
+        near = [j for j in tree.query_ball_point(new, reach) if j != i]
+        if near:
+            gap = np.linalg.norm(position[near] - new, axis=1) - radius[near] - radius[i]
+            if gap.min() < -tolerance:
+                continue
+        position[i] = new
+
+
 def rotating_drum(n: int = 1_000_000, seed: int = 3, ds: float = 1e-3, size_ratio: float = 3.0,
                   frac_small: float = 0.9, radius_d: float = 120.0, length_d: float = 60.0, omega: float = 1.0,
                   E: float = 1e7, nu: float = 0.3, mu: float = 0.4, mu_r: float = 0.05, eps: float = 0.7,
                   density: float = 2000.0, dt_factor: float = 0.02, site_spacing: float = 1.02,
                   jitter: float = 0.005, vstd: float = 0.0, touch_wall: float = 0.0, gravity: float = 9.81,
                   mu_o: float = 0.0, sliding_dissipation: float = 0.0, rolling_dissipation: float = 0.0,
-                  torsion_dissipation: float = 0.0) -> Scenario:
+                  torsion_dissipation: float = 0.0, wall_contact: bool = False) -> Scenario:
     """Rotating drum: n spheres, frac_small of them small (diameter ds), the
     rest size_ratio x larger, in a cylinder of radius radius_d ds and length
     length_d ds along x (AxisymmetricIntersectionOfWalls with setAxis(1,0,0)
@@ -317,7 +339,12 @@ def rotating_drum(n: int = 1_000_000, seed: int = 3, ds: float = 1e-3, size_rati
     the drum upwards, large cubes chosen in seeded random order, positions
     jittered by +-jitter ds. site_spacing < 1 starts the bed pre-compressed.
     touch_wall > 0 moves every sphere within touch_wall ds of the cylinder
-    radially onto it with an overlap of 0.1 touch_wall ds."""
+    radially onto it with an overlap of 0.1 touch_wall ds. wall_contact puts
+    the bed in contact with both walls the way the lattice's neighbours touch
+    each other (overlap 0.001 ds): spheres within 1.5 ds of the cylinder
+    is moved radially onto it (see _press_onto_cylinder), and each cap is
+    placed 0.001 ds inside the lattice's end face (the outermost sites' centre
+    plus radius)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     R, L = radius_d * ds, length_d * ds
     r_s, r_l = 0.5 * ds, 0.5 * ds * size_ratio
@@ -357,6 +384,12 @@ def rotating_drum(n: int = 1_000_000, seed: int = 3, ds: float = 1e-3, size_rati
         near = rho + radius > R - touch_wall * ds
         target = R - radius[near] + 0.1 * touch_wall * ds
         position[near, 1:] *= (target / rho[near])[:, None]
+    cap = L / 2
+    if wall_contact:
+        lap = 0.001 * ds
+        _press_onto_cylinder(position, radius, R, band=1.5 * ds, overlap=lap, tolerance=0.005 * ds)
+        # end face of the lattice: outermost block centre + (b-1)/2 sites + a small radius
+        cap = float(np.max(np.abs(cen[:, 0]))) + (b - 1) / 2 * s + r_s - lap
     velocity = rng.normal(0.0, vstd, size=(n, 3)) if vstd > 0 else np.zeros((n, 3))
     inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
     G = E / 2 * (1 + nu)
@@ -364,8 +397,8 @@ def rotating_drum(n: int = 1_000_000, seed: int = 3, ds: float = 1e-3, size_rati
                                torsion_dissipation)
     table = [sp] * 9  # species 0 small, 1 large, 2 wall; identical mixed entries
     walls = [axisymmetric_wall((1, 0, 0), [((1, 0, 0), (R, 0, 0))], species=2, angular_velocity=(omega, 0, 0)),
-             infinite_wall((-1, 0, 0), (-L / 2, 0, 0), species=2),
-             infinite_wall((1, 0, 0), (L / 2, 0, 0), species=2)]
+             infinite_wall((-1, 0, 0), (-cap, 0, 0), species=2),
+             infinite_wall((1, 0, 0), (cap, 0, 0), species=2)]
     m = 2 * R + 4 * r_l
     inst = Instance(domain_min=(-L / 2 - 2 * r_l, -m / 2, -m / 2), domain_max=(L / 2 + 2 * r_l, m / 2, m / 2),
                     gravity=(0.0, 0.0, -gravity), n_species=3)
@@ -506,6 +539,8 @@ def dense_drum(n: int = 1_000_000, seed: int = 3, radius_d: float = DRUM_RADIUS_
     rotating at 1 rad/s about x, two flat caps) with its bed started as a
     lattice whose neighbours overlap by 0.1 % of a diameter (jitter
     +-0.005 d), so that nearly every sphere is in contact from the first time
-    step. The first ~100 steps relax those overlaps (about 1.46 contacts per
-    sphere at the start); the bed then loosens."""
-    return rotating_drum(n=n, seed=seed, radius_d=radius_d, length_d=60.0, vstd=0.0, site_spacing=0.999)
+    step. The first ~100 steps relax those overlaps (about 1.6 contacts per
+    sphere then); the bed then loosens. The bed touches the cylinder and both
+    caps the same way (rotating_drum's wall_contact)."""
+    return rotating_drum(n=n, seed=seed, radius_d=radius_d, length_d=60.0, vstd=0.0, site_spacing=0.999,
+                         wall_contact=True)

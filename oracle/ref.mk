@@ -79,11 +79,11 @@ GOMP ?= $(firstword $(wildcard /usr/lib/x86_64-linux-gnu/libgomp.so.1 /usr/lib64
 SDRV := $(patsubst oracle/ref_drivers/%.cpp,$(OUT)/obj/serial/drv_%.o,$(DRIVERS)) $(OUT)/obj/serial/ref_stubs.o
 ODRV := $(patsubst oracle/ref_drivers/%.cpp,$(OUT)/obj/omp/drv_%.o,$(DRIVERS)) $(OUT)/obj/omp/ref_stubs.o
 
-$(OUT)/obj/serial/drv_%.o: oracle/ref_drivers/%.cpp include/dem_b200.h $(OUT)/gen/CMakeDefinitions.h
+$(OUT)/obj/serial/drv_%.o: oracle/ref_drivers/%.cpp oracle/ref_drivers/ref_driver.h include/dem_b200.h $(OUT)/gen/CMakeDefinitions.h
 	@mkdir -p $(@D)
 	$(CXX) $(SERIALFLAGS) -c $< -o $@
 
-$(OUT)/obj/omp/drv_%.o: oracle/ref_drivers/%.cpp include/dem_b200.h $(OUT)/gen/CMakeDefinitions.h
+$(OUT)/obj/omp/drv_%.o: oracle/ref_drivers/%.cpp oracle/ref_drivers/ref_driver.h include/dem_b200.h $(OUT)/gen/CMakeDefinitions.h
 	@mkdir -p $(@D)
 	$(CXX) $(OMPFLAGS) -c $< -o $@
 
@@ -111,6 +111,49 @@ $(OUT)/libmdpm_ref_omp.so: $(OUT)/libMercuryBase_omp.a $(ODRV)
 	$(LINKCXX) -shared -o $@ $(ODRV) $(OUT)/libMercuryBase_omp.a $(GOMP) -lpthread
 
 .PHONY: all
+
+# The engine's drop-in base class (mercurydpm_fork_b200/mercury/GpuTimeStep.h)
+# compiled into reference drivers, linked against the serial Kernel and the
+# engine library (found next to this checkout at run time through $ORIGIN):
+#   gpu_tangential_spring_unit_test : the reference's own
+#       Drivers/UnitTests/TangentialSpringUnitTest.cpp, unmodified, with its
+#       base class DPMBase replaced by GpuDPMBase (oracle/ref_drivers/gpu/)
+#   libmdpm_gpu_binding.so : RefDriverT<GpuMercury3D>, the checker's driver on
+#       the drop-in base class (solve() with the reference's .ene writer)
+ENGINE_LIB := mercurydpm_fork_b200/libdem_b200.so
+BINDING := mercurydpm_fork_b200/mercury/GpuTimeStep.h
+GPUFLAGS := $(SERIALFLAGS) -I$(REF) -Imercurydpm_fork_b200/mercury -Iinclude -Ioracle/ref_drivers
+GPULINK := $(OUT)/libMercuryBase_serial.a $(OUT)/obj/serial/ref_stubs.o -Lmercurydpm_fork_b200 -ldem_b200 \
+           -Wl,-rpath,'$$ORIGIN/../../mercurydpm_fork_b200'
+
+SELFTESTS := ForceSelfTest FreeFallSelfTest
+SELFTEST_SRC_ForceSelfTest := $(REF)/Drivers/SelfTests/Interactions/ForceSelfTest.cpp
+SELFTEST_SRC_FreeFallSelfTest := $(REF)/Drivers/SelfTests/Interactions/FreeFallSelfTest.cpp
+SELFTEST_GPU_ForceSelfTest := oracle/ref_drivers/gpu/force_self_test.cpp
+SELFTEST_GPU_FreeFallSelfTest := oracle/ref_drivers/gpu/free_fall_self_test.cpp
+
+gpu: $(OUT)/gpu_tangential_spring_unit_test $(OUT)/libmdpm_gpu_binding.so \
+     $(foreach t,$(SELFTESTS),$(OUT)/selftest_$(t)_reference $(OUT)/selftest_$(t)_gpu)
+
+# the reference's self tests as they are (the CPU reference run) ...
+$(OUT)/selftest_%_reference: $(OUT)/libMercuryBase_serial.a $(OUT)/obj/serial/ref_stubs.o
+	$(LINKCXX) $(SERIALFLAGS) $(SELFTEST_SRC_$*) -o $@ $(OUT)/libMercuryBase_serial.a $(OUT)/obj/serial/ref_stubs.o
+
+# ... and with their base class swapped for the engine's
+.SECONDEXPANSION:
+$(OUT)/selftest_%_gpu: $$(SELFTEST_GPU_$$*) $(BINDING) $(ENGINE_LIB) $(OUT)/libMercuryBase_serial.a \
+        $(OUT)/obj/serial/ref_stubs.o
+	$(LINKCXX) $(GPUFLAGS) $(SELFTEST_GPU_$*) -o $@ $(GPULINK)
+
+$(OUT)/gpu_tangential_spring_unit_test: oracle/ref_drivers/gpu/tangential_spring_unit_test.cpp $(BINDING) \
+        $(ENGINE_LIB) $(OUT)/libMercuryBase_serial.a $(OUT)/obj/serial/ref_stubs.o
+	$(LINKCXX) $(GPUFLAGS) $< -o $@ $(GPULINK)
+
+$(OUT)/libmdpm_gpu_binding.so: oracle/ref_drivers/gpu/gpu_binding_driver.cpp oracle/ref_drivers/ref_driver.h \
+        $(BINDING) $(ENGINE_LIB) $(OUT)/libMercuryBase_serial.a $(OUT)/obj/serial/ref_stubs.o
+	$(LINKCXX) $(GPUFLAGS) -shared $< -o $@ $(GPULINK)
+
+.PHONY: gpu
 
 objs: $(SOBJS) $(OOBJS)
 .PHONY: objs

@@ -14,6 +14,12 @@ tests never read the reference at run time).
   chaos envelope the GPU run is held to. Needs the reference build
   (oracle/_ref, `make -f oracle/ref.mk`).
 
+* selftest/*.gz: the gold files of the reference's own self tests that cover
+  the time step (Drivers/SelfTests/Interactions/SelfTestData/
+  ForceSelfTest{0..9}.{data,ene}, FreeFallSelfTest.{ene,restart}), copied
+  byte for byte and gzipped; the tests compare them with the reference's
+  fpdiff rule (0.1 % relative, 1e-14 numerical zero).
+
 Usage: python tests/golden/make_golden.py [REFERENCE_CHECKOUT] [fixture ...]
 (the checkout defaults to $MERCURYDPM_REF).
 """
@@ -73,7 +79,22 @@ def settling_box_ene():
             "serial": serial.tolist(), "omp8": omp.tolist()}
 
 
-FIXTURES = {"tangential_spring": tangential_spring, "settling_box_ene": settling_box_ene}
+def selftest():
+    import gzip
+    src = os.path.join(REF, "Drivers", "SelfTests", "Interactions", "SelfTestData")
+    names = [f"ForceSelfTest{k}.{ext}" for k in range(10) for ext in ("data", "ene")]
+    names += ["FreeFallSelfTest.ene", "FreeFallSelfTest.restart"]
+    out = os.path.join(HERE, "selftest")
+    os.makedirs(out, exist_ok=True)
+    for n in names:
+        with open(os.path.join(src, n), "rb") as f:
+            data = f.read()
+        with gzip.GzipFile(os.path.join(out, n + ".gz"), "wb", mtime=0) as g:
+            g.write(data)
+    return {"source": "Drivers/SelfTests/Interactions/SelfTestData", "files": names}
+
+
+FIXTURES = {"tangential_spring": tangential_spring, "settling_box_ene": settling_box_ene, "selftest": selftest}
 
 if __name__ == "__main__":
     if not REF:

@@ -341,3 +341,166 @@ def rel_err(a, b, scale=None):
     if s == 0:
         return float(np.max(np.abs(a - b)))
     return float(np.max(np.abs(a - b)) / s)
+
+
+def engine_ene(sc, steps: int, save: int, **engine_kw) -> np.ndarray:
+    """The .ene lines of the engine's run driven from Python (output.ene_line
+    from dem_reduce after dem_step(0) and every `save` further steps, 10
+    significant digits like the reference's file), parsed back."""
+    from mercurydpm_fork_b200 import output
+    e = sc.engine(**engine_kw)
+    try:
+        text = output.ene_header()
+        e.step(0)
+        for k in range(steps // save + 1):
+            if k:
+                e.step(save)
+            g = e.reduce()
+            text += output.ene_line(output.time_after(k * save, sc.time_step), sc.instance.gravity, g,
+                                    g["n_contacts"] + g["n_wall_contacts"])
+    finally:
+        e.close()
+    return parse_ene(text)
+
+
+def check_ene_against_golden(ours: np.ndarray, gold: dict):
+    """The settling box's .ene rows against the reference's (the fixture
+    tests/golden/settling_box_ene.json): while the reference's serial and
+    OpenMP builds still write identical lines, 1e-8 relative per column and
+    the exact interaction count; over the whole run, at most 3x the largest
+    difference between the reference's two builds in that column plus 1e-9 of
+    the column's magnitude."""
+    serial, omp = np.array(gold["serial"]), np.array(gold["omp8"])
+    assert ours.shape == serial.shape
+    np.testing.assert_array_equal(ours[:, 0], serial[:, 0])
+    agree = np.all(serial == omp, axis=1)
+    n_same = int(np.argmin(agree)) if not agree.all() else len(agree)
+    assert n_same >= 10
+    for col in range(1, 8):
+        scale = np.abs(serial[:n_same, col]).max()
+        err = np.abs(ours[:n_same, col] - serial[:n_same, col]).max()
+        assert err <= 1e-8 * max(scale, 1e-300), (gold["columns"][col], err, scale)
+    np.testing.assert_array_equal(ours[:n_same, 8], serial[:n_same, 8])
+    for col in range(1, 9):
+        mag = np.abs(serial[:, col]).max()
+        envelope = np.abs(serial[:, col] - omp[:, col]).max()
+        err = np.abs(ours[:, col] - serial[:, col]).max()
+        assert err <= 3.0 * envelope + 1e-9 * mag, (gold["columns"][col], err, envelope)
+
+
+GPU_BINDING_LIB = os.path.join(ROOT, "oracle", "_ref", "libmdpm_gpu_binding.so")
+GPU_UNIT_TEST = os.path.join(ROOT, "oracle", "_ref", "gpu_tangential_spring_unit_test")
+
+
+def gpu_binding_available() -> bool:
+    return os.path.exists(GPU_BINDING_LIB) and os.path.exists(GPU_UNIT_TEST)
+
+
+def _gpu_binding():
+    lib = C.CDLL(GPU_BINDING_LIB)
+    common = [C.POINTER(_abi.Config), C.POINTER(_abi.InstanceDesc), C.POINTER(_abi.SpeciesPair), _pd,
+              C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA), C.c_int]
+    lib.mdpm_gpu_solve_ene.restype = C.c_int
+    lib.mdpm_gpu_solve_ene.argtypes = common + [C.c_int, C.c_int, C.c_int, C.c_char_p]
+    lib.mdpm_gpu_solve_state.restype = C.c_int
+    lib.mdpm_gpu_solve_state.argtypes = common + [C.c_int, C.c_int, C.POINTER(_abi.ParticlesSoA)]
+    return lib
+
+
+def gpu_binding_ene(sc, nsteps: int, save_count: int, prefix: str, device: int = 0, sync_interval: int = 1):
+    """DPMBase::solve() of the checker's Mercury3D driver on the engine's
+    drop-in base class (GpuMercury3D), with the reference's .ene writer."""
+    inp = _Inputs(sc)
+    with quiet_stdout():
+        rc = _gpu_binding().mdpm_gpu_solve_ene(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density),
+                                               inp.walls, inp.nwalls, C.byref(inp.soa), nsteps, save_count, device,
+                                               sync_interval, prefix.encode())
+    assert rc == 0
+    return parse_ene(open(prefix + ".ene").read())
+
+
+def gpu_binding_state(sc, nsteps: int, device: int = 0, sync_interval: int = 1) -> dict:
+    """The host's particle state after DPMBase::solve() on GpuMercury3D."""
+    inp = _Inputs(sc)
+    n = sc.n
+    o = dict(position=np.zeros((n, 3)), velocity=np.zeros((n, 3)), angular_velocity=np.zeros((n, 3)))
+    soa = _abi.ParticlesSoA(n, _dp(o["position"]), _dp(o["velocity"]), _dp(o["angular_velocity"]), None, None,
+                            None, None, None, None, None)
+    with quiet_stdout():
+        rc = _gpu_binding().mdpm_gpu_solve_state(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density),
+                                                 inp.walls, inp.nwalls, C.byref(inp.soa), nsteps, device,
+                                                 sync_interval, C.byref(soa))
+    assert rc == 0
+    return o
+
+
+def fpdiff(text_a: str, text_b: str, relative_error: float = 0.1, small: float = 1e-14,
+           skip_first_line: bool = False, fields_of_b: bool = False) -> list:
+    """The self-test comparison rule of the reference's Configuration/fpdiff.py,
+    restated: the files must have the same lines and fields; identical fields
+    pass; otherwise both must be numbers, and pass if both magnitudes are at
+    most `small` or their difference is at most `relative_error` PERCENT of the
+    larger magnitude (.restart files: the first line, name and revision, is
+    not compared). fields_of_b: a line of text_a may carry more fields than
+    the line of text_b, and only text_b's are compared. Returns the mismatches
+    (line, field, a, b); empty = pass."""
+    import re
+    number = re.compile(r"(^[+-]?[0-9]*[.]?[0-9]+$)|(^[+-]?[0-9]+[.]?[0-9]*$)|(^[+-]?[0-9]?[.]?[0-9]+[EeDd][+-][0-9]+$)")
+    la, lb = text_a.splitlines(), text_b.splitlines()
+    if skip_first_line:
+        la, lb = la[1:], lb[1:]
+    bad = []
+    if len(la) != len(lb):
+        return [("lines", len(la), len(lb), None)]
+    for i, (a, b) in enumerate(zip(la, lb)):
+        fa, fb = a.split(), b.split()
+        if fields_of_b and len(fa) > len(fb):
+            fa = fa[:len(fb)]
+        if len(fa) != len(fb):
+            bad.append((i, "fields", len(fa), len(fb)))
+            continue
+        for j, (x, y) in enumerate(zip(fa, fb)):
+            if x == y:
+                continue
+            if not (number.match(x) and number.match(y)):
+                bad.append((i, j, x, y))
+                continue
+            u, v = float(x.lower().replace("d", "e")), float(y.lower().replace("d", "e"))
+            if abs(u) <= small and abs(v) <= small:
+                continue
+            if 100.0 * abs(u - v) / max(abs(u), abs(v)) > relative_error:
+                bad.append((i, j, x, y))
+    return bad
+
+
+SELFTEST_GOLD = os.path.join(ROOT, "tests", "golden", "selftest")
+# self test -> the output files its gold data covers
+SELFTESTS = {
+    "ForceSelfTest": [f"ForceSelfTest{k}.{ext}" for k in range(10) for ext in ("data", "ene")],
+    "FreeFallSelfTest": ["FreeFallSelfTest.ene", "FreeFallSelfTest.restart"],
+}
+
+
+def selftest_executable(name: str, variant: str) -> str:
+    """oracle/_ref/selftest_<name>_<variant>: variant "reference" is the
+    reference's self-test source as it is, "gpu" the same source on the
+    engine's drop-in base class."""
+    return os.path.join(ROOT, "oracle", "_ref", f"selftest_{name}_{variant}")
+
+
+def run_selftest(name: str, variant: str, workdir: str, timeout: float = 1800) -> dict:
+    """Runs a self-test executable in workdir; returns its output files'
+    texts (the ones the gold data covers) and its exit status."""
+    r = subprocess.run([selftest_executable(name, variant)], cwd=workdir, capture_output=True, text=True,
+                       timeout=timeout)
+    files = {}
+    for f in SELFTESTS[name]:
+        p = os.path.join(workdir, f)
+        files[f] = open(p).read() if os.path.exists(p) else None
+    return dict(returncode=r.returncode, log=r.stdout[-3000:] + r.stderr[-3000:], files=files)
+
+
+def selftest_gold(filename: str) -> str:
+    import gzip
+    with gzip.open(os.path.join(SELFTEST_GOLD, filename + ".gz"), "rt") as f:
+        return f.read()

@@ -27,7 +27,7 @@ import numpy as np
 import pytest
 
 import harness as H
-from mercurydpm_fork_b200 import output, scenarios
+from mercurydpm_fork_b200 import scenarios
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not H.reference_available("serial"), reason="reference build absent")]
@@ -97,24 +97,6 @@ def test_chute_200k_ten_steps(gpu, chute):
     assert H.rel_err(g["contacts"]["springs"], r["contacts"]["springs"]) < 1e-9
 
 
-def _engine_ene(sc, steps: int, save: int) -> np.ndarray:
-    """The .ene lines of the engine's run (output.ene_line from dem_reduce,
-    10 significant digits like the reference's file), parsed back."""
-    e = sc.engine()
-    try:
-        text = output.ene_header()
-        e.step(0)
-        for k in range(steps // save + 1):
-            if k:
-                e.step(save)
-            g = e.reduce()
-            text += output.ene_line(output.time_after(k * save, sc.time_step), sc.instance.gravity, g,
-                                    g["n_contacts"] + g["n_wall_contacts"])
-    finally:
-        e.close()
-    return H.parse_ene(text)
-
-
 def test_settling_box_balances(gpu):
     """The 5,000-sphere settling box (20 x 20 x 40 d, six walls, linear +
     sliding friction, dt = tc/50) over its full 20,000 steps: the engine's
@@ -132,21 +114,5 @@ def test_settling_box_balances(gpu):
       the envelope the reference's own rounding produces once the settling
       packing turns chaotic."""
     gold = json.load(open(os.path.join(GOLDEN, "settling_box_ene.json")))
-    serial, omp = np.array(gold["serial"]), np.array(gold["omp8"])
     sc = scenarios.settling_box()
-    ours = _engine_ene(sc, gold["steps"], gold["save_count"])
-    assert ours.shape == serial.shape
-    np.testing.assert_array_equal(ours[:, 0], serial[:, 0])
-    agree = np.all(serial == omp, axis=1)
-    n_same = int(np.argmin(agree)) if not agree.all() else len(agree)
-    assert n_same >= 10
-    for col in range(1, 8):
-        scale = np.abs(serial[:n_same, col]).max()
-        err = np.abs(ours[:n_same, col] - serial[:n_same, col]).max()
-        assert err <= 1e-8 * max(scale, 1e-300), (gold["columns"][col], err, scale)
-    np.testing.assert_array_equal(ours[:n_same, 8], serial[:n_same, 8])
-    for col in range(1, 9):
-        mag = np.abs(serial[:, col]).max()
-        envelope = np.abs(serial[:, col] - omp[:, col]).max()
-        err = np.abs(ours[:, col] - serial[:, col]).max()
-        assert err <= 3.0 * envelope + 1e-9 * mag, (gold["columns"][col], err, envelope)
+    H.check_ene_against_golden(H.engine_ene(sc, gold["steps"], gold["save_count"]), gold)

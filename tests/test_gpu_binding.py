@@ -1,0 +1,62 @@
+"""The reference-side binding: MercuryDPM drivers whose base class is the
+engine's drop-in GpuMercury3D / GpuDPMBase (mercurydpm_fork_b200/mercury/
+GpuTimeStep.h), compiled against the reference's headers and Kernel by
+oracle/ref.mk (target gpu) and run through the reference's own
+DPMBase::solve() -> computeOneTimeStep loop.
+
+* The reference's unit test Drivers/UnitTests/TangentialSpringUnitTest.cpp,
+  compiled from its own source with only its base class swapped (DPMBase ->
+  GpuDPMBase), passes its own golden assertions (position, velocity and
+  angular velocity to 1e-7) with every time step on the GPU.
+* The checker's Mercury3D driver on GpuMercury3D runs the 5,000-sphere
+  settling box through solve() and writes its .ene file with the reference's
+  File machinery; the lines equal those of the engine driven directly through
+  the C ABI, and lie within the reference's own chaos envelope
+  (tests/golden/settling_box_ene.json).
+* The host state the driver holds after solve() equals the engine's state
+  after the same number of steps, bit for bit, whatever the sync interval.
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import cases
+import harness as H
+from mercurydpm_fork_b200 import scenarios
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not H.gpu_binding_available(), reason="binding drivers not built (make -f oracle/ref.mk gpu)")]
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_reference_unit_test_on_gpu_base_class(gpu, tmp_path):
+    r = subprocess.run([H.GPU_UNIT_TEST], cwd=tmp_path, capture_output=True, text=True, timeout=900)
+    out = r.stdout + r.stderr
+    assert r.returncode == 0, out[-3000:]
+    assert "error has occured" not in out, out[-3000:]
+
+
+def test_settling_box_through_solve(gpu, tmp_path):
+    gold = json.load(open(os.path.join(GOLDEN, "settling_box_ene.json")))
+    sc = scenarios.settling_box()
+    rows = H.gpu_binding_ene(sc, gold["steps"], gold["save_count"], str(tmp_path / "box"),
+                             sync_interval=gold["save_count"])
+    direct = H.engine_ene(sc, gold["steps"], gold["save_count"])
+    np.testing.assert_array_equal(rows, direct)
+    H.check_ene_against_golden(rows, gold)
+
+
+@pytest.mark.parametrize("sync_interval", [1, 7])
+def test_host_state_after_solve_equals_engine(gpu, sync_interval):
+    """Periodic bidisperse chute (two HGrid levels, rough base): the state
+    GpuMercury3D leaves in the ParticleHandler after solve() is the engine's."""
+    sc = cases.small_chute()
+    steps = 40
+    host = H.gpu_binding_state(sc, steps, sync_interval=sync_interval)
+    g = H.run_gpu(sc, steps)
+    for k in ("position", "velocity", "angular_velocity"):
+        np.testing.assert_array_equal(host[k], g[k], err_msg=k)

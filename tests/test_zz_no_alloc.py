@@ -58,8 +58,9 @@ class _DeviceMemory:
     CUDA runtime (cuda-python)."""
 
     def __init__(self, device: int = 0):
-        from cuda.bindings import runtime as rt
+        from cuda.bindings import driver, runtime as rt
         self.rt = rt
+        self.u64 = driver.cuuint64_t
         err, = rt.cudaSetDevice(device)
         assert err == rt.cudaError_t.cudaSuccess
         err, self.pool = rt.cudaDeviceGetDefaultMemPool(device)
@@ -73,7 +74,7 @@ class _DeviceMemory:
     def reset_high_water(self):
         rt = self.rt
         err, = rt.cudaMemPoolSetAttribute(self.pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh,
-                                          rt.cuuint64_t(0))
+                                          self.u64(0))
         assert err == rt.cudaError_t.cudaSuccess
 
     def used(self) -> int:

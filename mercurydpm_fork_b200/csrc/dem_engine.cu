@@ -61,7 +61,9 @@ struct Handle {
     long long last_launches = 0;
     long long last_rebuilds = 0;
     long long launches_per_step = 0;
-    cudaGraphExec_t graph1 = nullptr, graphK = nullptr;
+    // time steps that are not the last of a dem_step call (1 and GRAPH_STEPS
+    // of them), and the last step, which also writes the contact records
+    cudaGraphExec_t graph1 = nullptr, graphK = nullptr, graphF = nullptr;
     int ncomp = 3;
     int law_variant = 0;
     int sm_count = 148;
@@ -100,7 +102,8 @@ void free_graphs(Handle* h)
 {
     if (h->graph1) cudaGraphExecDestroy(h->graph1);
     if (h->graphK) cudaGraphExecDestroy(h->graphK);
-    h->graph1 = h->graphK = nullptr;
+    if (h->graphF) cudaGraphExecDestroy(h->graphF);
+    h->graph1 = h->graphK = h->graphF = nullptr;
 }
 
 void free_particle_arrays(Handle* h)
@@ -141,8 +144,9 @@ constexpr int FORCE_LAUNCHES = 3;
 // specialised one when every species pair shares the same law pair.
 enum LawVariant { LAW_GENERIC = 0, LAW_LINEAR_SLIDING, LAW_LINEAR_ROLLING, LAW_HERTZ_MINDLIN, LAW_HERTZ_MINDLIN_RT };
 
-// one force evaluation: detect -> contacts -> sum (+ integration for MODE 1)
-template <int MODE, int NLAW, int FLAW, int NCOMP>
+// one force evaluation: detect -> contacts -> sum (+ integration for MODE 1);
+// RECORD: the evaluation may be the last of the call (contact records)
+template <int MODE, int NLAW, int FLAW, int NCOMP, bool RECORD>
 void launch_pipeline(Handle* h, cudaStream_t s)
 {
     DevPtrs& d = h->d;
@@ -150,7 +154,7 @@ void launch_pipeline(Handle* h, cudaStream_t s)
     // one resident wave (4 blocks of 128 per SM at 128 registers), grid-stride over the items
     const unsigned gc = (unsigned)std::max(1, std::min((d.item_cap + CONTACT_BLOCK - 1) / CONTACT_BLOCK,
                                                        h->sm_count * 4));
-    k_contacts<MODE, NLAW, FLAW, NCOMP><<<gc, CONTACT_BLOCK, 0, s>>>(d);
+    k_contacts<MODE, NLAW, FLAW, NCOMP, RECORD><<<gc, CONTACT_BLOCK, 0, s>>>(d);
     if (d.has_tri) { // at most one triangle item per particle
         const unsigned gt = (unsigned)std::max(1, std::min((d.n + TRI_BLOCK - 1) / TRI_BLOCK, h->sm_count * 4));
         k_tri<MODE, NLAW, FLAW, NCOMP><<<gt, TRI_BLOCK, 0, s>>>(d);
@@ -159,42 +163,47 @@ void launch_pipeline(Handle* h, cudaStream_t s)
 }
 int force_launches(const Handle* h) { return FORCE_LAUNCHES + (h->d.has_tri ? 1 : 0); }
 
-template <int MODE>
+template <int MODE, bool RECORD>
 void launch_force_mode(Handle* h, cudaStream_t s)
 {
     DevPtrs& d = h->d;
     switch (h->law_variant) {
     case LAW_LINEAR_SLIDING:
-        launch_pipeline<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_SLIDING, 3>(h, s);
+        launch_pipeline<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_SLIDING, 3, RECORD>(h, s);
         break;
     case LAW_LINEAR_ROLLING:
-        launch_pipeline<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_ROLLING_TORSION, 9>(h, s);
+        launch_pipeline<MODE, DEM_NORMAL_LINEAR_VISCOELASTIC, DEM_FRICTION_ROLLING_TORSION, 9, RECORD>(h, s);
         break;
     case LAW_HERTZ_MINDLIN:
-        launch_pipeline<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN, 3>(h, s);
+        launch_pipeline<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN, 3, RECORD>(h, s);
         break;
     case LAW_HERTZ_MINDLIN_RT:
-        launch_pipeline<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN_ROLLING_TORSION, 9>(h, s);
+        launch_pipeline<MODE, DEM_NORMAL_HERTZIAN_VISCOELASTIC, DEM_FRICTION_MINDLIN_ROLLING_TORSION, 9, RECORD>(h, s);
         break;
     default:
         if (d.ncomp == 3)
-            launch_pipeline<MODE, -1, -1, 3>(h, s);
+            launch_pipeline<MODE, -1, -1, 3, RECORD>(h, s);
         else
-            launch_pipeline<MODE, -1, -1, 9>(h, s);
+            launch_pipeline<MODE, -1, -1, 9, RECORD>(h, s);
     }
 }
 
-void launch_force(Handle* h, cudaStream_t s, int mode)
+// mode 0: the initial evaluation (always records); mode 1: a time step,
+// `last` when it is the last step of the dem_step call
+void launch_force(Handle* h, cudaStream_t s, int mode, bool last = true)
 {
     if (mode == 0)
-        launch_force_mode<0>(h, s);
+        launch_force_mode<0, true>(h, s);
+    else if (last)
+        launch_force_mode<1, true>(h, s);
     else
-        launch_force_mode<1>(h, s);
+        launch_force_mode<1, false>(h, s);
 }
 
 // Captures `steps` time steps: control -> rebuild (returns at once unless
-// the skin test fired) -> force.
-int build_graph(Handle* h, int steps, cudaGraphExec_t* out)
+// the skin test fired) -> force; `last`: the final step is the last of the
+// dem_step call (its force evaluation writes the contact records).
+int build_graph(Handle* h, int steps, bool last, cudaGraphExec_t* out)
 {
     cudaStream_t s = h->stream;
     CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -207,7 +216,7 @@ int build_graph(Handle* h, int steps, cudaGraphExec_t* out)
             if (g) cudaGraphDestroy(g);
             return fail(h, DEM_ERR_CUDA, std::string("rebuild launch in capture: ") + cudaGetErrorString(e));
         }
-        launch_force(h, s, 1);
+        launch_force(h, s, 1, last && k == steps - 1);
     }
     cudaGraph_t graph = nullptr;
     CU(cudaStreamEndCapture(s, &graph));
@@ -685,6 +694,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         for (int b = 0; b < 2; ++b) {
             d.pr[b] = kept.pr[b]; d.vm[b] = kept.vm[b]; d.wi[b] = kept.wi[b]; d.qo[b] = kept.qo[b];
             d.info[b] = kept.info[b]; d.caller[b] = kept.caller[b]; d.nbr[b] = kept.nbr[b]; d.cnt[b] = kept.cnt[b];
+            d.own[b] = kept.own[b];
             d.hist[b] = kept.hist[b]; d.act[b] = kept.act[b]; d.whist[b] = kept.whist[b]; d.wact[b] = kept.wact[b];
         }
         d.force = kept.force; d.torque = kept.torque; d.key = kept.key; d.perm = kept.perm; d.newidx = kept.newidx;
@@ -714,6 +724,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         if ((rc = dalloc(h, &d.caller[b], NC))) return rc;
         if ((rc = dalloc(h, &d.nbr[b], (size_t)cap * NC))) return rc;
         if ((rc = dalloc(h, &d.cnt[b], NC))) return rc;
+        if ((rc = dalloc(h, &d.own[b], (size_t)d.nwords * NC))) return rc;
         if ((rc = dalloc(h, &d.hist[b], (size_t)hist_stride(d.ncomp) * cap * NC))) return rc;
         if ((rc = dalloc(h, &d.act[b], (size_t)d.nwords * NC))) return rc;
         if ((rc = dalloc(h, &d.whist[b], (size_t)hist_stride(d.ncomp) * wmax * NC))) return rc;
@@ -945,21 +956,23 @@ int dem_step(dem_handle* hh, int nsteps)
             launches += 1;
             if (h->cfg.use_graphs) {
                 if (!h->graph1) {
-                    if ((rc = build_graph(h, 1, &h->graph1))) return rc;
-                    if ((rc = build_graph(h, GRAPH_STEPS, &h->graphK))) return rc;
+                    if ((rc = build_graph(h, 1, false, &h->graph1))) return rc;
+                    if ((rc = build_graph(h, GRAPH_STEPS, false, &h->graphK))) return rc;
+                    if ((rc = build_graph(h, 1, true, &h->graphF))) return rc;
                 }
-                int left = nsteps;
+                int left = nsteps - 1; // the last step: graphF
                 while (left >= GRAPH_STEPS) {
                     CU(cudaGraphLaunch(h->graphK, h->stream));
                     left -= GRAPH_STEPS;
                 }
                 while (left-- > 0) CU(cudaGraphLaunch(h->graph1, h->stream));
+                CU(cudaGraphLaunch(h->graphF, h->stream));
                 launches += (1ll + REBUILD_LAUNCHES + force_launches(h)) * nsteps;
             } else {
                 for (int k = 0; k < nsteps; ++k) {
                     k_control<<<1, CONTROL_THREADS, 0, h->stream>>>(h->d_ctl, d.walls, h->d_wgeom, d.n_walls, d.dt);
                     CU(launch_rebuild(h, h->stream));
-                    launch_force(h, h->stream, 1);
+                    launch_force(h, h->stream, 1, k == nsteps - 1);
                 }
                 CU(cudaGetLastError());
                 launches += (1ll + force_launches(h) + REBUILD_LAUNCHES) * nsteps;
@@ -1380,9 +1393,9 @@ int dem_time_force_kernel(dem_handle* hh, int reps, double* ms_per_launch)
     probe.pending_flip = 0;
     probe.record = 0;
     CU(cudaMemcpyAsync(h->d_ctl, &probe, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
-    launch_force(h, h->stream, 1); // warm-up
+    launch_force(h, h->stream, 1, false); // warm-up
     CU(cudaEventRecord(h->ev0, h->stream));
-    for (int r = 0; r < reps; ++r) launch_force(h, h->stream, 1);
+    for (int r = 0; r < reps; ++r) launch_force(h, h->stream, 1, false);
     CU(cudaEventRecord(h->ev1, h->stream));
     CU(cudaGetLastError());
     CU(cudaEventSynchronize(h->ev1));

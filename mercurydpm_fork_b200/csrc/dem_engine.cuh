@@ -131,6 +131,10 @@ struct DevPtrs {
     // neighbour lists, two buffers
     int *nbr[2];
     int *cnt[2];
+    // ownership bits of list buffer l, laid out like act: bit k%32 of word
+    // own[l][(k/32)*ncap + i] is set when particle i has the lower id of its
+    // entry k's pair (it is P unless the pair meets across a periodic boundary)
+    unsigned int *own[2];
     double *hist[2];
     unsigned int *act[2];
     double *whist[2];

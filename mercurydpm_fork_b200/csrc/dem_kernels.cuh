@@ -306,6 +306,7 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
     constexpr float U20 = 9.5367431640625e-07f; // 2^-20
     int count = 0;
     bool overflow = false;
+    unsigned int ownw = 0u; // ownership bits of the list word being filled
     for (int lvl = 0; lvl < I.n_levels; ++lvl) {
         const double reach = ps.w + I.level_rmax[lvl] + extra;
         int lox, hix, loy, hiy, loz, hiz;
@@ -376,6 +377,11 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
                             if (count < d.cap) {
                                 d.nbr[ln][nbr_at(d.ncap, s, count)] = t;
                                 d.rows[(size_t)s * d.cap + count] = t;
+                                if (is.x < d.info[nb][t].x) ownw |= 1u << (count & 31);
+                                if ((count & 31) == 31) {
+                                    d.own[ln][(size_t)(count >> 5) * d.ncap + s] = ownw;
+                                    ownw = 0u;
+                                }
                             } else {
                                 overflow = true;
                             }
@@ -390,6 +396,7 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
         atomicOr(&d.ctl->status, 1u << DEM_ERR_CAPACITY);
         count = d.cap;
     }
+    if (count & 31) d.own[ln][(size_t)(count >> 5) * d.ncap + s] = ownw; // the last, partial word
     d.cnt[ln][s] = count;
 
     // carry contact history from the old list (old order) to the new one, up

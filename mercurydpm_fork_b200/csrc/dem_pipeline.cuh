@@ -184,18 +184,44 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
         const V3 xs = xyz(ps);
         count = min(d.cnt[l][s], d.cap);
         const int ns = I.n_species;
-        constexpr int B = 2; // entries whose gathers are in flight together (divides 32; 2 keeps 80 registers)
+        constexpr int B = 2; // entries whose gathers are in flight together (2 keeps 80 registers)
         const int2* info2 = reinterpret_cast<const int2*>(d.info[c]); // (id, species) of each info record
+        // Without periodic boundaries a pair's owner (the lower id) is fixed
+        // for the life of a list, and the rebuild stored it (own bits): the
+        // partner-owned entries are marked without gathering the partner, and
+        // the owned ones are visited in list order, B at a time. With periodic
+        // boundaries every entry is visited (its image decides the owner).
+        const bool owner_known = I.per_mask == 0u;
         for (int w = 0; w < d.nwords; ++w) {
             unsigned int hitw = 0u, neww = 0u;
-            const unsigned int aw = first ? d.act[c][(size_t)w * d.ncap + s] : 0u;
-            const int kend = min(count, 32 * w + 32);
-            for (int k0 = 32 * w; k0 < kend; k0 += B) {
-                int tb[B];
+            const int kbeg = 32 * w, kend = min(count, kbeg + 32);
+            const unsigned int valid = kend <= kbeg ? 0u : (kend - kbeg == 32 ? 0xffffffffu : (1u << (kend - kbeg)) - 1u);
+            unsigned int todo = valid;
+            if (owner_known && valid) {
+                const unsigned int ow = d.own[l][(size_t)w * d.ncap + s];
+                unsigned int other = valid & ~ow;
+                while (other) {
+                    const int k = kbeg + __ffs(other) - 1;
+                    other &= other - 1;
+                    d.slot[nbr_at(d.ncap, s, k)] = SLOT_IS_I;
+                }
+                todo = valid & ow;
+            }
+            const unsigned int aw = (first && valid) ? d.act[c][(size_t)w * d.ncap + s] : 0u;
+            while (todo) {
+                int kb[B], tb[B];
                 double4 ptb[B];
                 int2 itb[B];
 #pragma unroll
-                for (int j = 0; j < B; ++j) tb[j] = (k0 + j < kend) ? d.nbr[l][nbr_at(d.ncap, s, k0 + j)] : -1;
+                for (int j = 0; j < B; ++j) {
+                    kb[j] = -1;
+                    if (todo) {
+                        kb[j] = kbeg + __ffs(todo) - 1;
+                        todo &= todo - 1;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < B; ++j) tb[j] = kb[j] >= 0 ? d.nbr[l][nbr_at(d.ncap, s, kb[j])] : -1;
 #pragma unroll
                 for (int j = 0; j < B; ++j)
                     if (tb[j] >= 0) {
@@ -204,8 +230,8 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
                     }
 #pragma unroll
                 for (int j = 0; j < B; ++j) {
-                    const int k = k0 + j;
-                    if (k >= kend) break;
+                    const int k = kb[j];
+                    if (k < 0) break;
                     const size_t e = nbr_at(d.ncap, s, k);
                     const double4 pt = ptb[j];
                     const int2 it = itb[j];
@@ -335,21 +361,28 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
     }
 }
 
-template <int MODE, int NLAW, int FLAW, int NCOMP>
+// RECORD: this launch may be the last force evaluation of a dem_step call,
+// which writes the contact records; the steps before it are launched with
+// RECORD = false, a variant without the record path (fewer registers).
+template <int MODE, int NLAW, int FLAW, int NCOMP, bool RECORD>
 __global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
 {
     Control* ctl = d.ctl;
     const int c = ctl->cur, nb = c ^ 1;
     const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
-    const bool record = final_step && ctl->record;
+    const bool record = RECORD && final_step && ctl->record;
     const bool first = (MODE == 1) && ctl->first_step;
     const int n_items = min((int)ctl->n_items, d.item_cap);
     const double dt = d.dt;
     __shared__ TableStage tables;
     stage_tables(d, tables);
     const dem_species_pair* species = staged_species(d, tables);
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += gridDim.x * blockDim.x) {
-        const int4 item = d.items[q];
+    const int stride = gridDim.x * blockDim.x;
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    int4 next = q < n_items ? d.items[q] : make_int4(0, 0, 0, 0);
+    for (; q < n_items; q += stride) {
+        const int4 item = next; // the next item is read while this one is evaluated
+        if (q + stride < n_items) next = d.items[q + stride];
         const int s = item.x, kq = item.y;
         if (d.has_tri && kq == ITEM_TRI) continue; // k_tri
         const double4 ps = d.pr[c][s];

@@ -18,12 +18,14 @@
 //                             every later call is one whole time step on the
 //                             device (dem_step(h, 1): half-kick, drift, walls,
 //                             forces, second half-kick)
-//   integrateBefore/AfterForceComputation, hGridActionsBeforeTimeStep /
-//   BeforeIntegration / AfterIntegration, checkInteractionWithBoundaries
+//   integrateBefore/AfterForceComputation, hGridActionsBeforeIntegration /
+//   AfterIntegration, checkInteractionWithBoundaries
 //                             nothing: the engine integrates, keeps its own
 //                             neighbour grid and wraps periodic positions
 //   hGridActionsBeforeTimeLoop  ends the engine of a previous solve(), then
 //                             the base's own set-up
+//   hGridActionsBeforeTimeStep  the base's own grid build in initialiseSolve
+//                             (restart files describe it), nothing afterwards
 //   writeEneTimeStep          the reference's .ene line (DPMBase.cc:2100-2123)
 //                             from the engine's balances (dem_reduce)
 //
@@ -148,7 +150,12 @@ protected:
         h_ = nullptr;
         Base::hGridActionsBeforeTimeLoop();
     }
-    void hGridActionsBeforeTimeStep() override {}
+    /// The base's grid is built once, by the call of initialiseSolve (Mercury3D /
+    /// Mercury2D size their cells there); the time steps use the engine's grid.
+    void hGridActionsBeforeTimeStep() override
+    {
+        if (!h_) Base::hGridActionsBeforeTimeStep();
+    }
     void hGridActionsBeforeIntegration() override {}
     void hGridActionsAfterIntegration() override {}
     void checkInteractionWithBoundaries() override {}

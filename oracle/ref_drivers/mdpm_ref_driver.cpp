@@ -191,6 +191,23 @@ int mdpm_ref_write_outputs(const dem_config* cfg, const dem_instance_desc* inst,
     return 0;
 }
 
+// The reference's restart file (DPMBase::write, DPMBase.cc:3550) after
+// `nsteps` time steps, written to `path` with the precision of its file
+// streams (10).
+int mdpm_ref_write_restart(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
+                           const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in,
+                           int nsteps, const char* path)
+{
+    RefDriver d;
+    setup(d, cfg, inst, species, density, walls, nwalls, in, 1);
+    d.initialiseSolve();
+    for (int k = 0; k < nsteps; ++k) d.computeOneTimeStep();
+    std::ofstream os(path);
+    os.precision(10);
+    d.write(os, true);
+    return 0;
+}
+
 // CPU baseline: builds the same simulation, runs `warmup` steps, then times
 // `nsteps` calls of computeOneTimeStep with std::chrono (set-up and output
 // excluded). `threads` is the OpenMP thread count (ignored by the serial build).

@@ -184,6 +184,9 @@ def run_ours(args):
     eng = DemEngine(sc.time_step, [sc.instance], sc.species, sc.walls, rotation=True, device=local)
     eng.upload(sc.position, sc.velocity, sc.radius, sc.inv_mass, sc.inv_inertia, sc.species_index, sc.ids)
     eng.step(0)  # the initial force evaluation (DPMBase::initialiseSolve)
+    # launch shapes of the force kernels measured on this state (dem_autotune:
+    # spare buffers only, the simulation state does not change)
+    tuning = eng.autotune(reps=10)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
 
     def barrier():
@@ -267,7 +270,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice bed in a rotating drum)",
         "config": dict(workload_config(args.steps, args.warmup), parallelism=f"replicas{world}", n_total=sc.n,
-                       n_moving=n_moving, contacts_window_start=cnt_start, contacts_window_end=cnt_end),
+                       n_moving=n_moving, contacts_window_start=cnt_start, contacts_window_end=cnt_end,
+                       tuning=tuning),
         "e2e": {"value": e2e_value, "unit": "particle-timesteps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
                 "step": f"upload + initial evaluation + {window} time steps + download, {e2e_runs} runs"},

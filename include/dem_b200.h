@@ -248,6 +248,19 @@ typedef struct dem_cg_grid {
     double  cutoff_factor;         /* cutoff = cutoff_factor * width (reference: 3)  */
 } dem_cg_grid;
 
+/* Launch shapes of the time step's force kernels (dem_autotune). They change
+ * how the work is spread over the GPU, never the arithmetic: results are
+ * bit-identical under every shape. */
+typedef struct dem_tuning {
+    int32_t detect_block;            /* threads per block of the contact predicate: 64, 128 or 256 */
+    int32_t contacts_blocks_per_sm;  /* resident blocks (of 128) per SM of the contact-law kernel,
+                                        3..6, with the register budget they leave (168 .. 85) */
+    int32_t sum_block;               /* threads per block of the sum/integration kernel: 64, 128, 256 */
+    int32_t reserved;
+    double  ms_before;               /* dem_autotune: one force evaluation with the shapes it found  */
+    double  ms_after;                /* and with the ones it chose (never slower)                    */
+} dem_tuning;
+
 typedef struct dem_handle dem_handle;
 
 /* DPMBase construction + setTimeStep/setGravity/setDomain. */
@@ -353,6 +366,18 @@ int  dem_time_force_kernel(dem_handle *h, int reps, double *ms_per_launch);
  * reports DEM_ERR_TIMEOUT; *status receives the status word the kernel wrote
  * (1 << DEM_ERR_TIMEOUT expected). The handle stays usable afterwards. */
 int  dem_selftest_wait_expiry(dem_handle *h, int64_t polls, uint32_t *status);
+/* Autotuner (the reference's HGridOptimiser, Kernel/HGridOptimiser.cc, picks
+ * cell sizes offline from a cost model; the engine's cells follow the
+ * reference's HGrid levels, and what is tuned instead are its kernels' launch
+ * shapes, measured on the live state): times each force kernel's variants
+ * (`reps` force evaluations each, best of three rounds, written to spare
+ * buffers so the simulation state is unchanged), one kernel at a time, keeps
+ * the fastest shape of each and recaptures the step graphs. Needs a force
+ * evaluation (after the first dem_step). */
+int  dem_autotune(dem_handle *h, int reps, dem_tuning *out);
+/* Applies shapes found earlier (e.g. cached per workload class). */
+int  dem_set_tuning(dem_handle *h, const dem_tuning *t);
+int  dem_get_tuning(dem_handle *h, dem_tuning *out);
 const char *dem_last_error(dem_handle *h);
 void dem_destroy(dem_handle *h);
 

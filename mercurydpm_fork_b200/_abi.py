@@ -121,6 +121,13 @@ class CGGrid(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("detect_block", _i32), ("contacts_blocks_per_sm", _i32), ("sum_block", _i32), ("reserved", _i32),
+        ("ms_before", _d), ("ms_after", _d),
+    ]
+
+
 _SIGNATURES = {
     "dem_create": (C.c_int, [C.POINTER(Config), C.POINTER(InstanceDesc), C.POINTER(C.c_void_p)]),
     "dem_set_species": (C.c_int, [C.c_void_p, C.POINTER(SpeciesPair), C.c_int]),
@@ -146,6 +153,9 @@ _SIGNATURES = {
     "dem_time_force_kernel": (C.c_int, [C.c_void_p, C.c_int, _pd]),
     "dem_selftest_wait_expiry": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_uint32)]),
     "dem_download_contact_geometry": (C.c_int, [C.c_void_p, _pd, _pd, _pd, C.c_int64, C.POINTER(C.c_int64)]),
+    "dem_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Tuning)]),
+    "dem_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    "dem_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "dem_last_error": (C.c_char_p, [C.c_void_p]),
     "dem_destroy": (None, [C.c_void_p]),
 }

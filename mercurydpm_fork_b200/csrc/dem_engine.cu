@@ -69,6 +69,11 @@ struct Handle {
     int sm_count = 148;
     int rb_grid = 148;                 // blocks of the cooperative rebuild (all resident)
     std::vector<int> level_buf;        // HGrid level of every particle (one-instance uploads)
+    // launch shapes of the force kernels (dem_autotune / dem_set_tuning)
+    dem_tuning tune{DETECT_BLOCK, 4, SUM_BLOCK, 0, 0.0, 0.0};
+    // optional events between the force kernels, for the autotuner's
+    // per-kernel times (null outside a measurement)
+    cudaEvent_t* kev = nullptr;
 };
 
 int fail(Handle* h, int code, const std::string& msg)
@@ -150,16 +155,39 @@ template <int MODE, int NLAW, int FLAW, int NCOMP, bool RECORD>
 void launch_pipeline(Handle* h, cudaStream_t s)
 {
     DevPtrs& d = h->d;
-    k_detect<MODE, NCOMP><<<grid_for(d.n, DETECT_BLOCK), DETECT_BLOCK, 0, s>>>(d);
-    // one resident wave (4 blocks of 128 per SM at 128 registers), grid-stride over the items
+    if (h->kev) cudaEventRecord(h->kev[0], s);
+    switch (h->tune.detect_block) {
+    case 64: k_detect<MODE, NCOMP, 64><<<grid_for(d.n, 64), 64, 0, s>>>(d); break;
+    case 256: k_detect<MODE, NCOMP, 256><<<grid_for(d.n, 256), 256, 0, s>>>(d); break;
+    default: k_detect<MODE, NCOMP, DETECT_BLOCK><<<grid_for(d.n, DETECT_BLOCK), DETECT_BLOCK, 0, s>>>(d);
+    }
+    if (h->kev) cudaEventRecord(h->kev[1], s);
+    // one resident wave of tune.contacts_blocks_per_sm blocks of 128 per SM,
+    // grid-stride over the items; the time-step variant without records is
+    // compiled with that many blocks' register budget (3 to 6), the others
+    // with 4 (128 registers)
+    const int bpsm = (MODE == 1 && !RECORD) ? h->tune.contacts_blocks_per_sm : 4;
     const unsigned gc = (unsigned)std::max(1, std::min((d.item_cap + CONTACT_BLOCK - 1) / CONTACT_BLOCK,
-                                                       h->sm_count * 4));
-    k_contacts<MODE, NLAW, FLAW, NCOMP, RECORD><<<gc, CONTACT_BLOCK, 0, s>>>(d);
+                                                       h->sm_count * bpsm));
+    if (MODE == 1 && !RECORD && bpsm == 3)
+        k_contacts<MODE, NLAW, FLAW, NCOMP, RECORD, 3><<<gc, CONTACT_BLOCK, 0, s>>>(d);
+    else if (MODE == 1 && !RECORD && bpsm == 5)
+        k_contacts<MODE, NLAW, FLAW, NCOMP, RECORD, 5><<<gc, CONTACT_BLOCK, 0, s>>>(d);
+    else if (MODE == 1 && !RECORD && bpsm == 6)
+        k_contacts<MODE, NLAW, FLAW, NCOMP, RECORD, 6><<<gc, CONTACT_BLOCK, 0, s>>>(d);
+    else
+        k_contacts<MODE, NLAW, FLAW, NCOMP, RECORD, 4><<<gc, CONTACT_BLOCK, 0, s>>>(d);
     if (d.has_tri) { // at most one triangle item per particle
         const unsigned gt = (unsigned)std::max(1, std::min((d.n + TRI_BLOCK - 1) / TRI_BLOCK, h->sm_count * 4));
         k_tri<MODE, NLAW, FLAW, NCOMP><<<gt, TRI_BLOCK, 0, s>>>(d);
     }
-    k_sum<MODE><<<grid_for(d.n, SUM_BLOCK), SUM_BLOCK, 0, s>>>(d);
+    if (h->kev) cudaEventRecord(h->kev[2], s);
+    switch (h->tune.sum_block) {
+    case 64: k_sum<MODE, 64><<<grid_for(d.n, 64), 64, 0, s>>>(d); break;
+    case 256: k_sum<MODE, 256><<<grid_for(d.n, 256), 256, 0, s>>>(d); break;
+    default: k_sum<MODE, SUM_BLOCK><<<grid_for(d.n, SUM_BLOCK), SUM_BLOCK, 0, s>>>(d);
+    }
+    if (h->kev) cudaEventRecord(h->kev[3], s);
 }
 int force_launches(const Handle* h) { return FORCE_LAUNCHES + (h->d.has_tri ? 1 : 0); }
 
@@ -1404,6 +1432,144 @@ int dem_time_force_kernel(dem_handle* hh, int reps, double* ms_per_launch)
     *ms_per_launch = ms / reps;
     CU(cudaMemcpyAsync(h->d_ctl, &saved, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
     CU(cudaStreamSynchronize(h->stream));
+    return DEM_OK;
+}
+
+} // extern "C"
+
+namespace {
+// Mean device time of each force kernel (detect, contacts + triangle walls,
+// sum) over `reps` time-step force evaluations on the current state, written
+// to the spare buffers (the probe control of dem_time_force_kernel); the best
+// of three rounds.
+int time_force_parts(Handle* h, int reps, double ms[3])
+{
+    std::vector<cudaEvent_t> ev(4 * (size_t)reps);
+    for (auto& e : ev) CU(cudaEventCreate(&e));
+    double best[3] = {1e30, 1e30, 1e30};
+    int rc = DEM_OK;
+    launch_force(h, h->stream, 1, false); // warm-up of this shape
+    for (int round = 0; round < 3 && rc == DEM_OK; ++round) {
+        for (int r = 0; r < reps; ++r) {
+            h->kev = ev.data() + 4 * r;
+            launch_force(h, h->stream, 1, false);
+        }
+        h->kev = nullptr;
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+            rc = fail(h, DEM_ERR_CUDA, "dem_autotune: a measured launch failed");
+            break;
+        }
+        double sum[3] = {0, 0, 0};
+        for (int r = 0; r < reps; ++r)
+            for (int k = 0; k < 3; ++k) {
+                float t = 0.f;
+                cudaEventElapsedTime(&t, ev[4 * r + k], ev[4 * r + k + 1]);
+                sum[k] += t;
+            }
+        for (int k = 0; k < 3; ++k) best[k] = std::min(best[k], sum[k] / reps);
+    }
+    h->kev = nullptr;
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 3; ++k) ms[k] = best[k];
+    return rc;
+}
+
+bool valid_tuning(const dem_tuning& t)
+{
+    const bool blk = (t.detect_block == 64 || t.detect_block == 128 || t.detect_block == 256) &&
+                     (t.sum_block == 64 || t.sum_block == 128 || t.sum_block == 256);
+    return blk && t.contacts_blocks_per_sm >= 3 && t.contacts_blocks_per_sm <= 6;
+}
+} // namespace
+
+extern "C" {
+
+int dem_autotune(dem_handle* hh, int reps, dem_tuning* out)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || reps <= 0 || !out) return fail(h, DEM_ERR_BAD_INPUT, "dem_autotune: bad arguments");
+    if (!h->uploaded || h->initial_pending) return fail(h, DEM_ERR_STATE, "no force evaluation yet (call dem_step)");
+    if (h->d.n == 0) return fail(h, DEM_ERR_STATE, "no particles");
+    CU(cudaSetDevice(h->device));
+    Control saved;
+    int rc = read_control(h, &saved);
+    if (rc) return rc;
+    Control probe = saved;
+    probe.final_step = 0;
+    probe.first_step = 0;
+    probe.pending_flip = 0;
+    probe.record = 0;
+    CU(cudaMemcpyAsync(h->d_ctl, &probe, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+    const dem_tuning start = h->tune;
+    double ms[3];
+    double before = 0.0;
+    if ((rc = time_force_parts(h, reps, ms)) == DEM_OK) {
+        before = ms[0] + ms[1] + ms[2];
+        // one kernel at a time, the others kept: the three kernels share no
+        // launch parameter, and each one's time is measured on its own
+        const int blocks[3] = {64, 128, 256};
+        const int per_sm[4] = {3, 4, 5, 6};
+        double best = 1e30;
+        int pick = h->tune.detect_block;
+        for (int b : blocks) {
+            h->tune.detect_block = b;
+            if ((rc = time_force_parts(h, reps, ms))) break;
+            if (ms[0] < best) { best = ms[0]; pick = b; }
+        }
+        h->tune.detect_block = pick;
+        best = 1e30;
+        pick = h->tune.contacts_blocks_per_sm;
+        for (int b : per_sm) {
+            if (rc) break;
+            h->tune.contacts_blocks_per_sm = b;
+            if ((rc = time_force_parts(h, reps, ms))) break;
+            if (ms[1] < best) { best = ms[1]; pick = b; }
+        }
+        h->tune.contacts_blocks_per_sm = pick;
+        best = 1e30;
+        pick = h->tune.sum_block;
+        for (int b : blocks) {
+            if (rc) break;
+            h->tune.sum_block = b;
+            if ((rc = time_force_parts(h, reps, ms))) break;
+            if (ms[2] < best) { best = ms[2]; pick = b; }
+        }
+        h->tune.sum_block = pick;
+        if (!rc) rc = time_force_parts(h, reps, ms);
+    }
+    CU(cudaMemcpyAsync(h->d_ctl, &saved, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if (rc) {
+        h->tune = start;
+        return rc;
+    }
+    const double after = ms[0] + ms[1] + ms[2];
+    if (after > before) h->tune = start; // the measurement did not find a faster shape
+    h->tune.ms_before = before;
+    h->tune.ms_after = std::min(after, before);
+    free_graphs(h); // captured with the previous shapes
+    *out = h->tune;
+    return DEM_OK;
+}
+
+int dem_set_tuning(dem_handle* hh, const dem_tuning* t)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !t) return DEM_ERR_BAD_INPUT;
+    if (!valid_tuning(*t))
+        return fail(h, DEM_ERR_BAD_INPUT, "dem_set_tuning: blocks of 64, 128 or 256 threads, 3-6 contact blocks per SM");
+    h->tune.detect_block = t->detect_block;
+    h->tune.contacts_blocks_per_sm = t->contacts_blocks_per_sm;
+    h->tune.sum_block = t->sum_block;
+    free_graphs(h);
+    return DEM_OK;
+}
+
+int dem_get_tuning(dem_handle* hh, dem_tuning* out)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !out) return DEM_ERR_BAD_INPUT;
+    *out = h->tune;
     return DEM_OK;
 }
 

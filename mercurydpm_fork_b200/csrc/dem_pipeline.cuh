@@ -39,9 +39,13 @@ constexpr int SLOT_NONE = -1;        // P entry without a contact this evaluatio
 constexpr int SLOT_IS_I = -2;        // entry whose partner owns the pair, no contact this evaluation
 constexpr int SLOT_I_BASE = -3;      // SLOT_I_BASE - q: I's share of the partner's item q
 constexpr int SHARE = 12;            // doubles per item: P force, P torque, I force, I torque
-constexpr int DETECT_BLOCK = 128;
+// Launch shapes. k_detect and k_sum are compiled for blocks of 64, 128 and
+// 256 threads and k_contacts' grid size is a run-time value; the handle keeps
+// the choice (dem_autotune measures the variants on the live state).
+constexpr int DETECT_BLOCK = 128;        // the default k_detect block
 constexpr int CONTACT_BLOCK = 128;
-constexpr int SUM_BLOCK = 128;
+constexpr int SUM_BLOCK = 128;           // the default k_sum block
+constexpr int SUM_THREADS_PER_SM = 640;  // k_sum's launch bounds: 640 / block resident blocks per SM
 
 // Shared-memory copies of the instance record (when there is one instance)
 // and of the species-pair table (when it has at most SP_STAGE_MAX entries),
@@ -137,7 +141,7 @@ __device__ __forceinline__ void rev_one(const DevPtrs& d, int s, int l)
     }
 }
 
-// Exclusive block scan of one int per thread (DETECT_BLOCK threads); returns
+// Exclusive block scan of one int per thread (any block of whole warps); returns
 // this thread's offset and the block total through `total`.
 __device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& total)
 {
@@ -159,13 +163,13 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& 
     return before + x - v;
 }
 
-template <int MODE, int NCOMP>
-__global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
+template <int MODE, int NCOMP, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
 {
     constexpr int HIT_KEEP = 16; // partner slots of the first hits, kept for the item pass
-    __shared__ int warp_sums[DETECT_BLOCK / 32];
+    __shared__ int warp_sums[BLOCK / 32];
     __shared__ int block_base;
-    __shared__ int kept_t[HIT_KEEP][DETECT_BLOCK];
+    __shared__ int kept_t[HIT_KEEP][BLOCK];
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     Control* ctl = d.ctl;
     const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
@@ -364,8 +368,11 @@ __global__ void __launch_bounds__(DETECT_BLOCK) k_detect(DevPtrs d)
 // RECORD: this launch may be the last force evaluation of a dem_step call,
 // which writes the contact records; the steps before it are launched with
 // RECORD = false, a variant without the record path (fewer registers).
-template <int MODE, int NLAW, int FLAW, int NCOMP, bool RECORD>
-__global__ void __launch_bounds__(CONTACT_BLOCK, 4) k_contacts(DevPtrs d)
+// MINB: resident blocks per SM the registers are budgeted for (4: 128
+// registers a thread; 5: 102; 6: 85; 3: 168), i.e. warps in flight against
+// spills; the time-step variant is compiled for 3 to 6 (dem_autotune).
+template <int MODE, int NLAW, int FLAW, int NCOMP, bool RECORD, int MINB = 4>
+__global__ void __launch_bounds__(CONTACT_BLOCK, MINB) k_contacts(DevPtrs d)
 {
     Control* ctl = d.ctl;
     const int c = ctl->cur, nb = c ^ 1;
@@ -728,8 +735,8 @@ __global__ void __launch_bounds__(TRI_BLOCK) k_tri(DevPtrs d)
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(SUM_BLOCK, 5) k_sum(DevPtrs d)
+template <int MODE, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, SUM_THREADS_PER_SM / BLOCK) k_sum(DevPtrs d)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     Control* ctl = d.ctl;

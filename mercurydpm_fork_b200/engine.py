@@ -201,6 +201,8 @@ class DemEngine:
         self.n_instances = len(instances)
         sp = (_abi.SpeciesPair * len(species))(*species)
         self._check(lib().dem_set_species(self._h, sp, len(species)))
+        self._species = list(species)
+        self._rmin = self._rmax = 0.0
         walls = walls or []
         wa = (_abi.Wall * max(1, len(walls)))(*walls)
         self._check(lib().dem_set_walls(self._h, wa, len(walls)))
@@ -249,6 +251,8 @@ class DemEngine:
                               _ip(k["species"]), _ip(k["id"]), _ip(k["instance"]))
         self._check(lib().dem_upload_particles(self._h, C.byref(p)))
         self.n = n
+        if n:
+            self._rmin, self._rmax = float(np.min(k["radius"])), float(np.max(k["radius"]))
 
     def upload_contacts(self, id_p, id_i, springs, is_wall=None, periodic=None):
         m = len(id_p)
@@ -404,6 +408,45 @@ class DemEngine:
         ms = C.c_double(0)
         self._check(lib().dem_time_force_kernel(self._h, int(reps), C.byref(ms)))
         return ms.value
+
+    def autotune(self, reps: int = 20, cache: dict | None = None, key=None) -> dict:
+        """dem_autotune: the fastest launch shape of each force kernel on the
+        current state. With a `cache` dict, shapes are looked up and stored
+        under `key` (default: workload_class() of this engine), so that
+        engines of the same class skip the measurement."""
+        t = _abi.Tuning()
+        if cache is not None:
+            key = key if key is not None else self.workload_class()
+            if key in cache:
+                t.detect_block, t.contacts_blocks_per_sm, t.sum_block = cache[key]
+                self._check(lib().dem_set_tuning(self._h, C.byref(t)))
+                return dict(detect_block=t.detect_block, contacts_blocks_per_sm=t.contacts_blocks_per_sm,
+                            sum_block=t.sum_block, cached=True)
+        self._check(lib().dem_autotune(self._h, int(reps), C.byref(t)))
+        out = dict(detect_block=t.detect_block, contacts_blocks_per_sm=t.contacts_blocks_per_sm,
+                   sum_block=t.sum_block, ms_before=t.ms_before, ms_after=t.ms_after, cached=False)
+        if cache is not None:
+            cache[key] = (t.detect_block, t.contacts_blocks_per_sm, t.sum_block)
+        return out
+
+    def set_tuning(self, detect_block: int, contacts_blocks_per_sm: int, sum_block: int):
+        t = _abi.Tuning(detect_block, contacts_blocks_per_sm, sum_block, 0, 0.0, 0.0)
+        self._check(lib().dem_set_tuning(self._h, C.byref(t)))
+
+    def tuning(self) -> dict:
+        t = _abi.Tuning()
+        self._check(lib().dem_get_tuning(self._h, C.byref(t)))
+        return dict(detect_block=t.detect_block, contacts_blocks_per_sm=t.contacts_blocks_per_sm,
+                    sum_block=t.sum_block)
+
+    def workload_class(self) -> tuple:
+        """(particles to the nearest power of 2, law variant of the species
+        table, size ratio to one decimal): the key the autotuner's cache uses."""
+        import math
+        st = self.stats()
+        laws = sorted({(int(p.normal_law), int(p.friction_law)) for p in self._species})
+        ratio = round(self._rmax / self._rmin, 1) if self._rmin > 0 else 1.0
+        return (int(round(math.log2(max(1, st["n"])))), tuple(laws), ratio)
 
     def stats(self) -> dict:
         ms = C.c_double(0)

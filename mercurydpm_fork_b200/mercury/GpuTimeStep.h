@@ -24,8 +24,9 @@
 //                             neighbour grid and wraps periodic positions
 //   hGridActionsBeforeTimeLoop  ends the engine of a previous solve(), then
 //                             the base's own set-up
-//   hGridActionsBeforeTimeStep  the base's own grid build in initialiseSolve
-//                             (restart files describe it), nothing afterwards
+//   hGridActionsBeforeTimeStep  the base's own grid in initialiseSolve and
+//                             the first step (restart files describe it),
+//                             nothing afterwards
 //   writeEneTimeStep          the reference's .ene line (DPMBase.cc:2100-2123)
 //                             from the engine's balances (dem_reduce)
 //
@@ -148,13 +149,19 @@ protected:
     {
         if (h_) dem_destroy(h_);
         h_ = nullptr;
+        baseGridCalls_ = 0;
         Base::hGridActionsBeforeTimeLoop();
     }
-    /// The base's grid is built once, by the call of initialiseSolve (Mercury3D /
-    /// Mercury2D size their cells there); the time steps use the engine's grid.
+    /// The base's own grid runs in initialiseSolve (Mercury3D / Mercury2D size
+    /// their cells there) and in the first time step (its first update resets
+    /// the displacement bookkeeping), so that restart files describe it as the
+    /// reference's do; later steps use the engine's grid only.
     void hGridActionsBeforeTimeStep() override
     {
-        if (!h_) Base::hGridActionsBeforeTimeStep();
+        if (baseGridCalls_ < 2) {
+            Base::hGridActionsBeforeTimeStep();
+            ++baseGridCalls_;
+        }
     }
     void hGridActionsBeforeIntegration() override {}
     void hGridActionsAfterIntegration() override {}
@@ -190,6 +197,7 @@ private:
     dem_handle* h_ = nullptr;
     int device_ = 0;
     unsigned syncInterval_ = 1;
+    int baseGridCalls_ = 0;
     unsigned sinceSync_ = 0;
     std::vector<BaseParticle*> real_;
     std::vector<double> x_, v_, w_, q_, f_, t_;

@@ -44,6 +44,8 @@ class Scenario:
     ids: np.ndarray
     rotation: bool = True
     info: dict = field(default_factory=dict)
+    angular_velocity: np.ndarray | None = None   # None: at rest
+    orientation: np.ndarray | None = None        # None: identity quaternions
 
     @property
     def n(self) -> int:
@@ -69,7 +71,7 @@ class Scenario:
         from .engine import DemEngine
         e = DemEngine(self.time_step, [self.instance], self.species, self.walls, rotation=self.rotation, **kw)
         e.upload(self.position, self.velocity, self.radius, self.inv_mass, self.inv_inertia, self.species_index,
-                 self.ids)
+                 self.ids, angular_velocity=self.angular_velocity, orientation=self.orientation)
         return e
 
 

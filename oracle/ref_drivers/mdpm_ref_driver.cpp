@@ -7,6 +7,8 @@
 // as the engine's C ABI (include/dem_b200.h), runs the reference's
 // initialiseSolve + computeOneTimeStep loop, and returns its state, forces and
 // contact list, or the wall time of a timed window (the CPU baseline).
+#include <limits>
+
 #include "ref_driver.h"
 
 namespace {
@@ -191,9 +193,97 @@ int mdpm_ref_write_outputs(const dem_config* cfg, const dem_instance_desc* inst,
     return 0;
 }
 
+// The reference restarted from a .restart file (DPMBase::readRestartFile,
+// DPMBase.cc:3015-3060, then initialiseSolve without setupInitialConditions)
+// and advanced `nsteps` time steps; returns its state (rows by particle id,
+// which the tests set to the upload index), forces, and the contacts of its
+// last force evaluation with their springs. The restart path must end in
+// ".restart".
+int mdpm_ref_restart_run(const char* path, int nsteps, int64_t n, dem_particles_soa* out, double* force,
+                         double* torque, dem_contacts_soa* contacts_out, int64_t contacts_capacity,
+                         int64_t* contacts_count)
+{
+    Mercury3D d;
+    d.setName("mdpm_ref_restart");
+    if (!d.readRestartFile(std::string(path))) return 1;
+    d.setFileType(FileType::NO_FILE);
+    d.setTimeMax(1e300);
+    const unsigned n0 = d.getNumberOfTimeSteps();
+    d.initialiseSolve();
+    for (int k = 0; k < nsteps; ++k) d.computeOneTimeStep();
+    unsigned per_mask = 0;
+    double per_lo[3] = {0, 0, 0}, per_hi[3] = {0, 0, 0};
+    for (BaseBoundary* b : d.boundaryHandler)
+        if (auto* pb = dynamic_cast<PeriodicBoundary*>(b))
+            for (int k = 0; k < 3; ++k)
+                if (pb->getNormal().getComponent(k) != 0) {
+                    per_mask |= 1u << k;
+                    per_lo[k] = pb->getDistanceLeft();
+                    per_hi[k] = pb->getDistanceRight();
+                }
+    for (int64_t r = 0; r < (int64_t)d.particleHandler.getSize(); ++r) {
+        const BaseParticle* p = d.particleHandler.getObject((unsigned)r);
+        const int64_t i = (int64_t)p->getId();
+        if (i < 0 || i >= n) continue;
+        const Vec3D x = p->getPosition(), v = p->getVelocity(), w = p->getAngularVelocity(), f = p->getForce(),
+                    t = p->getTorque();
+        for (int k = 0; k < 3; ++k) {
+            if (out && out->position) out->position[3 * i + k] = x.getComponent(k);
+            if (out && out->velocity) out->velocity[3 * i + k] = v.getComponent(k);
+            if (out && out->angular_velocity) out->angular_velocity[3 * i + k] = w.getComponent(k);
+            if (force) force[3 * i + k] = f.getComponent(k);
+            if (torque) torque[3 * i + k] = t.getComponent(k);
+        }
+    }
+    int64_t cnt = 0;
+    const unsigned last = n0 + (nsteps > 0 ? (unsigned)nsteps : 1u);
+    for (BaseInteraction* c : d.interactionHandler) {
+        if (c->getTimeStamp() != last) continue;
+        const bool wall = dynamic_cast<BaseParticle*>(c->getI()) == nullptr;
+        if (contacts_out && cnt < contacts_capacity) {
+            contacts_out->id_p[cnt] = (int)c->getP()->getId();
+            contacts_out->id_i[cnt] = (int)(wall ? c->getI()->getIndex() : c->getI()->getId());
+            if (contacts_out->is_wall) contacts_out->is_wall[cnt] = wall;
+            if (contacts_out->periodic) {
+                bool per = false;
+                if (!wall)
+                    for (int k = 0; k < 3; ++k)
+                        if ((per_mask >> k) & 1u) {
+                            const double dx = c->getP()->getPosition().getComponent(k) -
+                                              c->getI()->getPosition().getComponent(k);
+                            if (std::fabs(dx) > 0.5 * (per_hi[k] - per_lo[k])) per = true;
+                        }
+                contacts_out->periodic[cnt] = per;
+            }
+            if (contacts_out->overlap) contacts_out->overlap[cnt] = c->getOverlap();
+            if (contacts_out->force) {
+                const Vec3D f = c->getForce();
+                for (int k = 0; k < 3; ++k) contacts_out->force[3 * cnt + k] = f.getComponent(k);
+            }
+            if (contacts_out->springs) {
+                double* s = contacts_out->springs + 9 * cnt;
+                for (int k = 0; k < 9; ++k) s[k] = 0.0;
+                Vec3D sl(0, 0, 0), ro(0, 0, 0), to(0, 0, 0);
+                if (auto* fi = dynamic_cast<SlidingFrictionInteraction*>(c)) sl = fi->getSlidingSpring();
+                if (dynamic_cast<MindlinInteraction*>(c)) sl = mindlin_sliding_spring(c);
+                if (auto* fi = dynamic_cast<FrictionInteraction*>(c)) { ro = fi->getRollingSpring(); to = fi->getTorsionSpring(); }
+                if (auto* fi = dynamic_cast<MindlinRollingTorsionInteraction*>(c)) { ro = fi->getRollingSpring(); to = fi->getTorsionSpring(); }
+                for (int k = 0; k < 3; ++k) {
+                    s[k] = sl.getComponent(k);
+                    s[3 + k] = ro.getComponent(k);
+                    s[6 + k] = to.getComponent(k);
+                }
+            }
+        }
+        ++cnt;
+    }
+    if (contacts_count) *contacts_count = cnt;
+    return 0;
+}
+
 // The reference's restart file (DPMBase::write, DPMBase.cc:3550) after
-// `nsteps` time steps, written to `path` with the precision of its file
-// streams (10).
+// `nsteps` time steps, written to `path` with the precision of its restart
+// stream (std::numeric_limits<double>::digits10 = 15, DPMBase.cc:214-215).
 int mdpm_ref_write_restart(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
                            const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in,
                            int nsteps, const char* path)
@@ -203,7 +293,7 @@ int mdpm_ref_write_restart(const dem_config* cfg, const dem_instance_desc* inst,
     d.initialiseSolve();
     for (int k = 0; k < nsteps; ++k) d.computeOneTimeStep();
     std::ofstream os(path);
-    os.precision(10);
+    os.precision(std::numeric_limits<double>::digits10);
     d.write(os, true);
     return 0;
 }

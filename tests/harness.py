@@ -82,8 +82,12 @@ class _Inputs:
         self.ii = np.ascontiguousarray(sc.inv_inertia, np.float64)
         self.sp = np.ascontiguousarray(sc.species_index, np.int32)
         self.ids = np.ascontiguousarray(sc.ids, np.int32)
-        self.soa = _abi.ParticlesSoA(n, _dp(self.pos), _dp(self.vel), None, None, _dp(self.rad), _dp(self.im),
-                                     _dp(self.ii), _ip(self.sp), _ip(self.ids), None)
+        w = getattr(sc, "angular_velocity", None)
+        q = getattr(sc, "orientation", None)
+        self.ang = None if w is None else np.ascontiguousarray(w, np.float64)
+        self.ori = None if q is None else np.ascontiguousarray(q, np.float64)
+        self.soa = _abi.ParticlesSoA(n, _dp(self.pos), _dp(self.vel), _dp(self.ang), _dp(self.ori), _dp(self.rad),
+                                     _dp(self.im), _dp(self.ii), _ip(self.sp), _ip(self.ids), None)
         self.cfg = sc.config()
         self.inst = sc.instance.to_c()
         self.species = (_abi.SpeciesPair * len(sc.species))(*sc.species)
@@ -504,3 +508,40 @@ def selftest_gold(filename: str) -> str:
     import gzip
     with gzip.open(os.path.join(SELFTEST_GOLD, filename + ".gz"), "rt") as f:
         return f.read()
+
+
+def reference_restart(sc, nsteps: int, path: str) -> str:
+    """The reference's restart file (DPMBase::write, 15 digits) after nsteps
+    time steps of the scenario; returns its text."""
+    darr, nd = _deletions(None)
+    lib = ref_lib("serial")
+    lib.mdpm_ref_set_deletion(darr, nd)
+    fn = lib.mdpm_ref_write_restart
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(_abi.Config), C.POINTER(_abi.InstanceDesc), C.POINTER(_abi.SpeciesPair), _pd,
+                   C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA), C.c_int, C.c_char_p]
+    inp = _Inputs(sc)
+    with quiet_stdout():
+        rc = fn(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density), inp.walls, inp.nwalls,
+                C.byref(inp.soa), nsteps, path.encode())
+    assert rc == 0
+    return open(path).read()
+
+
+def reference_restart_run(path: str, nsteps: int, n: int) -> dict:
+    """The reference restarted from `path` (its own reader) and advanced
+    nsteps time steps: state, forces and the last evaluation's contacts."""
+    lib = ref_lib("serial")
+    fn = lib.mdpm_ref_restart_run
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_char_p, C.c_int, C.c_int64, C.POINTER(_abi.ParticlesSoA), _pd, _pd,
+                   C.POINTER(_abi.ContactsSoA), C.c_int64, C.POINTER(C.c_int64)]
+    cap = _contact_rows(n)
+    o, c, soa, csoa = _outputs(n, cap)
+    cnt = C.c_int64(0)
+    with quiet_stdout():
+        rc = fn(path.encode(), nsteps, n, C.byref(soa), _dp(o["force"]), _dp(o["torque"]), C.byref(csoa), cap,
+                C.byref(cnt))
+    assert rc == 0
+    o["contacts"] = sort_contacts(_trim(c, cnt.value))
+    return o

@@ -312,3 +312,51 @@ def triangle_mesh(group: int = 1, n: int = 300, seed: int = 13, velocity=(0.0, 0
     dt = 0.02 * hertz_collision_time(d, density, 1e7)
     return Scenario(f"triangle_mesh_g{group}{'_dropped' if dropped else ''}", dt, inst, _hertz_mindlin_table(2), np.array([density, density]), walls,
                     pos, vel, radius, inv_mass, inv_inertia, np.zeros(m, np.int32), np.arange(m, dtype=np.int32))
+
+
+LAWS = ("linear", "linear_sliding", "linear_sliding_constant_restitution", "linear_rolling_torsion",
+        "hertz", "hertz_sliding", "hertz_mindlin", "hertz_mindlin_rolling_torsion")
+
+
+def drum_with_law(law: str, n: int = 600, seed: int = 5):
+    """small_drum (bidisperse 1:3, a rotating AxisymmetricIntersectionOfWalls
+    cylinder and two InfiniteWall caps, compressed bed pressed onto the
+    cylinder) with every species pair on one contact law, so that each law's
+    branches run: normal force, sliding spring with the Coulomb cap (mu 0.2),
+    rolling (mu_r 0.05) and torsion (mu_o 0.02) springs, dissipation on every
+    spring. Linear laws: tc = 1e-4 s, restitution 0.7 for two small spheres,
+    k_t = 2/7 k, k_r = k_o = 2/5 k (Calibration.h's ratios), dt = tc/50
+    (constant restitution: the same k and gamma per unit mass). Hertz laws:
+    the drum's E, G and restitution, dt 0.02 of the Hertz collision time."""
+    import dataclasses
+    from mercurydpm_fork_b200 import _abi
+    from mercurydpm_fork_b200.engine import species_pair
+    from mercurydpm_fork_b200.host import hertz_dissipation_from_restitution
+    sc = small_drum(n=n, seed=seed)
+    m_small = 4.0 / 3.0 * PI * (0.5e-3) ** 3 * 2000.0
+    k, g = linear_collision_time_restitution(1e-4, 0.7, m_small)
+    E, G, eps = 1e7, 1e7 / 2 * 1.3, 0.7
+    L, H = _abi.DEM_NORMAL_LINEAR_VISCOELASTIC, _abi.DEM_NORMAL_HERTZIAN_VISCOELASTIC
+    base = dict(sliding_mu=0.2, sliding_mu_static=0.2, rolling_mu=0.05, rolling_mu_static=0.05, torsion_mu=0.02,
+                torsion_mu_static=0.02)
+    lin = dict(normal_law=L, stiffness=k, dissipation=g, sliding_stiffness=2 / 7 * k, sliding_dissipation=2 / 7 * g,
+               rolling_stiffness=2 / 5 * k, rolling_dissipation=2 / 5 * g, torsion_stiffness=2 / 5 * k,
+               torsion_dissipation=2 / 5 * g, **base)
+    hz = dict(normal_law=H, elastic_modulus=E, dissipation=hertz_dissipation_from_restitution(eps), shear_modulus=G,
+              sliding_dissipation=0.3, rolling_dissipation=0.2, torsion_dissipation=0.1, **base)
+    table = {
+        "linear": dict(lin, friction_law=_abi.DEM_FRICTION_NONE),
+        "linear_sliding": dict(lin, friction_law=_abi.DEM_FRICTION_SLIDING),
+        "linear_sliding_constant_restitution": dict(lin, friction_law=_abi.DEM_FRICTION_SLIDING, constant_restitution=1,
+                                                    stiffness=k / m_small, dissipation=g / m_small,
+                                                    sliding_stiffness=2 / 7 * k / m_small,
+                                                    sliding_dissipation=2 / 7 * g / m_small),
+        "linear_rolling_torsion": dict(lin, friction_law=_abi.DEM_FRICTION_ROLLING_TORSION),
+        "hertz": dict(hz, friction_law=_abi.DEM_FRICTION_NONE),
+        "hertz_sliding": dict(hz, friction_law=_abi.DEM_FRICTION_SLIDING, sliding_stiffness=2 / 7 * k),
+        "hertz_mindlin": dict(hz, friction_law=_abi.DEM_FRICTION_MINDLIN),
+        "hertz_mindlin_rolling_torsion": dict(hz, friction_law=_abi.DEM_FRICTION_MINDLIN_ROLLING_TORSION),
+    }[law]
+    sp = species_pair(**table)
+    dt = 2e-6 if law.startswith("linear") else sc.time_step
+    return dataclasses.replace(sc, name=f"drum_{law}", species=[sp] * len(sc.species), time_step=dt)

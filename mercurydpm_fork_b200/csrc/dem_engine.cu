@@ -629,6 +629,21 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         I.wall_end = wend[in];
         I.tri_mask = 0u;
         I.tri_static = 1;
+        I.wall_still_mask = 0u;
+        for (int w = wbegin[in]; w < wend[in]; ++w) {
+            const dem_wall& x = h->walls[w];
+            if (x.type == DEM_WALL_TRIANGLE) continue;
+            bool still = x.velocity[0] == 0.0 && x.velocity[1] == 0.0 && x.velocity[2] == 0.0;
+            const V3 om = v3(x.angular_velocity[0], x.angular_velocity[1], x.angular_velocity[2]);
+            if (still && len2(om) != 0.0) {
+                // a turn about the normal (infinite) or the axis (axisymmetric)
+                // through the wall's position maps the wall onto itself
+                const V3 ax = quat_axis(Q4{x.orientation[0], x.orientation[1], x.orientation[2], x.orientation[3]});
+                still = (x.type == DEM_WALL_INFINITE || x.type == DEM_WALL_AXISYMMETRIC) &&
+                        len2(cross(om, ax)) <= 1e-24 * len2(om) * len2(ax);
+            }
+            if (still) I.wall_still_mask |= 1u << (w - wbegin[in]);
+        }
         for (int k = 0; k < 3; ++k) {
             I.tri_lo[k] = DBL_MAX;
             I.tri_hi[k] = -DBL_MAX;
@@ -723,6 +738,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
             d.pr[b] = kept.pr[b]; d.vm[b] = kept.vm[b]; d.wi[b] = kept.wi[b]; d.qo[b] = kept.qo[b];
             d.info[b] = kept.info[b]; d.caller[b] = kept.caller[b]; d.nbr[b] = kept.nbr[b]; d.cnt[b] = kept.cnt[b];
             d.own[b] = kept.own[b];
+            d.wcand[b] = kept.wcand[b];
             d.hist[b] = kept.hist[b]; d.act[b] = kept.act[b]; d.whist[b] = kept.whist[b]; d.wact[b] = kept.wact[b];
         }
         d.force = kept.force; d.torque = kept.torque; d.key = kept.key; d.perm = kept.perm; d.newidx = kept.newidx;
@@ -753,6 +769,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         if ((rc = dalloc(h, &d.nbr[b], (size_t)cap * NC))) return rc;
         if ((rc = dalloc(h, &d.cnt[b], NC))) return rc;
         if ((rc = dalloc(h, &d.own[b], (size_t)d.nwords * NC))) return rc;
+        if ((rc = dalloc(h, &d.wcand[b], NC))) return rc;
         if ((rc = dalloc(h, &d.hist[b], (size_t)hist_stride(d.ncomp) * cap * NC))) return rc;
         if ((rc = dalloc(h, &d.act[b], (size_t)d.nwords * NC))) return rc;
         if ((rc = dalloc(h, &d.whist[b], (size_t)hist_stride(d.ncomp) * wmax * NC))) return rc;

@@ -58,6 +58,12 @@ struct InstanceDev {
     // DeletionBoundary planes: a particle is deleted when del_d - x . del_n < 0
     int n_del;
     uint32_t tri_mask;     // walls (bit w = wall_begin + w) that are triangle walls
+    // walls (same bits) whose distance field stays put while the simulation
+    // runs: no translation, and no rotation or one about the wall's own
+    // normal / symmetry axis (infinite and axisymmetric walls). The list
+    // rebuild records which of them are within reach + skin of a particle
+    // (wcand); k_detect tests the others not at all until the next rebuild
+    uint32_t wall_still_mask;
     int tri_static;        // every triangle wall of the instance stands still: tri_lo/hi hold
     double tri_lo[3], tri_hi[3]; // the bounding box of all their vertices
     double del_n[DEM_MAX_DELETION_PER_INSTANCE][3];
@@ -135,6 +141,10 @@ struct DevPtrs {
     // own[l][(k/32)*ncap + i] is set when particle i has the lower id of its
     // entry k's pair (it is P unless the pair meets across a periodic boundary)
     unsigned int *own[2];
+    // per particle of list buffer l: bit w set when still wall w (above) was
+    // within reach + skin at the rebuild (particles move less than skin / 2
+    // between rebuilds, so the other still walls cannot be touched)
+    unsigned int *wcand[2];
     double *hist[2];
     unsigned int *act[2];
     double *whist[2];

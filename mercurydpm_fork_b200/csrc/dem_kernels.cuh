@@ -287,6 +287,7 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
     const bool fixed_s = (is.w & FLAG_FIXED) != 0;
     if (is.w & FLAG_DELETED) {
         d.cnt[ln][s] = 0;
+        d.wcand[ln][s] = 0u;
         for (int w = 0; w < d.nwords; ++w) d.act[nb][(size_t)w * d.ncap + s] = 0u;
         d.wact[nb][s] = 0u;
         return;
@@ -398,6 +399,23 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
     }
     if (count & 31) d.own[ln][(size_t)(count >> 5) * d.ncap + s] = ownw; // the last, partial word
     d.cnt[ln][s] = count;
+
+    // still walls within reach + skin (k_detect tests only these until the next rebuild)
+    unsigned int wc = 0u;
+    if (!fixed_s) {
+        const int nwl = I.wall_end - I.wall_begin;
+        for (int w = 0; w < nwl; ++w) {
+            if (!((I.wall_still_mask >> w) & 1u)) continue;
+            const int wg = I.wall_begin + w;
+            const dem_wall& wall = d.walls[wg];
+            const double R = ps.w + d.species[I.species_offset + is.y * I.n_species + wall.species].interaction_distance +
+                             d.ctl->skin;
+            double dist;
+            V3 nrm;
+            if (wall_distance(wall, d.wgeom + wg, xs, R, dist, nrm)) wc |= 1u << w;
+        }
+    }
+    d.wcand[ln][s] = wc;
 
     // carry contact history from the old list (old order) to the new one, up
     // to 4 contacts per pass over the new list

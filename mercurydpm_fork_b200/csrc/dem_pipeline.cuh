@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
                            (xs.x > I.tri_lo[0] - R && xs.x < I.tri_hi[0] + R && xs.y > I.tri_lo[1] - R &&
                             xs.y < I.tri_hi[1] + R && xs.z > I.tri_lo[2] - R && xs.z < I.tri_hi[2] + R);
             }
+            const unsigned int far_still = I.wall_still_mask & ~d.wcand[l][s];
             for (int w = 0; w < nwalls; ++w) {
                 const int wg = I.wall_begin + w;
                 const unsigned int bit = 1u << w;
@@ -302,13 +303,17 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
                         if (hit) thit |= bit;
                     }
                 } else {
-                    const dem_wall& wall = d.walls[wg];
-                    const dem_species_pair& sp = d.species[I.species_offset + is.y * ns + wall.species];
-                    double dist;
-                    V3 nrm;
                     d.slotw[(size_t)w * d.ncap + s] = SLOT_NONE;
-                    hit = wall_distance(wall, d.wgeom + wg, xs, ps.w + sp.interaction_distance, dist, nrm);
-                    if (hit) whit |= bit;
+                    if (far_still & bit) { // farther than reach + skin at the last rebuild
+                        hit = false;
+                    } else {
+                        const dem_wall& wall = d.walls[wg];
+                        const dem_species_pair& sp = d.species[I.species_offset + is.y * ns + wall.species];
+                        double dist;
+                        V3 nrm;
+                        hit = wall_distance(wall, d.wgeom + wg, xs, ps.w + sp.interaction_distance, dist, nrm);
+                        if (hit) whit |= bit;
+                    }
                 }
                 if (hit) {
                     wnew |= bit;

@@ -188,7 +188,10 @@ typedef struct dem_config {
     int32_t  use_graphs;           /* capture the step loop in CUDA graphs           */
     double   skin;                 /* Verlet skin distance (0: 0.4 x smallest radius)*/
     int32_t  n_instances;          /* >= 1                                           */
-    int32_t  reserved;
+    int32_t  max_contacts;         /* contact capacity: mean contacts per particle in
+                                    * one evaluation (pairs once, plus wall contacts),
+                                    * which sizes the per-contact spring storage
+                                    * (0: auto, min(max_neighbors,16) + min(walls,4)) */
 } dem_config;
 
 /* Global balances (DPMBase::getKineticEnergy ... getCentreOfMass,
@@ -350,6 +353,9 @@ int  dem_last_step_stats(dem_handle *h, double *ms, int64_t *kernel_launches,
                          int64_t *rebuilds);
 int  dem_get_info(dem_handle *h, int64_t *n_particles, int64_t *max_neighbors,
                   int64_t *n_cells);
+/* Device memory held by the handle's particle, list and contact arrays, and
+ * the contact capacity (items of one evaluation) they were sized for. */
+int  dem_get_memory(dem_handle *h, int64_t *device_bytes, int64_t *contact_capacity);
 /* Neighbour-list entries, live particle contacts and wall contacts of the
  * current state (the sizes the per-step byte count is made of). */
 int  dem_get_counts(dem_handle *h, int64_t *list_entries, int64_t *contacts,

@@ -102,7 +102,7 @@ class InstanceDesc(C.Structure):
 class Config(C.Structure):
     _fields_ = [
         ("time_step", _d), ("background_drag", _d), ("rotation", _i32), ("device", _i32),
-        ("max_neighbors", _i32), ("use_graphs", _i32), ("skin", _d), ("n_instances", _i32), ("reserved", _i32),
+        ("max_neighbors", _i32), ("use_graphs", _i32), ("skin", _d), ("n_instances", _i32), ("max_contacts", _i32),
     ]
 
 
@@ -149,6 +149,7 @@ _SIGNATURES = {
     "dem_cg_eval": (C.c_int, [C.c_void_p, C.POINTER(CGGrid), _pd]),
     "dem_last_step_stats": (C.c_int, [C.c_void_p, _pd, C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_get_info": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
+    "dem_get_memory": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_get_counts": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_time_force_kernel": (C.c_int, [C.c_void_p, C.c_int, _pd]),
     "dem_selftest_wait_expiry": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_uint32)]),

@@ -163,14 +163,17 @@ def packing_fraction(pos: np.ndarray, radius: np.ndarray, base_radius: float, h0
 def run_heaps(b: Batch, base_radius: float, steps: int = 40_000, trace_every: int = 1_000, engine=None,
               max_neighbors: int = 0) -> dict:
     """Runs every instance of the batch for `steps` time steps in one handle;
-    returns the per-instance outputs and kinetic-energy traces."""
+    returns the per-instance outputs, kinetic-energy traces and the device
+    time of the time steps (device_ms, summed over the dem_step calls)."""
     e = engine if engine is not None else b.engine(max_neighbors=max_neighbors)
     e.step(0)
     ke = [e.reduce_batch()["kinetic_energy"]]
     done = 0
+    device_ms = 0.0
     while done < steps:
         k = min(trace_every, steps - done)
         e.step(k)
+        device_ms += e.stats()["ms"]
         done += k
         ke.append(e.reduce_batch()["kinetic_energy"])
     g = e.reduce_batch()
@@ -180,7 +183,7 @@ def run_heaps(b: Batch, base_radius: float, steps: int = 40_000, trace_every: in
     n_inst = len(b.members)
     out = dict(aor_reference=aor_com(g["centre_of_mass"][:, 2], base_radius), aor_surface=np.full(n_inst, np.nan),
                packing_fraction=np.full(n_inst, np.nan), kinetic_energy=np.array(ke).T,
-               elastic_energy=g["elastic_energy"], n_remaining=np.zeros(n_inst, np.int64))
+               elastic_energy=g["elastic_energy"], n_remaining=np.zeros(n_inst, np.int64), device_ms=device_ms)
     for k in range(n_inst):
         sl = b.member_slice(k)
         alive = st["instance"][sl] >= 0

@@ -42,6 +42,7 @@ struct Handle {
     DevPtrs d{};
     // device allocations
     std::vector<void*> allocs;
+    size_t alloc_bytes = 0;            // their sizes
     InstanceDev* d_inst = nullptr;
     dem_species_pair* d_species = nullptr;
     dem_wall* d_walls = nullptr;
@@ -99,6 +100,7 @@ int dalloc(Handle* h, T** p, size_t count)
     e = cudaMemsetAsync(ptr, 0, bytes, h->stream);
     if (e != cudaSuccess) return fail(h, DEM_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
     h->allocs.push_back(ptr);
+    h->alloc_bytes += bytes;
     *p = static_cast<T*>(ptr);
     return DEM_OK;
 }
@@ -116,6 +118,7 @@ void free_particle_arrays(Handle* h)
     free_graphs(h);
     for (void* p : h->allocs) cudaFree(p);
     h->allocs.clear();
+    h->alloc_bytes = 0;
     h->d_records = nullptr;
     h->record_capacity = 0;
     h->d_stage = nullptr;
@@ -694,14 +697,25 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     cap = ((cap + 31) / 32) * 32;
     if (cap > 128) return fail(h, DEM_ERR_BAD_INPUT, "max_neighbors above 128 is not supported");
 
+    // ---- contact capacity: items of one evaluation, and the springs of the
+    // contacts (one record per item, two pools). Auto: at most min(cap, 16)
+    // pairs owned per particle plus 4 walls; dem_config.max_contacts sets the
+    // mean per particle instead (a dense packing has 2 to 4 owned contacts
+    // per particle). Exceeding it is DEM_ERR_CAPACITY.
+    if (h->cfg.max_contacts < 0) return fail(h, DEM_ERR_BAD_INPUT, "max_contacts must be >= 0");
+    const long long item_cap =
+        std::min<long long>(2000000000ll, h->cfg.max_contacts > 0
+                                              ? (long long)n * h->cfg.max_contacts + 1024
+                                              : (long long)n * std::min(cap, 16) + (long long)n * std::min(wmax, 4) + 1024);
     // ---- (re)allocate: a re-upload with the same sizes keeps the device arrays
     // and the captured graphs (their kernel arguments stay valid)
-    const unsigned record_capacity =
-        (unsigned)std::min<long long>(2000000000ll, 8 * n + 1024 + (long long)n * std::min(wmax, 4));
+    const unsigned record_capacity = (unsigned)std::min<long long>(
+        item_cap, std::min<long long>(2000000000ll, 8 * n + 1024 + (long long)n * std::min(wmax, 4)));
     long long any_tri = 0;
     for (const auto& w : h->walls) any_tri = any_tri || w.type == DEM_WALL_TRIANGLE;
     const std::vector<long long> layout = {n, cap, wmax, ncells, (long long)h->inst.size(), (long long)h->species.size(),
-                                           (long long)h->walls.size(), (long long)record_capacity, h->ncomp, any_tri};
+                                           (long long)h->walls.size(), (long long)record_capacity, h->ncomp, any_tri,
+                                           item_cap};
     const bool reuse = !h->layout.empty() && h->layout == layout;
     if (!reuse) free_particle_arrays(h);
     const DevPtrs kept = h->d;
@@ -739,7 +753,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
             d.info[b] = kept.info[b]; d.caller[b] = kept.caller[b]; d.nbr[b] = kept.nbr[b]; d.cnt[b] = kept.cnt[b];
             d.own[b] = kept.own[b];
             d.wcand[b] = kept.wcand[b];
-            d.hist[b] = kept.hist[b]; d.act[b] = kept.act[b]; d.whist[b] = kept.whist[b]; d.wact[b] = kept.wact[b];
+            d.pool[b] = kept.pool[b]; d.hidx[b] = kept.hidx[b];
+            d.act[b] = kept.act[b]; d.whist[b] = kept.whist[b]; d.wact[b] = kept.wact[b];
         }
         d.force = kept.force; d.torque = kept.torque; d.key = kept.key; d.perm = kept.perm; d.newidx = kept.newidx;
         d.cell_count = kept.cell_count; d.cell_start = kept.cell_start; d.cell_cursor = kept.cell_cursor;
@@ -770,7 +785,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         if ((rc = dalloc(h, &d.cnt[b], NC))) return rc;
         if ((rc = dalloc(h, &d.own[b], (size_t)d.nwords * NC))) return rc;
         if ((rc = dalloc(h, &d.wcand[b], NC))) return rc;
-        if ((rc = dalloc(h, &d.hist[b], (size_t)hist_stride(d.ncomp) * cap * NC))) return rc;
+        if ((rc = dalloc(h, &d.pool[b], (size_t)hist_stride(d.ncomp) * item_cap))) return rc;
+        if ((rc = dalloc(h, &d.hidx[b], (size_t)cap * NC))) return rc;
         if ((rc = dalloc(h, &d.act[b], (size_t)d.nwords * NC))) return rc;
         if ((rc = dalloc(h, &d.whist[b], (size_t)hist_stride(d.ncomp) * wmax * NC))) return rc;
         if ((rc = dalloc(h, &d.wact[b], NC))) return rc;
@@ -780,9 +796,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     if ((rc = dalloc(h, &d.pf, NC))) return rc;
     if ((rc = dalloc(h, &d.slot, (size_t)cap * NC))) return rc;
     if ((rc = dalloc(h, &d.slotw, (size_t)wmax * NC))) return rc;
-    // contact items: at most min(cap, 16) pairs owned per particle plus 4 walls
-    d.item_cap = (int)std::min<long long>(2000000000ll, (long long)n * std::min(cap, 16) +
-                                                            (long long)n * std::min(wmax, 4) + 1024);
+    d.item_cap = (int)item_cap;
     if ((rc = dalloc(h, &d.items, (size_t)d.item_cap))) return rc;
     if ((rc = dalloc(h, &d.shares, (size_t)d.item_cap * SHARE))) return rc;
     if ((rc = dalloc(h, &d.tri_list, NC))) return rc;
@@ -895,16 +909,29 @@ int dem_upload_contacts(dem_handle* hh, const dem_contacts_soa* cs)
     std::vector<double4> pr(n);
     std::vector<int> cnt(n), nbr((size_t)d.cap * NC);
     std::vector<unsigned> act((size_t)d.nwords * NC), wact(NC);
-    std::vector<double> hist((size_t)hist_stride(d.ncomp) * d.cap * NC), whist((size_t)hist_stride(d.ncomp) * d.wmax * NC);
+    std::vector<int> hidx((size_t)d.cap * NC, 0);
+    std::vector<double> pool, whist((size_t)hist_stride(d.ncomp) * d.wmax * NC);
     CU(cudaMemcpyAsync(info.data(), d.info[cur], n * sizeof(int4), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaMemcpyAsync(pr.data(), d.pr[cur], n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaMemcpyAsync(cnt.data(), d.cnt[l], n * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaMemcpyAsync(nbr.data(), d.nbr[l], nbr.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaMemcpyAsync(act.data(), d.act[cur], act.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaMemcpyAsync(wact.data(), d.wact[cur], wact.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaMemcpyAsync(hist.data(), d.hist[cur], hist.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaMemcpyAsync(whist.data(), d.whist[cur], whist.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(hidx.data(), d.hidx[cur], hidx.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
+    // springs injected by an earlier call stay where they are in the pool
+    const int stride = hist_stride(d.ncomp);
+    long long used = 0;
+    for (int s = 0; s < n; ++s)
+        for (int k = 0; k < std::min(cnt[s], d.cap); ++k)
+            if ((act[(size_t)(k >> 5) * NC + s] >> (k & 31)) & 1u)
+                used = std::max<long long>(used, (long long)hidx[nbr_at(d.ncap, s, k)] + 1);
+    pool.resize((size_t)used * stride);
+    if (used) {
+        CU(cudaMemcpyAsync(pool.data(), d.pool[c.pcur], pool.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+    }
     // id -> sorted slot
     std::vector<std::pair<int, int>> ids(n);
     for (int s = 0; s < n; ++s) ids[s] = {info[s].x, s};
@@ -913,11 +940,16 @@ int dem_upload_contacts(dem_handle* hh, const dem_contacts_soa* cs)
         auto it = std::lower_bound(ids.begin(), ids.end(), std::make_pair(id, -1));
         return (it != ids.end() && it->first == id) ? it->second : -1;
     };
+    // an entry with a new spring gets the next record of the pool
     auto set_entry = [&](int s, int t, const double* spr, double sign) -> bool {
         for (int k = 0; k < cnt[s]; ++k) {
             if (nbr[nbr_at(d.ncap, s, k)] != t) continue;
-            for (int comp = 0; comp < d.ncomp; ++comp)
-                hist[hist_at(d.ncap, d.ncomp, s, k) + comp] = sign * spr[comp];
+            const size_t e = nbr_at(d.ncap, s, k);
+            if (!((act[(size_t)(k >> 5) * NC + s] >> (k & 31)) & 1u)) {
+                hidx[e] = (int)(pool.size() / stride);
+                pool.resize(pool.size() + stride, 0.0);
+            }
+            for (int comp = 0; comp < d.ncomp; ++comp) pool[(size_t)hidx[e] * stride + comp] = sign * spr[comp];
             act[(size_t)(k >> 5) * NC + s] |= 1u << (k & 31);
             return true;
         }
@@ -949,9 +981,13 @@ int dem_upload_contacts(dem_handle* hh, const dem_contacts_soa* cs)
         if (!set_entry(sp, si, spr, 1.0) || !set_entry(si, sp, spr, per ? -1.0 : 1.0))
             return fail(h, DEM_ERR_BAD_INPUT, "injected contact is not within the neighbour list");
     }
+    if (pool.size() / stride > (size_t)d.item_cap)
+        return fail(h, DEM_ERR_CAPACITY, "more contact springs than the contact capacity (raise dem_config.max_contacts)");
     CU(cudaMemcpyAsync(d.act[cur], act.data(), act.size() * sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(d.wact[cur], wact.data(), wact.size() * sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
-    CU(cudaMemcpyAsync(d.hist[cur], hist.data(), hist.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(d.hidx[cur], hidx.data(), hidx.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    if (!pool.empty())
+        CU(cudaMemcpyAsync(d.pool[c.pcur], pool.data(), pool.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(d.whist[cur], whist.data(), whist.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     return DEM_OK;
@@ -1045,6 +1081,7 @@ int dem_step(dem_handle* hh, int nsteps)
             void* p = nullptr;
             if (cudaMalloc(&p, (size_t)need * sizeof(ContactRecord)) == cudaSuccess) {
                 h->allocs.push_back(p);
+                h->alloc_bytes += (size_t)need * sizeof(ContactRecord);
                 h->d_records = static_cast<ContactRecord*>(p);
                 h->record_capacity = need;
                 d.records = h->d_records;
@@ -1393,6 +1430,15 @@ int dem_get_info(dem_handle* hh, int64_t* n_particles, int64_t* max_neighbors, i
     if (n_particles) *n_particles = h->d.n;
     if (max_neighbors) *max_neighbors = h->d.cap;
     if (n_cells) *n_cells = h->d.ncells;
+    return DEM_OK;
+}
+
+int dem_get_memory(dem_handle* hh, int64_t* device_bytes, int64_t* contact_capacity)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h) return DEM_ERR_BAD_INPUT;
+    if (device_bytes) *device_bytes = (int64_t)h->alloc_bytes;
+    if (contact_capacity) *contact_capacity = h->d.item_cap;
     return DEM_OK;
 }
 

@@ -13,15 +13,17 @@
 // Neighbour lists are fixed-capacity rows, one per particle: nbr[l][i*cap + k]
 // (k < count[l][i]); l = Control::lbuf flips at every rebuild. The force
 // kernel walks a warp's entries particle by particle, so a particle's entries
-// are contiguous. Contact history is stored per neighbour entry in the same
-// row order with its components contiguous, hist[b][(i*cap + k)*ncomp + c]
-// (3 components per spring), and an active bit per entry,
-// act[b][w*ncap + i] (bit k%32 of word k/32). The
-// history is double-buffered together with the state (b = Control::cur): a
-// force evaluation reads buffer b and writes b^1, so a thread may read its
-// partner's history of the previous step (needed for periodic pairs) while
-// the partner writes the next one. Reading b and writing b^1 moves the same
-// bytes as an in-place update.
+// are contiguous. Contact history is stored per contact, not per entry: the
+// springs of an evaluation's contacts sit in a pool indexed by the contact's
+// item number in that evaluation, pool[p][j*stride + c] (3 or 9 components
+// per spring, padded), and every list entry keeps the pool index of its
+// contact of the last evaluation, hidx[b][k*ncap + i], valid where its active
+// bit, act[b][w*ncap + i] (bit k%32 of word k/32), is set. hidx and act follow
+// the state buffer b = Control::cur (a rebuild carries them to the new order);
+// the pool flips with every force evaluation (p = Control::pcur: read p,
+// write p^1), and a rebuild leaves it in place. A thread may therefore read its
+// partner's spring of the previous step (needed for periodic pairs) while
+// the partner writes the next one.
 #pragma once
 #include <cstdint>
 #include "dem_math.cuh"
@@ -109,6 +111,8 @@ struct Control {
     unsigned int lost_history;
     unsigned int n_items;  // contact items of the current evaluation
     unsigned int n_tri;    // triangle-wall items of the current evaluation (tri_list)
+    int pcur;              // spring pool holding the springs of the last evaluation
+    unsigned int n_carry;  // first time step: springs kept without a contact (pool top)
 };
 
 // Entry-major layouts: entry k of every particle is contiguous, so threads
@@ -118,10 +122,7 @@ __host__ __device__ __forceinline__ size_t nbr_at(int ncap, int i, int k) { retu
 // A spring record holds ncomp doubles padded to an even count (3 -> 4,
 // 9 -> 10), so every record starts on 16 bytes and moves as 16-byte vectors.
 __host__ __device__ __forceinline__ int hist_stride(int ncomp) { return ncomp + (ncomp & 1); }
-__host__ __device__ __forceinline__ size_t hist_at(int ncap, int ncomp, int i, int k)
-{
-    return ((size_t)k * ncap + i) * hist_stride(ncomp);
-}
+__host__ __device__ __forceinline__ size_t pool_at(int ncomp, int j) { return (size_t)j * hist_stride(ncomp); }
 __host__ __device__ __forceinline__ size_t whist_at(int ncap, int ncomp, int i, int w)
 {
     return ((size_t)w * ncap + i) * hist_stride(ncomp);
@@ -145,7 +146,8 @@ struct DevPtrs {
     // within reach + skin at the rebuild (particles move less than skin / 2
     // between rebuilds, so the other still walls cannot be touched)
     unsigned int *wcand[2];
-    double *hist[2];
+    double *pool[2];        // springs per contact (item_cap records each)
+    int *hidx[2];           // per entry: pool index of its contact's spring
     unsigned int *act[2];
     double *whist[2];
     unsigned int *wact[2];

@@ -52,8 +52,9 @@ __global__ void k_control(Control* ctl, dem_wall* walls, WallGeom* wgeom, int n_
         if (w.type == DEM_WALL_TRIANGLE && !still) triangle_geometry(w, wgeom[k]);
     }
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (ctl->pending_flip) {
+    if (ctl->pending_flip) { // a force evaluation wrote the other state buffer and spring pool
         ctl->cur ^= 1;
+        ctl->pcur ^= 1;
         ctl->pending_flip = 0;
     }
     const double d = sqrt(__longlong_as_double((long long)ctl->step_disp2_bits));
@@ -73,8 +74,9 @@ __global__ void k_control(Control* ctl, dem_wall* walls, WallGeom* wgeom, int n_
 __global__ void k_flip(Control* ctl)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (ctl->pending_flip) {
+    if (ctl->pending_flip) { // a force evaluation wrote the other state buffer and spring pool
         ctl->cur ^= 1;
+        ctl->pcur ^= 1;
         ctl->pending_flip = 0;
     }
 }
@@ -463,9 +465,8 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
                     atomicAdd(&d.ctl->lost_history, 1u);
                     continue;
                 }
-                for (int comp = 0; comp < d.ncomp; ++comp)
-                    d.hist[nb][hist_at(d.ncap, d.ncomp, s, m[j]) + comp] =
-                        d.hist[hc][hist_at(d.ncap, d.ncomp, o, kk[j]) + comp];
+                // the spring stays where it is in the pool; the new entry points at it
+                d.hidx[nb][nbr_at(d.ncap, s, m[j])] = d.hidx[hc][nbr_at(d.ncap, o, kk[j])];
                 set_bit4(n0, n1, n2, n3, m[j]);
             }
         }
@@ -491,7 +492,7 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
 // ---------------------------------------------------------------------------
 // force + integration
 // ---------------------------------------------------------------------------
-// One spring record (hist_at / whist_at: 16-byte aligned, padded to an even
+// One spring record (pool_at / whist_at: 16-byte aligned, padded to an even
 // count) as 16-byte vectors.
 __device__ __forceinline__ void load_springs(const double* h, size_t base, int ncomp, Springs& s)
 {

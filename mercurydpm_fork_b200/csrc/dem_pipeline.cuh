@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
     __shared__ int kept_t[HIT_KEEP][BLOCK];
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     Control* ctl = d.ctl;
-    const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1;
+    const int c = ctl->cur, l = ctl->lbuf, nb = c ^ 1, pc = ctl->pcur;
     const bool first = (MODE == 1) && ctl->first_step;
     const bool active = s < d.n;
     // hit bits of the (at most 4) list words, in registers: each word is
@@ -258,10 +258,20 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
                         neww |= bit;
                     } else if (first && (aw & bit) && !(periodic && is.x > it.x)) {
                         // an interaction of the initial evaluation outlives step 0
-                        // (InteractionHandler::eraseOldInteractions erases stamps <= 0 only)
-                        for (int q = 0; q < NCOMP; ++q)
-                            d.hist[nb][hist_at(d.ncap, NCOMP, s, k) + q] = d.hist[c][hist_at(d.ncap, NCOMP, s, k) + q];
-                        neww |= bit;
+                        // (InteractionHandler::eraseOldInteractions erases stamps <= 0 only):
+                        // its spring moves to the top of the next pool, below which the
+                        // items of this evaluation stay (k_sum checks that they met no carry)
+                        const int top = d.item_cap - 1 - (int)atomicAdd(&ctl->n_carry, 1u);
+                        if (top >= 0) {
+                            const double2* from = reinterpret_cast<const double2*>(d.pool[pc] + pool_at(NCOMP, d.hidx[c][e]));
+                            double2* to = reinterpret_cast<double2*>(d.pool[pc ^ 1] + pool_at(NCOMP, top));
+#pragma unroll
+                            for (int q = 0; q < hist_stride(NCOMP) / 2; ++q) to[q] = from[q];
+                            d.hidx[nb][e] = top;
+                            neww |= bit;
+                        } else {
+                            atomicOr(&ctl->status, 1u << DEM_ERR_CAPACITY);
+                        }
                     }
                 }
             }
@@ -345,13 +355,20 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
 #pragma unroll
     for (int w = 0; w < 4; ++w) {
         unsigned int b = hits[w];
+        // the entry's spring of the last evaluation, where it had one, goes into
+        // the item (its pool index; -1: a new contact), and its spring of this
+        // evaluation will sit at the item's own index
+        const unsigned int aw = b ? d.act[c][(size_t)w * d.ncap + s] : 0u;
         while (b) {
             const int k = w * 32 + __ffs(b) - 1;
             b &= b - 1;
-            const int t = (nh_seen < HIT_KEEP) ? kept_t[nh_seen][threadIdx.x] : d.nbr[l][nbr_at(d.ncap, s, k)];
+            const size_t e = nbr_at(d.ncap, s, k);
+            const int t = (nh_seen < HIT_KEEP) ? kept_t[nh_seen][threadIdx.x] : d.nbr[l][e];
             ++nh_seen;
-            d.items[q] = make_int4(s, k, t, 0);
-            d.slot[nbr_at(d.ncap, s, k)] = q;
+            const int prev = ((aw >> (k & 31)) & 1u) ? d.hidx[c][e] : -1;
+            d.items[q] = make_int4(s, k, t, prev);
+            d.slot[e] = q;
+            d.hidx[nb][e] = q;
             ++q;
         }
     }
@@ -380,7 +397,7 @@ template <int MODE, int NLAW, int FLAW, int NCOMP, bool RECORD, int MINB = 4>
 __global__ void __launch_bounds__(CONTACT_BLOCK, MINB) k_contacts(DevPtrs d)
 {
     Control* ctl = d.ctl;
-    const int c = ctl->cur, nb = c ^ 1;
+    const int c = ctl->cur, nb = c ^ 1, pc = ctl->pcur;
     const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
     const bool record = RECORD && final_step && ctl->record;
     const bool first = (MODE == 1) && ctl->first_step;
@@ -446,9 +463,11 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, MINB) k_contacts(DevPtrs d)
             const size_t e = nbr_at(d.ncap, s, kq);
             tq = item.z;
             rv = d.rev[e];
-            hb = hist_at(d.ncap, NCOMP, s, kq);
-            Springs own; // read before the active bit is known: one less dependent load
-            load_springs(d.hist[c], hb, NCOMP, own);
+            hb = pool_at(NCOMP, q); // this evaluation's spring sits at the item's index
+            // the spring of the last evaluation (item.w; -1 for a new contact, whose
+            // record 0 is read and not used): read before anything else needs it
+            Springs own;
+            load_springs(d.pool[pc], pool_at(NCOMP, max(item.w, 0)), NCOMP, own);
             const double4 pt = d.pr[c][tq];
             const int4 it = d.info[c][tq];
             const double4 vt4 = d.vm[c][tq];
@@ -468,8 +487,8 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, MINB) k_contacts(DevPtrs d)
             g.curv_p = 1.0 / rq;
             g.curv_i = 1.0 / pt.w;
             g.i_is_wall = false;
-            hdst = d.hist[nb];
-            was_active = (d.act[c][(size_t)(kq >> 5) * d.ncap + s] >> (kq & 31)) & 1u;
+            hdst = d.pool[pc ^ 1];
+            was_active = item.w >= 0;
             // the higher-id side of a periodic pair restarts every step from the
             // reversed spring of the lower-id side (InteractionHandler.cc:316-368,
             // BaseInteraction::copySwitchPointer / reverseHistory)
@@ -477,7 +496,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, MINB) k_contacts(DevPtrs d)
             if (derived) {
                 const int m = rv;
                 if ((d.act[c][(size_t)(m >> 5) * d.ncap + tq] >> (m & 31)) & 1u) {
-                    load_springs(d.hist[c], hist_at(d.ncap, NCOMP, tq, m), NCOMP, spr);
+                    load_springs(d.pool[pc], pool_at(NCOMP, d.hidx[c][nbr_at(d.ncap, tq, m)]), NCOMP, spr);
                     spr.slide = -spr.slide; spr.roll = -spr.roll; spr.tors = -spr.tors;
                 }
             } else if (was_active) {
@@ -492,7 +511,7 @@ __global__ void __launch_bounds__(CONTACT_BLOCK, MINB) k_contacts(DevPtrs d)
         // that side is not derived and was active, so its old spring is its own
         // stored one, read again here instead of kept in registers
         Springs kept = spr;
-        if (first && periodic && !(is.x > pid_i) && was_active) load_springs(d.hist[c], hb, NCOMP, kept);
+        if (first && periodic && !(is.x > pid_i) && was_active) load_springs(d.pool[pc], pool_at(NCOMP, item.w), NCOMP, kept);
         store_springs(hdst, hb, NCOMP, kept);
         // shares as 16-byte stores (96-byte items: every item and half is 16-byte aligned)
         double2* sh = reinterpret_cast<double2*>(d.shares + (size_t)q * SHARE);
@@ -749,6 +768,11 @@ __global__ void __launch_bounds__(BLOCK, SUM_THREADS_PER_SM / BLOCK) k_sum(DevPt
     const bool final_step = (MODE == 0) ? true : (ctl->final_step != 0);
     const double dt = d.dt;
     if (s == 0) { // k_contacts and k_tri are done: the next evaluation starts new lists
+        // the springs kept at the pool top in the first time step must not have
+        // met this evaluation's items
+        if (ctl->n_carry && (unsigned long long)ctl->n_items + ctl->n_carry > (unsigned long long)d.item_cap)
+            atomicOr(&ctl->status, 1u << DEM_ERR_CAPACITY);
+        ctl->n_carry = 0u;
         ctl->n_items = 0u;
         ctl->n_tri = 0u;
     }

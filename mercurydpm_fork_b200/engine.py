@@ -180,7 +180,7 @@ class DemEngine:
     def __init__(self, time_step: float, instances: list[Instance], species: list[_abi.SpeciesPair],
                  walls: list[_abi.Wall] | None = None, rotation: bool = True, background_drag: float = 0.0,
                  max_neighbors: int = 0, skin: float = 0.0, use_graphs: bool = True, device: int = 0,
-                 deletions: list | None = None, batch_api: bool = False):
+                 deletions: list | None = None, batch_api: bool = False, max_contacts: int = 0):
         self._h = C.c_void_p()
         cfg = _abi.Config()
         cfg.time_step = time_step
@@ -191,6 +191,7 @@ class DemEngine:
         cfg.use_graphs = 1 if use_graphs else 0
         cfg.skin = skin
         cfg.n_instances = len(instances)
+        cfg.max_contacts = max_contacts
         arr = (_abi.InstanceDesc * len(instances))(*[i.to_c() for i in instances])
         if batch_api:
             rc = lib().dem_batch_create(C.byref(cfg), len(instances), arr, C.byref(self._h))
@@ -459,3 +460,11 @@ class DemEngine:
         self._check(lib().dem_get_info(self._h, C.byref(n), C.byref(cap), C.byref(cells)))
         return dict(ms=ms.value, kernel_launches=launches.value, rebuilds=rebuilds.value, n=n.value,
                     max_neighbors=cap.value, n_cells=cells.value)
+
+    def memory(self) -> dict:
+        """Device bytes held by the handle's arrays and the contact capacity
+        (items of one evaluation) the spring storage was sized for."""
+        b = C.c_int64(0)
+        cap = C.c_int64(0)
+        self._check(lib().dem_get_memory(self._h, C.byref(b), C.byref(cap)))
+        return dict(device_bytes=b.value, contact_capacity=cap.value)

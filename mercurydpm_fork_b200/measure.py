@@ -3,9 +3,10 @@
     python -m mercurydpm_fork_b200.measure chute       # 200k periodic chute, linear + sliding friction, 2 HGrid levels
     python -m mercurydpm_fork_b200.measure drum        # 1M-sphere rotating drum, Hertz-Mindlin (loose start)
     python -m mercurydpm_fork_b200.measure drum_dense  # the same drum started as a touching lattice bed
-    python -m mercurydpm_fork_b200.measure heaps       # 1,024 batched calibration heaps
+    python -m mercurydpm_fork_b200.measure heaps       # 4,096 calibration heaps in one handle (steps=40000: the whole run)
     python -m mercurydpm_fork_b200.measure surrogate   # MLP inference / training on the tensor cores
     python -m mercurydpm_fork_b200.measure calibration # calibrations per hour at 2 % response error
+    python -m mercurydpm_fork_b200.measure c5          # wall time to 2 %: surrogate-guided / plain batched DEM
     python -m mercurydpm_fork_b200.measure cg          # Gaussian CG of the 200k chute (XZ 100 x 1 x 50)
     python -m mercurydpm_fork_b200.measure triangles   # 200k spheres settling on a 32-triangle mesh floor
 
@@ -75,16 +76,44 @@ def drum_dense():
     return drum(site_spacing=0.999, workload="rotating_drum_dense_bed")
 
 
-def heaps(n_instances=1024, seed=1):
+def heaps(n_instances=4096, seed=1, steps=0, max_contacts=6):
+    """The calibration batch of heaps in ONE engine handle: n_instances heaps
+    of U[500, 8000] spheres (17.4M spheres for 4,096), each with its own
+    floor, deletion plane and species. Spring history is stored per contact,
+    sized by max_contacts per sphere (a settled heap has about 3). With
+    steps = 0: throughput over 1,000 steps of the pouring phase; with
+    steps > 0: the whole run of that many steps (40,000 for the heap
+    procedure), device time summed over its dem_step calls, then the per-heap
+    outputs. Reports the device memory the handle holds."""
     from . import calibration as cal
+    n_instances, seed, steps, max_contacts = int(n_instances), int(seed), int(steps), int(max_contacts)
     t0 = time.perf_counter()
     b, params, R = cal.heap_batch(n_instances, seed=seed)
     t1 = time.perf_counter()
-    e = b.engine()
-    out = _time_dem(e, b.n, steps_per_call=200, calls=5)
-    e.close()
+    e = b.engine(max_contacts=max_contacts)
+    mem = e.memory()
+    if steps > 0:
+        t2 = time.perf_counter()
+        res = cal.run_heaps(b, R, steps=steps, engine=e)
+        wall = time.perf_counter() - t2
+        counts = e.counts()
+        e.close()
+        ms = res["device_ms"]
+        aor = res["aor_reference"]
+        out = dict(value=b.n * steps / (ms / 1e3), unit="particle-timesteps/s", steps=steps,
+                   ms_per_time_step=ms / steps, wall_s=wall, device_s=ms / 1e3,
+                   heaps_per_hour=n_instances * 3600.0 / wall,
+                   aor_reference_deg=dict(median=float(np.nanmedian(aor)), min=float(np.nanmin(aor)),
+                                          max=float(np.nanmax(aor)), finite=int(np.isfinite(aor).sum())),
+                   remaining_fraction=float(res["n_remaining"].sum() / b.n), counts=counts)
+    else:
+        out = _time_dem(e, b.n, steps_per_call=200, calls=5)
+        out["counts"] = e.counts()
+        e.close()
     out.update(workload="calibration_heaps", instances=n_instances, n_total=b.n, build_s=t1 - t0,
-               instance_timesteps_per_s=out["value"] / b.n * n_instances)
+               instance_timesteps_per_s=out["value"] / b.n * n_instances, device_bytes=mem["device_bytes"],
+               device_bytes_per_sphere=mem["device_bytes"] / b.n, contact_capacity=mem["contact_capacity"],
+               max_contacts=max_contacts)
     return out
 
 
@@ -153,6 +182,61 @@ def calibration(n_train=2048, n_targets=16, tol=0.02, rounds=4, proposals=256, s
                 heap="600 spheres, 20,000 steps, lognormal PSD, rough floor disk (calibration.heap_responses)")
 
 
+def c5(n=2000, steps=40_000, n_train=2048, n_targets=16, tol=0.02, proposals=256, rounds=4, plain_rounds=12,
+       seed=3, chunk=4096):
+    """The surrogate claim as a wall-time ratio: the same held-out targets
+    (responses of DEM heaps at parameters drawn from the box) calibrated to
+    `tol` twice on this GPU, timed host to host --
+      surrogate-guided: the training heaps (n_train DEM runs), the network's
+      training, then calibration.calibrate_batch with the surrogate;
+      plain: calibration.calibrate_batch without it (every round uniform
+      proposals judged by batched DEM), up to plain_rounds rounds.
+    Every heap has n spheres (a calibration campaign fixes the sample size;
+    C4's heaps range over U[500, 8000]) and runs `steps` time steps; a
+    round's proposals for all targets are one batched DEM call. ratio =
+    surrogate-guided seconds / plain seconds (if the plain search stopped at
+    its round cap before every target reached tol, its time is a lower bound
+    and the ratio an upper one)."""
+    from . import calibration as cal
+    from .surrogate import Surrogate
+    n, steps, n_train, n_targets, proposals = int(n), int(steps), int(n_train), int(n_targets), int(proposals)
+    rounds, plain_rounds, seed, chunk, tol = int(rounds), int(plain_rounds), int(seed), int(chunk), float(tol)
+    dem = lambda p: cal.heap_responses(p, n=n, steps=steps, chunk=chunk)
+    rng = np.random.default_rng(seed)
+    pt = cal.sample_params(rng, n_targets)
+    targets = dem(pt)
+    # surrogate-guided
+    t0 = time.perf_counter()
+    x = cal.sample_params(rng, n_train)
+    y = dem(x)
+    t_data = time.perf_counter() - t0
+    s = Surrogate(capacity=65536, seed=0)
+    s.fit_normalisation(x, y)
+    s.fit(x, y, epochs=200, batch=1024)
+    t_train = time.perf_counter() - t0 - t_data
+    res_s = cal.calibrate_batch(targets, dem, s, rounds=rounds, proposals=proposals, candidates=65_536, tol=tol,
+                                seed=seed, data=(x, y))
+    t_surr = time.perf_counter() - t0
+    s.close()
+    # plain batched DEM
+    t0 = time.perf_counter()
+    res_p = cal.calibrate_batch(targets, dem, None, rounds=plain_rounds, proposals=proposals, tol=tol, seed=seed + 1)
+    t_plain = time.perf_counter() - t0
+    ok_s = [r["best_error"] <= tol for r in res_s]
+    ok_p = [r["best_error"] <= tol for r in res_p]
+    return dict(workload="calibration_c5", metric="wall-time ratio, surrogate-guided / plain batched DEM",
+                value=t_surr / t_plain, tol=tol, targets=n_targets, heap_spheres=n, heap_steps=steps,
+                proposals_per_round=proposals,
+                surrogate=dict(seconds=t_surr, training_data_s=t_data, training_s=t_train, succeeded=int(sum(ok_s)),
+                               rounds=[r["rounds"] for r in res_s],
+                               dem_runs=n_train + sum(r["dem_runs"] for r in res_s),
+                               best_errors=[round(r["best_error"], 5) for r in res_s]),
+                plain=dict(seconds=t_plain, succeeded=int(sum(ok_p)), rounds=[r["rounds"] for r in res_p],
+                           dem_runs=sum(r["dem_runs"] for r in res_p), round_cap=plain_rounds,
+                           best_errors=[round(r["best_error"], 5) for r in res_p]),
+                plain_time_is_lower_bound=not all(ok_p))
+
+
 def cg(reps=10, steps_between=1000):
     """Gaussian coarse-graining of the 200k periodic chute on an XZ grid of
     100 x 1 x 50 points, width one small diameter, cutoff 3 widths (the
@@ -209,5 +293,5 @@ if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "drum"
     kwargs = dict(a.split("=", 1) for a in sys.argv[2:])  # e.g. triangles n=20000 settle_steps=2000
     fn = dict(chute=chute, drum=drum, drum_dense=drum_dense, heaps=heaps, surrogate=surrogate, calibration=calibration,
-              cg=cg, triangles=triangles)[which]
+              c5=c5, cg=cg, triangles=triangles)[which]
     print(json.dumps(fn(**kwargs)))

@@ -360,3 +360,32 @@ def drum_with_law(law: str, n: int = 600, seed: int = 5):
     sp = species_pair(**table)
     dt = 2e-6 if law.startswith("linear") else sc.time_step
     return dataclasses.replace(sc, name=f"drum_{law}", species=[sp] * len(sc.species), time_step=dt)
+
+
+def recontact(owner_first: bool = True, vy: float = 0.1):
+    """Sphere P starts just touching the fixed sphere I (overlap 1e-5) while
+    moving away from it, with a tangential velocity vy, so the initial
+    evaluation builds a sliding spring. In the first time step P leaves I and
+    runs into the fixed sphere J, which throws it back onto I in the second.
+    The reference keeps the interaction of the initial evaluation through the
+    first time step although nothing touches it then (its time stamp is that
+    of the first step, InteractionHandler::eraseOldInteractions), so the
+    second step's contact continues from that spring. owner_first: P has the
+    lower id of the pair (it owns the pair's spring)."""
+    from mercurydpm_fork_b200 import _abi
+    from mercurydpm_fork_b200.engine import species_pair
+    sp = species_pair(normal_law=_abi.DEM_NORMAL_LINEAR_VISCOELASTIC, friction_law=_abi.DEM_FRICTION_SLIDING,
+                      stiffness=4e6, dissipation=10.0, sliding_stiffness=4e6 * 2 / 7, sliding_dissipation=0.0,
+                      sliding_mu=1e20, sliding_mu_static=1e20)
+    density = 6.0 / PI  # unit mass for r = 0.5
+    delta = 1e-5
+    pos = np.array([[1.0 - delta, 0.0, 0.0], [0.0, 0.0, 0.0], [2.0 - delta, 0.0, 0.0]]) + 5.0
+    vel = np.array([[1.0, vy, 0.0], [0.0, 0.0, 0.0], [0.0, 0.0, 0.0]])
+    radius = np.full(3, 0.5)
+    inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
+    inv_mass[1:] = 0.0
+    inv_inertia[1:] = 0.0
+    ids = np.array([0, 1, 2] if owner_first else [2, 0, 1], np.int32)
+    inst = Instance(domain_min=(0, 0, 0), domain_max=(10, 10, 10), gravity=(0, 0, 0), n_species=1)
+    return Scenario("recontact", 1e-3, inst, [sp], np.array([density]), [], pos, vel, radius, inv_mass, inv_inertia,
+                    np.zeros(3, np.int32), ids)

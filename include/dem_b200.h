@@ -281,8 +281,17 @@ int  dem_set_walls(dem_handle *h, const dem_wall *walls, int n);
  * dem_instance_desc's periodic_*; before dem_upload_particles. */
 int  dem_set_periodic(dem_handle *h, int instance, const double lo[3], const double hi[3], uint32_t mask);
 /* DeletionBoundary objects of BoundaryHandler, at most
- * DEM_MAX_DELETION_PER_INSTANCE per instance (before dem_upload_particles). */
+ * DEM_MAX_DELETION_PER_INSTANCE per instance. Before dem_upload_particles, or
+ * between dem_step calls (BoundaryHandler::copyAndAddObject during a run, as
+ * Drivers/Calibration/CalibrationHeap.cpp:128-131 does): the set replaces the
+ * previous one and applies from the next time step. */
 int  dem_set_deletion_boundaries(dem_handle *h, const dem_deletion_boundary *b, int n);
+/* WallHandler::removeObject / removeLastObject (Kernel/BaseHandler.h:131-136),
+ * wall = index in the dem_set_walls array: no contacts with the wall from the
+ * next time step on, its contacts' history dropped (as the removed wall's
+ * interactions are). Before the upload or between dem_step calls; not for
+ * triangle walls. */
+int  dem_remove_wall(dem_handle *h, int wall);
 /* ParticleHandler contents; triggers the first force evaluation on the next
  * dem_step (the one DPMBase::initialiseSolve performs, DPMBase.cc:4180). */
 int  dem_upload_particles(dem_handle *h, const dem_particles_soa *p);

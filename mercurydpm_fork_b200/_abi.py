@@ -150,6 +150,7 @@ _SIGNATURES = {
     "dem_last_step_stats": (C.c_int, [C.c_void_p, _pd, C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_get_info": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_get_memory": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64)]),
+    "dem_remove_wall": (C.c_int, [C.c_void_p, C.c_int]),
     "dem_get_counts": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_time_force_kernel": (C.c_int, [C.c_void_p, C.c_int, _pd]),
     "dem_selftest_wait_expiry": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_uint32)]),

@@ -104,6 +104,126 @@ def heap_scenario(p: HeapParams, d50: float = 1e-3, density: float = 2000.0, tc:
     return sc, [((0, 0, -1), 0.0)], R  # DeletionBoundary set({0,0,-1}, 0): z < 0 leaves
 
 
+def heap_species_cased(tc: float, eps: float, mass_min: float, mu: float, mu_r: float) -> list:
+    """Species table of a heap poured inside a casing, as Calibration::
+    setSpecies builds it (Calibration.h:147-186): 0 = particles, 1 = the
+    casing's frictionless wall species (mixed sliding and rolling friction 0),
+    2 = the floor's frictional wall species (mixed rolling friction
+    max(1, sliding), sliding max(1, rolling))."""
+    k, g = linear_collision_time_restitution(tc, eps, mass_min)
+
+    def sp(mu_s, mu_roll):
+        return species_pair(normal_law=_abi.DEM_NORMAL_LINEAR_VISCOELASTIC, friction_law=_abi.DEM_FRICTION_ROLLING_TORSION,
+                            stiffness=k, dissipation=g,
+                            sliding_stiffness=2. / 7. * k, sliding_dissipation=2. / 7. * g,
+                            sliding_mu=mu_s, sliding_mu_static=mu_s,
+                            rolling_stiffness=2. / 5. * k, rolling_dissipation=2. / 5. * g,
+                            rolling_mu=mu_roll, rolling_mu_static=mu_roll,
+                            torsion_stiffness=2. / 5. * k, torsion_dissipation=2. / 5. * g,
+                            torsion_mu=0.0, torsion_mu_static=0.0)
+    pp = sp(mu, mu_r)
+    smooth = sp(0.0, 0.0)
+    rough = sp(max(1.0, mu_r), max(1.0, mu))
+    return [pp, smooth, rough,
+            smooth, pp, pp,
+            rough, pp, pp]
+
+
+def cased_heap_scenario(p: HeapParams, d50: float = 1e-3, density: float = 2000.0, tc: float = 5e-4,
+                        base_radius_d: float = 7.5, spacing: float = 1.05):
+    """The set-up of Drivers/Calibration/CalibrationHeap.cpp (GranuHeap,
+    CalibrationHeap.cpp:70-115) for one heap: spheres in a column of radius
+    R_base inside the frictionless casing (AxisymmetricIntersectionOfWalls,
+    face (1, 0, 0) at R_base), standing on the frictional floor disk (faces
+    (-1, 0, 0) at R_base and (0, 0, -1) at 0), time step 0.05 collision
+    times. The reference fills the column by random insertion
+    (CubeInsertionBoundary); here the column is a seeded jittered lattice.
+    Returns (Scenario, R_base); wall 1 is the casing."""
+    rng = np.random.Generator(np.random.PCG64(p.seed))
+    radius = lognormal_radii(rng, p.n, p.sigma, 0.5 * d50)
+    R = base_radius_d * d50
+    s = spacing * 2.0 * radius.max()
+    m = int(R // s) + 1
+    g = np.arange(-m, m + 1) * s
+    X, Y = np.meshgrid(g, g, indexing="ij")
+    keep = np.hypot(X, Y) <= R - 0.5 * s
+    layer = np.stack([X[keep], Y[keep]], 1)
+    nl = len(layer)
+    layers = (p.n + nl - 1) // nl
+    sites = np.concatenate([np.column_stack([layer, np.full(nl, (k + 0.5) * s + 0.5 * s)]) for k in range(layers)])
+    pos = sites[: p.n] + rng.uniform(-0.02 * s, 0.02 * s, size=(p.n, 3))
+    pos = pos[rng.permutation(p.n)]
+    mass_min = 4.0 / 3.0 * PI * radius.min() ** 3 * density
+    species = heap_species_cased(tc, p.restitution, mass_min, p.mu, p.mu_r)
+    inv_mass, inv_inertia = sphere_inv_mass_inertia(radius, density)
+    top = float(pos[:, 2].max()) + 4 * radius.max()
+    inst = Instance(domain_min=(-R - 4 * d50, -R - 4 * d50, -2 * d50), domain_max=(R + 4 * d50, R + 4 * d50, top),
+                    gravity=(0.0, 0.0, -9.8), n_species=3)
+    floor = axisymmetric_wall((0, 0, 1), [((-1, 0, 0), (R, 0, 0)), ((0, 0, -1), (0, 0, 0))], species=2)
+    casing = axisymmetric_wall((0, 0, 1), [((1, 0, 0), (R, 0, 0))], species=1)
+    sc = Scenario("cased_heap", 0.05 * tc, inst, species, np.array([density] * 3), [floor, casing], pos,
+                  np.zeros((p.n, 3)), radius, inv_mass, inv_inertia, np.zeros(p.n, np.int32),
+                  np.arange(p.n, dtype=np.int32), info=dict(params=p, base_radius=R))
+    return sc, R
+
+
+def heap_procedure(sc: Scenario, R: float, casing: int = 1, check_every: int = 1000, max_steps: int = 400_000,
+                   engine=None) -> dict:
+    """Drivers/Calibration/CalibrationHeap.cpp's run (GranuHeap::
+    actionsAfterTimeStep, CalibrationHeap.cpp:119-160) on the engine: every
+    `check_every` time steps the reference's hook values -- the time before
+    the step's increment, the translational kinetic energy at the step's
+    half-kick velocities v - F dt / 2m, the elastic energy of the step's
+    contacts -- decide: at the first quiet check (kinetic < 1e-2 elastic) the
+    casing is removed and a DeletionBoundary z < 0 added between the steps;
+    from twice that time on, every quiet check measures the angle of repose
+    atan(4 COM_z / R_base) and the first one ends the run 0.05 s later. (The
+    reference keeps the removal time in an uninitialised local variable; the
+    time the casing was removed is what its code intends.) Returns the angle
+    of repose, the removal and end times and the particles left."""
+    from .engine import deletion_boundary
+    e = engine if engine is not None else sc.engine()
+    dt = sc.time_step
+    e.step(0)
+    fill, first, removal, aor = True, True, 0.0, float("nan")
+    # DPMBase::solve steps while time < timeMax, time accumulated step by
+    # step (time_ += timeStep_); the hook sees the time before the increment
+    t_max, steps, time_ = float("inf"), 0, 0.0
+    while time_ < t_max and steps < max_steps:
+        k, t = 0, time_
+        while k < check_every - steps % check_every and time_ < t_max:
+            t = time_
+            time_ += dt
+            k += 1
+        e.step(k)
+        steps += k
+        if steps % check_every:
+            continue
+        st = e.download()
+        f, _ = e.forces()
+        alive = st["instance"] >= 0
+        im = sc.inv_mass[alive]
+        vmid = st["velocity"][alive] - f[alive] * (im * 0.5 * dt)[:, None]
+        ke = float(np.sum(0.5 / im * np.sum(vmid * vmid, axis=1)))
+        g = e.reduce()
+        ee = g["elastic_energy"]
+        if fill:
+            if ke < 1e-2 * ee:
+                fill, removal = False, t
+                e.remove_wall(casing)
+                e.set_deletion_boundaries([deletion_boundary((0, 0, -1), 0.0)])
+        elif t > 2.0 * removal and ke < 1e-2 * ee:
+            aor = math.degrees(math.atan(4.0 * g["centre_of_mass"][2] / R))
+            if first:
+                t_max, first = t + 0.05, False
+    st = e.download()
+    g = e.reduce()
+    if engine is None:
+        e.close()
+    return dict(aor=aor, removal_time=removal, end_time=time_, steps=steps,
+                n_remaining=int((st["instance"] >= 0).sum()), com_z=float(g["centre_of_mass"][2]))
+
+
 def heap_batch(n_instances: int, seed: int = 1, n_range=(500, 8000), sigma_range=(0.0, 0.2), mu_range=(0.1, 0.8),
                mu_r_range=(0.0, 0.3), e_range=(0.3, 0.9), **kw):
     """Batch of heap instances with parameters drawn uniformly from the given

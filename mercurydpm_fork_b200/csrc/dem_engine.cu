@@ -35,6 +35,7 @@ struct Handle {
     std::vector<int> wall_caller;      // grouped index -> caller index
     std::vector<int> wall_grouped;     // caller index -> grouped index
     std::vector<dem_deletion_boundary> deletions;
+    std::vector<char> wall_removed;    // per wall (grouped order): taken out by dem_remove_wall
     std::string err;
     int device = 0;
     cudaStream_t stream = nullptr, stream2 = nullptr;
@@ -506,14 +507,53 @@ int dem_set_walls(dem_handle* hh, const dem_wall* walls, int n)
     h->wgeom = std::move(g);
     h->wall_caller = std::move(order);
     h->wall_grouped = std::move(grouped);
+    h->wall_removed.assign(n, 0);
     return DEM_OK;
+}
+
+// DeletionBoundary planes of instance `in` (DeletionBoundary::set normalises,
+// DeletionBoundary.cc:86-91).
+static void fill_deletions(const Handle* h, InstanceDev& I, int in)
+{
+    I.n_del = 0;
+    for (const auto& db : h->deletions)
+        if (db.instance == in) {
+            const double sf = 1. / std::sqrt(db.normal[0] * db.normal[0] + db.normal[1] * db.normal[1] +
+                                             db.normal[2] * db.normal[2]);
+            for (int a = 0; a < 3; ++a) I.del_n[I.n_del][a] = db.normal[a] * sf;
+            I.del_d[I.n_del] = db.distance * sf;
+            ++I.n_del;
+        }
+}
+
+// The instance table changed between steps: the next launches read the new one.
+static int push_instances(Handle* h)
+{
+    CU(cudaSetDevice(h->device));
+    CU(cudaMemcpyAsync(h->d_inst, h->inst.data(), h->inst.size() * sizeof(InstanceDev), cudaMemcpyHostToDevice,
+                       h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return DEM_OK;
+}
+
+int dem_remove_wall(dem_handle* hh, int wall)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || wall < 0 || wall >= (int)h->walls.size()) return fail(h, DEM_ERR_BAD_INPUT, "dem_remove_wall: no such wall");
+    const int g = h->wall_grouped[wall];
+    if (h->walls[g].type == DEM_WALL_TRIANGLE)
+        return fail(h, DEM_ERR_BAD_INPUT, "dem_remove_wall: triangle walls cannot be taken out");
+    h->wall_removed[g] = 1;
+    if (!h->uploaded) return DEM_OK; // applied when the particles are uploaded
+    const int in = h->walls[g].instance;
+    h->inst[in].wall_off_mask |= 1u << (g - h->inst[in].wall_begin);
+    return push_instances(h);
 }
 
 int dem_set_deletion_boundaries(dem_handle* hh, const dem_deletion_boundary* b, int n)
 {
     Handle* h = reinterpret_cast<Handle*>(hh);
     if (!h || n < 0 || (n > 0 && !b)) return fail(h, DEM_ERR_BAD_INPUT, "dem_set_deletion_boundaries: bad arguments");
-    if (h->uploaded) return fail(h, DEM_ERR_STATE, "dem_set_deletion_boundaries must come before dem_upload_particles");
     std::vector<int> per(h->inst_desc.size(), 0);
     for (int k = 0; k < n; ++k) {
         if (b[k].instance < 0 || b[k].instance >= (int)h->inst_desc.size())
@@ -527,7 +567,11 @@ int dem_set_deletion_boundaries(dem_handle* hh, const dem_deletion_boundary* b, 
         if (!finite || !(l2 > 0.0)) return fail(h, DEM_ERR_BAD_INPUT, "bad deletion boundary");
     }
     h->deletions.assign(b, b + n);
-    return DEM_OK;
+    if (!h->uploaded) return DEM_OK;
+    // during the run (BoundaryHandler::copyAndAddObject between time steps):
+    // the planes apply from the next drift on
+    for (int in = 0; in < (int)h->inst.size(); ++in) fill_deletions(h, h->inst[in], in);
+    return push_instances(h);
 }
 
 int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
@@ -633,6 +677,9 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         I.tri_mask = 0u;
         I.tri_static = 1;
         I.wall_still_mask = 0u;
+        I.wall_off_mask = 0u;
+        for (int w = wbegin[in]; w < wend[in]; ++w)
+            if (h->wall_removed[w]) I.wall_off_mask |= 1u << (w - wbegin[in]);
         for (int w = wbegin[in]; w < wend[in]; ++w) {
             const dem_wall& x = h->walls[w];
             if (x.type == DEM_WALL_TRIANGLE) continue;
@@ -661,15 +708,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
                 I.tri_hi[k] = std::max(I.tri_hi[k], h->wgeom[w].thi[k]);
             }
         }
-        I.n_del = 0;
-        for (const auto& db : h->deletions)
-            if (db.instance == in) { // DeletionBoundary::set normalises (DeletionBoundary.cc:86-91)
-                const double sf = 1. / std::sqrt(db.normal[0] * db.normal[0] + db.normal[1] * db.normal[1] +
-                                                 db.normal[2] * db.normal[2]);
-                for (int a = 0; a < 3; ++a) I.del_n[I.n_del][a] = db.normal[a] * sf;
-                I.del_d[I.n_del] = db.distance * sf;
-                ++I.n_del;
-            }
+        fill_deletions(h, I, in);
         std::vector<int> lv_multi;
         std::vector<int>& lv = one ? h->level_buf : lv_multi;
         const double* rad = one ? p->radius : radii[in].data();

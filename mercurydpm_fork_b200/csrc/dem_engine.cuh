@@ -66,6 +66,9 @@ struct InstanceDev {
     // rebuild records which of them are within reach + skin of a particle
     // (wcand); k_detect tests the others not at all until the next rebuild
     uint32_t wall_still_mask;
+    // walls (same bits) taken out during the run (WallHandler::removeObject):
+    // no contacts with them from the next time step on
+    uint32_t wall_off_mask;
     int tri_static;        // every triangle wall of the instance stands still: tri_lo/hi hold
     double tri_lo[3], tri_hi[3]; // the bounding box of all their vertices
     double del_n[DEM_MAX_DELETION_PER_INSTANCE][3];

@@ -292,7 +292,8 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
                            (xs.x > I.tri_lo[0] - R && xs.x < I.tri_hi[0] + R && xs.y > I.tri_lo[1] - R &&
                             xs.y < I.tri_hi[1] + R && xs.z > I.tri_lo[2] - R && xs.z < I.tri_hi[2] + R);
             }
-            const unsigned int far_still = I.wall_still_mask & ~d.wcand[l][s];
+            // farther than reach + skin at the last rebuild, or taken out
+            const unsigned int far_still = (I.wall_still_mask & ~d.wcand[l][s]) | I.wall_off_mask;
             for (int w = 0; w < nwalls; ++w) {
                 const int wg = I.wall_begin + w;
                 const unsigned int bit = 1u << w;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
                     }
                 } else {
                     d.slotw[(size_t)w * d.ncap + s] = SLOT_NONE;
-                    if (far_still & bit) { // farther than reach + skin at the last rebuild
+                    if (far_still & bit) {
                         hit = false;
                     } else {
                         const dem_wall& wall = d.walls[wg];
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
                 }
                 if (hit) {
                     wnew |= bit;
-                } else if (first && (wa & bit)) {
+                } else if (first && (wa & bit) && !(I.wall_off_mask & bit)) {
                     for (int q = 0; q < hist_stride(NCOMP); ++q) // with a triangle contact's creation key
                         d.whist[nb][whist_at(d.ncap, NCOMP, s, w) + q] = d.whist[c][whist_at(d.ncap, NCOMP, s, w) + q];
                     wnew |= bit;

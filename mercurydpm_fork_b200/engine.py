@@ -213,6 +213,17 @@ class DemEngine:
         self._check(lib().dem_set_deletion_boundaries(self._h, da, len(dels)))
         self.n = 0
 
+    def set_deletion_boundaries(self, deletions: list):
+        """Replaces the DeletionBoundary planes; between steps they apply from
+        the next time step (BoundaryHandler::copyAndAddObject during a run)."""
+        da = (_abi.DeletionBoundary * max(1, len(deletions)))(*deletions)
+        self._check(lib().dem_set_deletion_boundaries(self._h, da, len(deletions)))
+
+    def remove_wall(self, wall: int):
+        """WallHandler::removeObject: wall `wall` (index in the constructor's
+        list) makes no contacts from the next time step on."""
+        self._check(lib().dem_remove_wall(self._h, int(wall)))
+
     # ------------------------------------------------------------------
     def _check(self, rc: int):
         if rc:

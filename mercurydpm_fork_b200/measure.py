@@ -245,6 +245,7 @@ def cg(reps=10, steps_between=1000):
     interval."""
     from . import scenarios
     from ._abi import DEM_CG_XZ
+    reps, steps_between = int(reps), int(steps_between)
     sc = scenarios.periodic_chute(n_flow=200_000, seed=2, packing="layers", spacing_factor=1.0)
     e = sc.engine()
     e.step(0)

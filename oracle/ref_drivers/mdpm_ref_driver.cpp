@@ -19,6 +19,13 @@ extern "C" {
 
 // DeletionBoundary planes for the following runs (instance field ignored).
 void mdpm_ref_set_deletion(const dem_deletion_boundary* b, int n) { g_deletions.assign(b, b + n); }
+// the between-steps change of the next mdpm_ref_run (step < 0: none)
+void mdpm_ref_set_event(long long step, int wall, const dem_deletion_boundary* b, int n)
+{
+    g_event_step = step;
+    g_event_wall = wall;
+    g_event_deletions.assign(b, b + n);
+}
 
 } // extern "C"
 
@@ -34,7 +41,10 @@ int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem
     RefDriver d;
     setup(d, cfg, inst, species, density, walls, nwalls, in, 1);
     d.initialiseSolve();
-    for (int k = 0; k < nsteps; ++k) d.computeOneTimeStep();
+    for (int k = 0; k < nsteps; ++k) {
+        d.computeOneTimeStep();
+        apply_event(d, k + 1);
+    }
     const int64_t n = in->n;
     // deleted particles leave the handler (and reorder it): rows are matched by
     // id, which the tests set to the caller index; rows of deleted particles
@@ -349,6 +359,70 @@ int mdpm_ref_time_window(const dem_config* cfg, const dem_instance_desc* inst, c
     const auto t1 = std::chrono::steady_clock::now();
     *seconds = std::chrono::duration<double>(t1 - t0).count();
     *interactions_end = (int64_t)d.interactionHandler.getNumberOfObjects();
+    return 0;
+}
+
+} // extern "C"
+
+extern "C" {
+
+// The procedure of Drivers/Calibration/CalibrationHeap.cpp (GranuHeap::
+// actionsAfterTimeStep, CalibrationHeap.cpp:119-160) on the reference
+// Kernel, for a heap set up by the caller: a fill stage inside the casing
+// (wall `casing`, the last one), then, at the first check with kinetic
+// energy below 1e-2 of the elastic energy, the casing is removed and a
+// DeletionBoundary z < 0 added; from twice that time on, the first quiet
+// check gives the angle of repose atan(4 COM_z / R_base) and ends the run
+// 0.05 s later, every quiet check until then measuring it again. Checks
+// come every `check_every` time steps, as in the reference (every 1000th).
+// The reference keeps the removal time in an uninitialised local variable
+// (`double fillTime;`, read at a later call); this restatement uses the time
+// the casing was removed, which is what the code intends.
+// out: [angle of repose (deg, NaN if never measured), removal time, end time,
+//       time steps, particles left, centre of mass z]
+int mdpm_ref_heap_procedure(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
+                            const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in,
+                            int casing, double base_radius, int check_every, long long max_steps, int threads,
+                            double* out)
+{
+    RefDriver d;
+    setup(d, cfg, inst, species, density, walls, nwalls, in, threads);
+    bool fill = true, first_aor = true;
+    double removal_time = 0.0, aor = std::nan("");
+    long long count = 0;
+    d.setTimeMax(1e300);
+    d.after_step = [&]() {
+        if (++count % check_every) return;
+        const double ke = d.getKineticEnergy(), ee = d.getElasticEnergy();
+        if (fill) {
+            if (ke < 1e-2 * ee) {
+                fill = false;
+                removal_time = d.getTime();
+                d.wallHandler.removeObject((unsigned)casing);
+                DeletionBoundary b;
+                b.set(Vec3D(0, 0, -1), 0);
+                d.boundaryHandler.copyAndAddObject(b);
+            }
+        } else if (d.getTime() > 2.0 * removal_time && ke < 1e-2 * ee) {
+            aor = std::atan(4.0 * d.getCentreOfMass().Z / base_radius) * 180.0 / constants::pi;
+            if (first_aor) {
+                d.setTimeMax(d.getTime() + 0.05);
+                first_aor = false;
+            }
+        }
+    };
+    d.initialiseSolve();
+    long long steps = 0;
+    while (d.getTime() < d.getTimeMax() && steps < max_steps) {
+        d.computeOneTimeStep();
+        ++steps;
+    }
+    out[0] = aor;
+    out[1] = removal_time;
+    out[2] = d.getTime();
+    out[3] = (double)steps;
+    out[4] = (double)d.particleHandler.getSize();
+    out[5] = d.particleHandler.getSize() ? d.getCentreOfMass().Z : std::nan("");
     return 0;
 }
 

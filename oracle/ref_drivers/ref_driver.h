@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <sstream>
 #include <vector>
 #include "Boundaries/DeletionBoundary.h"
@@ -45,6 +46,26 @@ namespace {
 
 
 std::vector<dem_deletion_boundary> g_deletions; // DeletionBoundary planes of the next run
+
+// A change between two time steps of the next run (as a driver's
+// actionsAfterTimeStep makes it, e.g. Drivers/Calibration/CalibrationHeap.cpp:
+// 119-131): after step g_event_step, wall g_event_wall (handler index, -1:
+// none) is removed and the planes g_event_deletions are added.
+long long g_event_step = -1;
+int g_event_wall = -1;
+std::vector<dem_deletion_boundary> g_event_deletions;
+
+template <class Driver>
+void apply_event(Driver& d, long long step)
+{
+    if (step != g_event_step) return;
+    if (g_event_wall >= 0) d.wallHandler.removeObject((unsigned)g_event_wall);
+    for (const auto& db : g_event_deletions) {
+        DeletionBoundary b;
+        b.set(Vec3D(db.normal[0], db.normal[1], db.normal[2]), db.distance);
+        d.boundaryHandler.copyAndAddObject(b);
+    }
+}
 
 // MindlinInteraction keeps its sliding spring without a getter; its public
 // write() prints it after the token "slidingSpring" (MindlinInteraction.cc:166-170).
@@ -123,6 +144,15 @@ ParticleSpecies* make_species(const dem_species_pair& p)
 template <class Base>
 class RefDriverT : public Base {
 public:
+    // a driver's hook, run where the reference runs actionsAfterTimeStep
+    // (DPMBase::computeOneTimeStep: after the forces, before the second
+    // half-kick and the time increment)
+    std::function<void()> after_step;
+    void actionsAfterTimeStep() override
+    {
+        if (after_step) after_step();
+    }
+
     // The reference's own writers of the .ene, .fstat and .data outputs
     // (DPMBase::writeEneHeader / writeEneTimeStep, writeFstatHeader,
     // outputXBallsData) into the given streams.

@@ -66,6 +66,8 @@ def ref_lib(variant="serial"):
         lib.mdpm_ref_time.argtypes = common + [C.c_int, C.c_int, C.c_int, _pd]
         lib.mdpm_ref_set_deletion.restype = None
         lib.mdpm_ref_set_deletion.argtypes = [C.POINTER(_abi.DeletionBoundary), C.c_int]
+        lib.mdpm_ref_set_event.restype = None
+        lib.mdpm_ref_set_event.argtypes = [C.c_longlong, C.c_int, C.POINTER(_abi.DeletionBoundary), C.c_int]
         _ref[variant] = lib
     return _ref[variant]
 
@@ -169,9 +171,15 @@ def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated", deleti
     return o
 
 
-def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None) -> dict:
+def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None, event=None) -> dict:
+    """event = (step, wall, planes): after time step `step` the reference's
+    driver removes wall `wall` (handler index, -1: none) and adds the
+    DeletionBoundary planes [(normal, distance), ...]."""
     darr, nd = _deletions(deletions)
     ref_lib(variant).mdpm_ref_set_deletion(darr, nd)
+    step, wall, planes = event if event is not None else (-1, -1, [])
+    earr, ne = _deletions(planes)
+    ref_lib(variant).mdpm_ref_set_event(step, wall, earr, ne)
     inp = _Inputs(sc)
     cap = _contact_rows(sc.n)
     o, c, soa, csoa = _outputs(sc.n, cap)
@@ -184,6 +192,29 @@ def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None) -> d
     o["contacts"] = sort_contacts(_trim(c, cnt.value))
     o["energies"] = dict(kinetic=ene[0], rotational=ene[1], gravitational=ene[2], elastic=ene[3])
     return o
+
+
+def reference_heap_procedure(sc, base_radius: float, casing: int = 1, check_every: int = 1000,
+                             max_steps: int = 400_000, variant: str = "serial", threads: int = 1) -> dict:
+    """Drivers/Calibration/CalibrationHeap.cpp's procedure on the reference
+    Kernel (oracle/ref_drivers/mdpm_ref_driver.cpp, mdpm_ref_heap_procedure)
+    for the heap set up by `sc` (casing = the casing's wall index)."""
+    darr, nd = _deletions(None)
+    lib = ref_lib(variant)
+    lib.mdpm_ref_set_deletion(darr, nd)
+    lib.mdpm_ref_set_event(-1, -1, darr, 0)
+    fn = lib.mdpm_ref_heap_procedure
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(_abi.Config), C.POINTER(_abi.InstanceDesc), C.POINTER(_abi.SpeciesPair), _pd,
+                   C.POINTER(_abi.Wall), C.c_int, C.POINTER(_abi.ParticlesSoA), C.c_int, C.c_double, C.c_int,
+                   C.c_longlong, C.c_int, _pd]
+    inp = _Inputs(sc)
+    out = np.zeros(6)
+    rc = fn(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density), inp.walls, inp.nwalls,
+            C.byref(inp.soa), casing, base_radius, check_every, max_steps, threads, _dp(out))
+    assert rc == 0
+    return dict(aor=out[0], removal_time=out[1], end_time=out[2], steps=int(out[3]), n_remaining=int(out[4]),
+                com_z=out[5])
 
 
 def reference_outputs(sc, nsteps: int, prefix: str, variant: str = "serial"):
@@ -314,15 +345,24 @@ def time_reference_window(sc, warmup: int, nsteps: int, threads: int, variant: s
     return dict(seconds=sec.value, interactions_start=a.value, interactions_end=b.value)
 
 
-def run_gpu(sc, nsteps: int, contacts=None, deletions=None, **kw) -> dict:
+def run_gpu(sc, nsteps: int, contacts=None, deletions=None, event=None, **kw) -> dict:
+    """event: as in run_reference, made between two dem_step calls."""
+    from mercurydpm_fork_b200.engine import deletion_boundary
     if deletions:
-        from mercurydpm_fork_b200.engine import deletion_boundary
         kw["deletions"] = [deletion_boundary(nn, dd) for nn, dd in deletions]
     e = sc.engine(**kw)
     if contacts is not None:
         e.upload_contacts(contacts["id_p"], contacts["id_i"], contacts["springs"], contacts.get("is_wall"),
                           contacts.get("periodic"))
-    e.step(nsteps)
+    if event is not None and 0 <= event[0] < nsteps:
+        step, wall, planes = event
+        e.step(step)
+        if wall >= 0:
+            e.remove_wall(wall)
+        e.set_deletion_boundaries([deletion_boundary(nn, dd) for nn, dd in list(deletions or []) + list(planes)])
+        e.step(nsteps - step)
+    else:
+        e.step(nsteps)
     out = e.download()
     out["force"], out["torque"] = e.forces()
     out["contacts"] = sort_contacts(e.contacts())

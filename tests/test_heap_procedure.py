@@ -1,0 +1,76 @@
+"""Drivers/Calibration/CalibrationHeap.cpp's run on the engine, against the
+reference Kernel running the same procedure.
+
+* Changes between time steps (the casing removed with
+  dem_remove_wall, a DeletionBoundary added with dem_set_deletion_boundaries
+  while the run goes on) act as the reference's wallHandler.removeObject and
+  boundaryHandler.copyAndAddObject do in a driver's actionsAfterTimeStep:
+  a cased column pressed against its casing, the casing taken out and a
+  plane that deletes the bottom layer added after 100 steps, compared with
+  the reference after 100 more. Tolerances as in the law tests: the pair set
+  and the deleted particles exact, positions 1e-12 of a diameter, velocities
+  and forces 1e-9 of their largest magnitude.
+* The whole procedure (fill inside the casing, casing removal at the first
+  quiet check, angle of repose atan(4 COM_z / R_base) once quiet after
+  twice that time) on three heaps of 2,000 spheres, against the reference
+  Kernel's result in tests/golden/heap_aor.json (make_heap_aor.py). A heap
+  is chaotic: the reference itself, with its force sums in another order (4
+  OpenMP threads), measures another angle (0.3 to 1.0 deg apart on these
+  heaps); the engine's angle must lie within max(2 x that spread, 1.5 deg)
+  of the reference's serial one, its casing come off within one check of
+  either reference run, and its remaining particles match to 10 %.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import harness as H
+from mercurydpm_fork_b200 import calibration as cal
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "heap_aor.json")))
+
+
+def _pressed_column():
+    p = cal.HeapParams(n=400, sigma=0.1, mu=0.5, mu_r=0.1, restitution=0.5, seed=3)
+    sc, R = cal.cased_heap_scenario(p, spacing=0.98)  # the outer ring overlaps the casing
+    s = 0.98 * 2.0 * float(np.max(sc.radius))
+    return sc, R, [((0.0, 0.0, -1.0), -1.5 * s)]       # deletes z < 1.5 s: the bottom layer
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not H.reference_available("serial"), reason="reference build absent")
+def test_casing_removed_mid_run_matches_reference(gpu):
+    sc, R, planes = _pressed_column()
+    event = (100, 1, planes)
+    a = H.run_gpu(sc, 200, event=event)
+    r = H.run_reference(sc, 200, event=event)
+    assert (r["instance"] < 0).sum() > 20
+    np.testing.assert_array_equal(a["instance"] < 0, r["instance"] < 0)
+    assert H.pair_set(a["contacts"]) == H.pair_set(r["contacts"])
+    live = r["instance"] >= 0
+    assert H.rel_err(a["position"][live], r["position"][live], 1e-3) < 1e-12
+    for k in ("velocity", "force"):
+        assert H.rel_err(a[k][live], r[k][live]) < 1e-9, k
+    # the casing made contacts before the event, none after
+    before = H.run_gpu(sc, 100)
+    assert any(int(w) == 1 for w, iw in zip(before["contacts"]["id_i"], before["contacts"]["is_wall"]) if iw)
+    assert not any(int(w) == 1 for w, iw in zip(a["contacts"]["id_i"], a["contacts"]["is_wall"]) if iw)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", range(len(GOLDEN["heaps"])))
+def test_heap_angle_of_repose_matches_reference(gpu, k):
+    g = GOLDEN["heaps"][k]
+    sc, R = cal.cased_heap_scenario(cal.HeapParams(**g["params"]))
+    assert sc.time_step == g["time_step"] and R == g["base_radius"]
+    ours = cal.heap_procedure(sc, R)
+    ref, alt = g["serial"], g["omp4"]
+    spread = abs(ref["aor"] - alt["aor"])
+    assert np.isfinite(ours["aor"])
+    assert abs(ours["aor"] - ref["aor"]) <= max(2.0 * spread, 1.5), (ours, ref, alt)
+    # checks come every 1000 steps; the two reference runs may already differ by one
+    check = 1000 * sc.time_step * 1.0001
+    assert min(abs(ours["removal_time"] - ref["removal_time"]), abs(ours["removal_time"] - alt["removal_time"])) <= check
+    assert abs(ours["n_remaining"] - ref["n_remaining"]) <= 0.1 * ref["n_remaining"]

@@ -41,24 +41,36 @@
 // empty: contacts live on the device (dem_download_contacts), so .fstat and
 // .restart files written by the reference's writers carry no contacts.
 //
+// Between time steps a driver may take walls out (WallHandler::removeObject)
+// and add DeletionBoundary objects (BoundaryHandler::copyAndAddObject), as
+// Drivers/Calibration/CalibrationHeap.cpp does in its actionsAfterTimeStep:
+// the next computeAllForces hands the change to the engine (dem_remove_wall,
+// dem_set_deletion_boundaries). Particles the engine deletes leave the
+// ParticleHandler at the next refresh of the host copy.
+//
 // Supported set-ups: spherical particles; species whose normal law is
 // LinearViscoelastic or HertzianViscoelastic and whose friction law is none,
 // SlidingFriction, Friction (rolling and torsion), Mindlin or
-// MindlinRollingTorsion, with mixed species; InfiniteWall and TriangleWall;
-// PeriodicBoundary. Anything else (other walls and boundaries, particles
-// added or removed during the run) stops the run with logger(ERROR).
+// MindlinRollingTorsion, with mixed species (a ReversibleAdhesive part is
+// accepted when its maximum adhesive force is 0, where it exerts none);
+// InfiniteWall, IntersectionOfWalls, AxisymmetricIntersectionOfWalls and
+// TriangleWall; PeriodicBoundary and DeletionBoundary. Anything else (other
+// walls and boundaries, particles or walls added during the run) stops the
+// run with logger(ERROR).
 //
 // Build: compile the driver against the MercuryDPM Kernel as usual, with
 // -I<this repository>/include -I<this directory>, and link
 // mercurydpm_fork_b200/libdem_b200.so.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <iomanip>
 #include <sstream>
 #include <string>
 #include <vector>
 
+#include "Boundaries/DeletionBoundary.h"
 #include "Boundaries/PeriodicBoundary.h"
 #include "DPMBase.h"
 #include "Logger.h"
@@ -68,10 +80,13 @@
 #include "Species/FrictionForceSpecies/FrictionSpecies.h"
 #include "Species/FrictionForceSpecies/MindlinRollingTorsionSpecies.h"
 #include "Species/FrictionForceSpecies/MindlinSpecies.h"
+#include "Species/AdhesiveForceSpecies/ReversibleAdhesiveSpecies.h"
 #include "Species/FrictionForceSpecies/SlidingFrictionSpecies.h"
 #include "Species/NormalForceSpecies/HertzianViscoelasticNormalSpecies.h"
 #include "Species/NormalForceSpecies/LinearViscoelasticNormalSpecies.h"
+#include "Walls/AxisymmetricIntersectionOfWalls.h"
 #include "Walls/InfiniteWall.h"
+#include "Walls/IntersectionOfWalls.h"
 #include "Walls/TriangleWall.h"
 
 #include "dem_b200.h"
@@ -100,11 +115,18 @@ public:
         if (!h_) return;
         const size_t n = real_.size();
         dem_particles_soa s{(int64_t)n, x_.data(), v_.data(), w_.data(), q_.data(), nullptr, nullptr, nullptr,
-                            nullptr, nullptr, nullptr};
+                            nullptr, nullptr, inst_.data()};
         check(dem_download_particles(h_, &s), "dem_download_particles");
         check(dem_download_forces(h_, f_.data(), t_.data()), "dem_download_forces");
         for (size_t i = 0; i < n; ++i) {
             BaseParticle* p = real_[i];
+            if (!p) continue;
+            if (inst_[i] < 0) { // deleted by a DeletionBoundary on the device
+                this->particleHandler.removeObject(p->getIndex());
+                real_[i] = nullptr;
+                --live_;
+                continue;
+            }
             p->setPosition(Vec3D(x_[3 * i], x_[3 * i + 1], x_[3 * i + 2]));
             p->setVelocity(Vec3D(v_[3 * i], v_[3 * i + 1], v_[3 * i + 2]));
             p->setAngularVelocity(Vec3D(w_[3 * i], w_[3 * i + 1], w_[3 * i + 2]));
@@ -128,8 +150,9 @@ protected:
             gpuSync();
             return;
         }
-        if (countReal() != real_.size())
+        if (countReal() != live_)
             logger(ERROR, "GpuTimeStep: particles were added or removed during the run (not supported)");
+        handOverChanges();
         check(dem_step(h_, 1), "dem_step");
         ++sinceSync_;
         // this step's time and counter are advanced after computeAllForces
@@ -199,8 +222,96 @@ private:
     unsigned syncInterval_ = 1;
     int baseGridCalls_ = 0;
     unsigned sinceSync_ = 0;
-    std::vector<BaseParticle*> real_;
+    std::vector<BaseParticle*> real_;  // engine order; nullptr once deleted
+    size_t live_ = 0;
     std::vector<double> x_, v_, w_, q_, f_, t_;
+    std::vector<int32_t> inst_;
+    std::vector<const BaseWall*> walls_;  // dem_set_walls order; nullptr once taken out
+    std::vector<const BaseBoundary*> deletions_;
+
+    // Walls taken out and DeletionBoundary objects added since the last step
+    // go to the engine before the next one.
+    void handOverChanges()
+    {
+        if (this->wallHandler.getSize() != countWalls()) {
+            std::vector<const BaseWall*> now(this->wallHandler.begin(), this->wallHandler.end());
+            for (const BaseWall* w : now)
+                if (std::find(walls_.begin(), walls_.end(), w) == walls_.end())
+                    logger(ERROR, "GpuTimeStep: walls were added during the run (not supported)");
+            for (size_t k = 0; k < walls_.size(); ++k)
+                if (walls_[k] && std::find(now.begin(), now.end(), walls_[k]) == now.end()) {
+                    check(dem_remove_wall(h_, (int)k), "dem_remove_wall");
+                    walls_[k] = nullptr;
+                }
+        }
+        std::vector<const BaseBoundary*> dels;
+        for (BaseBoundary* b : this->boundaryHandler)
+            if (dynamic_cast<DeletionBoundary*>(b)) dels.push_back(b);
+        if (dels != deletions_) {
+            std::vector<dem_deletion_boundary> planes;
+            for (BaseBoundary* b : this->boundaryHandler) {
+                if (dynamic_cast<DeletionBoundary*>(b))
+                    planes.push_back(deletionPlane(b));
+                else if (!dynamic_cast<PeriodicBoundary*>(b))
+                    logger(ERROR, "GpuTimeStep: boundary % is not supported", b->getName());
+            }
+            check(dem_set_deletion_boundaries(h_, planes.data(), (int)planes.size()), "dem_set_deletion_boundaries");
+            deletions_ = dels;
+        }
+    }
+
+    size_t countWalls() const
+    {
+        size_t n = 0;
+        for (const BaseWall* w : walls_)
+            if (w) ++n;
+        return n;
+    }
+
+    // DeletionBoundary::set keeps the unit normal and the scaled distance; its
+    // restart line carries both (DeletionBoundary::write)
+    static dem_deletion_boundary deletionPlane(const BaseBoundary* b)
+    {
+        dem_deletion_boundary d{};
+        std::ostringstream os;
+        os.precision(17);
+        b->write(os);
+        std::istringstream is(os.str());
+        std::string tok;
+        while (is >> tok) {
+            if (tok == "normal") is >> d.normal[0] >> d.normal[1] >> d.normal[2];
+            if (tok == "distance") is >> d.distance;
+        }
+        return d;
+    }
+
+    // The faces of an IntersectionOfWalls (AxisymmetricIntersectionOfWalls:
+    // in its (r, 0, a) frame): normal and point of each of its InfiniteWalls,
+    // read from the wall's restart line (IntersectionOfWalls::write) and the
+    // normal taken from the face's orientation as the face itself does
+    static void fillFaces(const BaseWall* w, dem_wall& d)
+    {
+        std::ostringstream os;
+        os.precision(17);
+        w->write(os);
+        std::istringstream is(os.str());
+        std::string tok;
+        while (is >> tok && tok != "numIntersectionOfWalls") {
+        }
+        unsigned n = 0;
+        is >> n;
+        if (n > DEM_MAX_WALL_FACES) logger(ERROR, "GpuTimeStep: wall % has more than % faces", w->getIndex(), DEM_MAX_WALL_FACES);
+        d.n_faces = (int)n;
+        for (unsigned f = 0; f < n; ++f) {
+            Vec3D p;
+            double q[4];
+            is >> tok >> p.X >> p.Y >> p.Z >> tok >> q[0] >> q[1] >> q[2] >> q[3];
+            InfiniteWall face;
+            face.setOrientation(Quaternion(q[0], q[1], q[2], q[3]));
+            copy3(d.faces[f], face.getNormal());
+            copy3(d.faces[f] + 3, p);
+        }
+    }
 
     void check(int rc, const char* what) const
     {
@@ -283,6 +394,9 @@ private:
             p.sliding_mu = f->getSlidingFrictionCoefficient();
             p.sliding_mu_static = f->getSlidingFrictionCoefficientStatic();
         }
+        if (auto* a = dynamic_cast<ReversibleAdhesiveSpecies*>(s))
+            if (a->getAdhesionForceMax() != 0)
+                logger(ERROR, "GpuTimeStep: species % has an adhesive force the engine does not have", s->getName());
         p.interaction_distance = s->getInteractionDistance();
     }
 
@@ -319,7 +433,14 @@ private:
             }
         const unsigned ns = this->speciesHandler.getSize();
         in.n_species = (int)ns;
+        std::vector<dem_deletion_boundary> planes;
+        deletions_.clear();
         for (BaseBoundary* b : this->boundaryHandler) {
+            if (dynamic_cast<DeletionBoundary*>(b)) {
+                planes.push_back(deletionPlane(b));
+                deletions_.push_back(b);
+                continue;
+            }
             auto* pb = dynamic_cast<PeriodicBoundary*>(b);
             if (!pb) logger(ERROR, "GpuTimeStep: boundary % is not supported", b->getName());
             const Vec3D nrm = pb->getNormal();
@@ -346,6 +467,7 @@ private:
             }
         check(dem_set_species(h_, table.data(), (int)table.size()), "dem_set_species");
         std::vector<dem_wall> walls;
+        walls_.clear();
         for (BaseWall* w : this->wallHandler) {
             dem_wall d{};
             d.species = (int)w->getIndSpecies();
@@ -354,7 +476,13 @@ private:
             copy3(d.position, w->getPosition());
             copy3(d.velocity, w->getVelocity());
             copy3(d.angular_velocity, w->getAngularVelocity());
-            if (dynamic_cast<InfiniteWall*>(w)) {
+            if (dynamic_cast<AxisymmetricIntersectionOfWalls*>(w)) {
+                d.type = DEM_WALL_AXISYMMETRIC;
+                fillFaces(w, d);
+            } else if (dynamic_cast<IntersectionOfWalls*>(w)) {
+                d.type = DEM_WALL_INTERSECTION;
+                fillFaces(w, d);
+            } else if (dynamic_cast<InfiniteWall*>(w)) {
                 d.type = DEM_WALL_INFINITE;
             } else if (auto* tw = dynamic_cast<TriangleWall*>(w)) {
                 d.type = DEM_WALL_TRIANGLE;
@@ -365,12 +493,16 @@ private:
                 logger(ERROR, "GpuTimeStep: wall % is not supported", w->getName());
             }
             walls.push_back(d);
+            walls_.push_back(w);
         }
         check(dem_set_walls(h_, walls.data(), (int)walls.size()), "dem_set_walls");
+        check(dem_set_deletion_boundaries(h_, planes.data(), (int)planes.size()), "dem_set_deletion_boundaries");
         real_.clear();
         for (BaseParticle* p : this->particleHandler)
             if (isReal(p)) real_.push_back(p);
         const size_t n = real_.size();
+        live_ = n;
+        inst_.assign(n, 0);
         x_.assign(3 * n, 0.0); v_.assign(3 * n, 0.0); w_.assign(3 * n, 0.0); q_.assign(4 * n, 0.0);
         f_.assign(3 * n, 0.0); t_.assign(3 * n, 0.0);
         std::vector<double> r(n), im(n), ii(n);

@@ -35,6 +35,15 @@ int mdpm_gpu_solve_ene(const dem_config* cfg, const dem_instance_desc* inst, con
 // The same run, returning the final particle state the host holds after
 // solve() (caller order = upload order; position 3n, velocity 3n,
 // angular_velocity 3n).
+// the between-steps change of the next mdpm_gpu_solve_state (step < 0: none),
+// made by the driver's actionsAfterTimeStep as a MercuryDPM driver makes it
+void mdpm_gpu_set_event(long long step, int wall, const dem_deletion_boundary* b, int n)
+{
+    g_event_step = step;
+    g_event_wall = wall;
+    g_event_deletions.assign(b, b + n);
+}
+
 int mdpm_gpu_solve_state(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
                          const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in,
                          int nsteps, int device, int sync_interval, dem_particles_soa* out)
@@ -44,11 +53,15 @@ int mdpm_gpu_solve_state(const dem_config* cfg, const dem_instance_desc* inst, c
     d.setGpuDevice(device);
     d.setGpuSyncInterval((unsigned)sync_interval);
     d.setTimeMax((nsteps - 0.5) * cfg->time_step);
+    d.after_step = [&d]() { apply_event(d, (long long)d.getNumberOfTimeSteps() + 1); };
     d.solve_writing_ene("/dev/null", 1u << 30);
+    if (out->instance)
+        for (int64_t i = 0; i < in->n; ++i) out->instance[i] = -1; // deleted particles left the handler
     for (int64_t r = 0; r < (int64_t)d.particleHandler.getSize(); ++r) {
         const BaseParticle* p = d.particleHandler.getObject((unsigned)r);
         const int64_t i = (int64_t)p->getId();
         if (i < 0 || i >= in->n) continue;
+        if (out->instance) out->instance[i] = 0;
         const Vec3D x = p->getPosition(), v = p->getVelocity(), w = p->getAngularVelocity();
         for (int k = 0; k < 3; ++k) {
             out->position[3 * i + k] = x.getComponent(k);

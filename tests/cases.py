@@ -389,3 +389,15 @@ def recontact(owner_first: bool = True, vy: float = 0.1):
     inst = Instance(domain_min=(0, 0, 0), domain_max=(10, 10, 10), gravity=(0, 0, 0), n_species=1)
     return Scenario("recontact", 1e-3, inst, [sp], np.array([density]), [], pos, vel, radius, inv_mass, inv_inertia,
                     np.zeros(3, np.int32), ids)
+
+
+def pressed_column():
+    """400 spheres in a cased heap column whose outer ring presses on the
+    casing (lattice spacing 0.98 diameters), and a deletion plane z < 1.5
+    spacings that takes the bottom layer: (Scenario, R_base, [plane]). Wall 1
+    is the casing."""
+    from mercurydpm_fork_b200 import calibration as cal
+    p = cal.HeapParams(n=400, sigma=0.1, mu=0.5, mu_r=0.1, restitution=0.5, seed=3)
+    sc, R = cal.cased_heap_scenario(p, spacing=0.98)
+    s = 0.98 * 2.0 * float(np.max(sc.radius))
+    return sc, R, [((0.0, 0.0, -1.0), -1.5 * s)]

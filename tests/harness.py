@@ -463,13 +463,22 @@ def gpu_binding_ene(sc, nsteps: int, save_count: int, prefix: str, device: int =
     return parse_ene(open(prefix + ".ene").read())
 
 
-def gpu_binding_state(sc, nsteps: int, device: int = 0, sync_interval: int = 1) -> dict:
-    """The host's particle state after DPMBase::solve() on GpuMercury3D."""
+def gpu_binding_state(sc, nsteps: int, device: int = 0, sync_interval: int = 1, event=None) -> dict:
+    """The host's particle state after DPMBase::solve() on GpuMercury3D
+    (instance -1: the particle left the handler). event: as in
+    run_reference, made by the driver's actionsAfterTimeStep."""
     inp = _Inputs(sc)
     n = sc.n
-    o = dict(position=np.zeros((n, 3)), velocity=np.zeros((n, 3)), angular_velocity=np.zeros((n, 3)))
+    o = dict(position=np.zeros((n, 3)), velocity=np.zeros((n, 3)), angular_velocity=np.zeros((n, 3)),
+             instance=np.zeros(n, np.int32))
     soa = _abi.ParticlesSoA(n, _dp(o["position"]), _dp(o["velocity"]), _dp(o["angular_velocity"]), None, None,
-                            None, None, None, None, None)
+                            None, None, None, None, o["instance"].ctypes.data_as(C.POINTER(C.c_int32)))
+    step, wall, planes = event if event is not None else (-1, -1, [])
+    earr, ne = _deletions(planes)
+    lib = _gpu_binding()
+    lib.mdpm_gpu_set_event.restype = None
+    lib.mdpm_gpu_set_event.argtypes = [C.c_longlong, C.c_int, C.POINTER(_abi.DeletionBoundary), C.c_int]
+    lib.mdpm_gpu_set_event(step, wall, earr, ne)
     with quiet_stdout():
         rc = _gpu_binding().mdpm_gpu_solve_state(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density),
                                                  inp.walls, inp.nwalls, C.byref(inp.soa), nsteps, device,

@@ -14,7 +14,11 @@ DPMBase::solve() -> computeOneTimeStep loop.
   the C ABI, and lie within the reference's own chaos envelope
   (tests/golden/settling_box_ene.json).
 * The host state the driver holds after solve() equals the engine's state
-  after the same number of steps, bit for bit, whatever the sync interval.
+  after the same number of steps, bit for bit, whatever the sync interval:
+  on the periodic chute, on the rotating drum (AxisymmetricIntersectionOfWalls
+  and InfiniteWall caps), and on a cased column whose driver takes the casing
+  out and adds a DeletionBoundary in its actionsAfterTimeStep (the deleted
+  particles leave its ParticleHandler).
 """
 import json
 import os
@@ -60,3 +64,24 @@ def test_host_state_after_solve_equals_engine(gpu, sync_interval):
     g = H.run_gpu(sc, steps)
     for k in ("position", "velocity", "angular_velocity"):
         np.testing.assert_array_equal(host[k], g[k], err_msg=k)
+
+
+def test_drum_through_solve_equals_engine(gpu):
+    sc = cases.small_drum()
+    host = H.gpu_binding_state(sc, 40)
+    g = H.run_gpu(sc, 40)
+    for k in ("position", "velocity", "angular_velocity"):
+        np.testing.assert_array_equal(host[k], g[k], err_msg=k)
+
+
+@pytest.mark.parametrize("sync_interval", [1, 25])
+def test_casing_taken_out_by_the_driver(gpu, sync_interval):
+    sc, R, planes = cases.pressed_column()
+    event = (100, 1, planes)
+    host = H.gpu_binding_state(sc, 200, sync_interval=sync_interval, event=event)
+    g = H.run_gpu(sc, 200, event=event)
+    gone = g["instance"] < 0
+    assert gone.sum() > 20
+    np.testing.assert_array_equal(host["instance"] < 0, gone)
+    for k in ("position", "velocity", "angular_velocity"):
+        np.testing.assert_array_equal(host[k][~gone], g[k][~gone], err_msg=k)

@@ -26,23 +26,17 @@ import os
 import numpy as np
 import pytest
 
+import cases
 import harness as H
 from mercurydpm_fork_b200 import calibration as cal
 
 GOLDEN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "heap_aor.json")))
 
 
-def _pressed_column():
-    p = cal.HeapParams(n=400, sigma=0.1, mu=0.5, mu_r=0.1, restitution=0.5, seed=3)
-    sc, R = cal.cased_heap_scenario(p, spacing=0.98)  # the outer ring overlaps the casing
-    s = 0.98 * 2.0 * float(np.max(sc.radius))
-    return sc, R, [((0.0, 0.0, -1.0), -1.5 * s)]       # deletes z < 1.5 s: the bottom layer
-
-
 @pytest.mark.gpu
 @pytest.mark.skipif(not H.reference_available("serial"), reason="reference build absent")
 def test_casing_removed_mid_run_matches_reference(gpu):
-    sc, R, planes = _pressed_column()
+    sc, R, planes = cases.pressed_column()
     event = (100, 1, planes)
     a = H.run_gpu(sc, 200, event=event)
     r = H.run_reference(sc, 200, event=event)

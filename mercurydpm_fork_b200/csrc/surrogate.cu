@@ -20,6 +20,7 @@
 
 #include "../../include/dem_surrogate.h"
 #include "surrogate_gemm.cuh"
+#include "surrogate_fused.cuh"
 
 using namespace surrogate;
 
@@ -183,9 +184,30 @@ int gemm(Mlp* h, const __nv_bfloat16* A, long long a_sm, long long a_sk, const _
 // ---------------------------------------------------------------------------
 namespace {
 
-// keep_z: store the pre-activations for a backward pass (training)
+// Inference: the whole pass in one kernel (surrogate_fused.cuh), one CTA per
+// SM over 128-sample tiles; the activations stay on the SM.
+int forward_fused(Mlp* h, int n)
+{
+    static bool configured[64] = {false};
+    static int sms[64] = {0};
+    if (!configured[h->device & 63]) {
+        CK(cudaFuncSetAttribute(k_mlp_forward_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, FUSED_SMEM));
+        CK(cudaDeviceGetAttribute(&sms[h->device & 63], cudaDevAttrMultiProcessorCount, h->device));
+        configured[h->device & 63] = true;
+    }
+    const int tiles = (n + FUSED_TILE - 1) / FUSED_TILE;
+    FusedArgs a{h->x, h->d_norm, h->wb, h->p, OFF_W1, OFF_B1, OFF_W2, OFF_B2, OFF_W3, OFF_B3, OFF_W4, OFF_B4,
+                n, h->y, h->d_error};
+    k_mlp_forward_fused<<<std::min(tiles, sms[h->device & 63]), FUSED_THREADS, FUSED_SMEM, h->stream>>>(a);
+    CK(cudaGetLastError());
+    return DEM_MLP_OK;
+}
+
+// keep_z: store the pre-activations for a backward pass (training, one GEMM
+// per layer); without, the fused inference kernel
 int forward(Mlp* h, int n, bool keep_z = true)
 {
+    if (!keep_z) return forward_fused(h, n);
     const int epi = keep_z ? EPI_BIAS_GELU : EPI_BIAS_GELU_H;
     int rc;
     const __nv_bfloat16* W = h->wb;

@@ -1,6 +1,8 @@
 """The calibration surrogate on the GPU (tcgen05 BF16 GEMMs with FP32
 accumulation) against the CPU oracle with BF16 rounding at the same points.
 
+Inference runs as one fused kernel (layers 1 and 4 on the CUDA cores, 2 and 3
+on the tensor cores); training passes run one GEMM per layer.
 Tolerances: the oracle accumulates in FP64 and evaluates erf/exp in double;
 the GPU accumulates in FP32 and rounds the pre-activations it turns into BF16
 from FP32, so a few BF16 values differ by one unit (2^-8 relative). Outputs
@@ -45,6 +47,20 @@ def test_forward_matches_oracle(gpu, n):
     yo = yo * s.norm[3] + s.norm[2]
     s.close()
     assert np.linalg.norm(y - yo) <= 1e-2 * np.linalg.norm(yo)
+
+
+@pytest.mark.parametrize("n", [4097, 65536])
+def test_fused_forward_at_size_matches_oracle(gpu, n):
+    """Inference runs as one fused kernel (one CTA per SM over 128-sample
+    tiles): several tiles per CTA, and a last tile that is not full."""
+    s = _net(capacity=65536)
+    x, _ = _data(n, seed=5)
+    y = s.predict(x)
+    yo, _ = M.forward(s.params().astype(np.float64), x, s.norm)
+    yo = yo * s.norm[3] + s.norm[2]
+    s.close()
+    assert np.linalg.norm(y - yo) <= 1e-2 * np.linalg.norm(yo)
+    assert np.all(np.isfinite(y))
 
 
 @pytest.mark.parametrize("n", [64, 300, 1024])

@@ -37,9 +37,15 @@
 // that hooks, the .data writer and the caller read the engine's state.
 // Hooks that run between computeAllForces and integrateAfterForceComputation
 // in the reference (actionsAfterTimeStep) see the state after the whole step
-// (velocities after the second half-kick). The host's InteractionHandler stays
-// empty: contacts live on the device (dem_download_contacts), so .fstat and
-// .restart files written by the reference's writers carry no contacts.
+// (velocities after the second half-kick). At the same refreshes the
+// InteractionHandler is rebuilt from the engine's contacts of the last step
+// (dem_download_contacts, dem_download_contact_geometry): one interaction of
+// the pair's mixed species per contact with its force, contact point,
+// normal, overlap, distance and springs, so that hooks and the reference's
+// writers (getElasticEnergy, .fstat, .restart) see them. Between refreshes it
+// holds the last refresh's contacts. The refresh interval defaults to 1, or
+// to the value of the environment variable MERCURYDPM_GPU_SYNC_INTERVAL (for
+// drivers that read the state only every k steps and are built unmodified).
 //
 // Between time steps a driver may take walls out (WallHandler::removeObject)
 // and add DeletionBoundary objects (BoundaryHandler::copyAndAddObject), as
@@ -65,6 +71,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <iomanip>
 #include <sstream>
 #include <string>
@@ -81,6 +88,9 @@
 #include "Species/FrictionForceSpecies/MindlinRollingTorsionSpecies.h"
 #include "Species/FrictionForceSpecies/MindlinSpecies.h"
 #include "Species/AdhesiveForceSpecies/ReversibleAdhesiveSpecies.h"
+#include "Interactions/FrictionForceInteractions/FrictionInteraction.h"
+#include "Interactions/FrictionForceInteractions/MindlinRollingTorsionInteraction.h"
+#include "Interactions/FrictionForceInteractions/SlidingFrictionInteraction.h"
 #include "Species/FrictionForceSpecies/SlidingFrictionSpecies.h"
 #include "Species/NormalForceSpecies/HertzianViscoelasticNormalSpecies.h"
 #include "Species/NormalForceSpecies/LinearViscoelasticNormalSpecies.h"
@@ -122,6 +132,8 @@ public:
             BaseParticle* p = real_[i];
             if (!p) continue;
             if (inst_[i] < 0) { // deleted by a DeletionBoundary on the device
+                const unsigned id = p->getId();
+                if (id < byId_.size()) byId_[id] = nullptr;
                 this->particleHandler.removeObject(p->getIndex());
                 real_[i] = nullptr;
                 --live_;
@@ -135,6 +147,7 @@ public:
             p->setTorque(Vec3D(t_[3 * i], t_[3 * i + 1], t_[3 * i + 2]));
         }
         sinceSync_ = 0;
+        mirrorInteractions();
     }
 
     /// The engine's handle (after the first force evaluation), for the rest of
@@ -219,14 +232,66 @@ protected:
 private:
     dem_handle* h_ = nullptr;
     int device_ = 0;
-    unsigned syncInterval_ = 1;
+    unsigned syncInterval_ = defaultSyncInterval();
     int baseGridCalls_ = 0;
     unsigned sinceSync_ = 0;
     std::vector<BaseParticle*> real_;  // engine order; nullptr once deleted
     size_t live_ = 0;
     std::vector<double> x_, v_, w_, q_, f_, t_;
     std::vector<int32_t> inst_;
-    std::vector<const BaseWall*> walls_;  // dem_set_walls order; nullptr once taken out
+    std::vector<BaseWall*> walls_;        // dem_set_walls order; nullptr once taken out
+    std::vector<BaseParticle*> byId_;     // particle of each id (nullptr: none, or deleted)
+
+    static unsigned defaultSyncInterval()
+    {
+        const char* e = std::getenv("MERCURYDPM_GPU_SYNC_INTERVAL");
+        const long k = e ? std::strtol(e, nullptr, 10) : 1;
+        return k > 0 ? (unsigned)k : 1u;
+    }
+
+    // The engine's contacts of the last time step as the InteractionHandler's
+    // interactions (InteractionHandler::getInteraction creates each with the
+    // pair's mixed species, as the reference's contact detection does).
+    void mirrorInteractions()
+    {
+        int64_t count = 0;
+        check(dem_download_contacts(h_, nullptr, 0, &count), "dem_download_contacts");
+        std::vector<int32_t> ip(count), ii(count), iw(count), per(count);
+        std::vector<double> spr(9 * count), f(3 * count), ov(count), cp(3 * count), nr(3 * count);
+        dem_contacts_soa c{count, ip.data(), ii.data(), iw.data(), per.data(), spr.data(), f.data(), ov.data()};
+        check(dem_download_contacts(h_, &c, count, &count), "dem_download_contacts");
+        check(dem_download_contact_geometry(h_, cp.data(), nr.data(), nullptr, count, &count),
+              "dem_download_contact_geometry");
+        this->interactionHandler.clear();
+        const unsigned stamp = this->getNumberOfTimeSteps() + 1;
+        for (int64_t r = 0; r < count; ++r) {
+            BaseParticle* P = (ip[r] >= 0 && ip[r] < (int)byId_.size()) ? byId_[ip[r]] : nullptr;
+            BaseInteractable* I = nullptr;
+            if (iw[r]) {
+                if (ii[r] >= 0 && ii[r] < (int)walls_.size()) I = walls_[ii[r]];
+            } else if (ii[r] >= 0 && ii[r] < (int)byId_.size()) {
+                I = byId_[ii[r]];
+            }
+            if (!P || !I) continue;
+            BaseInteraction* x = this->interactionHandler.getInteraction(P, I, stamp);
+            x->setForce(Vec3D(f[3 * r], f[3 * r + 1], f[3 * r + 2]));
+            x->setContactPoint(Vec3D(cp[3 * r], cp[3 * r + 1], cp[3 * r + 2]));
+            x->setNormal(Vec3D(nr[3 * r], nr[3 * r + 1], nr[3 * r + 2]));
+            x->setOverlap(ov[r]);
+            const double reach = P->getRadius() + (iw[r] ? 0.0 : static_cast<BaseParticle*>(I)->getRadius());
+            x->setDistance(reach - ov[r]);
+            const double* sp = &spr[9 * r];
+            if (auto* sf = dynamic_cast<SlidingFrictionInteraction*>(x)) sf->setSlidingSpring(Vec3D(sp[0], sp[1], sp[2]));
+            if (auto* fr = dynamic_cast<FrictionInteraction*>(x)) {
+                fr->setRollingSpring(Vec3D(sp[3], sp[4], sp[5]));
+                fr->setTorsionSpring(Vec3D(sp[6], sp[7], sp[8]));
+            }
+            if (auto* mr = dynamic_cast<MindlinRollingTorsionInteraction*>(x)) {
+                mr->setRollingSpring(Vec3D(sp[3], sp[4], sp[5]));
+                mr->setTorsionSpring(Vec3D(sp[6], sp[7], sp[8]));
+            }
+        }
+    }
     std::vector<const BaseBoundary*> deletions_;
 
     // Walls taken out and DeletionBoundary objects added since the last step
@@ -502,6 +567,11 @@ private:
             if (isReal(p)) real_.push_back(p);
         const size_t n = real_.size();
         live_ = n;
+        byId_.clear();
+        for (BaseParticle* p : real_) {
+            if (p->getId() >= byId_.size()) byId_.resize(p->getId() + 1, nullptr);
+            byId_[p->getId()] = p;
+        }
         inst_.assign(n, 0);
         x_.assign(3 * n, 0.0); v_.assign(3 * n, 0.0); w_.assign(3 * n, 0.0); q_.assign(4 * n, 0.0);
         f_.assign(3 * n, 0.0); t_.assign(3 * n, 0.0);

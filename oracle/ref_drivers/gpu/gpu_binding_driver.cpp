@@ -46,7 +46,7 @@ void mdpm_gpu_set_event(long long step, int wall, const dem_deletion_boundary* b
 
 int mdpm_gpu_solve_state(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
                          const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in,
-                         int nsteps, int device, int sync_interval, dem_particles_soa* out)
+                         int nsteps, int device, int sync_interval, dem_particles_soa* out, double* host)
 {
     GpuRefDriver d;
     setup(d, cfg, inst, species, density, walls, nwalls, in, 1);
@@ -55,6 +55,10 @@ int mdpm_gpu_solve_state(const dem_config* cfg, const dem_instance_desc* inst, c
     d.setTimeMax((nsteps - 0.5) * cfg->time_step);
     d.after_step = [&d]() { apply_event(d, (long long)d.getNumberOfTimeSteps() + 1); };
     d.solve_writing_ene("/dev/null", 1u << 30);
+    if (host) { // what the driver's InteractionHandler holds: elastic energy, interactions
+        host[0] = d.getElasticEnergy();
+        host[1] = (double)d.interactionHandler.getNumberOfObjects();
+    }
     if (out->instance)
         for (int64_t i = 0; i < in->n; ++i) out->instance[i] = -1; // deleted particles left the handler
     for (int64_t r = 0; r < (int64_t)d.particleHandler.getSize(); ++r) {

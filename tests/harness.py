@@ -447,7 +447,7 @@ def _gpu_binding():
     lib.mdpm_gpu_solve_ene.restype = C.c_int
     lib.mdpm_gpu_solve_ene.argtypes = common + [C.c_int, C.c_int, C.c_int, C.c_char_p]
     lib.mdpm_gpu_solve_state.restype = C.c_int
-    lib.mdpm_gpu_solve_state.argtypes = common + [C.c_int, C.c_int, C.POINTER(_abi.ParticlesSoA)]
+    lib.mdpm_gpu_solve_state.argtypes = common + [C.c_int, C.c_int, C.POINTER(_abi.ParticlesSoA), _pd]
     return lib
 
 
@@ -479,11 +479,13 @@ def gpu_binding_state(sc, nsteps: int, device: int = 0, sync_interval: int = 1, 
     lib.mdpm_gpu_set_event.restype = None
     lib.mdpm_gpu_set_event.argtypes = [C.c_longlong, C.c_int, C.POINTER(_abi.DeletionBoundary), C.c_int]
     lib.mdpm_gpu_set_event(step, wall, earr, ne)
+    host = np.zeros(2)
     with quiet_stdout():
         rc = _gpu_binding().mdpm_gpu_solve_state(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density),
                                                  inp.walls, inp.nwalls, C.byref(inp.soa), nsteps, device,
-                                                 sync_interval, C.byref(soa))
+                                                 sync_interval, C.byref(soa), _dp(host))
     assert rc == 0
+    o["host_elastic_energy"], o["host_interactions"] = float(host[0]), int(host[1])
     return o
 
 

@@ -18,7 +18,8 @@ DPMBase::solve() -> computeOneTimeStep loop.
   on the periodic chute, on the rotating drum (AxisymmetricIntersectionOfWalls
   and InfiniteWall caps), and on a cased column whose driver takes the casing
   out and adds a DeletionBoundary in its actionsAfterTimeStep (the deleted
-  particles leave its ParticleHandler).
+  particles leave its ParticleHandler); its InteractionHandler holds the
+  engine's contacts of the last step, whose elastic energy is the engine's.
 """
 import json
 import os
@@ -67,11 +68,18 @@ def test_host_state_after_solve_equals_engine(gpu, sync_interval):
 
 
 def test_drum_through_solve_equals_engine(gpu):
+    """Also the InteractionHandler: after solve() it holds the engine's
+    contacts of the last step, and DPMBase::getElasticEnergy over them (the
+    reference's sum over interactions of the laws' energies) agrees with the
+    engine's own balance."""
     sc = cases.small_drum()
     host = H.gpu_binding_state(sc, 40)
     g = H.run_gpu(sc, 40)
     for k in ("position", "velocity", "angular_velocity"):
         np.testing.assert_array_equal(host[k], g[k], err_msg=k)
+    assert host["host_interactions"] == len(g["contacts"]["id_p"]) > 100
+    ee = g["globals"]["elastic_energy"]
+    assert abs(host["host_elastic_energy"] - ee) <= 1e-9 * ee
 
 
 @pytest.mark.parametrize("sync_interval", [1, 25])

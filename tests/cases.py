@@ -392,12 +392,18 @@ def recontact(owner_first: bool = True, vy: float = 0.1):
 
 
 def pressed_column():
-    """400 spheres in a cased heap column whose outer ring presses on the
-    casing (lattice spacing 0.98 diameters), and a deletion plane z < 1.5
+    """400 spheres in a cased heap column (lattice spacing 0.98 diameters)
+    whose outer ring presses on the casing, and a deletion plane z < 1.5
     spacings that takes the bottom layer: (Scenario, R_base, [plane]). Wall 1
     is the casing."""
     from mercurydpm_fork_b200 import calibration as cal
     p = cal.HeapParams(n=400, sigma=0.1, mu=0.5, mu_r=0.1, restitution=0.5, seed=3)
     sc, R = cal.cased_heap_scenario(p, spacing=0.98)
     s = 0.98 * 2.0 * float(np.max(sc.radius))
+    # the outer ring moved out radially until it overlaps the casing by 1 % of a radius
+    rxy = np.hypot(sc.position[:, 0], sc.position[:, 1])
+    outer = rxy > R - 1.5 * s
+    scale = (R - 0.99 * sc.radius[outer]) / rxy[outer]
+    sc.position[outer, 0] *= scale
+    sc.position[outer, 1] *= scale
     return sc, R, [((0.0, 0.0, -1.0), -1.5 * s)]

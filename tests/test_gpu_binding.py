@@ -85,9 +85,9 @@ def test_drum_through_solve_equals_engine(gpu):
 @pytest.mark.parametrize("sync_interval", [1, 25])
 def test_casing_taken_out_by_the_driver(gpu, sync_interval):
     sc, R, planes = cases.pressed_column()
-    event = (100, 1, planes)
-    host = H.gpu_binding_state(sc, 200, sync_interval=sync_interval, event=event)
-    g = H.run_gpu(sc, 200, event=event)
+    event = (10, 1, planes)
+    host = H.gpu_binding_state(sc, 110, sync_interval=sync_interval, event=event)
+    g = H.run_gpu(sc, 110, event=event)
     gone = g["instance"] < 0
     assert gone.sum() > 20
     np.testing.assert_array_equal(host["instance"] < 0, gone)

@@ -5,9 +5,9 @@ reference Kernel running the same procedure.
   dem_remove_wall, a DeletionBoundary added with dem_set_deletion_boundaries
   while the run goes on) act as the reference's wallHandler.removeObject and
   boundaryHandler.copyAndAddObject do in a driver's actionsAfterTimeStep:
-  a cased column pressed against its casing, the casing taken out and a
-  plane that deletes the bottom layer added after 100 steps, compared with
-  the reference after 100 more. Tolerances as in the law tests: the pair set
+  a cased column pressed against its casing, the casing taken out (with
+  124 contacts) and a plane that deletes the bottom layer added after 10
+  steps, compared with the reference 100 steps later. Tolerances as in the law tests: the pair set
   and the deleted particles exact, positions 1e-12 of a diameter, velocities
   and forces 1e-9 of their largest magnitude.
 * The whole procedure (fill inside the casing, casing removal at the first
@@ -37,9 +37,9 @@ GOLDEN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
 @pytest.mark.skipif(not H.reference_available("serial"), reason="reference build absent")
 def test_casing_removed_mid_run_matches_reference(gpu):
     sc, R, planes = cases.pressed_column()
-    event = (100, 1, planes)
-    a = H.run_gpu(sc, 200, event=event)
-    r = H.run_reference(sc, 200, event=event)
+    event = (10, 1, planes)   # the casing still holds 124 contacts then
+    a = H.run_gpu(sc, 110, event=event)
+    r = H.run_reference(sc, 110, event=event)
     assert (r["instance"] < 0).sum() > 20
     np.testing.assert_array_equal(a["instance"] < 0, r["instance"] < 0)
     assert H.pair_set(a["contacts"]) == H.pair_set(r["contacts"])
@@ -48,7 +48,7 @@ def test_casing_removed_mid_run_matches_reference(gpu):
     for k in ("velocity", "force"):
         assert H.rel_err(a[k][live], r[k][live]) < 1e-9, k
     # the casing made contacts before the event, none after
-    before = H.run_gpu(sc, 100)
+    before = H.run_gpu(sc, 10)
     assert any(int(w) == 1 for w, iw in zip(before["contacts"]["id_i"], before["contacts"]["is_wall"]) if iw)
     assert not any(int(w) == 1 for w, iw in zip(a["contacts"]["id_i"], a["contacts"]["is_wall"]) if iw)
 

@@ -16,9 +16,9 @@
 // filed in the bin of the first point of its range, and the bins are sorted
 // by (bin, particle slot) and (bin, contact pair) with stable radix sorts
 // (contact records arrive in launch order; the pair key makes their order
-// canonical). One block per point then walks the bins that can reach it in
-// index order, each thread a fixed stride of every bin, and sums the threads
-// in a fixed tree. The host divides by the volume of the averaged dimensions
+// canonical). One warp per point then walks the bins that can reach it in
+// index order, each lane a fixed stride of every bin, and sums the lanes in a
+// fixed butterfly. The host divides by the volume of the averaged dimensions
 // (CG::volumeAverageVariables).
 // The contact records are those of the last force evaluation, i.e. the
 // interactions the reference holds when writeOutputFiles evaluates CG at the
@@ -313,18 +313,20 @@ __global__ void k_cg_bin_bounds(const unsigned* sorted_bin, int m, int npts, int
     if (p == m - 1 || sorted_bin[p + 1] != b) end[b] = p + 1;
 }
 
-constexpr int CG_GATHER = 128;
+constexpr int CG_GATHER = 128; // 4 points per block
 constexpr int CG_ACC = 29;
 
-// One block per point: every particle and contact whose range covers the
-// point, bins in index order, thread t taking entries t, t + 128, ... of each
-// bin; the threads' sums are added in a fixed tree.
+// One warp per point: every particle and contact whose range covers the
+// point, bins in index order, lane l taking entries l, l + 32, ... of each
+// bin; the lanes' sums are added in a fixed butterfly.
 __global__ void __launch_bounds__(CG_GATHER) k_cg_gather(CGDev g, const CGParticle* prec, const int* porder,
                                                          const int* pstart, const int* pend, const CGContact* crec,
                                                          const int* corder, const int* cstart, const int* cend,
                                                          int3 pw, int3 cw, double* out)
 {
-    const int pt = blockIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int pt = blockIdx.x * (CG_GATHER / 32) + (threadIdx.x >> 5);
+    if (pt >= g.n[0] * g.n[1] * g.n[2]) return; // whole warps leave; no block barrier follows
     const int pk_ = pt % g.n[2], pj = (pt / g.n[2]) % g.n[1], pi = pt / (g.n[2] * g.n[1]);
     const int pidx[3] = {pi, pj, pk_};
     const V3 r = cg_point(g, pi, pj, pk_);
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(CG_GATHER) k_cg_gather(CGDev g, const CGPartic
         for (int j = plo[1]; j <= pj; ++j)
             for (int k = plo[2]; k <= pk_; ++k) {
                 const int b = (i * g.n[1] + j) * g.n[2] + k;
-                for (int e = pstart[b] + threadIdx.x; e < pend[b]; e += CG_GATHER) {
+                for (int e = pstart[b] + lane; e < pend[b]; e += 32) {
                     const CGParticle& q = prec[porder[e]];
                     bool in = true;
                     for (int dd = 0; dd < 3; ++dd) in = in && pidx[dd] < q.hi[dd];
@@ -354,7 +356,7 @@ __global__ void __launch_bounds__(CG_GATHER) k_cg_gather(CGDev g, const CGPartic
         for (int j = clo[1]; j <= pj; ++j)
             for (int k = clo[2]; k <= pk_; ++k) {
                 const int b = (i * g.n[1] + j) * g.n[2] + k;
-                for (int e = cstart[b] + threadIdx.x; e < cend[b]; e += CG_GATHER) {
+                for (int e = cstart[b] + lane; e < cend[b]; e += 32) {
                     const CGContact& q = crec[corder[e]];
                     bool in = true;
                     for (int dd = 0; dd < 3; ++dd) in = in && pidx[dd] < q.hi[dd];
@@ -402,22 +404,16 @@ __global__ void __launch_bounds__(CG_GATHER) k_cg_gather(CGDev g, const CGPartic
                     }
                 }
             }
-    // fixed tree: a butterfly within each warp, then the warps in order
-    __shared__ double part[CG_GATHER / 32][CG_ACC];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    // fixed butterfly over the lanes; lane f writes field f
+    double mine = 0.0;
 #pragma unroll
     for (int f = 0; f < CG_ACC; ++f) {
         double v = acc[f];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) part[wid][f] = v;
+        if (lane == f) mine = v;
     }
-    __syncthreads();
-    if (threadIdx.x < CG_ACC) {
-        double v = part[0][threadIdx.x];
-        for (int w = 1; w < CG_GATHER / 32; ++w) v += part[w][threadIdx.x];
-        out[(size_t)pt * DEM_CG_NFIELDS + threadIdx.x] = v;
-    }
+    if (lane < CG_ACC) out[(size_t)pt * DEM_CG_NFIELDS + lane] = mine;
 }
 
 } // namespace dem
@@ -537,7 +533,7 @@ extern "C" int dem_cg_eval(dem_handle* hh, const dem_cg_grid* grid, double* fiel
     int w[6];
     CU(cudaMemcpyAsync(w, wmax, sizeof(w), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
-    k_cg_gather<<<(unsigned)npts, CG_GATHER, 0, h->stream>>>(g, prec, pslot1, pstart, pend, crec, cpos1, cstart, cend,
+    k_cg_gather<<<(unsigned)((npts + CG_GATHER / 32 - 1) / (CG_GATHER / 32)), CG_GATHER, 0, h->stream>>>(g, prec, pslot1, pstart, pend, crec, cpos1, cstart, cend,
                                                             make_int3(w[0], w[1], w[2]), make_int3(w[3], w[4], w[5]),
                                                             dout);
     CU(cudaGetLastError());

@@ -2,7 +2,7 @@
 // (4 -> 256 -> 256 -> 256 -> 3, GELU, BF16 weights and activations, FP32
 // accumulation) in one persistent kernel.
 //
-// One CTA of 256 threads per SM walks tiles of 128 samples. A tile's
+// One CTA of 512 threads per SM walks tiles of 128 samples. A tile's
 // activations never leave the SM:
 //   layer 1 (K = 4, too short for the tensor cores): CUDA cores, from the raw
 //     inputs normalised as the unfused path does, written as BF16 into the
@@ -13,7 +13,7 @@
 //     epilogue reads it back with tcgen05.ld, adds the bias, applies GELU and
 //     writes the BF16 activations over the tile they came from;
 //   layer 4 (N = 3): folded into layer 3's epilogue, each thread summing its
-//     row's products over its 128 columns, the two halves of a row added in a
+//     row's products over its 64 columns, the four parts of a row added in a
 //     fixed order.
 // The four weight halves of a tile (64 KB each, two of layer 2, two of layer
 // 3) stream from L2 into two shared buffers with cp.async while the other
@@ -28,7 +28,7 @@
 
 namespace surrogate {
 
-constexpr int FUSED_THREADS = 256;
+constexpr int FUSED_THREADS = 512;   // 16 warps: 4 per tensor-memory lane quarter
 constexpr int FUSED_TILE = 128;       // samples per tile (UMMA M)
 constexpr int FUSED_NH = 256;         // hidden width
 constexpr int FUSED_HALF = 128;       // output features per weight half (UMMA N)
@@ -99,11 +99,11 @@ __device__ __forceinline__ uint4 fused_pack8(const float* f)
 __global__ void __launch_bounds__(FUSED_THREADS, 1) k_mlp_forward_fused(FusedArgs a)
 {
     extern __shared__ unsigned char smem_raw[];
-    __shared__ float w1s[FUSED_NH][4];
-    __shared__ float b1s[FUSED_NH], b2s[FUSED_NH], b3s[FUSED_NH];
-    __shared__ float w4s[3][FUSED_NH];
+    __shared__ float4 w1s[FUSED_NH];               // layer 1: the 4 weights of each feature
+    __shared__ __align__(16) float b1s[FUSED_NH], b2s[FUSED_NH], b3s[FUSED_NH];
+    __shared__ float4 w4s[FUSED_NH];               // layer 4: (w0, w1, w2, 0) of each input column
     __shared__ float b4s[3];
-    __shared__ float part[FUSED_TILE][3];
+    __shared__ float part[3][FUSED_TILE][3];       // layer 4 sums of column parts 1..3
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_slot;
     __shared__ int failed;
@@ -112,18 +112,20 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_mlp_forward_fused(FusedArg
     unsigned char* sA = smem;
     unsigned char* const sW[2] = {smem + FUSED_OPERAND, smem + 2 * FUSED_OPERAND};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int quarter = warp & 3, half = warp >> 2;
+    const int quarter = warp & 3, cpart = warp >> 2; // lane quarter, 64-column part
     const int ntiles = (a.n + FUSED_TILE - 1) / FUSED_TILE;
 
-    for (int i = threadIdx.x; i < FUSED_NH * 4; i += FUSED_THREADS)
-        w1s[i >> 2][i & 3] = __bfloat162float(a.wb[a.off_w1 + i]);
+    for (int i = threadIdx.x; i < FUSED_NH; i += FUSED_THREADS)
+        w1s[i] = make_float4(__bfloat162float(a.wb[a.off_w1 + 4 * i]), __bfloat162float(a.wb[a.off_w1 + 4 * i + 1]),
+                             __bfloat162float(a.wb[a.off_w1 + 4 * i + 2]), __bfloat162float(a.wb[a.off_w1 + 4 * i + 3]));
     for (int i = threadIdx.x; i < FUSED_NH; i += FUSED_THREADS) {
         b1s[i] = a.p[a.off_b1 + i];
         b2s[i] = a.p[a.off_b2 + i];
         b3s[i] = a.p[a.off_b3 + i];
     }
-    for (int i = threadIdx.x; i < 3 * FUSED_NH; i += FUSED_THREADS)
-        w4s[i / FUSED_NH][i % FUSED_NH] = __bfloat162float(a.wb[a.off_w4 + i]);
+    for (int i = threadIdx.x; i < FUSED_NH; i += FUSED_THREADS)
+        w4s[i] = make_float4(__bfloat162float(a.wb[a.off_w4 + i]), __bfloat162float(a.wb[a.off_w4 + FUSED_NH + i]),
+                             __bfloat162float(a.wb[a.off_w4 + 2 * FUSED_NH + i]), 0.0f);
     if (threadIdx.x < 3) b4s[threadIdx.x] = a.p[a.off_b4 + threadIdx.x];
     if (threadIdx.x == 0) {
         mbar_init(&bar, 1);
@@ -150,9 +152,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_mlp_forward_fused(FusedArg
     }
     for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
         const int m0 = tile * FUSED_TILE;
-        // ---- layer 1: thread = (row, half of the features) ----
+        // ---- layer 1: thread = (row, quarter of the features) ----
         {
-            const int r = threadIdx.x & (FUSED_TILE - 1), fh = threadIdx.x >> 7;
+            constexpr int FQ = FUSED_NH / (FUSED_THREADS / FUSED_TILE); // 64 features
+            const int r = threadIdx.x & (FUSED_TILE - 1), fq = threadIdx.x >> 7;
             const int m = m0 + r;
             float xn[4];
 #pragma unroll
@@ -161,13 +164,16 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_mlp_forward_fused(FusedArg
                 xn[k] = __bfloat162float(__float2bfloat16_rn((raw - a.norm[k]) / a.norm[4 + k]));
             }
 #pragma unroll 1
-            for (int j0 = fh * FUSED_HALF; j0 < fh * FUSED_HALF + FUSED_HALF; j0 += 8) {
+            for (int j0 = fq * FQ; j0 < fq * FQ + FQ; j0 += 8) {
                 float h[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
+                    const float4 w = w1s[j0 + j];
                     float acc = 0.0f;
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) acc = fmaf(xn[k], w1s[j0 + j][k], acc);
+                    acc = fmaf(xn[0], w.x, acc);
+                    acc = fmaf(xn[1], w.y, acc);
+                    acc = fmaf(xn[2], w.z, acc);
+                    acc = fmaf(xn[3], w.w, acc);
                     h[j] = gelu_f(acc + b1s[j0 + j]);
                 }
                 *reinterpret_cast<uint4*>(sA + fused_at(r, j0)) = fused_pack8(h);
@@ -194,17 +200,24 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_mlp_forward_fused(FusedArg
                 fused_load_half(sW[1], wn, 1);
                 asm volatile("cp.async.commit_group;" ::: "memory");
             }
-            // ---- epilogue: thread = row (tensor-memory lane), its half of the columns ----
+            // ---- epilogue: thread = row (tensor-memory lane), its 64-column part ----
             const int row = quarter * 32 + lane;
             const float* bias = layer == 2 ? b2s : b3s;
             float y0 = 0.0f, y1 = 0.0f, y2 = 0.0f;
 #pragma unroll 1
-            for (int cc = 0; cc < FUSED_HALF / 32; ++cc) {
-                const int c0 = half * FUSED_HALF + cc * 32;
+            for (int cc = 0; cc < 2; ++cc) {
+                const int c0 = cpart * 64 + cc * 32;
                 float v[32];
                 tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, v);
+                const float4* b4 = reinterpret_cast<const float4*>(bias + c0);
 #pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] = gelu_f(v[i] + bias[c0 + i]);
+                for (int i = 0; i < 8; ++i) {
+                    const float4 bb = b4[i];
+                    v[4 * i] = gelu_f(v[4 * i] + bb.x);
+                    v[4 * i + 1] = gelu_f(v[4 * i + 1] + bb.y);
+                    v[4 * i + 2] = gelu_f(v[4 * i + 2] + bb.z);
+                    v[4 * i + 3] = gelu_f(v[4 * i + 3] + bb.w);
+                }
                 if (layer == 2) {
 #pragma unroll
                     for (int g = 0; g < 4; ++g)
@@ -213,24 +226,25 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_mlp_forward_fused(FusedArg
 #pragma unroll
                     for (int i = 0; i < 32; ++i) { // layer 4 on the BF16 activations
                         const float hb = __bfloat162float(__float2bfloat16_rn(v[i]));
-                        y0 = fmaf(hb, w4s[0][c0 + i], y0);
-                        y1 = fmaf(hb, w4s[1][c0 + i], y1);
-                        y2 = fmaf(hb, w4s[2][c0 + i], y2);
+                        const float4 w = w4s[c0 + i];
+                        y0 = fmaf(hb, w.x, y0);
+                        y1 = fmaf(hb, w.y, y1);
+                        y2 = fmaf(hb, w.z, y2);
                     }
                 }
             }
             if (layer == 3) {
-                if (half == 1) {
-                    part[row][0] = y0;
-                    part[row][1] = y1;
-                    part[row][2] = y2;
+                if (cpart > 0) {
+                    part[cpart - 1][row][0] = y0;
+                    part[cpart - 1][row][1] = y1;
+                    part[cpart - 1][row][2] = y2;
                 }
                 __syncthreads();
                 const int m = m0 + row;
-                if (half == 0 && m < a.n) {
-                    a.y[(long long)m * 3 + 0] = (y0 + part[row][0]) + b4s[0];
-                    a.y[(long long)m * 3 + 1] = (y1 + part[row][1]) + b4s[1];
-                    a.y[(long long)m * 3 + 2] = (y2 + part[row][2]) + b4s[2];
+                if (cpart == 0 && m < a.n) { // the parts in column order
+                    a.y[(long long)m * 3 + 0] = (((y0 + part[0][row][0]) + part[1][row][0]) + part[2][row][0]) + b4s[0];
+                    a.y[(long long)m * 3 + 1] = (((y1 + part[0][row][1]) + part[1][row][1]) + part[2][row][1]) + b4s[1];
+                    a.y[(long long)m * 3 + 2] = (((y2 + part[0][row][2]) + part[1][row][2]) + part[2][row][2]) + b4s[2];
                 }
             }
         }

@@ -117,6 +117,25 @@ def heaps(n_instances=4096, seed=1, steps=0, max_contacts=6):
     return out
 
 
+def heap_pin():
+    """The three cased heaps of tests/golden/heap_aor.json through
+    CalibrationHeap's procedure on the engine (calibration.heap_procedure):
+    angle of repose, casing removal time and particles left, next to the
+    reference Kernel's serial and 4-thread results in that file."""
+    import os
+    from . import calibration as cal
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    gold = json.load(open(os.path.join(root, "tests", "golden", "heap_aor.json")))
+    rows = []
+    for g in gold["heaps"]:
+        sc, R = cal.cased_heap_scenario(cal.HeapParams(**g["params"]))
+        t0 = time.perf_counter()
+        ours = cal.heap_procedure(sc, R)
+        rows.append(dict(params=g["params"], engine=ours, engine_wall_s=time.perf_counter() - t0,
+                         reference_serial=g["serial"], reference_omp4=g["omp4"]))
+    return dict(workload="calibration_heap_procedure", heaps=rows)
+
+
 def surrogate(batch=65536, train_batch=1024, reps=20):
     import torch
     from .surrogate import Surrogate
@@ -294,5 +313,5 @@ if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "drum"
     kwargs = dict(a.split("=", 1) for a in sys.argv[2:])  # e.g. triangles n=20000 settle_steps=2000
     fn = dict(chute=chute, drum=drum, drum_dense=drum_dense, heaps=heaps, surrogate=surrogate, calibration=calibration,
-              c5=c5, cg=cg, triangles=triangles)[which]
+              c5=c5, cg=cg, triangles=triangles, heap_pin=heap_pin)[which]
     print(json.dumps(fn(**kwargs)))

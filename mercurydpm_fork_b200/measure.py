@@ -201,15 +201,17 @@ def calibration(n_train=2048, n_targets=16, tol=0.02, rounds=4, proposals=256, s
                 heap="600 spheres, 20,000 steps, lognormal PSD, rough floor disk (calibration.heap_responses)")
 
 
-def c5(n=2000, steps=40_000, n_train=2048, n_targets=16, tol=0.02, proposals=256, rounds=4, plain_rounds=12,
-       seed=3, chunk=4096):
+def c5(n=2000, steps=40_000, n_train=1024, n_targets=128, tol=0.02, proposals=64, surrogate_proposals=8, rounds=4,
+       plain_rounds=8, seed=3, chunk=4096):
     """The surrogate claim as a wall-time ratio: the same held-out targets
     (responses of DEM heaps at parameters drawn from the box) calibrated to
     `tol` twice on this GPU, timed host to host --
       surrogate-guided: the training heaps (n_train DEM runs), the network's
-      training, then calibration.calibrate_batch with the surrogate;
-      plain: calibration.calibrate_batch without it (every round uniform
-      proposals judged by batched DEM), up to plain_rounds rounds.
+      training, then calibration.calibrate_batch with the surrogate, each
+      target proposing its `surrogate_proposals` best-predicted candidates per
+      round;
+      plain: calibration.calibrate_batch without it, each target proposing
+      `proposals` uniform parameter sets per round, up to plain_rounds rounds.
     Every heap has n spheres (a calibration campaign fixes the sample size;
     C4's heaps range over U[500, 8000]) and runs `steps` time steps; a
     round's proposals for all targets are one batched DEM call. ratio =
@@ -218,7 +220,8 @@ def c5(n=2000, steps=40_000, n_train=2048, n_targets=16, tol=0.02, proposals=256
     and the ratio an upper one)."""
     from . import calibration as cal
     from .surrogate import Surrogate
-    n, steps, n_train, n_targets, proposals = int(n), int(steps), int(n_train), int(n_targets), int(proposals)
+    n, steps, n_train, n_targets = int(n), int(steps), int(n_train), int(n_targets)
+    proposals, surrogate_proposals = int(proposals), int(surrogate_proposals)
     rounds, plain_rounds, seed, chunk, tol = int(rounds), int(plain_rounds), int(seed), int(chunk), float(tol)
     dem = lambda p: cal.heap_responses(p, n=n, steps=steps, chunk=chunk)
     rng = np.random.default_rng(seed)
@@ -233,8 +236,8 @@ def c5(n=2000, steps=40_000, n_train=2048, n_targets=16, tol=0.02, proposals=256
     s.fit_normalisation(x, y)
     s.fit(x, y, epochs=200, batch=1024)
     t_train = time.perf_counter() - t0 - t_data
-    res_s = cal.calibrate_batch(targets, dem, s, rounds=rounds, proposals=proposals, candidates=65_536, tol=tol,
-                                seed=seed, data=(x, y))
+    res_s = cal.calibrate_batch(targets, dem, s, rounds=rounds, proposals=surrogate_proposals, candidates=65_536,
+                                tol=tol, seed=seed, data=(x, y))
     t_surr = time.perf_counter() - t0
     s.close()
     # plain batched DEM
@@ -245,14 +248,15 @@ def c5(n=2000, steps=40_000, n_train=2048, n_targets=16, tol=0.02, proposals=256
     ok_p = [r["best_error"] <= tol for r in res_p]
     return dict(workload="calibration_c5", metric="wall-time ratio, surrogate-guided / plain batched DEM",
                 value=t_surr / t_plain, tol=tol, targets=n_targets, heap_spheres=n, heap_steps=steps,
-                proposals_per_round=proposals,
                 surrogate=dict(seconds=t_surr, training_data_s=t_data, training_s=t_train, succeeded=int(sum(ok_s)),
-                               rounds=[r["rounds"] for r in res_s],
+                               proposals_per_round=surrogate_proposals, rounds_histogram=np.bincount(
+                                   [r["rounds"] for r in res_s]).tolist(),
                                dem_runs=n_train + sum(r["dem_runs"] for r in res_s),
-                               best_errors=[round(r["best_error"], 5) for r in res_s]),
-                plain=dict(seconds=t_plain, succeeded=int(sum(ok_p)), rounds=[r["rounds"] for r in res_p],
+                               median_best_error=float(np.median([r["best_error"] for r in res_s]))),
+                plain=dict(seconds=t_plain, succeeded=int(sum(ok_p)), proposals_per_round=proposals,
+                           rounds_histogram=np.bincount([r["rounds"] for r in res_p]).tolist(),
                            dem_runs=sum(r["dem_runs"] for r in res_p), round_cap=plain_rounds,
-                           best_errors=[round(r["best_error"], 5) for r in res_p]),
+                           median_best_error=float(np.median([r["best_error"] for r in res_p]))),
                 plain_time_is_lower_bound=not all(ok_p))
 
 

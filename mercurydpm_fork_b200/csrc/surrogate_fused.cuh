@@ -85,14 +85,15 @@ __device__ __forceinline__ void fused_mma_layer(uint32_t tmem, const unsigned ch
     umma_commit(bar);
 }
 
-// 8 consecutive BF16 values as one 16-byte word
+// 8 consecutive BF16 values (rounded to nearest, two per conversion) as one 16-byte word
 __device__ __forceinline__ uint4 fused_pack8(const float* f)
 {
     uint32_t w[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-        w[j] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f[2 * j])) |
-               ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f[2 * j + 1])) << 16);
+    for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+        w[j] = *reinterpret_cast<const uint32_t*>(&h);
+    }
     return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
@@ -224,12 +225,15 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_mlp_forward_fused(FusedArg
                         *reinterpret_cast<uint4*>(sA + fused_at(row, c0 + 8 * g)) = fused_pack8(v + 8 * g);
                 } else {
 #pragma unroll
-                    for (int i = 0; i < 32; ++i) { // layer 4 on the BF16 activations
-                        const float hb = __bfloat162float(__float2bfloat16_rn(v[i]));
-                        const float4 w = w4s[c0 + i];
-                        y0 = fmaf(hb, w.x, y0);
-                        y1 = fmaf(hb, w.y, y1);
-                        y2 = fmaf(hb, w.z, y2);
+                    for (int i = 0; i < 32; i += 2) { // layer 4 on the BF16 activations
+                        const float2 hb = __bfloat1622float2(__floats2bfloat162_rn(v[i], v[i + 1]));
+                        const float4 wa = w4s[c0 + i], wb = w4s[c0 + i + 1];
+                        y0 = fmaf(hb.x, wa.x, y0);
+                        y1 = fmaf(hb.x, wa.y, y1);
+                        y2 = fmaf(hb.x, wa.z, y2);
+                        y0 = fmaf(hb.y, wb.x, y0);
+                        y1 = fmaf(hb.y, wb.y, y1);
+                        y2 = fmaf(hb.y, wb.z, y2);
                     }
                 }
             }

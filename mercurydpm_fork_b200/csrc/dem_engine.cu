@@ -791,7 +791,6 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
             d.pr[b] = kept.pr[b]; d.vm[b] = kept.vm[b]; d.wi[b] = kept.wi[b]; d.qo[b] = kept.qo[b];
             d.info[b] = kept.info[b]; d.caller[b] = kept.caller[b]; d.nbr[b] = kept.nbr[b]; d.cnt[b] = kept.cnt[b];
             d.own[b] = kept.own[b];
-            d.near[b] = kept.near[b];
             d.wcand[b] = kept.wcand[b];
             d.pool[b] = kept.pool[b]; d.hidx[b] = kept.hidx[b];
             d.act[b] = kept.act[b]; d.whist[b] = kept.whist[b]; d.wact[b] = kept.wact[b];
@@ -824,7 +823,6 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         if ((rc = dalloc(h, &d.nbr[b], (size_t)cap * NC))) return rc;
         if ((rc = dalloc(h, &d.cnt[b], NC))) return rc;
         if ((rc = dalloc(h, &d.own[b], (size_t)d.nwords * NC))) return rc;
-        if ((rc = dalloc(h, &d.near[b], (size_t)4 * d.nwords * NC))) return rc;
         if ((rc = dalloc(h, &d.wcand[b], NC))) return rc;
         if ((rc = dalloc(h, &d.pool[b], (size_t)hist_stride(d.ncomp) * item_cap))) return rc;
         if ((rc = dalloc(h, &d.hidx[b], (size_t)cap * NC))) return rc;

@@ -149,13 +149,6 @@ struct DevPtrs {
     // within reach + skin at the rebuild (particles move less than skin / 2
     // between rebuilds, so the other still walls cannot be touched)
     unsigned int *wcand[2];
-    // per list word of list buffer l, four masks: bit k%32 of
-    // near[l][((k/32)*4 + q)*ncap + i] is set when entry k's clearance at the
-    // rebuild (distance - radii - interaction distance, FP64) was at most
-    // (q + 1) skin / 4 (plus 1e-9 of the radii); particles move less than the
-    // accumulated displacement each, so an entry outside the mask for
-    // 2 x that displacement cannot be in contact (k_detect skips its gathers)
-    unsigned int *near[2];
     double *pool[2];        // springs per contact (item_cap records each)
     int *hidx[2];           // per entry: pool index of its contact's spring
     unsigned int *act[2];

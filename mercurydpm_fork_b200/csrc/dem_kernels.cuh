@@ -310,8 +310,6 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
     int count = 0;
     bool overflow = false;
     unsigned int ownw = 0u; // ownership bits of the list word being filled
-    unsigned int nq0 = 0u, nq1 = 0u, nq2 = 0u, nq3 = 0u; // clearance masks of that word
-    const double band = 0.25 * d.ctl->skin;
     for (int lvl = 0; lvl < I.n_levels; ++lvl) {
         const double reach = ps.w + I.level_rmax[lvl] + extra;
         int lox, hix, loy, hiy, loz, hiz;
@@ -382,32 +380,10 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
                             if (count < d.cap) {
                                 d.nbr[ln][nbr_at(d.ncap, s, count)] = t;
                                 d.rows[(size_t)s * d.cap + count] = t;
-                                const int4 it = d.info[nb][t];
-                                const unsigned int bit = 1u << (count & 31);
-                                if (is.x < it.x) ownw |= bit;
-                                // clearance of the pair now (the predicate's distance, FP64)
-                                {
-                                    const double4 pt = d.pr[nb][t];
-                                    bool per;
-                                    const V3 xt = image_of(I, xs, xyz(pt), per);
-                                    double idist = 0.0;
-                                    if (!d.zero_idist)
-                                        idist = d.species[I.species_offset + is.y * I.n_species + it.y].interaction_distance;
-                                    const double c = sqrt(len2(xs - xt)) - (ps.w + pt.w + idist);
-                                    const double margin = 1e-9 * (ps.w + pt.w);
-                                    if (c <= band + margin) nq0 |= bit;
-                                    if (c <= 2.0 * band + margin) nq1 |= bit;
-                                    if (c <= 3.0 * band + margin) nq2 |= bit;
-                                    if (c <= 4.0 * band + margin) nq3 |= bit;
-                                }
+                                if (is.x < d.info[nb][t].x) ownw |= 1u << (count & 31);
                                 if ((count & 31) == 31) {
-                                    const size_t w = (size_t)(count >> 5);
-                                    d.own[ln][w * d.ncap + s] = ownw;
-                                    d.near[ln][(w * 4 + 0) * d.ncap + s] = nq0;
-                                    d.near[ln][(w * 4 + 1) * d.ncap + s] = nq1;
-                                    d.near[ln][(w * 4 + 2) * d.ncap + s] = nq2;
-                                    d.near[ln][(w * 4 + 3) * d.ncap + s] = nq3;
-                                    ownw = nq0 = nq1 = nq2 = nq3 = 0u;
+                                    d.own[ln][(size_t)(count >> 5) * d.ncap + s] = ownw;
+                                    ownw = 0u;
                                 }
                             } else {
                                 overflow = true;
@@ -423,14 +399,7 @@ __device__ __forceinline__ void build_one(const DevPtrs& d, int s, int hc, int l
         atomicOr(&d.ctl->status, 1u << DEM_ERR_CAPACITY);
         count = d.cap;
     }
-    if (count & 31) { // the last, partial word
-        const size_t w = (size_t)(count >> 5);
-        d.own[ln][w * d.ncap + s] = ownw;
-        d.near[ln][(w * 4 + 0) * d.ncap + s] = nq0;
-        d.near[ln][(w * 4 + 1) * d.ncap + s] = nq1;
-        d.near[ln][(w * 4 + 2) * d.ncap + s] = nq2;
-        d.near[ln][(w * 4 + 3) * d.ncap + s] = nq3;
-    }
+    if (count & 31) d.own[ln][(size_t)(count >> 5) * d.ncap + s] = ownw; // the last, partial word
     d.cnt[ln][s] = count;
 
     // still walls within reach + skin (k_detect tests only these until the next rebuild)

@@ -196,15 +196,6 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
         // the owned ones are visited in list order, B at a time. With periodic
         // boundaries every entry is visited (its image decides the owner).
         const bool owner_known = I.per_mask == 0u;
-        // entries whose clearance at the rebuild exceeds twice the accumulated
-        // displacement cannot be in contact: their gathers are skipped (not in
-        // the first time step, which keeps interactions that nothing touches)
-        int nq = 4;
-        if (!first) {
-            const double thr = 2.0 * ctl->disp_acc * (1.0 + 1e-9);
-            const double band = 0.25 * ctl->skin;
-            nq = thr <= band ? 0 : (thr <= 2.0 * band ? 1 : (thr <= 3.0 * band ? 2 : (thr <= 4.0 * band ? 3 : 4)));
-        }
         for (int w = 0; w < d.nwords; ++w) {
             unsigned int hitw = 0u, neww = 0u;
             const int kbeg = 32 * w, kend = min(count, kbeg + 32);
@@ -219,16 +210,6 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
                     d.slot[nbr_at(d.ncap, s, k)] = SLOT_IS_I;
                 }
                 todo = valid & ow;
-            }
-            if (nq < 4 && todo) {
-                const unsigned int reach = d.near[l][((size_t)w * 4 + nq) * d.ncap + s];
-                unsigned int far = todo & ~reach;
-                todo &= reach;
-                while (far) {
-                    const int k = kbeg + __ffs(far) - 1;
-                    far &= far - 1;
-                    d.slot[nbr_at(d.ncap, s, k)] = SLOT_NONE;
-                }
             }
             const unsigned int aw = (first && valid) ? d.act[c][(size_t)w * d.ncap + s] : 0u;
             while (todo) {

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -589,42 +590,49 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     std::vector<std::vector<long long>> members(ninst);
     const bool one = ninst == 1; // one instance: members are 0..n-1, radii the caller's array itself
     double rmin_all = 1e300;
-    // one instance: branch-free checks over whole arrays first (fast for
-    // millions of particles); the loop below runs only to name a failure
+    // one instance: the host reads only the radii (their minimum sets the skin
+    // and the grid); k_pack checks every other array on the device, and the
+    // loop below runs only to name a failure it reports
     bool checked = false;
     if (one) {
-        const int nsp = h->inst_desc[0].n_species;
-        int bad = 0;
+        bool bad = false;
         double rmin = 1e300;
         for (long long i = 0; i < n; ++i) {
             const double r = p->radius[i];
-            bad |= !(r > 0.0) | !(r <= DBL_MAX) | (p->species[i] < 0) | (p->species[i] >= nsp) | !(p->inv_mass[i] >= 0.0);
-            if (p->instance) bad |= p->instance[i] != 0;
+            bad |= !(r > 0.0) | !(r <= DBL_MAX);
             rmin = r < rmin ? r : rmin;
         }
-        for (long long i = 0; i < 3 * n; ++i)
-            bad |= !(std::fabs(p->position[i]) <= DBL_MAX) | !(std::fabs(p->velocity[i]) <= DBL_MAX);
         if (!bad) {
             checked = true;
             rmin_all = n > 0 ? rmin : rmin_all;
         }
     }
-    for (long long i = 0; i < n && !checked; ++i) {
-        const int in = p->instance ? p->instance[i] : 0;
-        if (in < 0 || in >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "particle instance out of range");
-        const double r = p->radius[i];
-        if (!(r > 0.0) || !std::isfinite(r)) return fail(h, DEM_ERR_BAD_INPUT, "particle radius must be positive");
-        if (p->species[i] < 0 || p->species[i] >= h->inst_desc[in].n_species)
-            return fail(h, DEM_ERR_BAD_INPUT, "particle species out of range");
-        if (!(p->inv_mass[i] >= 0.0)) return fail(h, DEM_ERR_BAD_INPUT, "inverse mass must be >= 0");
-        for (int k = 0; k < 3; ++k)
-            if (!std::isfinite(p->position[3 * i + k]) || !std::isfinite(p->velocity[3 * i + k]))
-                return fail(h, DEM_ERR_BAD_INPUT, "non-finite particle state");
-        if (!one) {
-            radii[in].push_back(r);
-            members[in].push_back(i);
+    auto validate = [&]() -> int { // every particle on the host, in caller order: names the first violation
+        for (long long i = 0; i < n; ++i) {
+            const int in = p->instance ? p->instance[i] : 0;
+            if (in < 0 || in >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "particle instance out of range");
+            const double r = p->radius[i];
+            if (!(r > 0.0) || !std::isfinite(r)) return fail(h, DEM_ERR_BAD_INPUT, "particle radius must be positive");
+            if (p->species[i] < 0 || p->species[i] >= h->inst_desc[in].n_species)
+                return fail(h, DEM_ERR_BAD_INPUT, "particle species out of range");
+            if (!(p->inv_mass[i] >= 0.0)) return fail(h, DEM_ERR_BAD_INPUT, "inverse mass must be >= 0");
+            for (int k = 0; k < 3; ++k)
+                if (!std::isfinite(p->position[3 * i + k]) || !std::isfinite(p->velocity[3 * i + k]))
+                    return fail(h, DEM_ERR_BAD_INPUT, "non-finite particle state");
         }
-        rmin_all = std::min(rmin_all, r);
+        return DEM_OK;
+    };
+    if (!checked) {
+        if (int rc0 = validate()) return rc0;
+        for (long long i = 0; i < n; ++i) {
+            const int in = p->instance ? p->instance[i] : 0;
+            const double r = p->radius[i];
+            if (!one) {
+                radii[in].push_back(r);
+                members[in].push_back(i);
+            }
+            rmin_all = std::min(rmin_all, r);
+        }
     }
     // ---- walls per instance
     std::vector<int> wbegin(ninst, 0), wend(ninst, 0);
@@ -885,10 +893,19 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         (rc = put(st.ii, p->inv_inertia, dn)) || (rc = put(st.sp, p->species, in4)) || (rc = put(st.id, p->id, in4)) ||
         (rc = put(st.inst, p->instance, in4)) || (rc = put(st.lvl, level.data(), in4)))
         return rc;
+    Control c{};
+    c.cur = 0;
+    c.lbuf = 0;
+    c.skin = skin;
+    c.force_rebuild = 1;
+    c.record = 1;
+    c.record_capacity = h->record_capacity;
+    CU(cudaMemcpyAsync(h->d_ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
     if (n > 0)
         k_pack<<<grid_for(n, 256), 256, 0, h->stream>>>(d, st, p->angular_velocity != nullptr,
                                                         p->orientation != nullptr, p->inv_inertia != nullptr,
-                                                        p->instance != nullptr);
+                                                        p->instance != nullptr,
+                                                        one ? h->inst_desc[0].n_species : INT_MAX, one ? 1 : 0);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(h->d_inst, h->inst.data(), h->inst.size() * sizeof(InstanceDev), cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(h->d_species, h->species.data(), h->species.size() * sizeof(dem_species_pair),
@@ -899,16 +916,15 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         CU(cudaMemcpyAsync(h->d_wgeom, h->wgeom.data(), h->wgeom.size() * sizeof(WallGeom), cudaMemcpyHostToDevice,
                            h->stream));
     }
-    Control c{};
-    c.cur = 0;
-    c.lbuf = 0;
-    c.skin = skin;
-    c.force_rebuild = 1;
-    c.record = 1;
-    c.record_capacity = h->record_capacity;
-    CU(cudaMemcpyAsync(h->d_ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemsetAsync(d.tri_first_n, 0, NC * sizeof(int), h->stream)); // filled by the initial evaluation
+    unsigned int status = 0;
+    CU(cudaMemcpyAsync(&status, &h->d_ctl->status, sizeof(status), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
+    if (status & (1u << DEM_ERR_BAD_INPUT)) { // k_pack found bad input: name it
+        h->uploaded = false;
+        const int rc1 = validate();
+        return rc1 ? rc1 : fail(h, DEM_ERR_BAD_INPUT, "particle arrays out of range");
+    }
     h->uploaded = true;
     h->initial_pending = true;
     h->records_valid = false;

@@ -776,13 +776,24 @@ __host__ __device__ inline StagePtrs stage_ptrs(double* base, size_t nc)
     return s;
 }
 
-// caller order -> state buffer 0 (identity permutation until the first rebuild)
+// caller order -> state buffer 0 (identity permutation until the first rebuild).
+// It also checks what it packs (finite positions and velocities, radius > 0,
+// species below nsp, inverse mass >= 0, instance 0 where one_instance) and
+// reports a violation as DEM_ERR_BAD_INPUT in the control status.
 __global__ void __launch_bounds__(256) k_pack(DevPtrs d, StagePtrs s, int has_ang, int has_ori, int has_ii,
-                                              int has_inst)
+                                              int has_inst, int nsp, int one_instance)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n) return;
     const double im = s.im[i];
+    {
+        bool bad = !(s.rad[i] > 0.0) || !(s.rad[i] <= DBL_MAX) || !(im >= 0.0) || s.sp[i] < 0 || s.sp[i] >= nsp ||
+                   (one_instance && has_inst && s.inst[i] != 0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            bad = bad || !(fabs(s.pos[3 * i + k]) <= DBL_MAX) || !(fabs(s.vel[3 * i + k]) <= DBL_MAX);
+        if (bad) atomicOr(&d.ctl->status, 1u << DEM_ERR_BAD_INPUT);
+    }
     d.pr[0][i] = make_double4(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], s.rad[i]);
     d.vm[0][i] = make_double4(s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2], im);
     d.wi[0][i] = make_double4(has_ang ? s.ang[3 * i] : 0.0, has_ang ? s.ang[3 * i + 1] : 0.0,

@@ -64,6 +64,8 @@ extern "C" {
 #define DEM_MAX_WALL_FACES  8
 #define DEM_MAX_WALLS_PER_INSTANCE 32
 #define DEM_MAX_DELETION_PER_INSTANCE 2
+#define DEM_MAX_INSERTION_PER_INSTANCE 4
+#define DEM_MAX_PSD_POINTS 64
 
 /* Parameters of one (mixed) species pair, as held by the reference's
  * Species<Normal,Friction,Adhesive> objects and the mixed-species triangle
@@ -224,6 +226,54 @@ typedef struct dem_deletion_boundary {
     double  distance;
 } dem_deletion_boundary;
 
+/* A CubeInsertionBoundary. Every time step, after the drift and before the
+ * forces (DPMBase::computeOneTimeStep, Kernel/DPMBase.cc:4348-4352),
+ * InsertionBoundary::checkBoundaryBeforeTimeStep (Kernel/Boundaries/
+ * InsertionBoundary.cc:184-296) places new particles until max_failed
+ * successive placements have failed or the inserted volume reaches
+ * volume_flow_rate x (time + dt) + initial_volume (insertParticle, :150-176):
+ *  - a new particle (InsertionBoundary::generateParticle, :103-142) takes
+ *    one draw of the instance's random number generator (the species choice
+ *    of a single template) and its radius from the cumulative number
+ *    distribution psd_* with the PSD's own generator (PSD::drawSample,
+ *    Kernel/Math/PSD.cc:114-128); it is drawn again only after it was placed;
+ *  - a placement draws the position in [pos_min, pos_max] and the velocity in
+ *    [vel_min, vel_max], x, y, z each (CubeInsertionBoundary::placeParticle,
+ *    Kernel/Boundaries/CubeInsertionBoundary.cc:173-184), and succeeds when
+ *    the particle touches no wall and no particle, its periodic images
+ *    included (DPMBase::checkParticleForInteractionLocalPeriodic and
+ *    checkParticleForInteractionLocal, DPMBase.cc:4868-4958);
+ *  - mass and inertia are BaseParticle::computeMass's (Kernel/Particles/
+ *    BaseParticle.cc:874-883) for the density; the angular velocity is zero
+ *    and the orientation the identity.
+ * The instance's generator (DPMBase::random) is in the state
+ * RNG::setRandomSeed(seed) leaves it in (Kernel/Math/RNG.cc: the lagged
+ * Fibonacci generator 607/273 seeded by the linear congruential one) when
+ * the particles are uploaded, and carries on from step to step; a boundary's
+ * PSD generator starts from psd_seed (the PSD's default is 0).
+ * Inserted particles take the free rows of the upload: rows of the
+ * boundary's instance with radius 0, in row order, each keeping its row's
+ * id (give free rows the ids the reference's ParticleHandler hands out:
+ * consecutive after the largest id in use). A free row is reported with
+ * instance -1 until a particle is placed in it; with none left, dem_step
+ * returns DEM_ERR_CAPACITY. */
+typedef struct dem_insertion_boundary {
+    int32_t  instance;
+    int32_t  species;              /* the template particle's species (index in the instance) */
+    int32_t  max_failed;           /* InsertionBoundary::maxFailed_                   */
+    int32_t  n_psd;                /* points of the PSD: 2 .. DEM_MAX_PSD_POINTS      */
+    double   pos_min[3];           /* CubeInsertionBoundary::setGeometry              */
+    double   pos_max[3];
+    double   vel_min[3];
+    double   vel_max[3];
+    double   density;              /* ParticleSpecies::getDensity of the species      */
+    double   volume_flow_rate;     /* setVolumeFlowRate; +infinity (the default): none */
+    double   initial_volume;       /* setInitialVolume                                */
+    double   psd_radius[DEM_MAX_PSD_POINTS];      /* PSD::getParticleSizeDistribution(): radii    */
+    double   psd_probability[DEM_MAX_PSD_POINTS]; /* and cumulative probabilities, from 0 to 1    */
+    uint64_t psd_seed;             /* PSD::setRandomSeed                              */
+} dem_insertion_boundary;
+
 /* Gaussian coarse-graining grid (CG<XZ|XYZ|O, Gauss, StandardFields>,
  * Kernel/CG/CG.hcc:233-528, Kernel/CG/Fields/StandardFields.cc:184-250).
  * The fields of StandardFields per grid point, in this order (29 doubles):
@@ -292,6 +342,24 @@ int  dem_set_deletion_boundaries(dem_handle *h, const dem_deletion_boundary *b, 
  * interactions are). Before the upload or between dem_step calls; not for
  * triangle walls. */
 int  dem_remove_wall(dem_handle *h, int wall);
+/* InsertionBoundary objects of BoundaryHandler (CubeInsertionBoundary, above),
+ * at most DEM_MAX_INSERTION_PER_INSTANCE per instance, run in array order
+ * after the deletion boundaries' checks. seeds[i] is instance i's
+ * RNG::setRandomSeed value (NULL: 0 for every instance, DPMBase's own,
+ * DPMBase.cc:279). Before dem_upload_particles, which sizes the cell grid for
+ * the PSD's radii, reserves the free rows and starts the generators. */
+int  dem_set_insertion_boundaries(dem_handle *h, const dem_insertion_boundary *b, int n,
+                                  const uint64_t *seeds);
+/* Per boundary (the order given): particles placed so far and their volume
+ * (InsertionBoundary::getNumberOfParticlesInserted / getVolumeOfParticlesInserted). */
+int  dem_get_insertion_counts(dem_handle *h, int64_t *inserted, double *volume, int n);
+/* The first n values of RNG::getRandomNumber(0, 1) after RNG::setRandomSeed(seed)
+ * (Kernel/Math/RNG.cc), from the generator the insertion kernel runs, here on
+ * the host: a check of the restatement that needs no device. */
+int  dem_rng_draws(uint64_t seed, int n, double *out);
+/* The first n radii PSD::drawSample (Kernel/Math/PSD.cc:114-128) gives for
+ * the boundary's PSD and psd_seed, from the kernel's code run on the host. */
+int  dem_psd_draws(const dem_insertion_boundary *b, int n, double *out);
 /* ParticleHandler contents; triggers the first force evaluation on the next
  * dem_step (the one DPMBase::initialiseSolve performs, DPMBase.cc:4180). */
 int  dem_upload_particles(dem_handle *h, const dem_particles_soa *p);

@@ -39,6 +39,8 @@ DEM_MAX_TRIANGLE_CONTACTS = 8
 DEM_MAX_LEVELS = 4
 DEM_MAX_WALL_FACES = 8
 DEM_MAX_DELETION_PER_INSTANCE = 2
+DEM_MAX_INSERTION_PER_INSTANCE = 4
+DEM_MAX_PSD_POINTS = 64
 
 DEM_CG_NFIELDS = 29
 DEM_CG_O = 0
@@ -89,6 +91,15 @@ class ContactsSoA(C.Structure):
 
 class DeletionBoundary(C.Structure):
     _fields_ = [("instance", _i32), ("reserved", _i32), ("normal", _d * 3), ("distance", _d)]
+
+
+class InsertionBoundary(C.Structure):
+    _fields_ = [
+        ("instance", _i32), ("species", _i32), ("max_failed", _i32), ("n_psd", _i32), ("pos_min", _d * 3),
+        ("pos_max", _d * 3), ("vel_min", _d * 3), ("vel_max", _d * 3), ("density", _d), ("volume_flow_rate", _d),
+        ("initial_volume", _d), ("psd_radius", _d * DEM_MAX_PSD_POINTS), ("psd_probability", _d * DEM_MAX_PSD_POINTS),
+        ("psd_seed", C.c_uint64),
+    ]
 
 
 class InstanceDesc(C.Structure):
@@ -151,6 +162,11 @@ _SIGNATURES = {
     "dem_get_info": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_get_memory": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_remove_wall": (C.c_int, [C.c_void_p, C.c_int]),
+    "dem_set_insertion_boundaries": (C.c_int, [C.c_void_p, C.POINTER(InsertionBoundary), C.c_int,
+                                               C.POINTER(C.c_uint64)]),
+    "dem_get_insertion_counts": (C.c_int, [C.c_void_p, C.POINTER(_i64), _pd, C.c_int]),
+    "dem_rng_draws": (C.c_int, [C.c_uint64, C.c_int, _pd]),
+    "dem_psd_draws": (C.c_int, [C.POINTER(InsertionBoundary), C.c_int, _pd]),
     "dem_get_counts": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "dem_time_force_kernel": (C.c_int, [C.c_void_p, C.c_int, _pd]),
     "dem_selftest_wait_expiry": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_uint32)]),

@@ -17,12 +17,14 @@
 #include "dem_kernels.cuh"
 #include "dem_pipeline.cuh"
 #include "dem_rebuild.cuh"
+#include "dem_insert.cuh"
 
 using namespace dem;
 
 namespace {
 
-constexpr unsigned FATAL_STATUS = (1u << DEM_ERR_CAPACITY) | (1u << DEM_ERR_NAN) | (1u << DEM_ERR_TIMEOUT);
+constexpr unsigned FATAL_STATUS =
+    (1u << DEM_ERR_CAPACITY) | (1u << DEM_ERR_NAN) | (1u << DEM_ERR_TIMEOUT) | (1u << INS_STATUS_NO_ROW);
 constexpr int GRAPH_STEPS = 16;
 constexpr int CONTROL_THREADS = 128;
 
@@ -37,6 +39,15 @@ struct Handle {
     std::vector<int> wall_grouped;     // caller index -> grouped index
     std::vector<dem_deletion_boundary> deletions;
     std::vector<char> wall_removed;    // per wall (grouped order): taken out by dem_remove_wall
+    // insertion boundaries (the caller's order) and the generators' seeds per
+    // instance; they take effect at the next upload
+    std::vector<dem_insertion_boundary> ins;
+    std::vector<uint64_t> ins_seeds;
+    std::vector<int> ins_order;        // device order (grouped by instance) -> caller index
+    InsInstanceDev* d_ins_inst = nullptr;
+    InsBoundaryDev* d_ins_bnd = nullptr;
+    int* d_ins_rows = nullptr;
+    int n_ins_inst = 0;                // instances with insertion boundaries (blocks of k_insert)
     std::string err;
     int device = 0;
     cudaStream_t stream = nullptr, stream2 = nullptr;
@@ -125,6 +136,9 @@ void free_particle_arrays(Handle* h)
     h->record_capacity = 0;
     h->d_stage = nullptr;
     h->d_batch = nullptr;
+    h->d_ins_inst = nullptr;
+    h->d_ins_bnd = nullptr;
+    h->d_ins_rows = nullptr;
     h->layout.clear();
 }
 
@@ -148,6 +162,14 @@ cudaError_t launch_rebuild(Handle* h, cudaStream_t s)
     return cudaLaunchKernelEx(&cfg, k_rebuild, h->d, h->d.rb_barrier);
 }
 constexpr int REBUILD_LAUNCHES = 1;
+
+// Insertion boundaries: one block per instance that has some (dem_insert.cuh),
+// after k_control and before the rebuild it may request.
+void launch_insert(Handle* h, cudaStream_t s)
+{
+    if (h->n_ins_inst > 0)
+        k_insert<<<h->n_ins_inst, INS_THREADS, 0, s>>>(h->d, InsPtrs{h->d_ins_inst, h->d_ins_bnd, h->d_ins_rows});
+}
 constexpr int FORCE_LAUNCHES = 3;
 
 // Law variants the force kernel is instantiated for; the handle uses a
@@ -242,6 +264,7 @@ int build_graph(Handle* h, int steps, bool last, cudaGraphExec_t* out)
     CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < steps; ++k) {
         k_control<<<1, CONTROL_THREADS, 0, s>>>(h->d_ctl, h->d.walls, h->d_wgeom, h->d.n_walls, h->d.dt);
+        launch_insert(h, s);
         const cudaError_t e = launch_rebuild(h, s);
         if (e != cudaSuccess) {
             cudaGraph_t g = nullptr;
@@ -274,6 +297,8 @@ int check_status(Handle* h, const Control& c)
         return fail(h, DEM_ERR_CAPACITY, "neighbour-list capacity exceeded (max_neighbors=" +
                                              std::to_string(h->d.cap) + "); raise dem_config.max_neighbors");
     if (st & (1u << DEM_ERR_NAN)) return fail(h, DEM_ERR_NAN, "non-finite force detected");
+    if (st & (1u << INS_STATUS_NO_ROW))
+        return fail(h, DEM_ERR_CAPACITY, "an insertion boundary found no free row (upload more rows of radius 0)");
     // a rebuild block gave up at a grid barrier: the arrival counter no longer
     // sits on a multiple of the launch's barriers, so it starts again at zero
     if (h->d.rb_barrier) cudaMemsetAsync(h->d.rb_barrier, 0, sizeof(unsigned long long), h->stream);
@@ -284,12 +309,21 @@ int check_status(Handle* h, const Control& c)
 // MercuryBase.cc:204-306, restated as dense per-level grids): radii are
 // grouped in geometric bands of ratio 2 starting at the smallest radius; a
 // level's cell edge is at least 2 r_max(level) + interaction distance + skin.
+// [psd_lo, psd_hi] (psd_hi > 0): radii insertion boundaries may place later;
+// every band they reach gets a level sized for its largest radius.
 void setup_instance_grid(const dem_instance_desc& in, const double* radii, size_t count, double skin, double dmax,
-                         InstanceDev& I, std::vector<int>& level_of, int& cell_base)
+                         double psd_lo, double psd_hi, InstanceDev& I, std::vector<int>& level_of, int& cell_base)
 {
     double rmin = 1e300, rmax = 0.0;
     for (size_t i = 0; i < count; ++i) { rmin = std::min(rmin, radii[i]); rmax = std::max(rmax, radii[i]); }
-    const bool empty = count == 0;
+    const bool psd = psd_hi > 0.0;
+    // a little above the largest PSD radius: PSD::drawSample's interpolation rounds
+    const double phi = psd_hi * (1.0 + 1e-12);
+    if (psd) {
+        rmin = std::min(rmin, psd_lo);
+        rmax = std::max(rmax, phi);
+    }
+    const bool empty = count == 0 && !psd;
     if (empty) { rmin = rmax = 1.0; }
     int nl = 1;
     while (nl < DEM_MAX_LEVELS && rmax >= rmin * std::pow(2.0, nl)) ++nl;
@@ -309,6 +343,19 @@ void setup_instance_grid(const dem_instance_desc& in, const double* radii, size_
         lrmax[l] = std::max(lrmax[l], radii[i]);
         used[l] = 1;
     }
+    if (psd) {
+        auto band = [&](double r) {
+            const double x = r / rmin;
+            uint64_t bits;
+            std::memcpy(&bits, &x, sizeof(bits));
+            return std::max(0, std::min(nl - 1, (int)((bits >> 52) & 0x7ffu) - 1023));
+        };
+        const int b0 = band(psd_lo), b1 = band(phi);
+        for (int l = b0; l <= b1; ++l) { // a band's radii lie below rmin 2^(l+1)
+            used[l] = 1;
+            lrmax[l] = std::max(lrmax[l], l == b1 ? phi : std::min(phi, std::ldexp(rmin, l + 1)));
+        }
+    }
     // drop empty levels
     std::vector<int> remap(nl, -1);
     int nu = 0;
@@ -318,6 +365,9 @@ void setup_instance_grid(const dem_instance_desc& in, const double* radii, size_
     if (nu != nl) // some level is empty: renumber (usually every level is used)
         for (size_t i = 0; i < count; ++i) level_of[i] = remap[level_of[i]];
     I.n_levels = nu;
+    I.level_rmin = rmin;
+    I.level_bands = nl;
+    for (int l = 0; l < DEM_MAX_LEVELS; ++l) I.level_remap[l] = l < nl ? remap[l] : -1;
     for (int l = 0; l < nu; ++l) {
         const double cs = 2.0 * lr[l] + dmax + skin;
         I.level_rmax[l] = lr[l];
@@ -551,6 +601,84 @@ int dem_remove_wall(dem_handle* hh, int wall)
     return push_instances(h);
 }
 
+int dem_set_insertion_boundaries(dem_handle* hh, const dem_insertion_boundary* b, int n, const uint64_t* seeds)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || n < 0 || (n > 0 && !b)) return fail(h, DEM_ERR_BAD_INPUT, "dem_set_insertion_boundaries: bad arguments");
+    const int ninst = (int)h->inst_desc.size();
+    std::vector<int> per(ninst, 0);
+    auto finite = [](double x) { return std::isfinite(x); };
+    for (int k = 0; k < n; ++k) {
+        const dem_insertion_boundary& x = b[k];
+        if (x.instance < 0 || x.instance >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: instance out of range");
+        if (++per[x.instance] > DEM_MAX_INSERTION_PER_INSTANCE)
+            return fail(h, DEM_ERR_BAD_INPUT, "more than DEM_MAX_INSERTION_PER_INSTANCE insertion boundaries in an instance");
+        if (x.species < 0 || x.species >= h->inst_desc[x.instance].n_species)
+            return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: species out of range");
+        if (x.max_failed < 0) return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: max_failed must be >= 0");
+        if (x.n_psd < 2 || x.n_psd > DEM_MAX_PSD_POINTS)
+            return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: n_psd must be in 2..DEM_MAX_PSD_POINTS");
+        if (!(x.density > 0.0) || !finite(x.density)) return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: bad density");
+        if (!(x.volume_flow_rate >= 0.0) || !finite(x.initial_volume))
+            return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: bad volume flow rate or initial volume");
+        for (int a = 0; a < 3; ++a)
+            if (!finite(x.pos_min[a]) || !finite(x.pos_max[a]) || !(x.pos_min[a] <= x.pos_max[a]) ||
+                !finite(x.vel_min[a]) || !finite(x.vel_max[a]) || !(x.vel_min[a] <= x.vel_max[a]))
+                return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: bad position or velocity range");
+        // a cumulative number distribution from 0 to 1 over positive radii
+        // (PSD::validateCumulativeDistribution's result)
+        for (int j = 0; j < x.n_psd; ++j) {
+            if (!(x.psd_radius[j] > 0.0) || !finite(x.psd_radius[j]))
+                return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: PSD radii must be positive");
+            if (j > 0 && !(x.psd_probability[j] >= x.psd_probability[j - 1]))
+                return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: PSD probabilities must not decrease");
+        }
+        if (x.psd_probability[0] != 0.0 || x.psd_probability[x.n_psd - 1] != 1.0)
+            return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: PSD probabilities must run from 0 to 1");
+    }
+    h->ins.assign(b, b + n);
+    h->ins_seeds.assign(ninst, 0);
+    if (seeds) h->ins_seeds.assign(seeds, seeds + ninst);
+    return DEM_OK;
+}
+
+int dem_get_insertion_counts(dem_handle* hh, int64_t* inserted, double* volume, int n)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || n < 0 || n > (int)h->ins.size()) return fail(h, DEM_ERR_BAD_INPUT, "dem_get_insertion_counts: bad arguments");
+    if (!h->uploaded || h->n_ins_inst == 0 || h->ins_order.size() != h->ins.size())
+        return fail(h, DEM_ERR_STATE, "no insertion boundaries uploaded");
+    CU(cudaSetDevice(h->device));
+    std::vector<InsBoundaryDev> bnd(h->ins.size());
+    CU(cudaMemcpyAsync(bnd.data(), h->d_ins_bnd, bnd.size() * sizeof(InsBoundaryDev), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    for (size_t k = 0; k < bnd.size(); ++k) {
+        const int i = h->ins_order[k];
+        if (i >= n) continue;
+        if (inserted) inserted[i] = bnd[k].n_inserted;
+        if (volume) volume[i] = bnd[k].volume_inserted;
+    }
+    return DEM_OK;
+}
+
+int dem_psd_draws(const dem_insertion_boundary* b, int n, double* out)
+{
+    if (!b || n < 0 || (n > 0 && !out) || b->n_psd < 2 || b->n_psd > DEM_MAX_PSD_POINTS) return DEM_ERR_BAD_INPUT;
+    Lfg g;
+    lfg_seed(b->psd_seed, g);
+    for (int i = 0; i < n; ++i) out[i] = psd_draw(*b, g.v, g.head);
+    return DEM_OK;
+}
+
+int dem_rng_draws(uint64_t seed, int n, double* out)
+{
+    if (n < 0 || (n > 0 && !out)) return DEM_ERR_BAD_INPUT;
+    Lfg g;
+    lfg_seed(seed, g);
+    for (int i = 0; i < n; ++i) out[i] = lfg_uniform(g.v, g.head, 0.0, 1.0);
+    return DEM_OK;
+}
+
 int dem_set_deletion_boundaries(dem_handle* hh, const dem_deletion_boundary* b, int n)
 {
     Handle* h = reinterpret_cast<Handle*>(hh);
@@ -588,13 +716,29 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     // ---- validate and collect per-instance radii
     std::vector<std::vector<double>> radii(ninst);
     std::vector<std::vector<long long>> members(ninst);
-    const bool one = ninst == 1; // one instance: members are 0..n-1, radii the caller's array itself
+    const bool one = ninst == 1;
+    // insertion boundaries: the radius range of each instance's PSDs; rows of
+    // such an instance with radius 0 are its free rows
+    std::vector<double> psd_lo(ninst, 0.0), psd_hi(ninst, 0.0);
+    std::vector<char> has_ins(ninst, 0);
+    for (const auto& b : h->ins) {
+        if (b.instance >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary instance out of range");
+        for (int k = 0; k < b.n_psd; ++k) {
+            const double r = b.psd_radius[k];
+            psd_lo[b.instance] = has_ins[b.instance] ? std::min(psd_lo[b.instance], r) : r;
+            psd_hi[b.instance] = std::max(psd_hi[b.instance], r);
+            has_ins[b.instance] = 1;
+        }
+    }
+    std::vector<std::vector<int>> free_rows(ninst);
+    // one instance without insertion: members are 0..n-1, radii the caller's array itself
+    const bool fast = one && h->ins.empty();
     double rmin_all = 1e300;
     // one instance: the host reads only the radii (their minimum sets the skin
     // and the grid); k_pack checks every other array on the device, and the
     // loop below runs only to name a failure it reports
     bool checked = false;
-    if (one) {
+    if (fast) {
         bool bad = false;
         double rmin = 1e300;
         for (long long i = 0; i < n; ++i) {
@@ -612,6 +756,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
             const int in = p->instance ? p->instance[i] : 0;
             if (in < 0 || in >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "particle instance out of range");
             const double r = p->radius[i];
+            if (r == 0.0 && has_ins[in]) continue; // a free row
             if (!(r > 0.0) || !std::isfinite(r)) return fail(h, DEM_ERR_BAD_INPUT, "particle radius must be positive");
             if (p->species[i] < 0 || p->species[i] >= h->inst_desc[in].n_species)
                 return fail(h, DEM_ERR_BAD_INPUT, "particle species out of range");
@@ -627,13 +772,19 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         for (long long i = 0; i < n; ++i) {
             const int in = p->instance ? p->instance[i] : 0;
             const double r = p->radius[i];
-            if (!one) {
+            if (r == 0.0 && has_ins[in]) {
+                free_rows[in].push_back((int)i);
+                continue;
+            }
+            if (!fast) {
                 radii[in].push_back(r);
                 members[in].push_back(i);
             }
             rmin_all = std::min(rmin_all, r);
         }
     }
+    for (int in = 0; in < ninst; ++in)
+        if (has_ins[in]) rmin_all = std::min(rmin_all, psd_lo[in]);
     // ---- walls per instance
     std::vector<int> wbegin(ninst, 0), wend(ninst, 0);
     {
@@ -656,8 +807,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     h->inst.assign(ninst, InstanceDev{});
     // levels of all particles; one instance fills the handle's buffer, which
     // keeps its size between uploads (no allocation or zeroing per upload)
-    std::vector<int> level_multi(one ? 0 : n, 0);
-    std::vector<int>& level = one ? h->level_buf : level_multi;
+    std::vector<int> level_multi(fast ? 0 : n, 0);
+    std::vector<int>& level = fast ? h->level_buf : level_multi;
     double rmax_all = 0.0;
     int cell_base = 0;
     for (int in = 0; in < ninst; ++in) {
@@ -718,15 +869,16 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         }
         fill_deletions(h, I, in);
         std::vector<int> lv_multi;
-        std::vector<int>& lv = one ? h->level_buf : lv_multi;
-        const double* rad = one ? p->radius : radii[in].data();
-        const size_t nrad = one ? (size_t)n : radii[in].size();
-        setup_instance_grid(D, rad, nrad, skin, dmax, I, lv, cell_base);
-        if (!one)
+        std::vector<int>& lv = fast ? h->level_buf : lv_multi;
+        const double* rad = fast ? p->radius : radii[in].data();
+        const size_t nrad = fast ? (size_t)n : radii[in].size();
+        setup_instance_grid(D, rad, nrad, skin, dmax, psd_lo[in], psd_hi[in], I, lv, cell_base);
+        if (!fast)
             for (size_t k = 0; k < members[in].size(); ++k) level[members[in][k]] = lv[k];
+        for (int r : free_rows[in]) level[r] = -1; // k_pack parks it dormant
         // a periodic dimension must be longer than twice the largest reach
         double rm = 0.0;
-        if (nrad > 0)
+        if (nrad > 0 || has_ins[in])
             for (int l = 0; l < I.n_levels; ++l) rm = std::max(rm, I.level_rmax[l]);
         rmax_all = std::max(rmax_all, rm);
         for (int k = 0; k < 3; ++k)
@@ -758,11 +910,13 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     // and the captured graphs (their kernel arguments stay valid)
     const unsigned record_capacity = (unsigned)std::min<long long>(
         item_cap, std::min<long long>(2000000000ll, 8 * n + 1024 + (long long)n * std::min(wmax, 4)));
+    int n_ins_inst = 0;
+    for (int in = 0; in < ninst; ++in) n_ins_inst += has_ins[in];
     long long any_tri = 0;
     for (const auto& w : h->walls) any_tri = any_tri || w.type == DEM_WALL_TRIANGLE;
     const std::vector<long long> layout = {n, cap, wmax, ncells, (long long)h->inst.size(), (long long)h->species.size(),
                                            (long long)h->walls.size(), (long long)record_capacity, h->ncomp, any_tri,
-                                           item_cap};
+                                           item_cap, (long long)h->ins.size(), (long long)n_ins_inst};
     const bool reuse = !h->layout.empty() && h->layout == layout;
     if (!reuse) free_particle_arrays(h);
     const DevPtrs kept = h->d;
@@ -808,7 +962,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         d.block_sums = kept.block_sums; d.rb_barrier = kept.rb_barrier; d.inst = kept.inst; d.species = kept.species; d.walls = kept.walls;
         d.wgeom = kept.wgeom; d.n_walls = kept.n_walls; d.ctl = kept.ctl; d.records = kept.records;
         d.n_instances = kept.n_instances;
-        d.pf = kept.pf; d.rows = kept.rows;
+        d.pf = kept.pf; d.rows = kept.rows; d.row_slot = kept.row_slot;
         d.rev = kept.rev; d.slot = kept.slot; d.slotw = kept.slotw; d.items = kept.items; d.shares = kept.shares;
         d.item_cap = kept.item_cap;
         d.tri_list = kept.tri_list;
@@ -841,6 +995,12 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     if ((rc = dalloc(h, &d.rev, (size_t)cap * NC))) return rc;
     if ((rc = dalloc(h, &d.rows, (size_t)cap * NC))) return rc;
     if ((rc = dalloc(h, &d.pf, NC))) return rc;
+    if (!h->ins.empty()) {
+        if ((rc = dalloc(h, &d.row_slot, NC))) return rc;
+        if ((rc = dalloc(h, &h->d_ins_inst, (size_t)n_ins_inst))) return rc;
+        if ((rc = dalloc(h, &h->d_ins_bnd, h->ins.size()))) return rc;
+        if ((rc = dalloc(h, &h->d_ins_rows, NC))) return rc;
+    }
     if ((rc = dalloc(h, &d.slot, (size_t)cap * NC))) return rc;
     if ((rc = dalloc(h, &d.slotw, (size_t)wmax * NC))) return rc;
     d.item_cap = (int)item_cap;
@@ -917,6 +1077,44 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
                            h->stream));
     }
     CU(cudaMemsetAsync(d.tri_first_n, 0, NC * sizeof(int), h->stream)); // filled by the initial evaluation
+    // insertion boundaries: generators seeded, counters zero, free rows listed
+    // per instance (InsertionBoundary's state at the start of a run)
+    std::vector<InsInstanceDev> ins_inst;
+    std::vector<InsBoundaryDev> ins_bnd;
+    std::vector<int> ins_rows;
+    h->ins_order.clear();
+    for (int in = 0; in < ninst && !h->ins.empty(); ++in) {
+        if (!has_ins[in]) continue;
+        InsInstanceDev S{};
+        lfg_seed(h->ins_seeds[in], S.rng);
+        S.time = 0.0;
+        S.instance = in;
+        S.first = (int)ins_bnd.size();
+        for (size_t k = 0; k < h->ins.size(); ++k) {
+            if (h->ins[k].instance != in) continue;
+            InsBoundaryDev B{};
+            B.b = h->ins[k];
+            lfg_seed(B.b.psd_seed, B.psd);
+            ins_bnd.push_back(B);
+            h->ins_order.push_back((int)k);
+        }
+        S.count = (int)ins_bnd.size() - S.first;
+        S.rows_begin = (int)ins_rows.size();
+        ins_rows.insert(ins_rows.end(), free_rows[in].begin(), free_rows[in].end());
+        S.rows_end = (int)ins_rows.size();
+        S.next_row = S.rows_begin;
+        ins_inst.push_back(S);
+    }
+    h->n_ins_inst = (int)ins_inst.size();
+    if (h->n_ins_inst > 0) {
+        CU(cudaMemcpyAsync(h->d_ins_inst, ins_inst.data(), ins_inst.size() * sizeof(InsInstanceDev),
+                           cudaMemcpyHostToDevice, h->stream));
+        CU(cudaMemcpyAsync(h->d_ins_bnd, ins_bnd.data(), ins_bnd.size() * sizeof(InsBoundaryDev),
+                           cudaMemcpyHostToDevice, h->stream));
+        if (!ins_rows.empty())
+            CU(cudaMemcpyAsync(h->d_ins_rows, ins_rows.data(), ins_rows.size() * sizeof(int), cudaMemcpyHostToDevice,
+                               h->stream));
+    }
     unsigned int status = 0;
     CU(cudaMemcpyAsync(&status, &h->d_ctl->status, sizeof(status), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
@@ -1103,15 +1301,16 @@ int dem_step(dem_handle* hh, int nsteps)
                 }
                 while (left-- > 0) CU(cudaGraphLaunch(h->graph1, h->stream));
                 CU(cudaGraphLaunch(h->graphF, h->stream));
-                launches += (1ll + REBUILD_LAUNCHES + force_launches(h)) * nsteps;
+                launches += (1ll + REBUILD_LAUNCHES + force_launches(h) + (h->n_ins_inst > 0)) * nsteps;
             } else {
                 for (int k = 0; k < nsteps; ++k) {
                     k_control<<<1, CONTROL_THREADS, 0, h->stream>>>(h->d_ctl, d.walls, h->d_wgeom, d.n_walls, d.dt);
+                    launch_insert(h, h->stream);
                     CU(launch_rebuild(h, h->stream));
                     launch_force(h, h->stream, 1, k == nsteps - 1);
                 }
                 CU(cudaGetLastError());
-                launches += (1ll + force_launches(h) + REBUILD_LAUNCHES) * nsteps;
+                launches += (1ll + force_launches(h) + REBUILD_LAUNCHES + (h->n_ins_inst > 0)) * nsteps;
             }
             k_flip<<<1, 32, 0, h->stream>>>(h->d_ctl);
             launches += 1;

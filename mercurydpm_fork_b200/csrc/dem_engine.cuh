@@ -36,6 +36,9 @@ constexpr int FLAG_FIXED = 1;
 // deleted by a DeletionBoundary: also FLAG_FIXED, parked at DELETED_COORD,
 // sorted into the graveyard cell (the last cell) at the next rebuild
 constexpr int FLAG_DELETED = 2;
+// a free row of an insertion boundary: parked like a deleted particle (also
+// FLAG_DELETED and FLAG_FIXED) until a placement fills it
+constexpr int FLAG_DORMANT = 4;
 constexpr double DELETED_COORD = 1e300;
 constexpr int LEVEL_SHIFT = 8;
 
@@ -56,6 +59,12 @@ struct InstanceDev {
     int dims[DEM_MAX_LEVELS][3];
     double inv_cell[DEM_MAX_LEVELS][3];
     double level_rmax[DEM_MAX_LEVELS];
+    // the banding that assigned the levels (radius r: binary exponent of
+    // r / level_rmin, clamped to level_bands - 1, through level_remap), for
+    // particles placed by insertion boundaries
+    double level_rmin;
+    int level_bands;
+    int level_remap[DEM_MAX_LEVELS];
     double max_interaction_distance;
     // DeletionBoundary planes: a particle is deleted when del_d - x . del_n < 0
     int n_del;
@@ -158,6 +167,7 @@ struct DevPtrs {
     int *key, *perm, *newidx, *cell_count, *cell_start, *cell_cursor, *block_sums;
     unsigned long long *rb_barrier; // arrivals at the rebuild's grid barriers (only grows)
     float4 *pf;              // (x, y, z, r) in FP32 of the gathered state: the list build's prefilter
+    int *row_slot;           // caller row -> slot of the current order (insertion boundaries only, else null)
     int *rows;               // neighbour lists particle-major (rows[s * cap + k]), for the reverse index
     // tables
     const InstanceDev *inst;

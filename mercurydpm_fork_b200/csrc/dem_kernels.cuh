@@ -165,6 +165,7 @@ __device__ __forceinline__ void gather_one(const DevPtrs& d, int s, int c)
     d.qo[nb][s] = d.qo[c][o];
     d.info[nb][s] = inf;
     d.caller[nb][s] = d.caller[c][o];
+    if (d.row_slot) d.row_slot[d.caller[c][o]] = s;
     d.newidx[o] = s;
 }
 
@@ -779,12 +780,23 @@ __host__ __device__ inline StagePtrs stage_ptrs(double* base, size_t nc)
 // caller order -> state buffer 0 (identity permutation until the first rebuild).
 // It also checks what it packs (finite positions and velocities, radius > 0,
 // species below nsp, inverse mass >= 0, instance 0 where one_instance) and
-// reports a violation as DEM_ERR_BAD_INPUT in the control status.
+// reports a violation as DEM_ERR_BAD_INPUT in the control status. Rows the
+// host gave level -1 are free rows of insertion boundaries: packed dormant.
 __global__ void __launch_bounds__(256) k_pack(DevPtrs d, StagePtrs s, int has_ang, int has_ori, int has_ii,
                                               int has_inst, int nsp, int one_instance)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n) return;
+    if (d.row_slot) d.row_slot[i] = i;
+    if (s.lvl[i] < 0) { // a free row of an insertion boundary (radius 0): dormant until filled
+        d.pr[0][i] = make_double4(DELETED_COORD, DELETED_COORD, DELETED_COORD, 0.0);
+        d.vm[0][i] = make_double4(0.0, 0.0, 0.0, 0.0);
+        d.wi[0][i] = make_double4(0.0, 0.0, 0.0, 0.0);
+        d.qo[0][i] = make_double4(1.0, 0.0, 0.0, 0.0);
+        d.info[0][i] = make_int4(s.id[i], 0, has_inst ? s.inst[i] : 0, FLAG_FIXED | FLAG_DELETED | FLAG_DORMANT);
+        d.caller[0][i] = i;
+        return;
+    }
     const double im = s.im[i];
     {
         bool bad = !(s.rad[i] > 0.0) || !(s.rad[i] <= DBL_MAX) || !(im >= 0.0) || s.sp[i] < 0 || s.sp[i] >= nsp ||

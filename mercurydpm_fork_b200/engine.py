@@ -92,6 +92,60 @@ def deletion_boundary(normal, distance, instance=0) -> _abi.DeletionBoundary:
     return b
 
 
+def insertion_boundary(pos_min, pos_max, density: float, radius: float | None = None, psd=None, species: int = 0,
+                       instance: int = 0, max_failed: int = 0, vel_min=(0, 0, 0), vel_max=(0, 0, 0),
+                       volume_flow_rate: float = float("inf"), initial_volume: float = 0.0,
+                       psd_seed: int = 0) -> _abi.InsertionBoundary:
+    """CubeInsertionBoundary::set(particleToCopy, maxFailed, posMin, posMax,
+    velMin, velMax) for a template particle of `species` (its density given
+    here). Radii: `psd` = (radii, cumulative probabilities), e.g.
+    host.psd_uniform(rmin, rmax, 2) for the set(..., rMin, rMax) form; with
+    psd None the template's `radius` through the PSD InsertionBoundary::
+    generateParticle builds when none is set (uniform from radius to radius,
+    50 points)."""
+    from .host import psd_uniform
+    if psd is None:
+        if radius is None:
+            raise ValueError("give radius or psd")
+        psd = psd_uniform(radius, radius, 50)
+    radii, probs = psd
+    if not 2 <= len(radii) == len(probs) <= _abi.DEM_MAX_PSD_POINTS:
+        raise ValueError("a PSD needs 2 to DEM_MAX_PSD_POINTS points")
+    b = _abi.InsertionBoundary()
+    b.instance, b.species, b.max_failed, b.n_psd = int(instance), int(species), int(max_failed), len(radii)
+    b.pos_min[:] = list(map(float, pos_min))
+    b.pos_max[:] = list(map(float, pos_max))
+    b.vel_min[:] = list(map(float, vel_min))
+    b.vel_max[:] = list(map(float, vel_max))
+    b.density = float(density)
+    b.volume_flow_rate = float(volume_flow_rate)
+    b.initial_volume = float(initial_volume)
+    for k, (r, q) in enumerate(zip(radii, probs)):
+        b.psd_radius[k] = float(r)
+        b.psd_probability[k] = float(q)
+    b.psd_seed = int(psd_seed)
+    return b
+
+
+def rng_draws(seed: int, n: int) -> np.ndarray:
+    """RNG::getRandomNumber(0, 1), n times after RNG::setRandomSeed(seed), from
+    the engine's generator (computed on the host; no device needed)."""
+    out = np.zeros(n)
+    rc = lib().dem_rng_draws(int(seed), int(n), _dp(out))
+    if rc:
+        raise DemError(rc, "dem_rng_draws failed")
+    return out
+
+
+def psd_draws(boundary: _abi.InsertionBoundary, n: int) -> np.ndarray:
+    """The first n radii the boundary's PSD gives (PSD::drawSample), computed on the host."""
+    out = np.zeros(n)
+    rc = lib().dem_psd_draws(C.byref(boundary), int(n), _dp(out))
+    if rc:
+        raise DemError(rc, "dem_psd_draws failed")
+    return out
+
+
 def species_pair(**kw) -> _abi.SpeciesPair:
     s = _abi.SpeciesPair()
     for k, v in kw.items():
@@ -180,7 +234,8 @@ class DemEngine:
     def __init__(self, time_step: float, instances: list[Instance], species: list[_abi.SpeciesPair],
                  walls: list[_abi.Wall] | None = None, rotation: bool = True, background_drag: float = 0.0,
                  max_neighbors: int = 0, skin: float = 0.0, use_graphs: bool = True, device: int = 0,
-                 deletions: list | None = None, batch_api: bool = False, max_contacts: int = 0):
+                 deletions: list | None = None, batch_api: bool = False, max_contacts: int = 0,
+                 insertions: list | None = None, insertion_seeds=None):
         self._h = C.c_void_p()
         cfg = _abi.Config()
         cfg.time_step = time_step
@@ -211,7 +266,29 @@ class DemEngine:
         dels = deletions or []
         da = (_abi.DeletionBoundary * max(1, len(dels)))(*dels)
         self._check(lib().dem_set_deletion_boundaries(self._h, da, len(dels)))
+        self._n_ins = 0
+        if insertions:
+            self.set_insertion_boundaries(insertions, insertion_seeds)
         self.n = 0
+
+    def set_insertion_boundaries(self, insertions: list, seeds=None):
+        """InsertionBoundary objects (see :func:`insertion_boundary`) and the
+        per-instance RNG::setRandomSeed values; they take effect at the next
+        upload, whose rows of radius 0 are the free rows they fill."""
+        ia = (_abi.InsertionBoundary * max(1, len(insertions)))(*insertions)
+        sa = None
+        if seeds is not None:
+            sa = (C.c_uint64 * self.n_instances)(*[int(x) for x in seeds])
+        self._check(lib().dem_set_insertion_boundaries(self._h, ia, len(insertions), sa))
+        self._n_ins = len(insertions)
+
+    def insertion_counts(self):
+        """(particles placed, their volume) per insertion boundary."""
+        n = self._n_ins
+        cnt = np.zeros(n, np.int64)
+        vol = np.zeros(n)
+        self._check(lib().dem_get_insertion_counts(self._h, cnt.ctypes.data_as(C.POINTER(C.c_int64)), _dp(vol), n))
+        return cnt, vol
 
     def set_deletion_boundaries(self, deletions: list):
         """Replaces the DeletionBoundary planes; between steps they apply from

@@ -16,6 +16,9 @@ evaluates the same expressions on identical operands:
   (HertzianViscoelasticNormalSpecies.cc:109-132).
 * :func:`average` -- BaseSpecies::average (harmonic mean used when two
   species are mixed, Kernel/Species/BaseSpecies.cc:110-115).
+* :func:`psd_uniform` -- PSD::setDistributionUniform (Kernel/Math/PSD.cc:
+  316-330, with PSD::linspace :1288-1302), the cumulative number distribution
+  an InsertionBoundary draws radii from.
 """
 from __future__ import annotations
 
@@ -68,3 +71,19 @@ def hertz_dissipation_from_restitution(eps: float) -> float:
 
 def average(a: float, b: float) -> float:
     return 0.0 if (a == 0 or b == 0) else (2. / (1.0 / a + 1.0 / b))
+
+
+def psd_uniform(rmin: float, rmax: float, bins: int):
+    """(radii, cumulative probabilities) of PSD::setDistributionUniform(rmin,
+    rmax, bins): both from PSD::linspace (a running sum of the step, the last
+    value replaced by the end point); PSD::validateCumulativeDistribution
+    leaves such a table as it is (it starts at 0, ends at 1 and rises)."""
+    def linspace(lo: float, hi: float, n: int):
+        dx = (hi - lo) / float(n - 1)
+        out, val = [], lo
+        for _ in range(n):
+            out.append(val)
+            val += dx
+        out[-1] = hi
+        return out
+    return linspace(float(rmin), float(rmax), bins), linspace(0.0, 1.0, bins)

@@ -7,7 +7,9 @@
 // as the engine's C ABI (include/dem_b200.h), runs the reference's
 // initialiseSolve + computeOneTimeStep loop, and returns its state, forces and
 // contact list, or the wall time of a timed window (the CPU baseline).
+#include <algorithm>
 #include <limits>
+#include <utility>
 
 #include "ref_driver.h"
 
@@ -25,6 +27,38 @@ void mdpm_ref_set_event(long long step, int wall, const dem_deletion_boundary* b
     g_event_step = step;
     g_event_wall = wall;
     g_event_deletions.assign(b, b + n);
+}
+// CubeInsertionBoundary objects of the following runs and DPMBase::random's seed
+// (the input rows of radius 0 are then skipped: they are the engine's free rows)
+void mdpm_ref_set_insertion(const dem_insertion_boundary* b, int n, unsigned long long seed)
+{
+    g_insertions.assign(b, b + n);
+    g_insertion_seed = (unsigned long)seed;
+}
+// RNG::getRandomNumber(0, 1) n times after RNG::setRandomSeed(seed)
+void mdpm_ref_rng_draws(unsigned long long seed, int n, double* out)
+{
+    RNG r;
+    r.setRandomSeed((unsigned long)seed);
+    for (int i = 0; i < n; ++i) out[i] = r.getRandomNumber(0, 1);
+}
+// PSD::drawSample n times from setDistributionUniform(rmin, rmax, bins) and setFixedSeed(seed)
+void mdpm_ref_psd_draws(double rmin, double rmax, int bins, int seed, int n, double* out)
+{
+    PSD psd;
+    psd.setDistributionUniform(rmin, rmax, bins);
+    psd.setFixedSeed(seed);
+    for (int i = 0; i < n; ++i) out[i] = psd.drawSample();
+}
+// particles and volume placed by each insertion boundary in the last run
+int mdpm_ref_insertion_counts(long long* inserted, double* volume, int capacity)
+{
+    const int n = (int)g_inserted.size();
+    for (int k = 0; k < n && k < capacity; ++k) {
+        inserted[k] = g_inserted[k];
+        volume[k] = g_inserted_volume[k];
+    }
+    return n;
 }
 
 } // extern "C"
@@ -45,15 +79,40 @@ int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem
         d.computeOneTimeStep();
         apply_event(d, k + 1);
     }
+    collect_insertions(d);
     const int64_t n = in->n;
     // deleted particles leave the handler (and reorder it): rows are matched by
-    // id, which the tests set to the caller index; rows of deleted particles
-    // keep instance -1
+    // id. The uploaded particles have ids 0, 1, ... in the order of the rows
+    // (of nonzero radius, when insertion boundaries are set); inserted particles
+    // have the ids after them, with gaps where periodic ghost particles drew
+    // ids, and take the rows of radius 0 in id order, whose ids the engine
+    // uses (the ids of contacts are reported as those). Rows of deleted or
+    // never filled particles keep instance -1.
+    std::vector<int64_t> live_rows, free_rows;
+    for (int64_t i = 0; i < n; ++i)
+        ((!g_insertions.empty() && in->radius[i] == 0.0) ? free_rows : live_rows).push_back(i);
+    std::vector<std::pair<unsigned, int64_t>> id_row; // reference id -> row
+    {
+        std::vector<unsigned> inserted;
+        for (unsigned r = 0; r < d.particleHandler.getSize(); ++r) {
+            const unsigned id = d.particleHandler.getObject(r)->getId();
+            if (id < live_rows.size()) id_row.emplace_back(id, live_rows[id]);
+            else inserted.push_back(id);
+        }
+        std::sort(inserted.begin(), inserted.end());
+        for (size_t k = 0; k < inserted.size() && k < free_rows.size(); ++k) id_row.emplace_back(inserted[k], free_rows[k]);
+        std::sort(id_row.begin(), id_row.end());
+    }
+    auto row_of = [&](unsigned id) -> int64_t {
+        auto it = std::lower_bound(id_row.begin(), id_row.end(), std::make_pair(id, (int64_t)-1));
+        return (it != id_row.end() && it->first == id) ? it->second : -1;
+    };
+    auto our_id = [&](unsigned id) -> int { const int64_t r = row_of(id); return r < 0 ? -1 : in->id[r]; };
     if (out && out->instance)
         for (int64_t i = 0; i < n; ++i) out->instance[i] = -1;
     for (int64_t r = 0; r < (int64_t)d.particleHandler.getSize(); ++r) {
         const BaseParticle* p = d.particleHandler.getObject((unsigned)r);
-        const int64_t i = (int64_t)p->getId();
+        const int64_t i = row_of(p->getId());
         if (i < 0 || i >= n) continue;
         if (out && out->instance) out->instance[i] = 0;
         const Vec3D x = p->getPosition(), v = p->getVelocity(), w = p->getAngularVelocity();
@@ -69,6 +128,7 @@ int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem
         }
         if (out && out->inv_mass) out->inv_mass[i] = p->getInvMass();
         if (out && out->inv_inertia) out->inv_inertia[i] = p->getInvInertia().XX;
+        if (out && out->radius) out->radius[i] = p->getRadius();
         const Vec3D f = p->getForce(), t = p->getTorque();
         if (force) { force[3 * i] = f.X; force[3 * i + 1] = f.Y; force[3 * i + 2] = f.Z; }
         if (torque) { torque[3 * i] = t.X; torque[3 * i + 1] = t.Y; torque[3 * i + 2] = t.Z; }
@@ -79,8 +139,8 @@ int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem
         if (c->getTimeStamp() != last) continue;
         const bool wall = dynamic_cast<BaseParticle*>(c->getI()) == nullptr;
         if (contacts_out && cnt < contacts_capacity) {
-            contacts_out->id_p[cnt] = (int)c->getP()->getId();
-            contacts_out->id_i[cnt] = (int)(wall ? c->getI()->getIndex() : c->getI()->getId());
+            contacts_out->id_p[cnt] = our_id(c->getP()->getId());
+            contacts_out->id_i[cnt] = wall ? (int)c->getI()->getIndex() : our_id(c->getI()->getId());
             if (contacts_out->is_wall) contacts_out->is_wall[cnt] = wall;
             if (contacts_out->periodic) {
                 bool per = false;

@@ -16,6 +16,7 @@
 #include <functional>
 #include <sstream>
 #include <vector>
+#include "Boundaries/CubeInsertionBoundary.h"
 #include "Boundaries/DeletionBoundary.h"
 #include "Boundaries/PeriodicBoundary.h"
 #include "CG/CG.h"
@@ -46,6 +47,12 @@ namespace {
 
 
 std::vector<dem_deletion_boundary> g_deletions; // DeletionBoundary planes of the next run
+// CubeInsertionBoundary objects of the next run and the seed of DPMBase::random
+std::vector<dem_insertion_boundary> g_insertions;
+unsigned long g_insertion_seed = 0;
+// particles and volume each insertion boundary placed in the last run
+std::vector<long long> g_inserted;
+std::vector<double> g_inserted_volume;
 
 // A change between two time steps of the next run (as a driver's
 // actionsAfterTimeStep makes it, e.g. Drivers/Calibration/CalibrationHeap.cpp:
@@ -240,8 +247,33 @@ public:
             b.set(Vec3D(db.normal[0], db.normal[1], db.normal[2]), db.distance);
             this->boundaryHandler.copyAndAddObject(b);
         }
+        if (!g_insertions.empty()) this->random.setRandomSeed(g_insertion_seed);
+        for (const auto& ib : g_insertions) {
+            // the engine's PSD table is the reference's own setDistributionUniform
+            // here; a 50-point table of one radius is left to generateParticle's
+            // default (InsertionBoundary.cc:119-124)
+            CubeInsertionBoundary b;
+            SphericalParticle tmpl;
+            tmpl.setSpecies(this->speciesHandler.getObject(ib.species));
+            tmpl.setRadius(ib.psd_radius[0]);
+            b.set(&tmpl, (unsigned)ib.max_failed, Vec3D(ib.pos_min[0], ib.pos_min[1], ib.pos_min[2]),
+                  Vec3D(ib.pos_max[0], ib.pos_max[1], ib.pos_max[2]), Vec3D(ib.vel_min[0], ib.vel_min[1], ib.vel_min[2]),
+                  Vec3D(ib.vel_max[0], ib.vel_max[1], ib.vel_max[2]));
+            const bool default_psd = ib.n_psd == 50 && ib.psd_radius[0] == ib.psd_radius[49] && ib.psd_seed == 0;
+            if (!default_psd) {
+                PSD psd;
+                psd.setDistributionUniform(ib.psd_radius[0], ib.psd_radius[ib.n_psd - 1], ib.n_psd);
+                psd.setFixedSeed((int)ib.psd_seed);
+                b.setPSD(psd);
+            }
+            // setInitialVolume zeroes an infinite flow rate: the rate is set after it
+            b.setInitialVolume(ib.initial_volume);
+            b.setVolumeFlowRate(ib.volume_flow_rate);
+            this->boundaryHandler.copyAndAddObject(b);
+        }
         SphericalParticle p;
         for (int64_t i = 0; i < in->n; ++i) {
+            if (!g_insertions.empty() && in->radius[i] == 0.0) continue; // a free row of the engine
             p.setSpecies(this->speciesHandler.getObject(in->species[i]));
             p.setRadius(in->radius[i]);
             p.setPosition(Vec3D(in->position[3 * i], in->position[3 * i + 1], in->position[3 * i + 2]));
@@ -261,6 +293,19 @@ public:
         }
     }
 };
+
+// The insertion boundaries' counters after a run (g_inserted, g_inserted_volume).
+template <class Driver>
+void collect_insertions(Driver& d)
+{
+    g_inserted.clear();
+    g_inserted_volume.clear();
+    for (BaseBoundary* b : d.boundaryHandler)
+        if (auto* ib = dynamic_cast<InsertionBoundary*>(b)) {
+            g_inserted.push_back(ib->getNumberOfParticlesInserted());
+            g_inserted_volume.push_back(ib->getVolumeOfParticlesInserted());
+        }
+}
 
 template <class Driver>
 void setup(Driver& d, const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,

@@ -407,3 +407,43 @@ def pressed_column():
     sc.position[outer, 0] *= scale
     sc.position[outer, 1] *= scale
     return sc, R, [((0.0, 0.0, -1.0), -1.5 * s)]
+
+
+def insertion_box(n_live=300, n_free=800, periodic=False, psd="range", rate=float("inf"), seed=11, max_failed=20,
+                  psd_seed=0):
+    """A box 10 x 10 x 30 diameters whose bottom holds n_live settling spheres
+    and a CubeInsertionBoundary over z = 3 .. 12 diameters, overlapping the
+    top of that bed (candidates meet particles and, near the sides, walls).
+    periodic: x and y are periodic instead of walled (candidates near the
+    sides have periodic images). psd: "range" = set(..., rMin, rMax) with
+    0.4 d .. 0.6 d; "single" = the default PSD of a 0.5 d template; "bins" =
+    setDistributionUniform(0.45 d, 0.55 d, 8) with the PSD seed psd_seed.
+    rate: the volume flow rate. The n_free rows after the bed have radius 0
+    and the ids the reference hands out next. Returns (scenario, [boundary])."""
+    import dataclasses
+    from mercurydpm_fork_b200.engine import insertion_boundary
+    from mercurydpm_fork_b200.host import psd_uniform
+    d = 1e-3
+    sc = scenarios.settling_box(n=n_live, seed=seed, box=(10, 10, 30), spacing=1.05, jitter=0.02, vstd=0.05)
+    L = 10 * d
+    if periodic:
+        sc.walls = sc.walls[4:]  # floor and lid only
+        sc.instance = dataclasses.replace(sc.instance, periodic_mask=0b011, periodic_min=(0.0, 0.0, 0.0),
+                                          periodic_max=(L, L, 0.0))
+    m = n_free
+    sc.position = np.vstack([sc.position, np.zeros((m, 3))])
+    sc.velocity = np.vstack([sc.velocity, np.zeros((m, 3))])
+    sc.radius = np.concatenate([sc.radius, np.zeros(m)])
+    sc.inv_mass = np.concatenate([sc.inv_mass, np.zeros(m)])
+    sc.inv_inertia = np.concatenate([sc.inv_inertia, np.zeros(m)])
+    sc.species_index = np.concatenate([sc.species_index, np.zeros(m, np.int32)])
+    sc.ids = np.arange(n_live + m, dtype=np.int32)
+    if psd == "range":
+        kw = dict(psd=psd_uniform(0.4 * d, 0.6 * d, 2))
+    elif psd == "single":
+        kw = dict(radius=0.5 * d)
+    else:
+        kw = dict(psd=psd_uniform(0.45 * d, 0.55 * d, 8), psd_seed=psd_seed)
+    b = insertion_boundary((0.0, 0.0, 3 * d), (L, L, 12 * d), float(sc.density[0]), max_failed=max_failed,
+                           vel_min=(-0.05, -0.05, -1.0), vel_max=(0.05, 0.05, 0.0), volume_flow_rate=rate, **kw)
+    return sc, [b]

@@ -68,6 +68,14 @@ def ref_lib(variant="serial"):
         lib.mdpm_ref_set_deletion.argtypes = [C.POINTER(_abi.DeletionBoundary), C.c_int]
         lib.mdpm_ref_set_event.restype = None
         lib.mdpm_ref_set_event.argtypes = [C.c_longlong, C.c_int, C.POINTER(_abi.DeletionBoundary), C.c_int]
+        lib.mdpm_ref_set_insertion.restype = None
+        lib.mdpm_ref_set_insertion.argtypes = [C.POINTER(_abi.InsertionBoundary), C.c_int, C.c_ulonglong]
+        lib.mdpm_ref_insertion_counts.restype = C.c_int
+        lib.mdpm_ref_insertion_counts.argtypes = [C.POINTER(C.c_longlong), _pd, C.c_int]
+        lib.mdpm_ref_rng_draws.restype = None
+        lib.mdpm_ref_rng_draws.argtypes = [C.c_ulonglong, C.c_int, _pd]
+        lib.mdpm_ref_psd_draws.restype = None
+        lib.mdpm_ref_psd_draws.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _pd]
         _ref[variant] = lib
     return _ref[variant]
 
@@ -120,13 +128,13 @@ def _deletions(planes):
 
 def _outputs(n, cap):
     o = dict(position=np.zeros((n, 3)), velocity=np.zeros((n, 3)), angular_velocity=np.zeros((n, 3)),
-             orientation=np.zeros((n, 4)), inv_mass=np.zeros(n), inv_inertia=np.zeros(n),
+             orientation=np.zeros((n, 4)), radius=np.zeros(n), inv_mass=np.zeros(n), inv_inertia=np.zeros(n),
              force=np.zeros((n, 3)), torque=np.zeros((n, 3)), instance=np.zeros(n, np.int32))
     c = dict(id_p=np.zeros(cap, np.int32), id_i=np.zeros(cap, np.int32), is_wall=np.zeros(cap, np.int32),
              periodic=np.zeros(cap, np.int32), springs=np.zeros((cap, 9)), force=np.zeros((cap, 3)),
              overlap=np.zeros(cap))
     soa = _abi.ParticlesSoA(n, _dp(o["position"]), _dp(o["velocity"]), _dp(o["angular_velocity"]),
-                            _dp(o["orientation"]), None, _dp(o["inv_mass"]), _dp(o["inv_inertia"]), None, None,
+                            _dp(o["orientation"]), _dp(o["radius"]), _dp(o["inv_mass"]), _dp(o["inv_inertia"]), None, None,
                             _ip(o["instance"]))
     csoa = _abi.ContactsSoA(cap, _ip(c["id_p"]), _ip(c["id_i"]), _ip(c["is_wall"]), _ip(c["periodic"]),
                             _dp(c["springs"]), _dp(c["force"]), _dp(c["overlap"]))
@@ -171,12 +179,24 @@ def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated", deleti
     return o
 
 
-def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None, event=None) -> dict:
+def _insertions(insertions):
+    ins = list(insertions or [])
+    return (_abi.InsertionBoundary * max(1, len(ins)))(*ins), len(ins)
+
+
+def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None, event=None, insertions=None,
+                  seed: int = 0) -> dict:
     """event = (step, wall, planes): after time step `step` the reference's
     driver removes wall `wall` (handler index, -1: none) and adds the
-    DeletionBoundary planes [(normal, distance), ...]."""
+    DeletionBoundary planes [(normal, distance), ...]. insertions:
+    dem_insertion_boundary structures made CubeInsertionBoundary objects, with
+    DPMBase::random seeded by `seed`; rows of radius 0 are left out (the
+    engine's free rows) and the output "inserted" / "inserted_volume" are the
+    boundaries' counters."""
     darr, nd = _deletions(deletions)
     ref_lib(variant).mdpm_ref_set_deletion(darr, nd)
+    iarr, ni = _insertions(insertions)
+    ref_lib(variant).mdpm_ref_set_insertion(iarr, ni, seed)
     step, wall, planes = event if event is not None else (-1, -1, [])
     earr, ne = _deletions(planes)
     ref_lib(variant).mdpm_ref_set_event(step, wall, earr, ne)
@@ -188,10 +208,31 @@ def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None, even
     rc = ref_lib(variant).mdpm_ref_run(C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density), inp.walls,
                                        inp.nwalls, C.byref(inp.soa), nsteps, C.byref(soa), _dp(o["force"]),
                                        _dp(o["torque"]), C.byref(csoa), cap, C.byref(cnt), _dp(ene))
+    ref_lib(variant).mdpm_ref_set_insertion(iarr, 0, 0)
     assert rc == 0
     o["contacts"] = sort_contacts(_trim(c, cnt.value))
     o["energies"] = dict(kinetic=ene[0], rotational=ene[1], gravitational=ene[2], elastic=ene[3])
+    if ni:
+        k = np.zeros(ni, np.int64)
+        v = np.zeros(ni)
+        m = ref_lib(variant).mdpm_ref_insertion_counts(k.ctypes.data_as(C.POINTER(C.c_longlong)), _dp(v), ni)
+        assert m == ni
+        o["inserted"], o["inserted_volume"] = k, v
     return o
+
+
+def reference_rng_draws(seed: int, n: int, variant: str = "serial") -> np.ndarray:
+    """RNG::getRandomNumber(0, 1) after RNG::setRandomSeed(seed), from the reference build."""
+    out = np.zeros(n)
+    ref_lib(variant).mdpm_ref_rng_draws(seed, n, _dp(out))
+    return out
+
+
+def reference_psd_draws(rmin: float, rmax: float, bins: int, seed: int, n: int, variant: str = "serial"):
+    """PSD::drawSample after setDistributionUniform(rmin, rmax, bins) and setFixedSeed(seed)."""
+    out = np.zeros(n)
+    ref_lib(variant).mdpm_ref_psd_draws(rmin, rmax, bins, seed, n, _dp(out))
+    return out
 
 
 def reference_heap_procedure(sc, base_radius: float, casing: int = 1, check_every: int = 1000,
@@ -345,11 +386,16 @@ def time_reference_window(sc, warmup: int, nsteps: int, threads: int, variant: s
     return dict(seconds=sec.value, interactions_start=a.value, interactions_end=b.value)
 
 
-def run_gpu(sc, nsteps: int, contacts=None, deletions=None, event=None, **kw) -> dict:
-    """event: as in run_reference, made between two dem_step calls."""
+def run_gpu(sc, nsteps: int, contacts=None, deletions=None, event=None, insertions=None, seed: int = 0,
+            **kw) -> dict:
+    """event: as in run_reference, made between two dem_step calls.
+    insertions / seed: as in run_reference (the engine fills the rows of radius 0)."""
     from mercurydpm_fork_b200.engine import deletion_boundary
     if deletions:
         kw["deletions"] = [deletion_boundary(nn, dd) for nn, dd in deletions]
+    if insertions:
+        kw["insertions"] = list(insertions)
+        kw["insertion_seeds"] = [seed]
     e = sc.engine(**kw)
     if contacts is not None:
         e.upload_contacts(contacts["id_p"], contacts["id_i"], contacts["springs"], contacts.get("is_wall"),
@@ -368,6 +414,8 @@ def run_gpu(sc, nsteps: int, contacts=None, deletions=None, event=None, **kw) ->
     out["contacts"] = sort_contacts(e.contacts())
     out["globals"] = e.reduce()
     out["stats"] = e.stats()
+    if insertions:
+        out["inserted"], out["inserted_volume"] = e.insertion_counts()
     e.close()
     return out
 

@@ -45,6 +45,8 @@ def test_struct_layouts_match_c():
              sizeof(dem_globals), sizeof(dem_cg_grid));
       printf("%zu %zu %zu %zu\n", offsetof(dem_wall, faces), offsetof(dem_instance_desc, periodic_min),
              offsetof(dem_cg_grid, width), offsetof(dem_species_pair, interaction_distance));
+      printf("%zu %zu %zu %zu\n", sizeof(dem_insertion_boundary), offsetof(dem_insertion_boundary, density),
+             offsetof(dem_insertion_boundary, psd_probability), offsetof(dem_insertion_boundary, psd_seed));
       return 0; }
     """
     import tempfile
@@ -60,6 +62,9 @@ def test_struct_layouts_match_c():
                                            _abi.InstanceDesc, _abi.Config, _abi.Globals, _abi.CGGrid)]
     assert offs == [_abi.Wall.faces.offset, _abi.InstanceDesc.periodic_min.offset, _abi.CGGrid.width.offset,
                     _abi.SpeciesPair.interaction_distance.offset]
+    ins = list(map(int, lines[2].split()))
+    B = _abi.InsertionBoundary
+    assert ins == [C.sizeof(B), B.density.offset, B.psd_probability.offset, B.psd_seed.offset]
 
 
 def test_create_without_gpu_reports_error():

@@ -1,0 +1,114 @@
+"""Insertion boundaries (CubeInsertionBoundary, Kernel/Boundaries/
+InsertionBoundary.cc:184-296) on the engine against the reference build.
+
+* CPU: the engine's restatements of the reference's generators -- RNG
+  (Kernel/Math/RNG.cc, lagged Fibonacci 607/273 seeded by the linear
+  congruential generator) and PSD::drawSample (Kernel/Math/PSD.cc:114-128)
+  after PSD::setDistributionUniform -- give bit-identical sequences to the
+  reference's own classes (dem_rng_draws / dem_psd_draws run the kernel's
+  code on the host).
+* GPU: a box whose bed fills its bottom, with a CubeInsertionBoundary over
+  the bed's top, run on the engine and on the reference Kernel from the same
+  inputs: the same particles are placed (count, volume, rows, radii, masses
+  bit for bit) and the run continues like the law tests (positions 1e-12 of
+  a diameter, velocities and forces 1e-9 of their largest magnitude). Walled
+  and periodic sides, the three PSD forms, a volume flow rate that stops the
+  insertion between steps (the drawn particle waits for the next step), and
+  a run out of free rows (DEM_ERR_CAPACITY).
+"""
+import numpy as np
+import pytest
+
+import cases
+import harness as H
+from mercurydpm_fork_b200 import _abi
+from mercurydpm_fork_b200.engine import DemError, insertion_boundary, psd_draws, rng_draws
+from mercurydpm_fork_b200.host import psd_uniform
+
+needs_ref = pytest.mark.skipif(not H.reference_available("serial"), reason="reference build absent")
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [0, 1, 12345, 2 ** 31 + 7])
+def test_rng_matches_reference(seed):
+    ours = rng_draws(seed, 5000)
+    ref = H.reference_rng_draws(seed, 5000)
+    np.testing.assert_array_equal(ours, ref)
+    assert 0.0 <= ours.min() and ours.max() < 1.0
+
+
+@needs_ref
+@pytest.mark.parametrize("rmin,rmax,bins,seed", [(0.4e-3, 0.6e-3, 2, 0), (0.5e-3, 0.5e-3, 50, 0),
+                                                 (0.45e-3, 0.55e-3, 8, 3), (1.0, 3.0, 64, 17)])
+def test_psd_draws_match_reference(rmin, rmax, bins, seed):
+    b = insertion_boundary((0, 0, 0), (1, 1, 1), 1.0, psd=psd_uniform(rmin, rmax, bins), psd_seed=seed)
+    ours = psd_draws(b, 3000)
+    ref = H.reference_psd_draws(rmin, rmax, bins, seed, 3000)
+    np.testing.assert_array_equal(ours, ref)
+
+
+def _compare(a, r):
+    live = r["instance"] >= 0
+    np.testing.assert_array_equal(a["instance"] >= 0, live)
+    np.testing.assert_array_equal(a["radius"][live], r["radius"][live])
+    np.testing.assert_array_equal(a["inv_mass"][live], r["inv_mass"][live])
+    np.testing.assert_array_equal(a["inv_inertia"][live], r["inv_inertia"][live])
+    assert H.pair_set(a["contacts"]) == H.pair_set(r["contacts"])
+    assert H.rel_err(a["position"][live], r["position"][live], 1e-3) < 1e-12
+    for k in ("velocity", "force"):
+        assert H.rel_err(a[k][live], r[k][live]) < 1e-9, k
+
+
+def _run_both(sc, bnd, steps, seed=0):
+    a = H.run_gpu(sc, steps, insertions=bnd, seed=seed)
+    r = H.run_reference(sc, steps, insertions=bnd, seed=seed)
+    return a, r
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("periodic", [False, True])
+@pytest.mark.parametrize("psd", ["range", "single", "bins"])
+def test_insertion_matches_reference(gpu, periodic, psd):
+    sc, bnd = cases.insertion_box(periodic=periodic, psd=psd, psd_seed=5)
+    a, r = _run_both(sc, bnd, 400, seed=3)
+    np.testing.assert_array_equal(a["inserted"], r["inserted"])
+    np.testing.assert_array_equal(a["inserted_volume"], r["inserted_volume"])
+    n_live0 = int(np.count_nonzero(sc.radius))
+    assert r["inserted"][0] > 100  # the first step fills much of the region
+    assert int((r["instance"] >= 0).sum()) == n_live0 + int(r["inserted"][0])
+    _compare(a, r)
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_insertion_flow_rate_limits_between_steps(gpu):
+    """A volume flow rate of about half a particle per time step: most steps
+    place one particle or none, and the particle drawn last waits (its radius
+    already drawn) for the step whose volume allows it."""
+    d = 1e-3
+    vp = 4.0 / 3.0 * np.pi * (0.5 * d) ** 3
+    sc, bnd = cases.insertion_box(rate=0.5 * vp / 2e-6, psd="range")
+    a, r = _run_both(sc, bnd, 80, seed=9)
+    np.testing.assert_array_equal(a["inserted"], r["inserted"])
+    assert 20 <= r["inserted"][0] <= 60
+    _compare(a, r)
+
+
+@pytest.mark.gpu
+def test_insertion_without_free_rows_reports_capacity(gpu):
+    sc, bnd = cases.insertion_box(n_free=5)
+    e = sc.engine(insertions=bnd, insertion_seeds=[0])
+    with pytest.raises(DemError) as err:
+        e.step(2)
+    assert err.value.code == _abi.DEM_ERR_CAPACITY
+    e.close()
+
+
+def test_insertion_boundary_validation():
+    """Bad PSDs and ranges are refused before anything reaches a device."""
+    with pytest.raises(ValueError):
+        insertion_boundary((0, 0, 0), (1, 1, 1), 1.0)  # neither radius nor PSD
+    b = insertion_boundary((0, 0, 0), (1, 1, 1), 1.0, psd=([1.0, 2.0], [0.0, 1.0]))
+    out = psd_draws(b, 100)
+    assert np.all((out >= 1.0 - 1e-12) & (out <= 2.0 + 1e-12))

@@ -67,6 +67,10 @@ extern "C" {
 #define DEM_MAX_INSERTION_PER_INSTANCE 4
 #define DEM_MAX_PSD_POINTS 64
 
+/* ---- insertion boundary kinds ----------------------------------------- */
+#define DEM_INSERTION_CUBE  0 /* CubeInsertionBoundary::placeParticle (CubeInsertionBoundary.cc:173-184) */
+#define DEM_INSERTION_CHUTE 1 /* ChuteInsertionBoundary::placeParticle (ChuteInsertionBoundary.cc:163-190) */
+
 /* Parameters of one (mixed) species pair, as held by the reference's
  * Species<Normal,Friction,Adhesive> objects and the mixed-species triangle
  * (SpeciesHandler::getMixedObject, Kernel/SpeciesHandler.cc:901-937).
@@ -226,7 +230,8 @@ typedef struct dem_deletion_boundary {
     double  distance;
 } dem_deletion_boundary;
 
-/* A CubeInsertionBoundary. Every time step, after the drift and before the
+/* An InsertionBoundary of the kind DEM_INSERTION_CUBE (CubeInsertionBoundary)
+ * or DEM_INSERTION_CHUTE (ChuteInsertionBoundary). Every time step, after the drift and before the
  * forces (DPMBase::computeOneTimeStep, Kernel/DPMBase.cc:4348-4352),
  * InsertionBoundary::checkBoundaryBeforeTimeStep (Kernel/Boundaries/
  * InsertionBoundary.cc:184-296) places new particles until max_failed
@@ -237,9 +242,15 @@ typedef struct dem_deletion_boundary {
  *    of a single template) and its radius from the cumulative number
  *    distribution psd_* with the PSD's own generator (PSD::drawSample,
  *    Kernel/Math/PSD.cc:114-128); it is drawn again only after it was placed;
- *  - a placement draws the position in [pos_min, pos_max] and the velocity in
- *    [vel_min, vel_max], x, y, z each (CubeInsertionBoundary::placeParticle,
- *    Kernel/Boundaries/CubeInsertionBoundary.cc:173-184), and succeeds when
+ *  - a placement of a cube boundary draws the position in [pos_min, pos_max]
+ *    and the velocity in [vel_min, vel_max], x, y, z each
+ *    (CubeInsertionBoundary::placeParticle, Kernel/Boundaries/
+ *    CubeInsertionBoundary.cc:173-184); one of a chute boundary puts the
+ *    particle at x = pos_min.x + r and draws y in [pos_min.y - r, pos_max.y + r],
+ *    z in [pos_min.z - r, pos_max.z + r + fixed_particle_radius] and the
+ *    velocity inflow_velocity (1 + U(-variance, variance), U(-variance, variance),
+ *    U(-variance, variance)) (ChuteInsertionBoundary::placeParticle,
+ *    ChuteInsertionBoundary.cc:163-190); a placement succeeds when
  *    the particle touches no wall and no particle, its periodic images
  *    included (DPMBase::checkParticleForInteractionLocalPeriodic and
  *    checkParticleForInteractionLocal, DPMBase.cc:4868-4958);
@@ -258,6 +269,8 @@ typedef struct dem_deletion_boundary {
  * instance -1 until a particle is placed in it; with none left, dem_step
  * returns DEM_ERR_CAPACITY. */
 typedef struct dem_insertion_boundary {
+    int32_t  kind;                 /* DEM_INSERTION_*                                 */
+    int32_t  reserved;
     int32_t  instance;
     int32_t  species;              /* the template particle's species (index in the instance) */
     int32_t  max_failed;           /* InsertionBoundary::maxFailed_                   */
@@ -269,10 +282,42 @@ typedef struct dem_insertion_boundary {
     double   density;              /* ParticleSpecies::getDensity of the species      */
     double   volume_flow_rate;     /* setVolumeFlowRate; +infinity (the default): none */
     double   initial_volume;       /* setInitialVolume                                */
+    double   fixed_particle_radius;    /* chute: ChuteInsertionBoundary::set's fixedParticleRadius */
+    double   inflow_velocity;          /* chute: inflowVelocity                           */
+    double   inflow_velocity_variance; /* chute: inflowVelocityVariance                   */
     double   psd_radius[DEM_MAX_PSD_POINTS];      /* PSD::getParticleSizeDistribution(): radii    */
     double   psd_probability[DEM_MAX_PSD_POINTS]; /* and cumulative probabilities, from 0 to 1    */
     uint64_t psd_seed;             /* PSD::setRandomSeed                              */
 } dem_insertion_boundary;
+
+/* The chute's compact inflow fill, Chute::addFlowParticlesCompactly with
+ * Chute::createFlowParticle (Kernel/Chute.cc:1083-1115), which a Chute
+ * driver runs from setupInitialConditions: with r_in = (min_radius +
+ * max_radius) / 2 it places particles until the instance holds
+ * N = (unsigned)(particles + x_max y_max inflow_height / r_in^3 / 8) of them.
+ * Each candidate draws its radius in [min_radius, max_radius], then z in
+ * [z_min + r + fixed_particle_radius, inflow height], y in [y_min + r,
+ * y_max - r] and x in [x_min + r, x_max - r] (the three coordinates are the
+ * arguments of one Vec3D constructor, which the reference's compiler, g++,
+ * evaluates last to first), at rest; it is kept when it touches no wall and
+ * no particle (DPMBase::checkParticleForInteraction, periodic images
+ * included), else the inflow height grows by 0.0001 max_radius. The draws
+ * come from the instance's generator (seeded as for insertion boundaries,
+ * dem_set_insertion_boundaries; the boundaries then continue from where the
+ * fill left it). The fill runs inside dem_upload_particles, placing the
+ * particles in the instance's free rows (radius 0, row order), before the
+ * initial force evaluation. */
+typedef struct dem_chute_fill {
+    int32_t instance;
+    int32_t species;               /* the flow particles' species (species 0 in Chute) */
+    double  density;               /* its ParticleSpecies::getDensity                 */
+    double  x_min, x_max;          /* getXMin, getXMax (= getChuteLength)             */
+    double  y_min, y_max;          /* getYMin, getYMax (= getChuteWidth)              */
+    double  z_min;                 /* getZMin                                         */
+    double  inflow_height;         /* getInflowHeight when the fill starts            */
+    double  min_radius, max_radius;/* get{Min,Max}InflowParticleRadius                */
+    double  fixed_particle_radius; /* getFixedParticleRadius                          */
+} dem_chute_fill;
 
 /* Gaussian coarse-graining grid (CG<XZ|XYZ|O, Gauss, StandardFields>,
  * Kernel/CG/CG.hcc:233-528, Kernel/CG/Fields/StandardFields.cc:184-250).
@@ -350,6 +395,11 @@ int  dem_remove_wall(dem_handle *h, int wall);
  * the PSD's radii, reserves the free rows and starts the generators. */
 int  dem_set_insertion_boundaries(dem_handle *h, const dem_insertion_boundary *b, int n,
                                   const uint64_t *seeds);
+/* Chute fills (dem_chute_fill, at most one per instance) for the next upload. */
+int  dem_set_chute_fills(dem_handle *h, const dem_chute_fill *f, int n);
+/* Per fill of the last upload: the inflow height it ended with and the
+ * particles it placed (Chute::getInflowHeight, the growth of ParticleHandler). */
+int  dem_get_chute_fill_results(dem_handle *h, double *inflow_height, int64_t *added, int n);
 /* Per boundary (the order given): particles placed so far and their volume
  * (InsertionBoundary::getNumberOfParticlesInserted / getVolumeOfParticlesInserted). */
 int  dem_get_insertion_counts(dem_handle *h, int64_t *inserted, double *volume, int n);

@@ -41,6 +41,8 @@ DEM_MAX_WALL_FACES = 8
 DEM_MAX_DELETION_PER_INSTANCE = 2
 DEM_MAX_INSERTION_PER_INSTANCE = 4
 DEM_MAX_PSD_POINTS = 64
+DEM_INSERTION_CUBE = 0
+DEM_INSERTION_CHUTE = 1
 
 DEM_CG_NFIELDS = 29
 DEM_CG_O = 0
@@ -95,10 +97,20 @@ class DeletionBoundary(C.Structure):
 
 class InsertionBoundary(C.Structure):
     _fields_ = [
-        ("instance", _i32), ("species", _i32), ("max_failed", _i32), ("n_psd", _i32), ("pos_min", _d * 3),
-        ("pos_max", _d * 3), ("vel_min", _d * 3), ("vel_max", _d * 3), ("density", _d), ("volume_flow_rate", _d),
-        ("initial_volume", _d), ("psd_radius", _d * DEM_MAX_PSD_POINTS), ("psd_probability", _d * DEM_MAX_PSD_POINTS),
+        ("kind", _i32), ("reserved", _i32), ("instance", _i32), ("species", _i32), ("max_failed", _i32),
+        ("n_psd", _i32), ("pos_min", _d * 3), ("pos_max", _d * 3), ("vel_min", _d * 3), ("vel_max", _d * 3),
+        ("density", _d), ("volume_flow_rate", _d), ("initial_volume", _d), ("fixed_particle_radius", _d),
+        ("inflow_velocity", _d), ("inflow_velocity_variance", _d),
+        ("psd_radius", _d * DEM_MAX_PSD_POINTS), ("psd_probability", _d * DEM_MAX_PSD_POINTS),
         ("psd_seed", C.c_uint64),
+    ]
+
+
+class ChuteFill(C.Structure):
+    _fields_ = [
+        ("instance", _i32), ("species", _i32), ("density", _d), ("x_min", _d), ("x_max", _d), ("y_min", _d),
+        ("y_max", _d), ("z_min", _d), ("inflow_height", _d), ("min_radius", _d), ("max_radius", _d),
+        ("fixed_particle_radius", _d),
     ]
 
 
@@ -165,6 +177,8 @@ _SIGNATURES = {
     "dem_set_insertion_boundaries": (C.c_int, [C.c_void_p, C.POINTER(InsertionBoundary), C.c_int,
                                                C.POINTER(C.c_uint64)]),
     "dem_get_insertion_counts": (C.c_int, [C.c_void_p, C.POINTER(_i64), _pd, C.c_int]),
+    "dem_set_chute_fills": (C.c_int, [C.c_void_p, C.POINTER(ChuteFill), C.c_int]),
+    "dem_get_chute_fill_results": (C.c_int, [C.c_void_p, _pd, C.POINTER(_i64), C.c_int]),
     "dem_rng_draws": (C.c_int, [C.c_uint64, C.c_int, _pd]),
     "dem_psd_draws": (C.c_int, [C.POINTER(InsertionBoundary), C.c_int, _pd]),
     "dem_get_counts": (C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),

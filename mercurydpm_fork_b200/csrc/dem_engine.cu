@@ -47,7 +47,10 @@ struct Handle {
     InsInstanceDev* d_ins_inst = nullptr;
     InsBoundaryDev* d_ins_bnd = nullptr;
     int* d_ins_rows = nullptr;
-    int n_ins_inst = 0;                // instances with insertion boundaries (blocks of k_insert)
+    int n_ins_inst = 0;                // instances with insertion boundaries or a fill (blocks of k_insert)
+    int n_ins_launch = 0;              // blocks of k_insert per step (0: no insertion boundary)
+    std::vector<dem_chute_fill> fills; // chute fills of the next upload
+    std::vector<FillDev> fill_results; // and their outcome at the last upload
     std::string err;
     int device = 0;
     cudaStream_t stream = nullptr, stream2 = nullptr;
@@ -167,7 +170,7 @@ constexpr int REBUILD_LAUNCHES = 1;
 // after k_control and before the rebuild it may request.
 void launch_insert(Handle* h, cudaStream_t s)
 {
-    if (h->n_ins_inst > 0)
+    if (h->n_ins_launch > 0)
         k_insert<<<h->n_ins_inst, INS_THREADS, 0, s>>>(h->d, InsPtrs{h->d_ins_inst, h->d_ins_bnd, h->d_ins_rows});
 }
 constexpr int FORCE_LAUNCHES = 3;
@@ -610,6 +613,8 @@ int dem_set_insertion_boundaries(dem_handle* hh, const dem_insertion_boundary* b
     auto finite = [](double x) { return std::isfinite(x); };
     for (int k = 0; k < n; ++k) {
         const dem_insertion_boundary& x = b[k];
+        if (x.kind != DEM_INSERTION_CUBE && x.kind != DEM_INSERTION_CHUTE)
+            return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: unknown kind");
         if (x.instance < 0 || x.instance >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: instance out of range");
         if (++per[x.instance] > DEM_MAX_INSERTION_PER_INSTANCE)
             return fail(h, DEM_ERR_BAD_INPUT, "more than DEM_MAX_INSERTION_PER_INSTANCE insertion boundaries in an instance");
@@ -625,6 +630,9 @@ int dem_set_insertion_boundaries(dem_handle* hh, const dem_insertion_boundary* b
             if (!finite(x.pos_min[a]) || !finite(x.pos_max[a]) || !(x.pos_min[a] <= x.pos_max[a]) ||
                 !finite(x.vel_min[a]) || !finite(x.vel_max[a]) || !(x.vel_min[a] <= x.vel_max[a]))
                 return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: bad position or velocity range");
+        if (!finite(x.fixed_particle_radius) || !finite(x.inflow_velocity) || !(x.inflow_velocity_variance >= 0.0) ||
+            !finite(x.inflow_velocity_variance))
+            return fail(h, DEM_ERR_BAD_INPUT, "insertion boundary: bad chute inflow parameters");
         // a cumulative number distribution from 0 to 1 over positive radii
         // (PSD::validateCumulativeDistribution's result)
         for (int j = 0; j < x.n_psd; ++j) {
@@ -639,6 +647,42 @@ int dem_set_insertion_boundaries(dem_handle* hh, const dem_insertion_boundary* b
     h->ins.assign(b, b + n);
     h->ins_seeds.assign(ninst, 0);
     if (seeds) h->ins_seeds.assign(seeds, seeds + ninst);
+    return DEM_OK;
+}
+
+int dem_set_chute_fills(dem_handle* hh, const dem_chute_fill* f, int n)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || n < 0 || (n > 0 && !f)) return fail(h, DEM_ERR_BAD_INPUT, "dem_set_chute_fills: bad arguments");
+    const int ninst = (int)h->inst_desc.size();
+    std::vector<int> per(ninst, 0);
+    for (int k = 0; k < n; ++k) {
+        const dem_chute_fill& x = f[k];
+        if (x.instance < 0 || x.instance >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "chute fill: instance out of range");
+        if (++per[x.instance] > 1) return fail(h, DEM_ERR_BAD_INPUT, "chute fill: at most one per instance");
+        if (x.species < 0 || x.species >= h->inst_desc[x.instance].n_species)
+            return fail(h, DEM_ERR_BAD_INPUT, "chute fill: species out of range");
+        const double v[] = {x.density, x.x_min, x.x_max, x.y_min, x.y_max, x.z_min, x.inflow_height, x.min_radius,
+                            x.max_radius, x.fixed_particle_radius};
+        for (double a : v)
+            if (!std::isfinite(a)) return fail(h, DEM_ERR_BAD_INPUT, "chute fill: non-finite parameter");
+        if (!(x.density > 0.0) || !(x.min_radius > 0.0) || !(x.max_radius >= x.min_radius) ||
+            !(x.fixed_particle_radius >= 0.0) || !(x.x_max > x.x_min) || !(x.y_max > x.y_min))
+            return fail(h, DEM_ERR_BAD_INPUT, "chute fill: bad radii, density or ranges");
+    }
+    h->fills.assign(f, f + n);
+    return DEM_OK;
+}
+
+int dem_get_chute_fill_results(dem_handle* hh, double* inflow_height, int64_t* added, int n)
+{
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || n < 0 || n > (int)h->fill_results.size())
+        return fail(h, DEM_ERR_BAD_INPUT, "dem_get_chute_fill_results: bad arguments");
+    for (int k = 0; k < n; ++k) {
+        if (inflow_height) inflow_height[k] = h->fill_results[k].height;
+        if (added) added[k] = h->fill_results[k].added;
+    }
     return DEM_OK;
 }
 
@@ -730,9 +774,21 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
             has_ins[b.instance] = 1;
         }
     }
+    std::vector<int> fill_of(ninst, -1);
+    for (size_t k = 0; k < h->fills.size(); ++k) {
+        const dem_chute_fill& f = h->fills[k];
+        if (f.instance >= ninst) return fail(h, DEM_ERR_BAD_INPUT, "chute fill instance out of range");
+        fill_of[f.instance] = (int)k;
+        for (double r : {f.min_radius, f.max_radius}) {
+            psd_lo[f.instance] = has_ins[f.instance] ? std::min(psd_lo[f.instance], r) : r;
+            psd_hi[f.instance] = std::max(psd_hi[f.instance], r);
+            has_ins[f.instance] = 1;
+        }
+    }
+    const bool any_free = !h->ins.empty() || !h->fills.empty();
     std::vector<std::vector<int>> free_rows(ninst);
     // one instance without insertion: members are 0..n-1, radii the caller's array itself
-    const bool fast = one && h->ins.empty();
+    const bool fast = one && !any_free;
     double rmin_all = 1e300;
     // one instance: the host reads only the radii (their minimum sets the skin
     // and the grid); k_pack checks every other array on the device, and the
@@ -916,7 +972,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     for (const auto& w : h->walls) any_tri = any_tri || w.type == DEM_WALL_TRIANGLE;
     const std::vector<long long> layout = {n, cap, wmax, ncells, (long long)h->inst.size(), (long long)h->species.size(),
                                            (long long)h->walls.size(), (long long)record_capacity, h->ncomp, any_tri,
-                                           item_cap, (long long)h->ins.size(), (long long)n_ins_inst};
+                                           item_cap, (long long)h->ins.size(), (long long)n_ins_inst,
+                                           (long long)h->fills.size()};
     const bool reuse = !h->layout.empty() && h->layout == layout;
     if (!reuse) free_particle_arrays(h);
     const DevPtrs kept = h->d;
@@ -995,7 +1052,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     if ((rc = dalloc(h, &d.rev, (size_t)cap * NC))) return rc;
     if ((rc = dalloc(h, &d.rows, (size_t)cap * NC))) return rc;
     if ((rc = dalloc(h, &d.pf, NC))) return rc;
-    if (!h->ins.empty()) {
+    if (any_free) {
         if ((rc = dalloc(h, &d.row_slot, NC))) return rc;
         if ((rc = dalloc(h, &h->d_ins_inst, (size_t)n_ins_inst))) return rc;
         if ((rc = dalloc(h, &h->d_ins_bnd, h->ins.size()))) return rc;
@@ -1083,11 +1140,12 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     std::vector<InsBoundaryDev> ins_bnd;
     std::vector<int> ins_rows;
     h->ins_order.clear();
-    for (int in = 0; in < ninst && !h->ins.empty(); ++in) {
+    for (int in = 0; in < ninst && any_free; ++in) {
         if (!has_ins[in]) continue;
         InsInstanceDev S{};
         lfg_seed(h->ins_seeds[in], S.rng);
         S.time = 0.0;
+        for (double r : radii[in]) S.grid_rmax = std::max(S.grid_rmax, r);
         S.instance = in;
         S.first = (int)ins_bnd.size();
         for (size_t k = 0; k < h->ins.size(); ++k) {
@@ -1106,6 +1164,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         ins_inst.push_back(S);
     }
     h->n_ins_inst = (int)ins_inst.size();
+    h->n_ins_launch = h->ins.empty() ? 0 : h->n_ins_inst;
     if (h->n_ins_inst > 0) {
         CU(cudaMemcpyAsync(h->d_ins_inst, ins_inst.data(), ins_inst.size() * sizeof(InsInstanceDev),
                            cudaMemcpyHostToDevice, h->stream));
@@ -1114,6 +1173,69 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         if (!ins_rows.empty())
             CU(cudaMemcpyAsync(h->d_ins_rows, ins_rows.data(), ins_rows.size() * sizeof(int), cudaMemcpyHostToDevice,
                                h->stream));
+    }
+    // chute fills (Chute::addFlowParticlesCompactly), in the order given
+    h->fill_results.assign(h->fills.size(), FillDev{});
+    for (size_t k = 0; k < h->fills.size(); ++k) {
+        const dem_chute_fill& f = h->fills[k];
+        const int in = f.instance;
+        const InstanceDev& I = h->inst[in];
+        FillDev F{};
+        F.f = f;
+        F.height = f.inflow_height;
+        for (size_t j = 0; j < ins_inst.size(); ++j)
+            if (ins_inst[j].instance == in) F.instance_slot = (int)j;
+        // N = ParticleHandler::getNumberOfObjects() + length width height / r_in^3 / 8 (Chute.cc:1086-1087)
+        const unsigned n_objects = (unsigned)(fast ? n : (long long)radii[in].size());
+        const double r_in = 0.5 * (f.min_radius + f.max_radius);
+        const unsigned N = (unsigned)(n_objects + f.x_max * f.y_max * f.inflow_height / (r_in * r_in * r_in) / 8);
+        F.target = N > n_objects ? (long long)(N - n_objects) : 0;
+        F.tries_left = 100 * F.target + 10000000ll;
+        // a linked-list grid of the instance, cells at least one reach wide
+        double rmax = 0.0;
+        for (int l = 0; l < I.n_levels; ++l) rmax = std::max(rmax, I.level_rmax[l]);
+        double cs = 2.0 * rmax + I.max_interaction_distance;
+        FillGrid g{};
+        const auto& D = h->inst_desc[in];
+        for (int pass = 0; pass < 64; ++pass) {
+            long long cells = 1;
+            for (int a = 0; a < 3; ++a) {
+                g.origin[a] = I.origin[a];
+                if ((D.periodic_mask >> a) & 1u) {
+                    const double L = I.per_L[a];
+                    g.dims[a] = std::max(1, (int)std::floor(L / cs));
+                    g.inv[a] = (double)g.dims[a] / L;
+                } else {
+                    const double ext = D.domain_max[a] - D.domain_min[a];
+                    g.dims[a] = (int)std::min(1024.0, std::max(1.0, std::ceil(ext / cs)));
+                    g.inv[a] = 1.0 / cs;
+                }
+                cells *= g.dims[a];
+            }
+            if (cells <= (1ll << 24)) break;
+            cs *= 2.0;
+        }
+        const size_t ncells = (size_t)g.dims[0] * g.dims[1] * g.dims[2];
+        FillDev* dF = nullptr;
+        CU(cudaMalloc(&g.head, ncells * sizeof(int)));
+        CU(cudaMalloc(&g.next, NC * sizeof(int)));
+        CU(cudaMalloc(&dF, sizeof(FillDev)));
+        CU(cudaMemsetAsync(g.head, 0xff, ncells * sizeof(int), h->stream)); // -1: empty
+        CU(cudaMemcpyAsync(dF, &F, sizeof(FillDev), cudaMemcpyHostToDevice, h->stream));
+        if (F.target > 0) {
+            k_fill_grid<<<grid_for(n, 256), 256, 0, h->stream>>>(d, g, in);
+            k_fill<<<1, INS_THREADS, 0, h->stream>>>(d, InsPtrs{h->d_ins_inst, h->d_ins_bnd, h->d_ins_rows}, dF, g);
+        }
+        CU(cudaGetLastError());
+        CU(cudaMemcpyAsync(&h->fill_results[k], dF, sizeof(FillDev), cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        cudaFree(g.head);
+        cudaFree(g.next);
+        cudaFree(dF);
+        if (h->fill_results[k].status == 1)
+            return fail(h, DEM_ERR_CAPACITY, "chute fill: no free row left (upload more rows of radius 0)");
+        if (h->fill_results[k].status == 2)
+            return fail(h, DEM_ERR_CAPACITY, "chute fill: gave up before placing every particle");
     }
     unsigned int status = 0;
     CU(cudaMemcpyAsync(&status, &h->d_ctl->status, sizeof(status), cudaMemcpyDeviceToHost, h->stream));
@@ -1301,7 +1423,7 @@ int dem_step(dem_handle* hh, int nsteps)
                 }
                 while (left-- > 0) CU(cudaGraphLaunch(h->graph1, h->stream));
                 CU(cudaGraphLaunch(h->graphF, h->stream));
-                launches += (1ll + REBUILD_LAUNCHES + force_launches(h) + (h->n_ins_inst > 0)) * nsteps;
+                launches += (1ll + REBUILD_LAUNCHES + force_launches(h) + (h->n_ins_launch > 0)) * nsteps;
             } else {
                 for (int k = 0; k < nsteps; ++k) {
                     k_control<<<1, CONTROL_THREADS, 0, h->stream>>>(h->d_ctl, d.walls, h->d_wgeom, d.n_walls, d.dt);
@@ -1310,7 +1432,7 @@ int dem_step(dem_handle* hh, int nsteps)
                     launch_force(h, h->stream, 1, k == nsteps - 1);
                 }
                 CU(cudaGetLastError());
-                launches += (1ll + force_launches(h) + REBUILD_LAUNCHES + (h->n_ins_inst > 0)) * nsteps;
+                launches += (1ll + force_launches(h) + REBUILD_LAUNCHES + (h->n_ins_launch > 0)) * nsteps;
             }
             k_flip<<<1, 32, 0, h->stream>>>(h->d_ctl);
             launches += 1;

@@ -39,6 +39,11 @@ constexpr int FLAG_DELETED = 2;
 // a free row of an insertion boundary: parked like a deleted particle (also
 // FLAG_DELETED and FLAG_FIXED) until a placement fills it
 constexpr int FLAG_DORMANT = 4;
+// the last drift moved the particle across a periodic boundary (set and
+// cleared by every drift): the reference's HGrid still files it under its
+// cell before the shift until the grid is next updated, which the insertion
+// check reproduces
+constexpr int FLAG_WRAPPED = 8;
 constexpr double DELETED_COORD = 1e300;
 constexpr int LEVEL_SHIFT = 8;
 

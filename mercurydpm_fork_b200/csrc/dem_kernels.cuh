@@ -626,6 +626,7 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevPtrs d)
             disp2 = len2(disp);
             q = quat_rotate(q, w * dt);
         }
+        bool wrapped = false;
         if (I.per_mask) {
             double* xc = &x.x;
 #pragma unroll
@@ -633,6 +634,7 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevPtrs d)
                 if ((I.per_mask >> k) & 1u) {
                     const double dl = xc[k] - I.per_lo[k], dr = I.per_hi[k] - xc[k];
                     if ((dl < dr ? dl : dr) < 0) {
+                        wrapped = true;
                         if (I.per_hi[k] - xc[k] > xc[k] - I.per_lo[k])
                             xc[k] = xc[k] + I.per_L[k];
                         else
@@ -644,12 +646,13 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevPtrs d)
         double4 pn = make_double4(x.x, x.y, x.z, ps.w);
         double4 vn = make_double4(v.x, v.y, v.z, vs.w);
         double4 wn = make_double4(w.x, w.y, w.z, ws.w);
+        int4 isn = is;
+        isn.w = wrapped ? (is.w | FLAG_WRAPPED) : (is.w & ~FLAG_WRAPPED);
         if (I.n_del && !(is.w & FLAG_DELETED) && deletion_check(I, x)) {
-            int4 isn = is;
             park_deleted(ctl, pn, vn, wn, isn);
-            d.info[c][s] = isn;
             disp2 = 0.0;
         }
+        if (isn.w != is.w) d.info[c][s] = isn;
         d.pr[c][s] = pn;
         d.vm[c][s] = vn;
         d.wi[c][s] = wn;

@@ -843,6 +843,7 @@ __global__ void __launch_bounds__(BLOCK, SUM_THREADS_PER_SM / BLOCK) k_sum(DevPt
 
         // ---- integration ----
         double4 pn = ps, vn = vs, wn = ws;
+        bool wrapped = false;
         if (final_step) {
             d.force[3 * (size_t)s + 0] = F.x;
             d.force[3 * (size_t)s + 1] = F.y;
@@ -886,6 +887,7 @@ __global__ void __launch_bounds__(BLOCK, SUM_THREADS_PER_SM / BLOCK) k_sum(DevPt
                     if ((I.per_mask >> k) & 1u) {
                         const double dl = xc[k] - I.per_lo[k], dr = I.per_hi[k] - xc[k];
                         if ((dl < dr ? dl : dr) < 0) {
+                            wrapped = true;
                             if (I.per_hi[k] - xc[k] > xc[k] - I.per_lo[k])
                                 xc[k] = xc[k] + I.per_L[k];
                             else
@@ -900,6 +902,7 @@ __global__ void __launch_bounds__(BLOCK, SUM_THREADS_PER_SM / BLOCK) k_sum(DevPt
             qs = make_double4(q.q0, q.q1, q.q2, q.q3);
         }
         int4 isn = is;
+        isn.w = wrapped ? (is.w | FLAG_WRAPPED) : (is.w & ~FLAG_WRAPPED);
         if (MODE == 1 && !final_step && I.n_del && !(is.w & FLAG_DELETED) && deletion_check(I, xyz(pn))) {
             park_deleted(ctl, pn, vn, wn, isn);
             disp2 = 0.0;

@@ -95,14 +95,17 @@ def deletion_boundary(normal, distance, instance=0) -> _abi.DeletionBoundary:
 def insertion_boundary(pos_min, pos_max, density: float, radius: float | None = None, psd=None, species: int = 0,
                        instance: int = 0, max_failed: int = 0, vel_min=(0, 0, 0), vel_max=(0, 0, 0),
                        volume_flow_rate: float = float("inf"), initial_volume: float = 0.0,
-                       psd_seed: int = 0) -> _abi.InsertionBoundary:
+                       psd_seed: int = 0, chute=None) -> _abi.InsertionBoundary:
     """CubeInsertionBoundary::set(particleToCopy, maxFailed, posMin, posMax,
     velMin, velMax) for a template particle of `species` (its density given
     here). Radii: `psd` = (radii, cumulative probabilities), e.g.
     host.psd_uniform(rmin, rmax, 2) for the set(..., rMin, rMax) form; with
     psd None the template's `radius` through the PSD InsertionBoundary::
     generateParticle builds when none is set (uniform from radius to radius,
-    50 points)."""
+    50 points). chute = (fixedParticleRadius, inflowVelocity,
+    inflowVelocityVariance) makes it a ChuteInsertionBoundary instead
+    (ChuteInsertionBoundary::set(particleToCopy, maxFailed, posMin, posMax,
+    fixedParticleRadius, inflowVelocity, inflowVelocityVariance))."""
     from .host import psd_uniform
     if psd is None:
         if radius is None:
@@ -113,6 +116,9 @@ def insertion_boundary(pos_min, pos_max, density: float, radius: float | None = 
         raise ValueError("a PSD needs 2 to DEM_MAX_PSD_POINTS points")
     b = _abi.InsertionBoundary()
     b.instance, b.species, b.max_failed, b.n_psd = int(instance), int(species), int(max_failed), len(radii)
+    b.kind = _abi.DEM_INSERTION_CUBE if chute is None else _abi.DEM_INSERTION_CHUTE
+    if chute is not None:
+        b.fixed_particle_radius, b.inflow_velocity, b.inflow_velocity_variance = (float(v) for v in chute)
     b.pos_min[:] = list(map(float, pos_min))
     b.pos_max[:] = list(map(float, pos_max))
     b.vel_min[:] = list(map(float, vel_min))
@@ -125,6 +131,22 @@ def insertion_boundary(pos_min, pos_max, density: float, radius: float | None = 
         b.psd_probability[k] = float(q)
     b.psd_seed = int(psd_seed)
     return b
+
+
+def chute_fill(x_max: float, y_max: float, inflow_height: float, min_radius: float, max_radius: float,
+               density: float, fixed_particle_radius: float = 0.0, x_min: float = 0.0, y_min: float = 0.0,
+               z_min: float = 0.0, species: int = 0, instance: int = 0) -> _abi.ChuteFill:
+    """Chute::addFlowParticlesCompactly for a chute of length x_max, width
+    y_max (getChuteLength / getChuteWidth) with the given inflow height,
+    inflow radii and fixed-particle radius (include/dem_b200.h,
+    dem_chute_fill)."""
+    f = _abi.ChuteFill()
+    f.instance, f.species = int(instance), int(species)
+    for k, v in dict(density=density, x_min=x_min, x_max=x_max, y_min=y_min, y_max=y_max, z_min=z_min,
+                     inflow_height=inflow_height, min_radius=min_radius, max_radius=max_radius,
+                     fixed_particle_radius=fixed_particle_radius).items():
+        setattr(f, k, float(v))
+    return f
 
 
 def rng_draws(seed: int, n: int) -> np.ndarray:
@@ -235,7 +257,7 @@ class DemEngine:
                  walls: list[_abi.Wall] | None = None, rotation: bool = True, background_drag: float = 0.0,
                  max_neighbors: int = 0, skin: float = 0.0, use_graphs: bool = True, device: int = 0,
                  deletions: list | None = None, batch_api: bool = False, max_contacts: int = 0,
-                 insertions: list | None = None, insertion_seeds=None):
+                 insertions: list | None = None, insertion_seeds=None, chute_fills: list | None = None):
         self._h = C.c_void_p()
         cfg = _abi.Config()
         cfg.time_step = time_step
@@ -267,8 +289,11 @@ class DemEngine:
         da = (_abi.DeletionBoundary * max(1, len(dels)))(*dels)
         self._check(lib().dem_set_deletion_boundaries(self._h, da, len(dels)))
         self._n_ins = 0
-        if insertions:
-            self.set_insertion_boundaries(insertions, insertion_seeds)
+        self._n_fill = 0
+        if insertions or insertion_seeds is not None:
+            self.set_insertion_boundaries(insertions or [], insertion_seeds)
+        if chute_fills:
+            self.set_chute_fills(chute_fills)
         self.n = 0
 
     def set_insertion_boundaries(self, insertions: list, seeds=None):
@@ -281,6 +306,20 @@ class DemEngine:
             sa = (C.c_uint64 * self.n_instances)(*[int(x) for x in seeds])
         self._check(lib().dem_set_insertion_boundaries(self._h, ia, len(insertions), sa))
         self._n_ins = len(insertions)
+
+    def set_chute_fills(self, fills: list):
+        """Chute fills (:func:`chute_fill`) the next upload performs."""
+        fa = (_abi.ChuteFill * max(1, len(fills)))(*fills)
+        self._check(lib().dem_set_chute_fills(self._h, fa, len(fills)))
+        self._n_fill = len(fills)
+
+    def chute_fill_results(self):
+        """(final inflow heights, particles placed) per chute fill of the last upload."""
+        n = self._n_fill
+        h = np.zeros(n)
+        k = np.zeros(n, np.int64)
+        self._check(lib().dem_get_chute_fill_results(self._h, _dp(h), k.ctypes.data_as(C.POINTER(C.c_int64)), n))
+        return h, k
 
     def insertion_counts(self):
         """(particles placed, their volume) per insertion boundary."""

@@ -13,8 +13,26 @@
 
 #include "ref_driver.h"
 
+#include "Chute.h"
+
 namespace {
 using RefDriver = RefDriverT<Mercury3D>;
+
+// A Chute driver whose set-up is the checker's, followed by the chute's
+// compact inflow fill (Chute.cc:1083-1115) from a freshly seeded generator.
+class ChuteFillDriver : public RefDriverT<Chute> {
+public:
+    void setupInitialConditions() override
+    {
+        RefDriverT<Chute>::setupInitialConditions();
+        this->setInflowParticleRadius(g_fill.min_radius, g_fill.max_radius);
+        this->setFixedParticleRadius(g_fill.fixed_particle_radius);
+        this->setInflowHeight(g_fill.inflow_height);
+        this->random.setRandomSeed(g_insertion_seed);
+        this->addFlowParticlesCompactly();
+        g_fill_height = this->getInflowHeight();
+    }
+};
 } // namespace
 
 extern "C" {
@@ -65,14 +83,16 @@ int mdpm_ref_insertion_counts(long long* inserted, double* volume, int capacity)
 
 extern "C" {
 
-// Same contract as oracle_run (oracle/dem_oracle.cpp), with the species
-// densities the reference needs to derive the particle masses.
-int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
-                 const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in, int nsteps,
-                 dem_particles_soa* out, double* force, double* torque, dem_contacts_soa* contacts_out,
-                 int64_t contacts_capacity, int64_t* contacts_count, double* energies /* kin, rot, grav, ela */)
+} // extern "C"
+
+namespace {
+template <class Driver>
+int run_and_report(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
+                   const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in, int nsteps,
+                   dem_particles_soa* out, double* force, double* torque, dem_contacts_soa* contacts_out,
+                   int64_t contacts_capacity, int64_t* contacts_count, double* energies)
 {
-    RefDriver d;
+    Driver d;
     setup(d, cfg, inst, species, density, walls, nwalls, in, 1);
     d.initialiseSolve();
     for (int k = 0; k < nsteps; ++k) {
@@ -89,8 +109,7 @@ int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem
     // uses (the ids of contacts are reported as those). Rows of deleted or
     // never filled particles keep instance -1.
     std::vector<int64_t> live_rows, free_rows;
-    for (int64_t i = 0; i < n; ++i)
-        ((!g_insertions.empty() && in->radius[i] == 0.0) ? free_rows : live_rows).push_back(i);
+    for (int64_t i = 0; i < n; ++i) ((free_rows_in_use() && in->radius[i] == 0.0) ? free_rows : live_rows).push_back(i);
     std::vector<std::pair<unsigned, int64_t>> id_row; // reference id -> row
     {
         std::vector<unsigned> inserted;
@@ -179,6 +198,39 @@ int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem
         energies[3] = d.getElasticEnergy();
     }
     return 0;
+}
+} // namespace
+
+extern "C" {
+
+// Same contract as oracle_run (oracle/dem_oracle.cpp), with the species
+// densities the reference needs to derive the particle masses.
+int mdpm_ref_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
+                 const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in, int nsteps,
+                 dem_particles_soa* out, double* force, double* torque, dem_contacts_soa* contacts_out,
+                 int64_t contacts_capacity, int64_t* contacts_count, double* energies /* kin, rot, grav, ela */)
+{
+    return run_and_report<RefDriver>(cfg, inst, species, density, walls, nwalls, in, nsteps, out, force, torque,
+                                     contacts_out, contacts_capacity, contacts_count, energies);
+}
+
+// mdpm_ref_run on a Chute whose set-up ends with the compact inflow fill
+// `fill` (DPMBase::random seeded with `seed` first); *inflow_height receives
+// the height the fill ended with.
+int mdpm_ref_run_chute_fill(const dem_config* cfg, const dem_instance_desc* inst, const dem_species_pair* species,
+                            const double* density, const dem_wall* walls, int nwalls, const dem_particles_soa* in,
+                            const dem_chute_fill* fill, unsigned long long seed, int nsteps, dem_particles_soa* out,
+                            double* force, double* torque, dem_contacts_soa* contacts_out, int64_t contacts_capacity,
+                            int64_t* contacts_count, double* inflow_height)
+{
+    g_fill = *fill;
+    g_fill_set = true;
+    g_insertion_seed = (unsigned long)seed;
+    const int rc = run_and_report<ChuteFillDriver>(cfg, inst, species, density, walls, nwalls, in, nsteps, out, force,
+                                                   torque, contacts_out, contacts_capacity, contacts_count, nullptr);
+    g_fill_set = false;
+    if (inflow_height) *inflow_height = g_fill_height;
+    return rc;
 }
 
 } // extern "C"

@@ -16,6 +16,7 @@
 #include <functional>
 #include <sstream>
 #include <vector>
+#include "Boundaries/ChuteInsertionBoundary.h"
 #include "Boundaries/CubeInsertionBoundary.h"
 #include "Boundaries/DeletionBoundary.h"
 #include "Boundaries/PeriodicBoundary.h"
@@ -50,6 +51,12 @@ std::vector<dem_deletion_boundary> g_deletions; // DeletionBoundary planes of th
 // CubeInsertionBoundary objects of the next run and the seed of DPMBase::random
 std::vector<dem_insertion_boundary> g_insertions;
 unsigned long g_insertion_seed = 0;
+// Chute::addFlowParticlesCompactly of the next Chute run (ChuteFillDriver)
+dem_chute_fill g_fill{};
+bool g_fill_set = false;
+double g_fill_height = 0.0; // Chute::getInflowHeight after it
+// rows of radius 0 are the engine's free rows, not particles
+inline bool free_rows_in_use() { return !g_insertions.empty() || g_fill_set; }
 // particles and volume each insertion boundary placed in the last run
 std::vector<long long> g_inserted;
 std::vector<double> g_inserted_volume;
@@ -252,13 +259,20 @@ public:
             // the engine's PSD table is the reference's own setDistributionUniform
             // here; a 50-point table of one radius is left to generateParticle's
             // default (InsertionBoundary.cc:119-124)
-            CubeInsertionBoundary b;
+            CubeInsertionBoundary cube;
+            ChuteInsertionBoundary chute;
+            InsertionBoundary& b = ib.kind == DEM_INSERTION_CHUTE ? static_cast<InsertionBoundary&>(chute)
+                                                                  : static_cast<InsertionBoundary&>(cube);
             SphericalParticle tmpl;
             tmpl.setSpecies(this->speciesHandler.getObject(ib.species));
             tmpl.setRadius(ib.psd_radius[0]);
-            b.set(&tmpl, (unsigned)ib.max_failed, Vec3D(ib.pos_min[0], ib.pos_min[1], ib.pos_min[2]),
-                  Vec3D(ib.pos_max[0], ib.pos_max[1], ib.pos_max[2]), Vec3D(ib.vel_min[0], ib.vel_min[1], ib.vel_min[2]),
-                  Vec3D(ib.vel_max[0], ib.vel_max[1], ib.vel_max[2]));
+            const Vec3D lo(ib.pos_min[0], ib.pos_min[1], ib.pos_min[2]), hi(ib.pos_max[0], ib.pos_max[1], ib.pos_max[2]);
+            if (ib.kind == DEM_INSERTION_CHUTE)
+                chute.set(&tmpl, (unsigned)ib.max_failed, lo, hi, ib.fixed_particle_radius, ib.inflow_velocity,
+                          ib.inflow_velocity_variance);
+            else
+                cube.set(&tmpl, (unsigned)ib.max_failed, lo, hi, Vec3D(ib.vel_min[0], ib.vel_min[1], ib.vel_min[2]),
+                         Vec3D(ib.vel_max[0], ib.vel_max[1], ib.vel_max[2]));
             const bool default_psd = ib.n_psd == 50 && ib.psd_radius[0] == ib.psd_radius[49] && ib.psd_seed == 0;
             if (!default_psd) {
                 PSD psd;
@@ -269,11 +283,14 @@ public:
             // setInitialVolume zeroes an infinite flow rate: the rate is set after it
             b.setInitialVolume(ib.initial_volume);
             b.setVolumeFlowRate(ib.volume_flow_rate);
-            this->boundaryHandler.copyAndAddObject(b);
+            if (ib.kind == DEM_INSERTION_CHUTE)
+                this->boundaryHandler.copyAndAddObject(chute);
+            else
+                this->boundaryHandler.copyAndAddObject(cube);
         }
         SphericalParticle p;
         for (int64_t i = 0; i < in->n; ++i) {
-            if (!g_insertions.empty() && in->radius[i] == 0.0) continue; // a free row of the engine
+            if (free_rows_in_use() && in->radius[i] == 0.0) continue; // a free row of the engine
             p.setSpecies(this->speciesHandler.getObject(in->species[i]));
             p.setRadius(in->radius[i]);
             p.setPosition(Vec3D(in->position[3 * i], in->position[3 * i + 1], in->position[3 * i + 2]));

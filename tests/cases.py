@@ -410,7 +410,7 @@ def pressed_column():
 
 
 def insertion_box(n_live=300, n_free=800, periodic=False, psd="range", rate=float("inf"), seed=11, max_failed=20,
-                  psd_seed=0):
+                  psd_seed=0, chute=False):
     """A box 10 x 10 x 30 diameters whose bottom holds n_live settling spheres
     and a CubeInsertionBoundary over z = 3 .. 12 diameters, overlapping the
     top of that bed (candidates meet particles and, near the sides, walls).
@@ -418,8 +418,11 @@ def insertion_box(n_live=300, n_free=800, periodic=False, psd="range", rate=floa
     sides have periodic images). psd: "range" = set(..., rMin, rMax) with
     0.4 d .. 0.6 d; "single" = the default PSD of a 0.5 d template; "bins" =
     setDistributionUniform(0.45 d, 0.55 d, 8) with the PSD seed psd_seed.
-    rate: the volume flow rate. The n_free rows after the bed have radius 0
-    and the ids the reference hands out next. Returns (scenario, [boundary])."""
+    rate: the volume flow rate. chute: a ChuteInsertionBoundary instead,
+    feeding the plane x = 0.5 d + r over z = 6 .. 12 d (fixed particle radius
+    0.5 d, inflow velocity 0.1 m/s, variance 0.2). The n_free rows after the
+    bed have radius 0 and the ids the reference hands out next. Returns
+    (scenario, [boundary])."""
     import dataclasses
     from mercurydpm_fork_b200.engine import insertion_boundary
     from mercurydpm_fork_b200.host import psd_uniform
@@ -444,6 +447,42 @@ def insertion_box(n_live=300, n_free=800, periodic=False, psd="range", rate=floa
         kw = dict(radius=0.5 * d)
     else:
         kw = dict(psd=psd_uniform(0.45 * d, 0.55 * d, 8), psd_seed=psd_seed)
-    b = insertion_boundary((0.0, 0.0, 3 * d), (L, L, 12 * d), float(sc.density[0]), max_failed=max_failed,
-                           vel_min=(-0.05, -0.05, -1.0), vel_max=(0.05, 0.05, 0.0), volume_flow_rate=rate, **kw)
+    if chute:
+        b = insertion_boundary((0.5 * d, 0.0, 6 * d), (2 * d, L, 12 * d), float(sc.density[0]), max_failed=max_failed,
+                               volume_flow_rate=rate, chute=(0.5 * d, 0.1, 0.2), **kw)
+    else:
+        b = insertion_boundary((0.0, 0.0, 3 * d), (L, L, 12 * d), float(sc.density[0]), max_failed=max_failed,
+                               vel_min=(-0.05, -0.05, -1.0), vel_max=(0.05, 0.05, 0.0), volume_flow_rate=rate, **kw)
     return sc, [b]
+
+
+def chute_fill_case(n_base_free=0, n_free=3000, lx=12, ly=6, height=6, seed=13):
+    """A periodic chute (x and y periodic, 12 x 6 diameters, domain z from 0
+    to twice the inflow height) whose base is the seeded rough base of fixed
+    spheres of scenarios.periodic_chute, and Chute::addFlowParticlesCompactly
+    filling it to an inflow height of `height` diameters with radii 0.45 d ..
+    0.55 d (fixed particle radius 0.5 d). Returns (scenario, fill)."""
+    from mercurydpm_fork_b200.engine import chute_fill
+    d = 1e-3
+    sc = scenarios.periodic_chute(n_flow=1, seed=seed, lx=lx, ly=ly)
+    base = sc.inv_mass == 0.0
+    for k in ("position", "velocity", "radius", "inv_mass", "inv_inertia", "species_index"):
+        setattr(sc, k, getattr(sc, k)[base])
+    nb = int(base.sum())
+    m = n_free
+    sc.position = np.vstack([sc.position, np.zeros((m, 3))])
+    sc.velocity = np.vstack([sc.velocity, np.zeros((m, 3))])
+    sc.radius = np.concatenate([sc.radius, np.zeros(m)])
+    sc.inv_mass = np.concatenate([sc.inv_mass, np.zeros(m)])
+    sc.inv_inertia = np.concatenate([sc.inv_inertia, np.zeros(m)])
+    sc.species_index = np.concatenate([sc.species_index, np.zeros(m, np.int32)])
+    sc.ids = np.arange(nb + m, dtype=np.int32)
+    import dataclasses
+    sc.instance = dataclasses.replace(sc.instance, domain_min=(0.0, 0.0, 0.0),
+                                      domain_max=(sc.instance.domain_max[0], sc.instance.domain_max[1], 2 * height * d))
+    inst = sc.instance
+    f = chute_fill(x_max=inst.periodic_max[0], y_max=inst.periodic_max[1], inflow_height=height * d,
+                   min_radius=0.45 * d, max_radius=0.55 * d, density=float(sc.density[0]),
+                   fixed_particle_radius=0.5 * d, x_min=inst.periodic_min[0], y_min=inst.periodic_min[1],
+                   z_min=inst.domain_min[2])
+    return sc, f

@@ -74,6 +74,11 @@ def ref_lib(variant="serial"):
         lib.mdpm_ref_insertion_counts.argtypes = [C.POINTER(C.c_longlong), _pd, C.c_int]
         lib.mdpm_ref_rng_draws.restype = None
         lib.mdpm_ref_rng_draws.argtypes = [C.c_ulonglong, C.c_int, _pd]
+        lib.mdpm_ref_run_chute_fill.restype = C.c_int
+        lib.mdpm_ref_run_chute_fill.argtypes = common + [C.POINTER(_abi.ChuteFill), C.c_ulonglong, C.c_int,
+                                                        C.POINTER(_abi.ParticlesSoA), _pd, _pd,
+                                                        C.POINTER(_abi.ContactsSoA), C.c_int64, C.POINTER(C.c_int64),
+                                                        _pd]
         lib.mdpm_ref_psd_draws.restype = None
         lib.mdpm_ref_psd_draws.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _pd]
         _ref[variant] = lib
@@ -218,6 +223,27 @@ def run_reference(sc, nsteps: int, variant: str = "serial", deletions=None, even
         m = ref_lib(variant).mdpm_ref_insertion_counts(k.ctypes.data_as(C.POINTER(C.c_longlong)), _dp(v), ni)
         assert m == ni
         o["inserted"], o["inserted_volume"] = k, v
+    return o
+
+
+def run_reference_chute_fill(sc, fill, seed: int, nsteps: int, variant: str = "serial") -> dict:
+    """The scenario on a reference Chute whose set-up ends with
+    Chute::addFlowParticlesCompactly (`fill`, DPMBase::random seeded with
+    `seed`); rows of radius 0 receive the placed particles in id order.
+    Adds "inflow_height", the height the fill ended with."""
+    inp = _Inputs(sc)
+    cap = _contact_rows(sc.n)
+    o, c, soa, csoa = _outputs(sc.n, cap)
+    cnt = C.c_int64(0)
+    hgt = np.zeros(1)
+    with quiet_stdout():
+        rc = ref_lib(variant).mdpm_ref_run_chute_fill(
+            C.byref(inp.cfg), C.byref(inp.inst), inp.species, _dp(inp.density), inp.walls, inp.nwalls,
+            C.byref(inp.soa), C.byref(fill), seed, nsteps, C.byref(soa), _dp(o["force"]), _dp(o["torque"]),
+            C.byref(csoa), cap, C.byref(cnt), _dp(hgt))
+    assert rc == 0
+    o["contacts"] = sort_contacts(_trim(c, cnt.value))
+    o["inflow_height"] = float(hgt[0])
     return o
 
 
@@ -387,7 +413,7 @@ def time_reference_window(sc, warmup: int, nsteps: int, threads: int, variant: s
 
 
 def run_gpu(sc, nsteps: int, contacts=None, deletions=None, event=None, insertions=None, seed: int = 0,
-            **kw) -> dict:
+            chute_fill=None, **kw) -> dict:
     """event: as in run_reference, made between two dem_step calls.
     insertions / seed: as in run_reference (the engine fills the rows of radius 0)."""
     from mercurydpm_fork_b200.engine import deletion_boundary
@@ -395,7 +421,10 @@ def run_gpu(sc, nsteps: int, contacts=None, deletions=None, event=None, insertio
         kw["deletions"] = [deletion_boundary(nn, dd) for nn, dd in deletions]
     if insertions:
         kw["insertions"] = list(insertions)
+    if insertions or chute_fill is not None:
         kw["insertion_seeds"] = [seed]
+    if chute_fill is not None:
+        kw["chute_fills"] = [chute_fill]
     e = sc.engine(**kw)
     if contacts is not None:
         e.upload_contacts(contacts["id_p"], contacts["id_i"], contacts["springs"], contacts.get("is_wall"),
@@ -416,6 +445,9 @@ def run_gpu(sc, nsteps: int, contacts=None, deletions=None, event=None, insertio
     out["stats"] = e.stats()
     if insertions:
         out["inserted"], out["inserted_volume"] = e.insertion_counts()
+    if chute_fill is not None:
+        hh, kk = e.chute_fill_results()
+        out["inflow_height"], out["filled"] = float(hh[0]), int(kk[0])
     e.close()
     return out
 

@@ -82,6 +82,21 @@ def test_insertion_matches_reference(gpu, periodic, psd):
 
 @pytest.mark.gpu
 @needs_ref
+@pytest.mark.parametrize("periodic", [False, True])
+def test_chute_insertion_matches_reference(gpu, periodic):
+    """ChuteInsertionBoundary (ChuteInsertionBoundary.cc:163-190): particles fed
+    into one plane of x, over a y range one radius wider than the boundary on
+    each side (with periodic y, candidates beyond the period meet the images)."""
+    sc, bnd = cases.insertion_box(periodic=periodic, psd="bins", psd_seed=2, chute=True)
+    a, r = _run_both(sc, bnd, 300, seed=4)
+    np.testing.assert_array_equal(a["inserted"], r["inserted"])
+    np.testing.assert_array_equal(a["inserted_volume"], r["inserted_volume"])
+    assert r["inserted"][0] > 20
+    _compare(a, r)
+
+
+@pytest.mark.gpu
+@needs_ref
 def test_insertion_flow_rate_limits_between_steps(gpu):
     """A volume flow rate of about half a particle per time step: most steps
     place one particle or none, and the particle drawn last waits (its radius
@@ -112,3 +127,24 @@ def test_insertion_boundary_validation():
     b = insertion_boundary((0, 0, 0), (1, 1, 1), 1.0, psd=([1.0, 2.0], [0.0, 1.0]))
     out = psd_draws(b, 100)
     assert np.all((out >= 1.0 - 1e-12) & (out <= 2.0 + 1e-12))
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_chute_fill_matches_reference(gpu):
+    """Chute::addFlowParticlesCompactly (Chute.cc:1083-1115) on a periodic
+    chute over a rough base: the same particles, in the same places (bit for
+    bit, before any step), the same final inflow height after some 70,000
+    rejected candidates; then 30 steps like the other runs."""
+    sc, f = cases.chute_fill_case()
+    a0 = H.run_gpu(sc, 0, chute_fill=f, seed=7)
+    r0 = H.run_reference_chute_fill(sc, f, 7, 0)
+    live = r0["instance"] >= 0
+    np.testing.assert_array_equal(a0["instance"] >= 0, live)
+    assert a0["filled"] == int(live.sum()) - int(np.count_nonzero(sc.radius)) > 400
+    assert a0["inflow_height"] == r0["inflow_height"] > f.inflow_height
+    for k in ("position", "radius", "inv_mass", "inv_inertia"):
+        np.testing.assert_array_equal(a0[k][live], r0[k][live], err_msg=k)
+    a = H.run_gpu(sc, 30, chute_fill=f, seed=7)
+    r = H.run_reference_chute_fill(sc, f, 7, 30)
+    _compare(a, r)

@@ -86,9 +86,16 @@ __global__ void k_flip(Control* ctl)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-__device__ __forceinline__ int cell_coord(double x, double origin, double inv, int dim)
+__device__ __forceinline__ int cell_coord(double x, double origin, double inv, int dim, bool periodic)
 {
     const double f = floor((x - origin) * inv);
+    // periodic: a particle just outside the period (an insertion may place one
+    // there; the next drift shifts it back) is filed in the cell the searches
+    // reach it in, the wrapped one
+    if (periodic && fabs(f) < 1e9) {
+        const int c = (int)f % dim;
+        return c < 0 ? c + dim : c;
+    }
     // positions far outside the grid are clamped into the edge cells
     if (!(f >= 0.0)) return 0;
     if (f >= (double)(dim - 1)) return dim - 1;
@@ -109,9 +116,9 @@ __device__ __forceinline__ void keys_one(const DevPtrs& d, int i, int c)
     }
     const InstanceDev& I = d.inst[inf.z];
     const int lvl = (inf.w >> LEVEL_SHIFT) & 0xff;
-    const int cx = cell_coord(p.x, I.origin[0], I.inv_cell[lvl][0], I.dims[lvl][0]);
-    const int cy = cell_coord(p.y, I.origin[1], I.inv_cell[lvl][1], I.dims[lvl][1]);
-    const int cz = cell_coord(p.z, I.origin[2], I.inv_cell[lvl][2], I.dims[lvl][2]);
+    const int cx = cell_coord(p.x, I.origin[0], I.inv_cell[lvl][0], I.dims[lvl][0], I.per_mask & 1u);
+    const int cy = cell_coord(p.y, I.origin[1], I.inv_cell[lvl][1], I.dims[lvl][1], (I.per_mask >> 1) & 1u);
+    const int cz = cell_coord(p.z, I.origin[2], I.inv_cell[lvl][2], I.dims[lvl][2], (I.per_mask >> 2) & 1u);
     const int key = I.cell_base[lvl] + (cz * I.dims[lvl][1] + cy) * I.dims[lvl][0] + cx;
     d.key[i] = key;
     atomicAdd(&d.cell_count[key], 1);

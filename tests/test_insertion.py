@@ -148,3 +148,43 @@ def test_chute_fill_matches_reference(gpu):
     a = H.run_gpu(sc, 30, chute_fill=f, seed=7)
     r = H.run_reference_chute_fill(sc, f, 7, 30)
     _compare(a, r)
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_insertion_in_batch_members(gpu):
+    """Two instances of one handle, each with its own insertion boundary and
+    generator seed (the k_insert blocks of one launch run side by side):
+    each member places what the reference places when run alone."""
+    from mercurydpm_fork_b200 import scenarios
+    s0, (b0,) = cases.insertion_box(seed=11, n_free=600)
+    s1, (b1,) = cases.insertion_box(periodic=True, seed=12, psd="bins", psd_seed=1, n_free=600)
+    bt = scenarios.batch([s0, s1])
+    b1.instance = 1
+    e = bt.engine(insertions=[b0, b1], insertion_seeds=[3, 5])
+    e.step(200)
+    g = e.download()
+    g["force"], g["torque"] = e.forces()
+    c = e.contacts()
+    cnt, vol = e.insertion_counts()
+    e.close()
+    for k, (sc, b, seed) in enumerate(((s0, b0, 3), (s1, b1, 5))):
+        b.instance = 0  # the reference runs the member alone
+        r = H.run_reference(sc, 200, insertions=[b], seed=seed)
+        assert cnt[k] == r["inserted"][0] and vol[k] == r["inserted_volume"][0]
+        sl = bt.member_slice(k)
+        a = {key: g[key][sl] for key in ("position", "velocity", "force", "radius", "inv_mass", "inv_inertia")}
+        a["instance"] = np.where(g["instance"][sl] == k, 0, -1)
+        a["contacts"] = _member_contacts(bt, c, k)
+        _compare(a, r)
+
+
+def _member_contacts(b, c, k):
+    lo, hi = b.offsets[k], b.offsets[k + 1]
+    wall_off = sum(len(m.walls) for m in b.members[:k])
+    sel = (c["id_p"] >= lo) & (c["id_p"] < hi)
+    out = {key: v[sel].copy() for key, v in c.items()}
+    out["id_p"] -= lo
+    w = out["is_wall"] != 0
+    out["id_i"] = np.where(w, out["id_i"] - wall_off, out["id_i"] - lo)
+    return H.sort_contacts(out)

@@ -287,7 +287,9 @@ __global__ void __launch_bounds__(BLOCK) k_detect(DevPtrs d)
             bool near_tri = false; // within reach of the instance's triangles (all of them, if they move)
             if (d.has_tri && I.tri_mask) {
                 d.slott[s] = SLOT_NONE;
-                const double R = ps.w + I.max_interaction_distance;
+                // widened by a relative 1e-12 so that rounding of tri_lo - R cannot
+                // skip a particle at exactly the reach
+                const double R = (ps.w + I.max_interaction_distance) * (1.0 + 1e-12);
                 near_tri = !I.tri_static ||
                            (xs.x > I.tri_lo[0] - R && xs.x < I.tri_hi[0] + R && xs.y > I.tri_lo[1] - R &&
                             xs.y < I.tri_hi[1] + R && xs.z > I.tri_lo[2] - R && xs.z < I.tri_hi[2] + R);

@@ -111,3 +111,59 @@ def test_periodic_triangle_floor_matches_reference(gpu):
     assert H.rel_err(g["position"], r["position"], 1e-3) < 1e-13
     assert H.rel_err(g["force"], r["force"]) < 1e-9
     assert H.rel_err(g["contacts"]["springs"], r["contacts"]["springs"]) < 1e-9
+
+
+@pytest.mark.gpu
+@needs_reference
+def test_static_mesh_box_margin_matches_reference(gpu):
+    """k_detect skips the triangle tests of a particle outside the bounding
+    box of a static mesh widened by its reach (radius + interaction distance).
+    Spheres placed around a 10 x 10 diameter patch at that margin (a hair
+    inside and outside it, and exactly on it), others a tenth of a diameter
+    out and moving in, others dropping onto the patch's corners: the
+    contacts, at the start and as they appear, are the reference's."""
+    import dataclasses
+    from mercurydpm_fork_b200 import scenarios
+    d = 1e-3
+    sc = scenarios.triangle_floor(n=1, l_d=10.0, amplitude_d=0.3)
+    L = 10 * d
+    zs = [w.faces[k][2] for w in sc.walls for k in range(3)]
+    lo = np.array([0.0, 0.0, min(zs)])
+    hi = np.array([L, L, max(zs)])
+    r = 0.5 * d
+    pos, vel = [], []
+    z = 0.5 * (lo[2] + hi[2])
+    # one side per margin offset: a hair inside, exactly on, a hair outside, inside again
+    sides = (((lambda s, f: (lo[0] - r * f, s, z)), (0.3, 0, 0), 1.0 - 1e-9),
+             ((lambda s, f: (hi[0] + r * f, s, z)), (-0.3, 0, 0), 1.0),
+             ((lambda s, f: (s, lo[1] - r * f, z)), (0, 0.3, 0), 1.0 + 1e-9),
+             ((lambda s, f: (s, hi[1] + r * f, z)), (0, -0.3, 0), 1.0 - 1e-12))
+    for place, v, frac in sides:
+        for s in np.linspace(1.0 * d, L - 1.0 * d, 5):  # on the margin, at rest
+            pos.append(place(s, frac))
+            vel.append((0, 0, 0))
+        for s in np.linspace(2.0 * d, L - 2.0 * d, 4):  # a tenth of a diameter out, moving in
+            pos.append(place(s, 1.2))
+            vel.append(v)
+    for cx, cy in ((lo[0], lo[1]), (hi[0], lo[1]), (lo[0], hi[1]), (hi[0], hi[1])):
+        pos.append((cx, cy, hi[2] + r * 1.05))
+        vel.append((0, 0, -0.3))
+    # spheres of one side column would touch their neighbours across the corner: spread them
+    n = len(pos)
+    sc.position, sc.velocity = pos, vel
+    sc.radius = np.full(n, r)
+    from mercurydpm_fork_b200.host import sphere_inv_mass_inertia
+    sc.inv_mass, sc.inv_inertia = sphere_inv_mass_inertia(sc.radius, float(sc.density[0]))
+    sc.species_index = np.zeros(n, np.int32)
+    sc.ids = np.arange(n, dtype=np.int32)
+    sc.instance = dataclasses.replace(sc.instance, periodic_mask=0, domain_min=(-3 * d, -3 * d, -2 * d),
+                                      domain_max=(L + 3 * d, L + 3 * d, 4 * d))
+    seen = 0
+    for steps in (0, 150, 180, 210, 240, 300):
+        g = H.run_gpu(sc, steps)
+        r_ = H.run_reference(sc, steps)
+        assert H.pair_set(g["contacts"]) == H.pair_set(r_["contacts"]), steps
+        assert H.rel_err(g["position"], r_["position"], 1e-3) < 1e-13
+        assert H.rel_err(g["force"], r_["force"]) < 1e-9
+        seen += _triangle_pairs(r_["contacts"])
+    assert seen > 10

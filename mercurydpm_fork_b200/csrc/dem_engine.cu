@@ -47,6 +47,7 @@ struct Handle {
     InsInstanceDev* d_ins_inst = nullptr;
     InsBoundaryDev* d_ins_bnd = nullptr;
     int* d_ins_rows = nullptr;
+    int* d_ovf = nullptr;              // per cell, then per slot twice: k_insert's lists of placed particles
     int n_ins_inst = 0;                // instances with insertion boundaries or a fill (blocks of k_insert)
     int n_ins_launch = 0;              // blocks of k_insert per step (0: no insertion boundary)
     std::vector<dem_chute_fill> fills; // chute fills of the next upload
@@ -142,6 +143,7 @@ void free_particle_arrays(Handle* h)
     h->d_ins_inst = nullptr;
     h->d_ins_bnd = nullptr;
     h->d_ins_rows = nullptr;
+    h->d_ovf = nullptr;
     h->layout.clear();
 }
 
@@ -166,12 +168,20 @@ cudaError_t launch_rebuild(Handle* h, cudaStream_t s)
 }
 constexpr int REBUILD_LAUNCHES = 1;
 
+InsPtrs ins_ptrs(Handle* h)
+{
+    const size_t nc = (size_t)h->d.ncells + 1;
+    int* o = h->d_ovf;
+    return InsPtrs{h->d_ins_inst, h->d_ins_bnd, h->d_ins_rows, o, o ? o + nc : nullptr,
+                   o ? o + nc + (size_t)h->d.ncap : nullptr};
+}
+
 // Insertion boundaries: one block per instance that has some (dem_insert.cuh),
 // after k_control and before the rebuild it may request.
 void launch_insert(Handle* h, cudaStream_t s)
 {
     if (h->n_ins_launch > 0)
-        k_insert<<<h->n_ins_inst, INS_THREADS, 0, s>>>(h->d, InsPtrs{h->d_ins_inst, h->d_ins_bnd, h->d_ins_rows});
+        k_insert<<<h->n_ins_inst, INS_THREADS, 0, s>>>(h->d, ins_ptrs(h));
 }
 constexpr int FORCE_LAUNCHES = 3;
 
@@ -1057,6 +1067,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         if ((rc = dalloc(h, &h->d_ins_inst, (size_t)n_ins_inst))) return rc;
         if ((rc = dalloc(h, &h->d_ins_bnd, h->ins.size()))) return rc;
         if ((rc = dalloc(h, &h->d_ins_rows, NC))) return rc;
+        if ((rc = dalloc(h, &h->d_ovf, (size_t)ncells + 1 + 2 * NC))) return rc;
     }
     if ((rc = dalloc(h, &d.slot, (size_t)cap * NC))) return rc;
     if ((rc = dalloc(h, &d.slotw, (size_t)wmax * NC))) return rc;
@@ -1161,11 +1172,13 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         ins_rows.insert(ins_rows.end(), free_rows[in].begin(), free_rows[in].end());
         S.rows_end = (int)ins_rows.size();
         S.next_row = S.rows_begin;
+        S.filed_from = S.rows_begin;
         ins_inst.push_back(S);
     }
     h->n_ins_inst = (int)ins_inst.size();
     h->n_ins_launch = h->ins.empty() ? 0 : h->n_ins_inst;
     if (h->n_ins_inst > 0) {
+        CU(cudaMemsetAsync(h->d_ovf, 0xff, ((size_t)d.ncells + 1) * sizeof(int), h->stream)); // lists empty
         CU(cudaMemcpyAsync(h->d_ins_inst, ins_inst.data(), ins_inst.size() * sizeof(InsInstanceDev),
                            cudaMemcpyHostToDevice, h->stream));
         CU(cudaMemcpyAsync(h->d_ins_bnd, ins_bnd.data(), ins_bnd.size() * sizeof(InsBoundaryDev),
@@ -1224,7 +1237,7 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         CU(cudaMemcpyAsync(dF, &F, sizeof(FillDev), cudaMemcpyHostToDevice, h->stream));
         if (F.target > 0) {
             k_fill_grid<<<grid_for(n, 256), 256, 0, h->stream>>>(d, g, in);
-            k_fill<<<1, INS_THREADS, 0, h->stream>>>(d, InsPtrs{h->d_ins_inst, h->d_ins_bnd, h->d_ins_rows}, dF, g);
+            k_fill<<<1, INS_THREADS, 0, h->stream>>>(d, ins_ptrs(h), dF, g);
         }
         CU(cudaGetLastError());
         CU(cudaMemcpyAsync(&h->fill_results[k], dF, sizeof(FillDev), cudaMemcpyDeviceToHost, h->stream));

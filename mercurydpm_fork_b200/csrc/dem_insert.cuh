@@ -18,8 +18,11 @@
 // than Control::disp_acc (the accumulated per-step maximum displacement)
 // since then, so a cell search widened by it finds every particle a
 // candidate can touch; the test itself is the exact one on the current
-// positions. Particles placed in this launch are not in any cell yet: they
-// are the free rows used so far, tested one by one.
+// positions. Particles placed in this launch are not in the cell table yet:
+// each is filed in a per-cell list of its own (ovf_head / ovf_next, the cell
+// its position and radius give, as keys_one would), which the search walks
+// with the cell; the next launch empties the lists it filled (the rebuild of
+// the step has put those particles into the table).
 //
 // One trait of the reference's search is kept: Mercury3D::hGridHasParticleContacts
 // (Mercury3D.cc:485-542) looks particles up in the HGrid cells filed at the
@@ -106,14 +109,26 @@ struct InsInstanceDev {
     int first, count;         // its boundaries in InsBoundaryDev order
     int rows_begin, rows_end; // its free rows in the row list
     int next_row;             // the next free row to fill
-    int pad;
+    int filed_from;           // rows filed in the per-cell lists by the last launch: filed_from .. next_row - 1
 };
 
 struct InsPtrs {
     InsInstanceDev* inst;
     InsBoundaryDev* bnd;
     const int* rows;          // free rows (caller order), grouped by instance
+    int* ovf_head;            // per cell: a particle placed in this launch, -1: none
+    int* ovf_next;            // per slot: the next placed particle of its cell
+    int* filed_key;           // per free-row index: the cell its particle was filed in
 };
+
+// The cell key keys_one gives a particle of radius r at x (level by radius).
+__device__ __forceinline__ int ins_cell_key(const InstanceDev& I, double x, double y, double z, int lvl)
+{
+    const int cx = cell_coord(x, I.origin[0], I.inv_cell[lvl][0], I.dims[lvl][0], I.per_mask & 1u);
+    const int cy = cell_coord(y, I.origin[1], I.inv_cell[lvl][1], I.dims[lvl][1], (I.per_mask >> 1) & 1u);
+    const int cz = cell_coord(z, I.origin[2], I.inv_cell[lvl][2], I.dims[lvl][2], (I.per_mask >> 2) & 1u);
+    return I.cell_base[lvl] + (cz * I.dims[lvl][1] + cy) * I.dims[lvl][0] + cx;
+}
 
 // PSD::drawSample (Kernel/Math/PSD.cc:114-128): std::lower_bound over the
 // cumulative probabilities, then a*r_low + (1 - a)*r_high.
@@ -242,6 +257,8 @@ __global__ void __launch_bounds__(INS_THREADS) k_insert(DevPtrs d, InsPtrs ip)
     __shared__ InsCandidate cand;
     __shared__ int s_go, s_stop, s_placed, s_next_row, s_fresh;
     for (int k = tid; k < LFG_P; k += blockDim.x) rng_v[k] = S.rng.v[k];
+    // empty the per-cell lists the last launch filled
+    for (int k = S.filed_from + tid; k < S.next_row; k += blockDim.x) ip.ovf_head[ip.filed_key[k]] = -1;
     if (tid == 0) {
         rng_head = S.rng.head;
         s_placed = 0;
@@ -306,15 +323,6 @@ __global__ void __launch_bounds__(INS_THREADS) k_insert(DevPtrs d, InsPtrs ip)
             const double rc = cand.r;
             const int nimg = cand.n_img;
             bool hit = ins_wall_hit(d, I, b.species, cand);
-            // particles placed earlier in this launch
-            for (int k = first_row + tid; k < s_next_row && !hit; k += blockDim.x) {
-                const int t = d.row_slot[ip.rows[k]];
-                const double4 pt = d.pr[c][t];
-                const int4 it = d.info[c][t];
-                const double idist = d.species[I.species_offset + b.species * ns + it.y].interaction_distance;
-                for (int m = 0; m < nimg && !hit; ++m)
-                    hit = ins_overlaps(v3(cand.x[m][0], cand.x[m][1], cand.x[m][2]), rc, pt, idist);
-            }
             // particles of the cells around the candidate and its images
             for (int m = 0; m < nimg && !__syncthreads_or(hit); ++m) {
                 const V3 xm = v3(cand.x[m][0], cand.x[m][1], cand.x[m][2]);
@@ -340,6 +348,11 @@ __global__ void __launch_bounds__(INS_THREADS) k_insert(DevPtrs d, InsPtrs ip)
                                 d.species[I.species_offset + b.species * ns + it.y].interaction_distance;
                             hit = ins_overlaps(xm, rc, d.pr[c][t], idist);
                         }
+                        for (int t = ip.ovf_head[key]; t >= 0 && !hit; t = ip.ovf_next[t]) { // placed in this launch
+                            const double idist =
+                                d.species[I.species_offset + b.species * ns + d.info[c][t].y].interaction_distance;
+                            hit = ins_overlaps(xm, rc, d.pr[c][t], idist);
+                        }
                     }
                 }
             }
@@ -352,6 +365,10 @@ __global__ void __launch_bounds__(INS_THREADS) k_insert(DevPtrs d, InsPtrs ip)
                         const int t = d.row_slot[ip.rows[s_next_row]];
                         const double r = cand.r;
                         ins_place(d, I, c, t, inst, b.species, b.density, cand.x[0], cand.v, r);
+                        const int key = ins_cell_key(I, cand.x[0][0], cand.x[0][1], cand.x[0][2], level_of_radius(I, r));
+                        ip.ovf_next[t] = ip.ovf_head[key];
+                        ip.ovf_head[key] = t;
+                        ip.filed_key[s_next_row] = key;
                         if (r > S.grid_rmax) { // the next test finds the grid rebuilt
                             S.grid_rmax = r;
                             s_fresh = 1;
@@ -387,6 +404,7 @@ __global__ void __launch_bounds__(INS_THREADS) k_insert(DevPtrs d, InsPtrs ip)
     for (int k = tid; k < LFG_P; k += blockDim.x) S.rng.v[k] = rng_v[k];
     if (tid == 0) {
         S.rng.head = rng_head;
+        S.filed_from = first_row;
         S.next_row = s_next_row;
         S.time = next_time; // DPMBase::time_ += timeStep_ at the end of the step
         if (s_placed) ctl->rebuild = 1; // the new particles need cells and lists
@@ -554,6 +572,7 @@ __global__ void __launch_bounds__(INS_THREADS) k_fill(DevPtrs d, InsPtrs ip, Fil
     if (tid == 0) {
         S.rng.head = rng_head;
         S.next_row = next_row;
+        S.filed_from = next_row; // the fill files in its own grid, not in the per-cell lists
         fd.height = height;
         fd.added = added;
         fd.tries_left = tries;

@@ -48,6 +48,11 @@ struct Handle {
     InsBoundaryDev* d_ins_bnd = nullptr;
     int* d_ins_rows = nullptr;
     int* d_ovf = nullptr;              // per cell, then per slot twice: k_insert's lists of placed particles
+    // radii of a one-instance upload and their statistics (the grid is laid
+    // out from them before the particle arrays are allocated)
+    double* d_rtmp = nullptr;
+    long long rtmp_cap = 0;
+    unsigned long long* d_rstats = nullptr;
     int n_ins_inst = 0;                // instances with insertion boundaries or a fill (blocks of k_insert)
     int n_ins_launch = 0;              // blocks of k_insert per step (0: no insertion boundary)
     std::vector<dem_chute_fill> fills; // chute fills of the next upload
@@ -302,6 +307,60 @@ int read_control(Handle* h, Control* c)
     return DEM_OK;
 }
 
+// Bands of radii (setup_instance_grid): ratio 2 from the smallest radius, at
+// most DEM_MAX_LEVELS of them.
+int band_count(double rmin, double rmax)
+{
+    int nl = 1;
+    while (nl < DEM_MAX_LEVELS && rmax >= rmin * std::pow(2.0, nl)) ++nl;
+    return nl;
+}
+
+// What setup_instance_grid needs of the radii, measured on the device for a
+// one-instance upload: extremes and the largest radius of each band.
+struct BandStats {
+    double rmin, rmax;
+    double lrmax[DEM_MAX_LEVELS];
+};
+
+// The radii of a one-instance upload on the device: extremes and validity
+// (k_radius_extremes), then, if all are positive and finite, the largest
+// radius of every band (k_radius_bands). `ok` is false when some radius is
+// bad (the host check then names it).
+int radius_stats(Handle* h, const double* radius, long long n, BandStats& st, bool& ok)
+{
+    if (n > h->rtmp_cap) {
+        if (h->d_rtmp) cudaFree(h->d_rtmp);
+        h->d_rtmp = nullptr;
+        h->rtmp_cap = 0;
+        CU(cudaMalloc(&h->d_rtmp, (size_t)n * sizeof(double)));
+        h->rtmp_cap = n;
+    }
+    if (!h->d_rstats) CU(cudaMalloc(&h->d_rstats, (3 + DEM_MAX_LEVELS) * sizeof(unsigned long long)));
+    unsigned long long init[3 + DEM_MAX_LEVELS] = {(unsigned long long)__builtin_bit_cast(long long, DBL_MAX), 0ull, 0ull};
+    for (int k = 0; k < DEM_MAX_LEVELS; ++k) init[3 + k] = 0ull;
+    CU(cudaMemcpyAsync(h->d_rtmp, radius, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->d_rstats, init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
+    const unsigned blocks = std::min<unsigned>(grid_for(n, 256), 4u * (unsigned)h->sm_count);
+    k_radius_extremes<<<blocks, 256, 0, h->stream>>>(h->d_rtmp, (int)n, h->d_rstats);
+    CU(cudaGetLastError());
+    unsigned long long out[3 + DEM_MAX_LEVELS];
+    CU(cudaMemcpyAsync(out, h->d_rstats, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    ok = out[2] == 0ull;
+    if (!ok) return DEM_OK;
+    st.rmin = __builtin_bit_cast(double, out[0]);
+    st.rmax = __builtin_bit_cast(double, out[1]);
+    const int nl = band_count(st.rmin, st.rmax);
+    k_radius_bands<<<blocks, 256, 0, h->stream>>>(h->d_rtmp, (int)n, st.rmin, nl, h->d_rstats + 3);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(out + 3, h->d_rstats + 3, DEM_MAX_LEVELS * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < DEM_MAX_LEVELS; ++k) st.lrmax[k] = __builtin_bit_cast(double, out[3 + k]);
+    return DEM_OK;
+}
+
 int check_status(Handle* h, const Control& c)
 {
     const unsigned st = c.status & FATAL_STATUS;
@@ -325,10 +384,16 @@ int check_status(Handle* h, const Control& c)
 // [psd_lo, psd_hi] (psd_hi > 0): radii insertion boundaries may place later;
 // every band they reach gets a level sized for its largest radius.
 void setup_instance_grid(const dem_instance_desc& in, const double* radii, size_t count, double skin, double dmax,
-                         double psd_lo, double psd_hi, InstanceDev& I, std::vector<int>& level_of, int& cell_base)
+                         double psd_lo, double psd_hi, InstanceDev& I, std::vector<int>& level_of, int& cell_base,
+                         const BandStats* pre = nullptr)
 {
     double rmin = 1e300, rmax = 0.0;
-    for (size_t i = 0; i < count; ++i) { rmin = std::min(rmin, radii[i]); rmax = std::max(rmax, radii[i]); }
+    if (pre) {
+        rmin = pre->rmin;
+        rmax = pre->rmax;
+    } else {
+        for (size_t i = 0; i < count; ++i) { rmin = std::min(rmin, radii[i]); rmax = std::max(rmax, radii[i]); }
+    }
     const bool psd = psd_hi > 0.0;
     // a little above the largest PSD radius: PSD::drawSample's interpolation rounds
     const double phi = psd_hi * (1.0 + 1e-12);
@@ -338,12 +403,17 @@ void setup_instance_grid(const dem_instance_desc& in, const double* radii, size_
     }
     const bool empty = count == 0 && !psd;
     if (empty) { rmin = rmax = 1.0; }
-    int nl = 1;
-    while (nl < DEM_MAX_LEVELS && rmax >= rmin * std::pow(2.0, nl)) ++nl;
+    const int nl = band_count(rmin, rmax);
     std::vector<double> lrmax(nl, 0.0);
     std::vector<int> used(nl, 0);
-    level_of.resize(count);
-    for (size_t i = 0; i < count; ++i) {
+    if (pre) // the levels themselves are computed by k_pack
+        for (int l = 0; l < nl; ++l) {
+            lrmax[l] = pre->lrmax[l];
+            used[l] = pre->lrmax[l] > 0.0;
+        }
+    else
+        level_of.resize(count);
+    for (size_t i = 0; i < count && !pre; ++i) {
         // floor(log2(r / rmin)) is the binary exponent of r / rmin >= 1 (a
         // normal number): exact, and far cheaper than log2 for millions of
         // particles
@@ -375,7 +445,7 @@ void setup_instance_grid(const dem_instance_desc& in, const double* radii, size_
     std::vector<double> lr;
     for (int l = 0; l < nl; ++l)
         if (used[l] || empty) { remap[l] = nu++; lr.push_back(lrmax[l] > 0 ? lrmax[l] : rmax); }
-    if (nu != nl) // some level is empty: renumber (usually every level is used)
+    if (nu != nl && !pre) // some level is empty: renumber (usually every level is used)
         for (size_t i = 0; i < count; ++i) level_of[i] = remap[level_of[i]];
     I.n_levels = nu;
     I.level_rmin = rmin;
@@ -804,19 +874,16 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
     // and the grid); k_pack checks every other array on the device, and the
     // loop below runs only to name a failure it reports
     bool checked = false;
-    if (fast) {
-        bool bad = false;
-        double rmin = 1e300;
-        for (long long i = 0; i < n; ++i) {
-            const double r = p->radius[i];
-            bad |= !(r > 0.0) | !(r <= DBL_MAX);
-            rmin = r < rmin ? r : rmin;
-        }
-        if (!bad) {
+    BandStats pre{};
+    if (fast && n > 0) { // the radii's extremes and bands from the device, not host loops
+        bool ok = false;
+        if (int rc0 = radius_stats(h, p->radius, n, pre, ok)) return rc0;
+        if (ok) {
             checked = true;
-            rmin_all = n > 0 ? rmin : rmin_all;
+            rmin_all = pre.rmin;
         }
     }
+    const bool levels_here = fast && checked; // k_pack computes the levels
     auto validate = [&]() -> int { // every particle on the host, in caller order: names the first violation
         for (long long i = 0; i < n; ++i) {
             const int in = p->instance ? p->instance[i] : 0;
@@ -938,7 +1005,8 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         std::vector<int>& lv = fast ? h->level_buf : lv_multi;
         const double* rad = fast ? p->radius : radii[in].data();
         const size_t nrad = fast ? (size_t)n : radii[in].size();
-        setup_instance_grid(D, rad, nrad, skin, dmax, psd_lo[in], psd_hi[in], I, lv, cell_base);
+        setup_instance_grid(D, rad, nrad, skin, dmax, psd_lo[in], psd_hi[in], I, lv, cell_base,
+                            levels_here ? &pre : nullptr);
         if (!fast)
             for (size_t k = 0; k < members[in].size(); ++k) level[members[in][k]] = lv[k];
         for (int r : free_rows[in]) level[r] = -1; // k_pack parks it dormant
@@ -1119,8 +1187,9 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         (rc = put(st.ang, p->angular_velocity, 3 * dn)) || (rc = put(st.ori, p->orientation, 4 * dn)) ||
         (rc = put(st.rad, p->radius, dn)) || (rc = put(st.im, p->inv_mass, dn)) ||
         (rc = put(st.ii, p->inv_inertia, dn)) || (rc = put(st.sp, p->species, in4)) || (rc = put(st.id, p->id, in4)) ||
-        (rc = put(st.inst, p->instance, in4)) || (rc = put(st.lvl, level.data(), in4)))
+        (rc = put(st.inst, p->instance, in4)) || (!levels_here && (rc = put(st.lvl, level.data(), in4))))
         return rc;
+    CU(cudaMemcpyAsync(h->d_inst, h->inst.data(), h->inst.size() * sizeof(InstanceDev), cudaMemcpyHostToDevice, h->stream));
     Control c{};
     c.cur = 0;
     c.lbuf = 0;
@@ -1133,9 +1202,9 @@ int dem_upload_particles(dem_handle* hh, const dem_particles_soa* p)
         k_pack<<<grid_for(n, 256), 256, 0, h->stream>>>(d, st, p->angular_velocity != nullptr,
                                                         p->orientation != nullptr, p->inv_inertia != nullptr,
                                                         p->instance != nullptr,
-                                                        one ? h->inst_desc[0].n_species : INT_MAX, one ? 1 : 0);
+                                                        one ? h->inst_desc[0].n_species : INT_MAX, one ? 1 : 0,
+                                                        levels_here ? 1 : 0);
     CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(h->d_inst, h->inst.data(), h->inst.size() * sizeof(InstanceDev), cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(h->d_species, h->species.data(), h->species.size() * sizeof(dem_species_pair),
                        cudaMemcpyHostToDevice, h->stream));
     if (!h->walls.empty()) {
@@ -2038,6 +2107,8 @@ void dem_destroy(dem_handle* hh)
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     free_particle_arrays(h);
+    if (h->d_rtmp) cudaFree(h->d_rtmp);
+    if (h->d_rstats) cudaFree(h->d_rstats);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);

@@ -144,17 +144,6 @@ __host__ __device__ __forceinline__ double psd_draw(const dem_insertion_boundary
     return a * rmin + (1.0 - a) * rmax;
 }
 
-// The HGrid level of radius r under the instance's banding (the host's
-// setup_instance_grid made sure every band the PSD reaches has a level).
-__device__ __forceinline__ int level_of_radius(const InstanceDev& I, double r)
-{
-    const double x = r / I.level_rmin;
-    int l = (int)((__double_as_longlong(x) >> 52) & 0x7ff) - 1023;
-    l = l < 0 ? 0 : (l > I.level_bands - 1 ? I.level_bands - 1 : l);
-    const int m = I.level_remap[l];
-    return m < 0 ? 0 : m;
-}
-
 // BaseParticle::isInContactWith / getSumOfInteractionRadii (BaseParticle.cc:
 // 863-871, BaseParticle.h:383-385): candidate c against particle t.
 __device__ __forceinline__ bool ins_overlaps(V3 c, double rc, double4 pt, double idist)

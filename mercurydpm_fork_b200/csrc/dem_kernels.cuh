@@ -787,18 +787,91 @@ __host__ __device__ inline StagePtrs stage_ptrs(double* base, size_t nc)
     return s;
 }
 
+// The HGrid level of radius r under the instance's banding: the binary
+// exponent of r / level_rmin, clamped to the bands, through the remap of
+// empty bands (setup_instance_grid; for insertion boundaries the host made
+// every band the PSD reaches a level).
+__device__ __forceinline__ int level_of_radius(const InstanceDev& I, double r)
+{
+    const double x = r / I.level_rmin;
+    int l = (int)((__double_as_longlong(x) >> 52) & 0x7ff) - 1023;
+    l = l < 0 ? 0 : (l > I.level_bands - 1 ? I.level_bands - 1 : l);
+    const int m = I.level_remap[l];
+    return m < 0 ? 0 : m;
+}
+
+// Radii of a one-instance upload, before the cell grid is laid out: their
+// extremes and whether any is not a positive finite number (stats[0], [1]:
+// bits of the smallest and largest positive radius, which order like the
+// values; stats[2]: nonzero if some radius is bad).
+__global__ void __launch_bounds__(256) k_radius_extremes(const double* r, int n, unsigned long long* stats)
+{
+    double lo = DBL_MAX, hi = 0.0;
+    bool bad = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double x = r[i];
+        if (!(x > 0.0) || !(x <= DBL_MAX)) {
+            bad = true;
+            continue;
+        }
+        lo = fmin(lo, x);
+        hi = fmax(hi, x);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&stats[0], (unsigned long long)__double_as_longlong(lo));
+        atomicMax(&stats[1], (unsigned long long)__double_as_longlong(hi));
+        if (bad) atomicOr(&stats[2], 1ull);
+    }
+}
+
+// The largest radius of every band (setup_instance_grid's bands: binary
+// exponent of r / rmin, clamped to nl - 1): band_max[l] gets its bits.
+__global__ void __launch_bounds__(256) k_radius_bands(const double* r, int n, double rmin, int nl,
+                                                      unsigned long long* band_max)
+{
+    unsigned long long m[DEM_MAX_LEVELS] = {0ull, 0ull, 0ull, 0ull};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double x = r[i] / rmin;
+        int l = (int)((__double_as_longlong(x) >> 52) & 0x7ff) - 1023;
+        l = l < 0 ? 0 : (l > nl - 1 ? nl - 1 : l);
+        const unsigned long long b = (unsigned long long)__double_as_longlong(r[i]);
+#pragma unroll
+        for (int k = 0; k < DEM_MAX_LEVELS; ++k)
+            if (k == l && b > m[k]) m[k] = b;
+    }
+#pragma unroll
+    for (int k = 0; k < DEM_MAX_LEVELS; ++k) {
+        unsigned long long v = m[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = w > v ? w : v;
+        }
+        if ((threadIdx.x & 31) == 0 && v) atomicMax(&band_max[k], v);
+    }
+}
+
 // caller order -> state buffer 0 (identity permutation until the first rebuild).
 // It also checks what it packs (finite positions and velocities, radius > 0,
 // species below nsp, inverse mass >= 0, instance 0 where one_instance) and
 // reports a violation as DEM_ERR_BAD_INPUT in the control status. Rows the
 // host gave level -1 are free rows of insertion boundaries: packed dormant.
 __global__ void __launch_bounds__(256) k_pack(DevPtrs d, StagePtrs s, int has_ang, int has_ori, int has_ii,
-                                              int has_inst, int nsp, int one_instance)
+                                              int has_inst, int nsp, int one_instance, int levels_here)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n) return;
     if (d.row_slot) d.row_slot[i] = i;
-    if (s.lvl[i] < 0) { // a free row of an insertion boundary (radius 0): dormant until filled
+    // levels_here: a one-instance upload without free rows, whose levels are
+    // computed here from the banding instead of sent by the host
+    const int lvl = levels_here ? level_of_radius(d.inst[0], s.rad[i]) : s.lvl[i];
+    if (lvl < 0) { // a free row of an insertion boundary (radius 0): dormant until filled
         d.pr[0][i] = make_double4(DELETED_COORD, DELETED_COORD, DELETED_COORD, 0.0);
         d.vm[0][i] = make_double4(0.0, 0.0, 0.0, 0.0);
         d.wi[0][i] = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -822,7 +895,7 @@ __global__ void __launch_bounds__(256) k_pack(DevPtrs d, StagePtrs s, int has_an
                               has_ang ? s.ang[3 * i + 2] : 0.0, has_ii ? s.ii[i] : 0.0);
     d.qo[0][i] = has_ori ? make_double4(s.ori[4 * i], s.ori[4 * i + 1], s.ori[4 * i + 2], s.ori[4 * i + 3])
                          : make_double4(1.0, 0.0, 0.0, 0.0);
-    const int flags = (im == 0.0 ? FLAG_FIXED : 0) | (s.lvl[i] << LEVEL_SHIFT);
+    const int flags = (im == 0.0 ? FLAG_FIXED : 0) | (lvl << LEVEL_SHIFT);
     d.info[0][i] = make_int4(s.id[i], s.sp[i], has_inst ? s.inst[i] : 0, flags);
     d.caller[0][i] = i;
 }

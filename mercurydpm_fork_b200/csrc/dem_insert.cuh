@@ -1,4 +1,6 @@
-// dem_insert.cuh -- insertion boundaries (CubeInsertionBoundary) on the device.
+// dem_insert.cuh -- insertion boundaries (CubeInsertionBoundary and
+// ChuteInsertionBoundary) and the chute's compact inflow fill
+// (Chute::addFlowParticlesCompactly) on the device.
 //
 // InsertionBoundary::checkBoundaryBeforeTimeStep (Kernel/Boundaries/
 // InsertionBoundary.cc:184-296) is sequential by nature: every draw of the

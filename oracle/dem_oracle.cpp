@@ -23,6 +23,21 @@
 // BaseInteraction::copySwitchPointer, BaseInteraction.cc:340-356).
 // The contact-law arithmetic is shared with the device code
 // (mercurydpm_fork_b200/csrc/dem_laws.cuh), compiled here for the host.
+//
+// Insertion boundaries (InsertionBoundary::checkBoundaryBeforeTimeStep,
+// Kernel/Boundaries/InsertionBoundary.cc:184-296) run after the periodic
+// wrap and the deletions, before the forces, with the reference's random
+// number generator restated here as the reference stores it (a vector of 607
+// lags from which every draw drops the oldest), the placement of a
+// CubeInsertionBoundary (CubeInsertionBoundary.cc:173-184) or
+// ChuteInsertionBoundary (ChuteInsertionBoundary.cc:163-190), and the test of
+// DPMBase::checkParticleForInteractionLocalPeriodic / ...Local
+// (DPMBase.cc:4868-4958) against every particle, its copies made as the
+// reference makes them. Input rows of radius 0 are free rows that placed
+// particles fill in row order. Like the reference's HGrid lookup, the test
+// does not see a particle that this step's drift shifted across a periodic
+// boundary until a particle larger than any before has been placed (which
+// rebuilds the reference's grid).
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -45,7 +60,55 @@ struct Particle {
     int species, id;
     bool fixed;
     bool deleted = false;
+    bool wrapped = false; // the last periodic wrap moved it
     V3 F, T;
+};
+
+// RNG (Kernel/Math/RNG.cc): setRandomSeed fills the 607 lags from the linear
+// congruential generator; getRandomNumber(lo, hi) appends
+// fmod(lags[0] + lags[607 - 273], 1), drops lags[0] and returns lo + (hi - lo) x.
+struct RefRng {
+    std::vector<double> lags;
+    explicit RefRng(unsigned long seed = 0)
+    {
+        const unsigned long a = 1103515245ul, c = 12345ul, m = 1024ul * 1024ul * 1024ul;
+        unsigned long s = seed;
+        for (int i = 0; i < 607; ++i) {
+            s = (a * s + c) % m;
+            lags.push_back(0.0 + 1.0 * (double)s / ((double)m + 1.0));
+        }
+    }
+    double draw(double lo, double hi)
+    {
+        const double x = std::fmod(lags[0] + lags[607 - 273], 1.0);
+        lags.erase(lags.begin());
+        lags.push_back(x);
+        const double range = hi - lo;
+        return lo + range * x;
+    }
+};
+
+// One insertion boundary and its state between steps.
+struct InsBoundary {
+    dem_insertion_boundary b;
+    RefRng psd_rng;       // PSD::random_
+    bool has_p0 = false;  // InsertionBoundary::p0
+    double p0_r = 0.0;
+    double volume = 0.0;  // volumeInserted_
+    long long inserted = 0;
+    // PSD::drawSample (Kernel/Math/PSD.cc:114-128)
+    double draw_radius()
+    {
+        const double prob = psd_rng.draw(0, 1);
+        const double* P = b.psd_probability;
+        const int n = b.n_psd;
+        const int high = (int)(std::lower_bound(P, P + n, prob) - P);
+        const int low = std::max(0, high - 1);
+        const double rMin = b.psd_radius[low], rMax = b.psd_radius[high];
+        const double pMin = P[low], pMax = P[high];
+        const double a = (prob - pMin) / (pMax - pMin);
+        return a * rMin + (1 - a) * rMax;
+    }
 };
 
 // Persistent interaction (InteractionHandler object). Key: (kind, P id, I id)
@@ -272,12 +335,14 @@ struct Sim {
 
     void wrap()
     {
+        for (auto& q : p) q.wrapped = false;
         for (int k = 0; k < 3; ++k) {
             if (!((inst.periodic_mask >> k) & 1u)) continue;
             const double lo = inst.periodic_min[k], hi = inst.periodic_max[k];
             for (auto& q : p) {
                 double* xc = &q.x.x;
                 if (std::min(xc[k] - lo, hi - xc[k]) < 0) {
+                    q.wrapped = true;
                     if (hi - xc[k] > xc[k] - lo)
                         xc[k] = xc[k] + L[k];
                     else
@@ -557,6 +622,190 @@ struct Sim {
         }
     }
 
+    // ---- insertion ---------------------------------------------------------
+    std::vector<InsBoundary> ins;
+    RefRng rng;                   // DPMBase::random
+    std::vector<int> free_rows;   // input rows of radius 0, in row order
+    size_t next_free = 0;
+    double time = 0.0;            // DPMBase::time_
+    double grid_rmax = 0.0;       // the largest radius the reference's HGrid was built for
+    bool grid_fresh = false;      // a placement in this step rebuilt it
+    bool no_row = false;
+
+    double max_idist(int a) const
+    {
+        double m = 0.0;
+        for (int b = 0; b < inst.n_species; ++b) m = std::max(m, sp(a, b).interaction_distance);
+        return m;
+    }
+
+    // DPMBase::checkParticleForInteractionLocal for a candidate of radius r
+    // and species a at x: no wall, then no particle, within reach
+    bool free_at(V3 x, double r, int a) const
+    {
+        for (int w = 0; w < (int)walls.size(); ++w) {
+            if (walls[w].type == DEM_WALL_TRIANGLE) continue;
+            double dist;
+            V3 nrm;
+            if (wall_dist(w, x, r + sp(a, walls[w].species).interaction_distance, dist, nrm)) return false;
+        }
+        for (const auto& q : p) {
+            if (q.deleted) continue;
+            if (q.wrapped && !grid_fresh) continue; // filed in the HGrid on the far side
+            const double X = x.x - q.x.x, Y = x.y - q.x.y, Z = x.z - q.x.z;
+            const double sum = r + q.r + sp(a, q.species).interaction_distance;
+            if (X * X + Y * Y + Z * Z < sum * sum) return false;
+        }
+        return true;
+    }
+
+    // DPMBase::checkParticleForInteractionLocalPeriodic: the candidate and its
+    // copies, made per periodic boundary within the largest reach
+    bool insertable(V3 x, double r, int a) const
+    {
+        std::vector<V3> copies;
+        double largest = 0.0; // ParticleHandler::getLargestParticle()->getMaxInteractionRadius()
+        bool any = false;
+        for (const auto& q : p)
+            if (!q.deleted) {
+                largest = std::max(largest, q.r + max_idist(q.species) * 0.5);
+                any = true;
+            }
+        for (int k = 0; k < 3 && any; ++k) {
+            if (!((inst.periodic_mask >> k) & 1u)) continue;
+            const double left = inst.periodic_min[k], right = inst.periodic_max[k];
+            const double maxDistance = (r + max_idist(a) * 0.5) + largest;
+            auto dist = [&](V3 y) { const double c = (&y.x)[k]; return std::min(c - left, right - c); };
+            auto shift = [&](V3& y) {
+                double& c = (&y.x)[k];
+                c = (right - c > c - left) ? c + (right - left) : c - (right - left);
+            };
+            for (int i = (int)copies.size() - 1; i >= 0; --i)
+                if (dist(copies[i]) < maxDistance) {
+                    copies.push_back(copies[i]);
+                    shift(copies.back());
+                }
+            if (dist(x) < maxDistance) {
+                copies.push_back(x);
+                shift(copies.back());
+            }
+        }
+        if (!free_at(x, r, a)) return false;
+        for (const V3& y : copies)
+            if (!free_at(y, r, a)) return false;
+        return true;
+    }
+
+    void insert()
+    {
+        const double next_time = time + cfg.time_step; // DPMBase::getNextTime
+        grid_fresh = false;
+        for (auto& B : ins) {
+            const dem_insertion_boundary& b = B.b;
+            auto generate = [&]() { // InsertionBoundary::generateParticle
+                rng.draw(0, 1);
+                B.p0_r = B.draw_radius();
+                B.has_p0 = true;
+            };
+            unsigned failed = 0;
+            while (failed <= (unsigned)b.max_failed && B.volume < b.volume_flow_rate * next_time + b.initial_volume) {
+                if (!B.has_p0) generate();
+                while (true) {
+                    const double r = B.p0_r;
+                    V3 x, v;
+                    if (b.kind == DEM_INSERTION_CHUTE) {
+                        x.x = b.pos_min[0] + r;
+                        x.y = rng.draw(b.pos_min[1] - r, b.pos_max[1] + r);
+                        x.z = rng.draw(b.pos_min[2] - r, b.pos_max[2] + r + b.fixed_particle_radius);
+                        const double u = b.inflow_velocity, var = b.inflow_velocity_variance;
+                        v.x = u * rng.draw(-var, var) + u;
+                        v.y = u * rng.draw(-var, var);
+                        v.z = u * rng.draw(-var, var);
+                    } else {
+                        x.x = rng.draw(b.pos_min[0], b.pos_max[0]);
+                        x.y = rng.draw(b.pos_min[1], b.pos_max[1]);
+                        x.z = rng.draw(b.pos_min[2], b.pos_max[2]);
+                        v.x = rng.draw(b.vel_min[0], b.vel_max[0]);
+                        v.y = rng.draw(b.vel_min[1], b.vel_max[1]);
+                        v.z = rng.draw(b.vel_min[2], b.vel_max[2]);
+                    }
+                    if (insertable(x, r, b.species)) {
+                        if (next_free >= free_rows.size()) {
+                            no_row = true;
+                            return;
+                        }
+                        Particle& q = p[free_rows[next_free++]];
+                        q.x = x;
+                        q.v = v;
+                        q.w = zero3();
+                        q.q = Q4{1.0, 0.0, 0.0, 0.0};
+                        q.r = r;
+                        // BaseParticle::computeMass (BaseParticle.cc:874-883), getVolume (:147-166)
+                        const double pi = 3.1415926535897932384626433832795;
+                        q.invm = 1.0 / (4.0 / 3.0 * pi * r * r * r * b.density);
+                        q.invI = 1.0 / (.4 * (1.0 / q.invm) * (r * r));
+                        q.species = b.species;
+                        q.fixed = false;
+                        q.deleted = false;
+                        q.wrapped = false;
+                        q.F = q.T = zero3();
+                        failed = 0;
+                        ++B.inserted;
+                        B.volume += 4.0 / 3.0 * pi * r * r * r;
+                        if (r > grid_rmax) { // HGrid::insertParticleToHgrid: too large, rebuild
+                            grid_rmax = r;
+                            grid_fresh = true;
+                        }
+                        generate();
+                        break;
+                    }
+                    ++failed;
+                    if (failed > (unsigned)b.max_failed) break;
+                }
+            }
+        }
+    }
+
+    // Chute::addFlowParticlesCompactly with Chute::createFlowParticle
+    // (Kernel/Chute.cc:1083-1115): candidates until the handler holds N
+    // particles; a rejected one raises the inflow height. Returns false when
+    // the free rows ran out.
+    bool chute_fill(const dem_chute_fill& f, double& height)
+    {
+        unsigned n_objects = 0;
+        for (const auto& q : p) n_objects += q.deleted ? 0u : 1u;
+        const double r_in = 0.5 * (f.min_radius + f.max_radius); // getInflowParticleRadius
+        const unsigned N = n_objects + f.x_max * f.y_max * height / (r_in * r_in * r_in) / 8;
+        unsigned size = n_objects;
+        while (size < N) {
+            const double r = rng.draw(f.min_radius, f.max_radius);
+            // the Vec3D constructor's arguments, evaluated last to first by g++
+            const double z = rng.draw(f.z_min + r + f.fixed_particle_radius, height);
+            const double y = rng.draw(f.y_min + r, f.y_max - r);
+            const double x = rng.draw(f.x_min + r, f.x_max - r);
+            if (insertable(v3(x, y, z), r, f.species)) {
+                if (next_free >= free_rows.size()) return false;
+                Particle& q = p[free_rows[next_free++]];
+                q.x = v3(x, y, z);
+                q.v = zero3();
+                q.w = zero3();
+                q.q = Q4{1.0, 0.0, 0.0, 0.0};
+                q.r = r;
+                const double pi = 3.1415926535897932384626433832795;
+                q.invm = 1.0 / (4.0 / 3.0 * pi * r * r * r * f.density);
+                q.invI = 1.0 / (.4 * (1.0 / q.invm) * (r * r));
+                q.species = f.species;
+                q.fixed = false;
+                q.deleted = false;
+                q.F = q.T = zero3();
+                ++size;
+            } else {
+                height = height + .0001 * f.max_radius; // Chute::setInflowHeight
+            }
+        }
+        return true;
+    }
+
     void erase_old(unsigned current)
     {
         for (auto it = inter.begin(); it != inter.end();) {
@@ -572,6 +821,13 @@ struct Sim {
 
 static int g_report_handler = 0;
 static std::vector<dem_deletion_boundary> g_deletions;
+static std::vector<dem_insertion_boundary> g_insertions;
+static unsigned long g_insertion_seed = 0;
+static std::vector<long long> g_inserted;
+static dem_chute_fill g_fill;
+static bool g_fill_set = false;
+static double g_fill_height = 0.0;
+static std::vector<double> g_inserted_volume;
 
 extern "C" {
 
@@ -583,6 +839,38 @@ void oracle_set_contact_report(int mode) { g_report_handler = mode; }
 
 // DeletionBoundary planes of the next oracle_run (the instance field is ignored).
 void oracle_set_deletion(const dem_deletion_boundary* b, int n) { g_deletions.assign(b, b + n); }
+
+// Insertion boundaries of the next oracle_run (instance fields ignored) and
+// the seed of DPMBase::random; input rows of radius 0 are then free rows.
+void oracle_set_insertion(const dem_insertion_boundary* b, int n, unsigned long long seed)
+{
+    g_insertions.assign(b, b + n);
+    g_insertion_seed = (unsigned long)seed;
+}
+
+// Chute::addFlowParticlesCompactly before the next oracle_run's initial force
+// evaluation (set = 0: none), from DPMBase::random seeded with `seed`; input
+// rows of radius 0 are the free rows. oracle_chute_fill_height: the inflow
+// height it ended with.
+void oracle_set_chute_fill(const dem_chute_fill* f, int set, unsigned long long seed)
+{
+    if (f) g_fill = *f;
+    g_fill_set = set != 0;
+    g_insertion_seed = (unsigned long)seed;
+}
+double oracle_chute_fill_height() { return g_fill_height; }
+
+// Particles and volume each insertion boundary placed in the last oracle_run;
+// returns the number of boundaries, -1 if a placement found no free row.
+int oracle_insertion_counts(long long* inserted, double* volume, int capacity)
+{
+    const int n = (int)g_inserted.size();
+    for (int k = 0; k < n && k < capacity; ++k) {
+        inserted[k] = g_inserted[k];
+        volume[k] = g_inserted_volume[k];
+    }
+    return n;
+}
 
 // Runs nsteps reference time steps from the given state (after the initial
 // force evaluation of DPMBase::initialiseSolve) and returns the final state
@@ -626,6 +914,21 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
         q.id = in->id[i];
         q.fixed = q.invm == 0.0;
         q.F = q.T = zero3();
+        if ((!g_insertions.empty() || g_fill_set) && q.r == 0.0) { // a free row: no particle until one is placed
+            q.deleted = true;
+            q.fixed = true;
+            q.invm = 0.0;
+            S.free_rows.push_back((int)i);
+        } else {
+            S.grid_rmax = std::max(S.grid_rmax, q.r);
+        }
+    }
+    S.rng = RefRng(g_insertion_seed);
+    for (const auto& b : g_insertions) {
+        InsBoundary B;
+        B.b = b;
+        B.psd_rng = RefRng((unsigned long)b.psd_seed);
+        S.ins.push_back(B);
     }
     std::map<int, int> index_of;
     for (int64_t i = 0; i < n; ++i) index_of[S.p[i].id] = (int)i;
@@ -650,6 +953,11 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
             }
         }
     }
+    if (g_fill_set) { // Chute::setupInitialConditions runs before the first force evaluation
+        double height = g_fill.inflow_height;
+        if (!S.chute_fill(g_fill, height)) return -3;
+        g_fill_height = height;
+    }
     // DPMBase::initialiseSolve: numberOfTimeSteps_ = 0, one force evaluation
     S.nt = 0;
     S.snapshot_periodic();
@@ -659,12 +967,23 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
         S.integrate_before();
         S.wrap();
         S.delete_particles();
+        if (!S.ins.empty()) {
+            S.insert();
+            if (S.no_row) return -3;
+        }
+        S.time += S.cfg.time_step; // the time the reference reaches at the end of the step
         S.snapshot_periodic();
         S.compute_forces();
         S.periodic_handover();
         S.integrate_after();
         S.erase_old(S.nt);
         S.nt += 1;
+    }
+    g_inserted.clear();
+    g_inserted_volume.clear();
+    for (const auto& B : S.ins) {
+        g_inserted.push_back(B.inserted);
+        g_inserted_volume.push_back(B.volume);
     }
     if (out) {
         for (int64_t i = 0; i < n; ++i) {
@@ -679,6 +998,9 @@ int oracle_run(const dem_config* cfg, const dem_instance_desc* inst, const dem_s
                 out->orientation[4 * i + 2] = q.q.q2; out->orientation[4 * i + 3] = q.q.q3;
             }
             if (out->instance) out->instance[i] = q.deleted ? -1 : 0;
+            if (out->radius) out->radius[i] = q.r;
+            if (out->inv_mass) out->inv_mass[i] = q.invm;
+            if (out->inv_inertia) out->inv_inertia[i] = q.invI;
         }
     }
     for (int64_t i = 0; i < n; ++i) {

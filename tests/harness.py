@@ -46,6 +46,14 @@ def oracle_lib():
         lib.oracle_set_contact_report.argtypes = [C.c_int]
         lib.oracle_set_deletion.restype = None
         lib.oracle_set_deletion.argtypes = [C.POINTER(_abi.DeletionBoundary), C.c_int]
+        lib.oracle_set_insertion.restype = None
+        lib.oracle_set_insertion.argtypes = [C.POINTER(_abi.InsertionBoundary), C.c_int, C.c_ulonglong]
+        lib.oracle_set_chute_fill.restype = None
+        lib.oracle_set_chute_fill.argtypes = [C.POINTER(_abi.ChuteFill), C.c_int, C.c_ulonglong]
+        lib.oracle_chute_fill_height.restype = C.c_double
+        lib.oracle_chute_fill_height.argtypes = []
+        lib.oracle_insertion_counts.restype = C.c_int
+        lib.oracle_insertion_counts.argtypes = [C.POINTER(C.c_longlong), _pd, C.c_int]
         _oracle = lib
     return _oracle
 
@@ -163,7 +171,8 @@ def sort_contacts(c):
     return {k: v[order] for k, v in c.items()}
 
 
-def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated", deletions=None) -> dict:
+def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated", deletions=None, insertions=None,
+               seed: int = 0, chute_fill=None) -> dict:
     """report="evaluated": contacts of the last force evaluation (what the
     engine records); "handler": every interaction the reference still holds.
     deletions: DeletionBoundary planes [(normal, distance), ...]; the output
@@ -171,6 +180,10 @@ def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated", deleti
     oracle_lib().oracle_set_contact_report(1 if report == "handler" else 0)
     darr, nd = _deletions(deletions)
     oracle_lib().oracle_set_deletion(darr, nd)
+    iarr, ni = _insertions(insertions)
+    oracle_lib().oracle_set_insertion(iarr, ni, seed)
+    oracle_lib().oracle_set_chute_fill(C.byref(chute_fill) if chute_fill is not None else None,
+                                       1 if chute_fill is not None else 0, seed)
     inp = _Inputs(sc, contacts)
     cap = _contact_rows(sc.n)
     o, c, soa, csoa = _outputs(sc.n, cap)
@@ -179,8 +192,18 @@ def run_oracle(sc, nsteps: int, contacts=None, report: str = "evaluated", deleti
                                  inp.nwalls, C.byref(inp.soa), C.byref(inp.contacts_in) if inp.contacts_in else None,
                                  nsteps, C.byref(soa), _dp(o["force"]), _dp(o["torque"]), C.byref(csoa), cap,
                                  C.byref(cnt))
+    oracle_lib().oracle_set_insertion(iarr, 0, 0)
+    oracle_lib().oracle_set_chute_fill(None, 0, 0)
     assert rc == 0
+    if chute_fill is not None:
+        o["inflow_height"] = float(oracle_lib().oracle_chute_fill_height())
     o["contacts"] = sort_contacts(_trim(c, cnt.value))
+    if ni:
+        k = np.zeros(ni, np.int64)
+        v = np.zeros(ni)
+        m = oracle_lib().oracle_insertion_counts(k.ctypes.data_as(C.POINTER(C.c_longlong)), _dp(v), ni)
+        assert m == ni
+        o["inserted"], o["inserted_volume"] = k, v
     return o
 
 

@@ -1,6 +1,8 @@
 """Insertion boundaries (CubeInsertionBoundary, Kernel/Boundaries/
 InsertionBoundary.cc:184-296) on the engine against the reference build.
 
+* CPU: the oracle's own restatement of the insertion and of the chute fill
+  against the reference build (placements bit for bit, then the run).
 * CPU: the engine's restatements of the reference's generators -- RNG
   (Kernel/Math/RNG.cc, lagged Fibonacci 607/273 seeded by the linear
   congruential generator) and PSD::drawSample (Kernel/Math/PSD.cc:114-128)
@@ -45,6 +47,39 @@ def test_psd_draws_match_reference(rmin, rmax, bins, seed):
     ours = psd_draws(b, 3000)
     ref = H.reference_psd_draws(rmin, rmax, bins, seed, 3000)
     np.testing.assert_array_equal(ours, ref)
+
+
+@needs_ref
+@pytest.mark.parametrize("periodic", [False, True])
+@pytest.mark.parametrize("psd", ["range", "single", "bins"])
+def test_oracle_insertion_matches_reference(periodic, psd):
+    """The oracle's own restatement of the insertion (oracle/dem_oracle.cpp:
+    the reference's generators kept as the reference stores them, every
+    candidate tested against every particle) places the reference's particles,
+    on the CPU."""
+    sc, bnd = cases.insertion_box(periodic=periodic, psd=psd, psd_seed=5)
+    o = H.run_oracle(sc, 400, insertions=bnd, seed=3)
+    r = H.run_reference(sc, 400, insertions=bnd, seed=3)
+    np.testing.assert_array_equal(o["inserted"], r["inserted"])
+    np.testing.assert_array_equal(o["inserted_volume"], r["inserted_volume"])
+    _compare(o, r)
+
+
+@needs_ref
+def test_oracle_chute_insertion_and_fill_match_reference():
+    """The oracle's ChuteInsertionBoundary and Chute::addFlowParticlesCompactly
+    against the reference, on the CPU."""
+    for periodic in (False, True):
+        sc, bnd = cases.insertion_box(periodic=periodic, psd="bins", psd_seed=2, chute=True)
+        o = H.run_oracle(sc, 300, insertions=bnd, seed=4)
+        r = H.run_reference(sc, 300, insertions=bnd, seed=4)
+        np.testing.assert_array_equal(o["inserted"], r["inserted"])
+        _compare(o, r)
+    sc, f = cases.chute_fill_case()
+    o = H.run_oracle(sc, 30, chute_fill=f, seed=7)
+    r = H.run_reference_chute_fill(sc, f, 7, 30)
+    assert o["inflow_height"] == r["inflow_height"] > f.inflow_height
+    _compare(o, r)
 
 
 def _compare(a, r):

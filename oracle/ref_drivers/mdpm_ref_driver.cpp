@@ -94,34 +94,47 @@ int run_and_report(const dem_config* cfg, const dem_instance_desc* inst, const d
 {
     Driver d;
     setup(d, cfg, inst, species, density, walls, nwalls, in, 1);
+    const int64_t n = in->n;
+    // Rows are matched by id. The uploaded particles have ids 0, 1, ... in the
+    // order of the rows (of nonzero radius, when insertion boundaries or a fill
+    // are set); placed particles take the rows of radius 0 in the order they
+    // were placed, whose ids the engine uses (the ids of contacts are reported
+    // as those). The reference gives them the ids after the uploaded ones, with
+    // gaps where periodic ghost particles drew ids, and a placed particle may
+    // be deleted later, so each one is given its row as soon as it appears: a
+    // particle placed in a step is still there at its end (deletions come
+    // before the placements of a step). Rows of deleted or never filled
+    // particles keep instance -1.
+    std::vector<int64_t> live_rows, free_rows;
+    for (int64_t i = 0; i < n; ++i) ((free_rows_in_use() && in->radius[i] == 0.0) ? free_rows : live_rows).push_back(i);
+    std::vector<std::pair<unsigned, int64_t>> placed_row; // reference id -> row, in placement order
+    unsigned next_new_id = (unsigned)live_rows.size();    // ids below were uploaded or already seen
+    auto note_placed = [&]() {
+        if (!free_rows_in_use()) return;
+        std::vector<unsigned> fresh;
+        for (unsigned r = 0; r < d.particleHandler.getSize(); ++r) {
+            const unsigned id = d.particleHandler.getObject(r)->getId();
+            if (id >= next_new_id) fresh.push_back(id);
+        }
+        std::sort(fresh.begin(), fresh.end());
+        for (unsigned id : fresh)
+            if (placed_row.size() < free_rows.size()) placed_row.emplace_back(id, free_rows[placed_row.size()]);
+        if (!fresh.empty()) next_new_id = fresh.back() + 1;
+    };
     d.initialiseSolve();
+    note_placed(); // a fill made by the set-up
     for (int k = 0; k < nsteps; ++k) {
         d.computeOneTimeStep();
+        note_placed();
         apply_event(d, k + 1);
     }
     collect_insertions(d);
-    const int64_t n = in->n;
-    // deleted particles leave the handler (and reorder it): rows are matched by
-    // id. The uploaded particles have ids 0, 1, ... in the order of the rows
-    // (of nonzero radius, when insertion boundaries are set); inserted particles
-    // have the ids after them, with gaps where periodic ghost particles drew
-    // ids, and take the rows of radius 0 in id order, whose ids the engine
-    // uses (the ids of contacts are reported as those). Rows of deleted or
-    // never filled particles keep instance -1.
-    std::vector<int64_t> live_rows, free_rows;
-    for (int64_t i = 0; i < n; ++i) ((free_rows_in_use() && in->radius[i] == 0.0) ? free_rows : live_rows).push_back(i);
-    std::vector<std::pair<unsigned, int64_t>> id_row; // reference id -> row
-    {
-        std::vector<unsigned> inserted;
-        for (unsigned r = 0; r < d.particleHandler.getSize(); ++r) {
-            const unsigned id = d.particleHandler.getObject(r)->getId();
-            if (id < live_rows.size()) id_row.emplace_back(id, live_rows[id]);
-            else inserted.push_back(id);
-        }
-        std::sort(inserted.begin(), inserted.end());
-        for (size_t k = 0; k < inserted.size() && k < free_rows.size(); ++k) id_row.emplace_back(inserted[k], free_rows[k]);
-        std::sort(id_row.begin(), id_row.end());
+    std::vector<std::pair<unsigned, int64_t>> id_row(placed_row); // reference id -> row
+    for (unsigned r = 0; r < d.particleHandler.getSize(); ++r) {
+        const unsigned id = d.particleHandler.getObject(r)->getId();
+        if (id < live_rows.size()) id_row.emplace_back(id, live_rows[id]);
     }
+    std::sort(id_row.begin(), id_row.end());
     auto row_of = [&](unsigned id) -> int64_t {
         auto it = std::lower_bound(id_row.begin(), id_row.end(), std::make_pair(id, (int64_t)-1));
         return (it != id_row.end() && it->first == id) ? it->second : -1;

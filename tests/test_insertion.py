@@ -66,6 +66,20 @@ def test_oracle_insertion_matches_reference(periodic, psd):
 
 
 @needs_ref
+def test_oracle_insertion_with_deletion_matches_reference():
+    """Particles placed above z = 10 d are removed by a DeletionBoundary at
+    the next step and placed again: some 2,000 of 2,500 placements are
+    deleted, and the survivors keep the rows their placement gave them."""
+    sc, bnd = cases.insertion_box(psd="range", n_free=4000)
+    dels = [((0, 0, 1), 10e-3)]
+    o = H.run_oracle(sc, 200, insertions=bnd, seed=6, deletions=dels)
+    r = H.run_reference(sc, 200, insertions=bnd, seed=6, deletions=dels)
+    np.testing.assert_array_equal(o["inserted"], r["inserted"])
+    assert r["inserted"][0] - ((r["instance"] >= 0).sum() - 300) > 1000
+    _compare(o, r)
+
+
+@needs_ref
 def test_oracle_chute_insertion_and_fill_match_reference():
     """The oracle's ChuteInsertionBoundary and Chute::addFlowParticlesCompactly
     against the reference, on the CPU."""
@@ -127,6 +141,19 @@ def test_chute_insertion_matches_reference(gpu, periodic):
     np.testing.assert_array_equal(a["inserted"], r["inserted"])
     np.testing.assert_array_equal(a["inserted_volume"], r["inserted_volume"])
     assert r["inserted"][0] > 20
+    _compare(a, r)
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_insertion_with_deletion_matches_reference(gpu):
+    """Placements above z = 10 d deleted at the next step and made again
+    (most of some 2,500): the placements, the deletions and the rows kept."""
+    sc, bnd = cases.insertion_box(psd="range", n_free=4000)
+    dels = [((0, 0, 1), 10e-3)]
+    a = H.run_gpu(sc, 200, insertions=bnd, seed=6, deletions=dels)
+    r = H.run_reference(sc, 200, insertions=bnd, seed=6, deletions=dels)
+    np.testing.assert_array_equal(a["inserted"], r["inserted"])
     _compare(a, r)
 
 
